@@ -1,0 +1,335 @@
+#!/usr/bin/env python3
+"""Benchmark of the grand-potential time step (cell-updates/s) on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload cfg2|cfg1|cfg4]
+
+Default workload (cfg2): the plain FP64 drop-in configuration -- 2048x2048
+grid, 3 phases, ternary alloy (2 chemical potentials), 4-fold anisotropy
+delta=0.02, periodic boundaries, 64 seeds (uniform centres, r ~ U[4,12],
+random solid phase, seed 0), liquid diffusivity diag(1, 0.5), solid 0, FP64.
+Synthetic data: the seed layout comes from a splitmix64 generator, the
+physical constants are fixed in eshwar_dipan_b200/workloads.py.
+
+A step is one explicit time step of the whole grid (phase-field pass +
+concentration pass + boundary handling).  Cell-updates count interior cells
+x steps.  With N>1 (torchrun) every rank runs its own replica of the workload
+(the single-grid step does not shard without a halo exchange); value is the
+sum over ranks, timed as the max over ranks.
+"""
+import argparse
+import json
+import os
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+
+import numpy as np  # noqa: E402
+
+from eshwar_dipan_b200.workloads import filling_text, input_text, random_seeds  # noqa: E402
+
+HARNESS = os.path.join(ROOT, "oracle", "_ref", "gp_ref_harness")
+PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+
+
+def workload(name, scale=1):
+    """(input text, filling text, description) of a benchmark configuration;
+    scale>1 shrinks the grid by that factor per axis with the same seed density."""
+    if name == "cfg2":
+        m = 2048 // scale
+        nseeds = max(1, 64 // (scale * scale))
+        kw = dict(N=3, K=2, mesh=(m, m), dab=0.02, bc_phi=(3, 3, 3, 3), d_liquid=[1.0, 0.5], d_solid=0.0,
+                  A_off=0.0, dt=0.02, eps=4.0, T=0.97)
+        seeds = random_seeds(nseeds, (m, m), 4.0, 12.0, 2, seed=0)
+        desc = "%dx%d ternary 3-phase FP64, aniso 0.02, periodic, %d seeds r~U[4,12]" % (m, m, nseeds)
+    elif name == "cfg4":
+        m = 4096 // scale
+        nseeds = max(1, 256 // (scale * scale))
+        kw = dict(N=3, K=2, mesh=(m, m), dab=0.0, aniso=False, bc_phi=(1, 1, 1, 1), d_liquid=[1.0, 0.5],
+                  d_solid=0.0, dt=0.02, eps=4.0, T=0.97)
+        seeds = random_seeds(nseeds, (m, m), 4.0, 12.0, 2, seed=0)
+        desc = "%dx%d ternary 3-phase FP64, isotropic, Neumann, %d seeds" % (m, m, nseeds)
+    elif name == "cfg1":
+        m = 256 // scale
+        kw = dict(N=2, K=1, mesh=(m, m), aniso=False, dab=0.0, d_solid=0.0, d_liquid=[1.0], dt=0.02, eps=4.0,
+                  T=1.0, liquid_c=[0.45])
+        seeds = [(0, m // 2, m // 2, 40.0 / scale)]
+        desc = "%dx%d binary 2-phase FP64, isotropic, Neumann, one supercritical seed r=40" % (m, m)
+    else:
+        raise SystemExit("unknown workload " + name)
+    return input_text(**kw), filling_text(seeds), desc, kw
+
+
+def write_workload(d, name, scale=1):
+    it, ft, desc, kw = workload(name, scale)
+    ip, fp = os.path.join(d, name + ".in"), os.path.join(d, name + "_fill.in")
+    open(ip, "w").write(it)
+    open(fp, "w").write(ft)
+    return ip, fp, desc, kw
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled every 200 ms in the background."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = str(gpu_index)
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        if shutil.which("nvidia-smi"):
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", self.idx, "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        return json.load(open(PEAKS))
+    except Exception:
+        return {}
+
+
+def run_reference(ip, fp, nsteps):
+    """The reference's own serial C implementation (built from its sources into
+    oracle/_ref): device-free, single thread.  Returns seconds of the time loop."""
+    with tempfile.TemporaryDirectory() as d:
+        for _ in range(4):   # the reference crashes at random at start-up; retry
+            r = subprocess.run([HARNESS, ip, fp, "time", str(nsteps)], capture_output=True, text=True, cwd=d)
+            if r.returncode == 0:
+                return float(r.stdout.strip().splitlines()[-1])
+    raise RuntimeError("reference harness failed: " + r.stderr[-400:])
+
+
+def run_oracle_port(ip, fp, nsteps):
+    """CPU restatement (oracle/liboracle.so), single thread; seconds of the steps."""
+    import eshwar_dipan_b200 as gp
+    from oracle_py import Oracle
+    p = gp.load_params(ip)
+    phi, mu = gp.fill(p, fp)
+    o = Oracle(p, recip_div=0)
+    o.set(phi, mu)
+    o.smooth(max(0, p.nsmooth - 1))
+    t0 = time.perf_counter()
+    o.step(nsteps)
+    return time.perf_counter() - t0
+
+
+def cpu_baseline(name, target_s=15.0):
+    """Reference timed on a bounded sample: the same configuration shrunk 4x per
+    axis (same seed density), enough steps for ~target_s of CPU time."""
+    scale = 4
+    with tempfile.TemporaryDirectory() as d:
+        ip, fp, desc, kw = write_workload(d, name, scale)
+        cells = kw["mesh"][0] * kw["mesh"][1]
+        kind = "reference" if os.path.exists(HARNESS) else "port"
+        runner = run_reference if kind == "reference" else run_oracle_port
+        t1 = runner(ip, fp, 2)
+        steps = max(2, min(400, int(target_s / max(t1 / 2, 1e-3))))
+        t = runner(ip, fp, steps)
+    return {"value": cells * steps / t, "unit": "cell-updates/s", "cores": 1, "kind": kind,
+            "sample": "%s, %d time steps (after the NSMOOTH-1 smoothing sweeps, untimed), %.1f s single-threaded"
+                      % (desc, steps, t)}
+
+
+def reference_arm(args, rank, world):
+    if rank != 0:
+        return 0
+    name = args.workload
+    base = cpu_baseline(name, target_s=min(60.0, 3.0 * max(1, args.steps)))
+    out = {"metric": "cell-updates/s", "value": base["value"], "unit": "cell-updates/s", "n_gpus": args.gpus,
+           "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "impl": "reference",
+           "dtype": "f64", "data": "synthetic", "scaling": "weak", "vs_baseline": None,
+           "config": {"workload": workload(name)[2]},
+           "cpu_baseline": base,
+           "e2e": {"value": base["value"], "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="cfg2", choices=["cfg1", "cfg2", "cfg4"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    else:
+        os.environ.setdefault("CUDA_VISIBLE_DEVICES", os.environ.get("CUDA_VISIBLE_DEVICES", "0"))
+
+    if args.impl == "reference":
+        rc = reference_arm(args, rank, world)
+        if dist:
+            dist.destroy_process_group()
+        return rc
+
+    import ctypes
+    import eshwar_dipan_b200 as gp
+    if world > 1:
+        # libgp uses the current CUDA device of the calling thread
+        import torch  # noqa: F401
+    work = tempfile.mkdtemp(prefix="gpbench")
+    ip, fp, desc, kw = write_workload(work, args.workload)
+    p = gp.load_params(ip)
+    phi0, mu0 = gp.fill(p, fp)
+    N, K = p.numphases, p.numcomponents - 1
+    cells = p.mesh_x * p.mesh_y
+    state_bytes = (N + K) * cells * 8
+
+    # ---- device-resident throughput (value) ---------------------------------
+    sim = gp.Simulation(p, phi0, mu0)
+    sim.smooth(p.nsmooth - 1)
+    sim.step(args.warmup, stats=False)
+
+    def barrier():
+        if dist:
+            dist.barrier()
+
+    barrier()
+    with ClockSampler(local) as clk:
+        tot_ms, ph_ms, up_ms, st = sim.step_timed(args.steps, stats=True)
+    barrier()
+    if dist:
+        import torch
+        t = torch.tensor([tot_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        tot_ms = float(t.item())
+    sim.close()
+
+    # ---- end to end through the C ABI with host buffers ----------------------
+    # gp_init uploads the host state, gp_smooth + gp_step run, and every SAVET=50
+    # steps the state is read back to the host (what the CLI does before writing
+    # a VTK file); wall clock around the whole sequence.
+    L = gp._abi.lib()
+    savet = 50
+    barrier()
+    t0 = time.perf_counter()
+    h = ctypes.c_void_p()
+    gp._abi.check(L.gp_init(ctypes.byref(h), ctypes.byref(p), phi0.ctypes.data_as(ctypes.c_void_p),
+                            mu0.ctypes.data_as(ctypes.c_void_p), gp.GP_FP64))
+    gp._abi.check(L.gp_smooth(h, p.nsmooth - 1), h)
+    gp._abi.check(L.gp_step(h, args.warmup, None), h)
+    phi_h = np.empty_like(phi0)
+    mu_h = np.empty_like(mu0)
+    done, ngets = 0, 0
+    while done < args.steps:
+        n = min(savet, args.steps - done)
+        gp._abi.check(L.gp_step(h, n, None), h)
+        gp._abi.check(L.gp_get(h, phi_h.ctypes.data_as(ctypes.c_void_p), mu_h.ctypes.data_as(ctypes.c_void_p)), h)
+        done += n
+        ngets += 1
+    t_e2e = time.perf_counter() - t0
+    L.gp_destroy(h)
+    barrier()
+    if dist:
+        import torch
+        t = torch.tensor([t_e2e], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_e2e = float(t.item())
+
+    if rank == 0:
+        peaks = measured_peaks()
+        hbm = peaks.get("hbm_gbs")
+        peak_src = "measured" if hbm else "fallback"
+        hbm = hbm or 6650.0
+        bytes_per_cell = 2 * (N + K) * 8
+        step_s = tot_ms / 1e3 / args.steps
+        achieved = bytes_per_cell * cells / step_s / 1e9
+        value = world * cells * args.steps / (tot_ms / 1e3)
+        e2e_steps = args.steps + args.warmup
+        out = {
+            "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": tot_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (splitmix64 seed layout, seed 0)",
+            "config": {"workload": args.workload + ": " + desc, "grid": [p.mesh_x, p.mesh_y], "phases": N,
+                       "components": K, "precision": "fp64 plain (bit-identical to the reference step)",
+                       "state_bytes": state_bytes,
+                       "l2": "inputs larger than L2: %.0f MB state + %.0f MB delta-phi per step"
+                             % (2 * state_bytes / 1e6, N * cells * 8 / 1e6),
+                       "parallelism": "replicas" if world > 1 else "single"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": achieved / hbm, "traffic": None, "peak_source": peak_src,
+                         "bytes_per_cell": bytes_per_cell,
+                         "kernels_ms_per_step": {"k_dphi": ph_ms / args.steps, "k_update": up_ms / args.steps},
+                         "note": "achieved = 2*(N+K)*8 B per cell-update / step time (both kernels); the FP64 "
+                                 "pipe, not HBM, bounds this step"},
+            "e2e": {"value": world * cells * e2e_steps / t_e2e, "unit": "cell-updates/s",
+                    "h2d_bytes_per_step": state_bytes / e2e_steps,
+                    "d2h_bytes_per_step": state_bytes * ngets / e2e_steps,
+                    "includes": "gp_init upload, %d smoothing sweeps, %d steps, a state read-back every %d steps"
+                                % (p.nsmooth - 1, e2e_steps, savet)},
+            "gpu_launches": 2 * args.steps + 1,
+            "clocks": clk.summary(),
+            "stats_last_step": st,
+        }
+        if not args.no_cpu_baseline:
+            out["cpu_baseline"] = cpu_baseline(args.workload)
+        print(json.dumps(out), flush=True)
+    shutil.rmtree(work, ignore_errors=True)
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

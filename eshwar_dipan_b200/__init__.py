@@ -1,0 +1,135 @@
+"""eshwar_dipan_b200 -- MicroSim's 2D grand-potential finite-difference step on B200.
+
+Python side of libgp (include/gp.h).  The physics runs in hand-written sm_100a
+CUDA kernels behind the C ABI; this module only marshals arguments:
+
+    p = load_params("Input.in")                 # reading_input_parameters()
+    phi, mu = fill(p, "Filling.in")             # fill_domain()
+    sim = Simulation(p, phi, mu)                # gp_init on the current device
+    sim.smooth(p.nsmooth - 1)                   # preconditioning sweeps
+    stats = sim.step(1000)                      # time steps
+    phi, mu = sim.get()
+
+Arrays are float64 numpy arrays shaped (N, MESH_X, MESH_Y) and (K, MESH_X, MESH_Y),
+y contiguous, as in the reference's VTK output.
+"""
+import ctypes
+
+import numpy as np
+
+from ._abi import (GP_FP32, GP_FP64, GpError, Params, Stats, check, lib)
+
+__all__ = ["Params", "Stats", "GpError", "Simulation", "load_params", "fill", "vtk_write", "vtk_read",
+           "GP_FP64", "GP_FP32", "version"]
+
+
+def version():
+    return lib().gp_version().decode()
+
+
+def _ptr(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def load_params(path):
+    """Parse an Input.in file (gp_params_load)."""
+    p = Params()
+    check(lib().gp_params_load(ctypes.byref(p), str(path).encode()))
+    return p
+
+
+def _shapes(p):
+    return (p.numphases, p.mesh_x, p.mesh_y), (p.numcomponents - 1, p.mesh_x, p.mesh_y)
+
+
+def fill(p, filling_path):
+    """Initial interior fields from a Filling.in file (gp_fill)."""
+    sp, sm = _shapes(p)
+    phi = np.zeros(sp, dtype=np.float64)
+    mu = np.zeros(sm, dtype=np.float64)
+    check(lib().gp_fill(ctypes.byref(p), str(filling_path).encode(), _ptr(phi), _ptr(mu)))
+    return phi, mu
+
+
+def vtk_write(p, path, phi, mu, ascii=None):
+    phi = np.ascontiguousarray(phi, dtype=np.float64)
+    mu = np.ascontiguousarray(mu, dtype=np.float64)
+    a = p.ascii if ascii is None else int(ascii)
+    check(lib().gp_vtk_write(ctypes.byref(p), str(path).encode(), _ptr(phi), _ptr(mu), a))
+
+
+def vtk_read(p, path, ascii=None):
+    sp, sm = _shapes(p)
+    phi = np.zeros(sp, dtype=np.float64)
+    mu = np.zeros(sm, dtype=np.float64)
+    a = p.ascii if ascii is None else int(ascii)
+    check(lib().gp_vtk_read(ctypes.byref(p), str(path).encode(), _ptr(phi), _ptr(mu), a))
+    return phi, mu
+
+
+class Simulation:
+    """One simulation resident on the current CUDA device (a gp_ctx)."""
+
+    def __init__(self, params, phi, mu, precision=GP_FP64):
+        self.params = params
+        self.N, self.K = params.numphases, params.numcomponents - 1
+        sp, sm = _shapes(params)
+        phi = np.ascontiguousarray(phi, dtype=np.float64)
+        mu = np.ascontiguousarray(mu, dtype=np.float64)
+        if phi.shape != sp or mu.shape != sm:
+            raise ValueError("phi/mu shapes %s/%s, expected %s/%s" % (phi.shape, mu.shape, sp, sm))
+        h = ctypes.c_void_p()
+        check(lib().gp_init(ctypes.byref(h), ctypes.byref(params), _ptr(phi), _ptr(mu), int(precision)))
+        self._h = h
+
+    @property
+    def handle(self):
+        return self._h
+
+    def smooth(self, n):
+        check(lib().gp_smooth(self._h, int(n)), self._h)
+
+    def step(self, n, stats=True):
+        if stats:
+            s = Stats()
+            check(lib().gp_step(self._h, int(n), ctypes.byref(s)), self._h)
+            return s.as_dict(self.N, self.K)
+        check(lib().gp_step(self._h, int(n), None), self._h)
+        return None
+
+    def step_timed(self, n, stats=False):
+        """Steps with device timing: (total_ms, phase_kernel_ms, update_kernel_ms, stats)."""
+        tot, a, b = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        s = Stats() if stats else None
+        check(lib().gp_step_timed(self._h, int(n), ctypes.byref(s) if stats else None, ctypes.byref(tot),
+                                  ctypes.byref(a), ctypes.byref(b)), self._h)
+        return tot.value, a.value, b.value, (s.as_dict(self.N, self.K) if stats else None)
+
+    def get(self):
+        sp, sm = _shapes(self.params)
+        phi = np.zeros(sp, dtype=np.float64)
+        mu = np.zeros(sm, dtype=np.float64)
+        check(lib().gp_get(self._h, _ptr(phi), _ptr(mu)), self._h)
+        return phi, mu
+
+    def set(self, phi, mu):
+        phi = np.ascontiguousarray(phi, dtype=np.float64)
+        mu = np.ascontiguousarray(mu, dtype=np.float64)
+        check(lib().gp_set(self._h, _ptr(phi), _ptr(mu)), self._h)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().gp_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()

@@ -1,0 +1,447 @@
+/*
+ * gp_device.cu -- libgp: the C ABI (include/gp.h) over the sm_100a kernels.
+ * Host orchestration only; the kernels are in gp_step64.cuh / gp_smooth64.cuh.
+ */
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+
+#include "gp_smooth64.cuh"
+
+
+extern "C" const char *gp_host_thread_error(void);
+
+struct gp_ctx {
+  gp_params p;
+  gp_derived d;
+  gp_precision prec;
+  int dev;
+  cudaStream_t stream;
+  gpd::Grid g;
+  double *phi[2], *mu[2];       /* ping-pong state planes */
+  int cur;
+  double *dphi;                 /* delta-phi over the interior plus a ring */
+  long long *minmax;            /* running extremes as ordered integers */
+  double *partials;             /* per-block sums of the last stats step */
+  double *sums;                 /* reduced sums */
+  int ublocks;                  /* blocks of k_update */
+  long long steps;
+  gp_stats last;
+  char err[256];
+};
+
+namespace {
+
+int fail(gp_ctx *c, int code, const char *fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  if (c) vsnprintf(c->err, sizeof c->err, fmt, ap);
+  else {
+    char buf[256];
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    gp_set_thread_error("%s", buf);
+  }
+  va_end(ap);
+  return code;
+}
+
+#define CK(call)                                                                        \
+  do {                                                                                  \
+    cudaError_t e_ = (call);                                                            \
+    if (e_ != cudaSuccess) return fail(c, GP_ECUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+  } while (0)
+
+bool pow2(double v) {
+  int e;
+  double m = frexp(fabs(v), &e);
+  return v != 0.0 && m == 0.5;
+}
+
+/* ---- kernel dispatch over the template parameters -------------------- */
+
+struct Kern {
+  void (*dphi)(const double *, const double *, double *, gpd::Grid);
+  void (*upd)(const double *, const double *, const double *, double *, double *, gpd::Grid, gpd::StatBufs);
+  void (*sdphi)(const double *, double *, gpd::Grid);
+  void (*supd)(const double *, const double *, const double *, double *, double *, gpd::Grid);
+  size_t smem_dphi, smem_upd;
+};
+
+template <int N, int K, bool A>
+Kern make() {
+  Kern k;
+  k.dphi = gpd::k_dphi<N, K, A>;
+  k.upd = gpd::k_update<N, K>;
+  k.sdphi = gpd::k_sdphi<N, A>;
+  k.supd = gpd::k_supdate<N, K>;
+  k.smem_dphi = sizeof(gpd::DphiSmem<N>);
+  k.smem_upd = sizeof(gpd::UpdSmem<N, K>);
+  return k;
+}
+
+bool pick(int N, int K, bool A, Kern *out) {
+#define CASE(n, k)                                   \
+  if (N == n && K == k) {                            \
+    *out = A ? make<n, k, true>() : make<n, k, false>(); \
+    return true;                                     \
+  }
+  CASE(2, 1) CASE(3, 1) CASE(4, 1) CASE(2, 2) CASE(3, 2) CASE(4, 2)
+#undef CASE
+  return false;
+}
+
+int setup_kernels(gp_ctx *c, const Kern &k) {
+  CK(cudaFuncSetAttribute(k.dphi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem_dphi));
+  CK(cudaFuncSetAttribute(k.upd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem_upd));
+  return GP_OK;
+}
+
+__global__ void k_reduce_partials(const double *__restrict__ part, int nblocks, int nsum, double *__restrict__ out) {
+  /* one thread per sum, blocks in order: deterministic */
+  int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= nsum) return;
+  double s = 0.0;
+  for (int b = 0; b < nblocks; b++) s += part[(long long)b * nsum + f];
+  out[f] = s;
+}
+
+double from_ord(long long i) {
+  if (i < 0) i ^= 0x7fffffffffffffffLL;
+  double v;
+  memcpy(&v, &i, 8);
+  return v;
+}
+long long to_ord(double v) {
+  long long i;
+  memcpy(&i, &v, 8);
+  return i < 0 ? i ^ 0x7fffffffffffffffLL : i;
+}
+
+int upload_state(gp_ctx *c, const double *phi, const double *mu, cudaMemcpyKind kind) {
+  const gp_derived &d = c->d;
+  for (int a = 0; a < d.N; a++)
+    CK(cudaMemcpy2DAsync(c->phi[c->cur] + a * c->g.plane, (size_t)c->g.pitch * 8, phi + (size_t)a * d.mx * d.my,
+                         (size_t)d.my * 8, (size_t)d.my * 8, (size_t)d.mx, kind, c->stream));
+  for (int k = 0; k < d.K; k++)
+    CK(cudaMemcpy2DAsync(c->mu[c->cur] + k * c->g.plane, (size_t)c->g.pitch * 8, mu + (size_t)k * d.mx * d.my,
+                         (size_t)d.my * 8, (size_t)d.my * 8, (size_t)d.mx, kind, c->stream));
+  return GP_OK;
+}
+
+int download_state(gp_ctx *c, double *phi, double *mu, cudaMemcpyKind kind) {
+  const gp_derived &d = c->d;
+  for (int a = 0; a < d.N; a++)
+    CK(cudaMemcpy2DAsync(phi + (size_t)a * d.mx * d.my, (size_t)d.my * 8, c->phi[c->cur] + a * c->g.plane,
+                         (size_t)c->g.pitch * 8, (size_t)d.my * 8, (size_t)d.mx, kind, c->stream));
+  for (int k = 0; k < d.K; k++)
+    CK(cudaMemcpy2DAsync(mu + (size_t)k * d.mx * d.my, (size_t)d.my * 8, c->mu[c->cur] + k * c->g.plane,
+                         (size_t)c->g.pitch * 8, (size_t)d.my * 8, (size_t)d.mx, kind, c->stream));
+  return GP_OK;
+}
+
+int reset_minmax(gp_ctx *c) {
+  long long h[2 * (GPK_MAXN + GPK_MAXK)];
+  const int N = c->d.N, K = c->d.K;
+  for (int a = 0; a < N; a++) { h[a] = to_ord(1.0); h[N + a] = to_ord(0.0); }
+  for (int k = 0; k < K; k++) { h[2 * N + k] = to_ord(1.0); h[2 * N + K + k] = to_ord(1.0); }
+  CK(cudaMemcpyAsync(c->minmax, h, sizeof(long long) * 2 * (N + K), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return GP_OK;
+}
+
+}  // namespace
+
+/* ======================================================================= */
+
+/* The constant block is per module and device; a context re-uploads it when
+ * another context was used last.  Contexts are not meant to be driven from
+ * several host threads at once. */
+static const gp_ctx *g_last_ctx = nullptr;
+
+extern "C" {
+
+const char *gp_version(void) { return "libgp 0.1 (sm_100a, FP64 plain step)"; }
+
+size_t gp_params_size(void) { return sizeof(gp_params); }
+
+const char *gp_last_error(const gp_ctx *ctx) { return ctx ? ctx->err : gp_host_thread_error(); }
+
+void *gp_stream(gp_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
+
+int gp_init(gp_ctx **out, const gp_params *p, const double *phi, const double *mu, gp_precision prec) {
+  gp_ctx *c = nullptr;
+  if (!out || !p || !phi || !mu) return fail(nullptr, GP_EINVAL, "gp_init: NULL argument");
+  *out = nullptr;
+  if (prec != GP_FP64) return fail(nullptr, GP_EUNSUPPORTED, "gp_init: only GP_FP64 is built in this context type");
+  c = (gp_ctx *)calloc(1, sizeof(gp_ctx));
+  if (!c) return fail(nullptr, GP_ENOMEM, "gp_init: out of host memory");
+  c->p = *p;
+  c->prec = prec;
+  char err[256] = "";
+  if (gp_host_derive(p, &c->d, err, sizeof err) != GP_OK) {
+    int r = fail(nullptr, GP_EINVAL, "gp_init: %s", err);
+    free(c);
+    return r;
+  }
+  Kern k;
+  if (!pick(c->d.N, c->d.K, c->d.aniso != 0, &k)) {
+    free(c);
+    return fail(nullptr, GP_EINVAL, "gp_init: no kernel for N=%d K=%d", c->d.N, c->d.K);
+  }
+  int rc;
+  cudaError_t e = cudaGetDevice(&c->dev);
+  if (e != cudaSuccess) {
+    free(c);
+    return fail(nullptr, GP_ECUDA, "gp_init: no CUDA device: %s", cudaGetErrorString(e));
+  }
+  e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    free(c);
+    return fail(nullptr, GP_ECUDA, "gp_init: %s", cudaGetErrorString(e));
+  }
+  const gp_derived &d = c->d;
+  gpd::Grid &g = c->g;
+  g.mx = (int)d.mx;
+  g.my = (int)d.my;
+  g.pitch = (int)((d.my + 31) / 32 * 32);
+  g.plane = (long long)g.pitch * d.mx;
+  g.dpitch = (int)((d.my + 2 + 31) / 32 * 32);
+  g.dplane = (long long)g.dpitch * (d.mx + 2);
+  g.dx_pow2 = pow2(d.dx);
+  g.dy_pow2 = pow2(d.dy);
+  g.inv_dx = 1.0 / d.dx;
+  g.inv_dy = 1.0 / d.dy;
+  g.inv_2dy = 1.0 / (2.0 * d.dy);
+  const int ublocks = (int)(((d.my + gpd::TY - 1) / gpd::TY) * ((d.mx + gpd::TX - 1) / gpd::TX));
+  c->ublocks = ublocks;
+  const int nsum = 2 * d.N + 2 * d.K + 1;
+#define ALLOC(ptr, bytes)                                                           \
+  do {                                                                              \
+    if (cudaMalloc((void **)&(ptr), (bytes)) != cudaSuccess) {                       \
+      rc = fail(c, GP_ENOMEM, "gp_init: cudaMalloc of %zu bytes failed", (size_t)(bytes)); \
+      goto bad;                                                                     \
+    }                                                                               \
+  } while (0)
+  ALLOC(c->phi[0], (size_t)g.plane * d.N * 8);
+  ALLOC(c->phi[1], (size_t)g.plane * d.N * 8);
+  ALLOC(c->mu[0], (size_t)g.plane * d.K * 8);
+  ALLOC(c->mu[1], (size_t)g.plane * d.K * 8);
+  ALLOC(c->dphi, (size_t)g.dplane * d.N * 8);
+  ALLOC(c->minmax, sizeof(long long) * 2 * (d.N + d.K));
+  ALLOC(c->partials, sizeof(double) * (size_t)ublocks * nsum);
+  ALLOC(c->sums, sizeof(double) * nsum);
+#undef ALLOC
+  if (cudaDeviceSynchronize() != cudaSuccess ||
+      cudaMemcpyToSymbol(cD, &c->d, sizeof(gp_derived)) != cudaSuccess) {
+    rc = fail(c, GP_ECUDA, "gp_init: constant upload failed");
+    goto bad;
+  }
+  g_last_ctx = c;
+  if ((rc = setup_kernels(c, k)) != GP_OK) goto bad;
+  if (cudaMemsetAsync(c->dphi, 0, (size_t)g.dplane * d.N * 8, c->stream) != cudaSuccess) {
+    rc = fail(c, GP_ECUDA, "gp_init: memset failed");
+    goto bad;
+  }
+  if ((rc = upload_state(c, phi, mu, cudaMemcpyHostToDevice)) != GP_OK) goto bad;
+  if ((rc = reset_minmax(c)) != GP_OK) goto bad;
+  *out = c;
+  return GP_OK;
+bad:
+  gp_set_thread_error("%s", c->err);
+  gp_destroy(c);
+  return rc;
+}
+
+
+static int bind(gp_ctx *c) {
+  if (g_last_ctx != c) {
+    /* another context's kernels may still read the constant block */
+    CK(cudaDeviceSynchronize());
+    CK(cudaMemcpyToSymbol(cD, &c->d, sizeof(gp_derived)));
+    g_last_ctx = c;
+  }
+  return GP_OK;
+}
+
+int gp_smooth(gp_ctx *c, long nsteps) {
+  if (!c || nsteps < 0) return fail(c, GP_EINVAL, "gp_smooth: bad argument");
+  Kern k;
+  pick(c->d.N, c->d.K, c->d.aniso != 0, &k);
+  int rc = bind(c);
+  if (rc) return rc;
+  const gpd::Grid &g = c->g;
+  dim3 grid((g.my + 127) / 128, g.mx);
+  for (long s = 0; s < nsteps; s++) {
+    k.sdphi<<<grid, 128, 0, c->stream>>>(c->phi[c->cur], c->dphi, g);
+    k.supd<<<grid, 128, 0, c->stream>>>(c->phi[c->cur], c->mu[c->cur], c->dphi, c->phi[c->cur ^ 1], c->mu[c->cur ^ 1], g);
+    c->cur ^= 1;
+  }
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(c->stream));
+  return GP_OK;
+}
+
+static int fill_stats(gp_ctx *c, gp_stats *s) {
+  const int N = c->d.N, K = c->d.K, nsum = 2 * N + 2 * K + 1;
+  long long mm[2 * (GPK_MAXN + GPK_MAXK)];
+  double sums[2 * GPK_MAXN + 2 * GPK_MAXK + 1];
+  gpd::Grid &g = c->g;
+  (void)g;
+  k_reduce_partials<<<1, 32, 0, c->stream>>>(c->partials, c->ublocks, nsum, c->sums);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(mm, c->minmax, sizeof(long long) * 2 * (N + K), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(sums, c->sums, sizeof(double) * nsum, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  gp_stats r;
+  memset(&r, 0, sizeof r);
+  for (int a = 0; a < N; a++) {
+    r.phi_max[a] = from_ord(mm[a]);
+    r.phi_min[a] = from_ord(mm[N + a]);
+    r.rel_change_phi[a] = sums[a];
+    r.phi_sum[a] = sums[N + K + a];
+  }
+  for (int k = 0; k < K; k++) {
+    r.mu_max[k] = from_ord(mm[2 * N + k]);
+    r.mu_min[k] = from_ord(mm[2 * N + K + k]);
+    r.rel_change_mu[k] = sums[N + k];
+    r.comp_sum[k] = sums[2 * N + K + k];
+  }
+  r.nonfinite = (long long)llround(sums[2 * N + 2 * K]);
+  r.steps_done = c->steps;
+  c->last = r;
+  if (s) *s = r;
+  return GP_OK;
+}
+
+static int step_impl(gp_ctx *c, long nsteps, gp_stats *stats, double *total_ms, double *ms_phase,
+                     double *ms_update);
+
+int gp_step(gp_ctx *c, long nsteps, gp_stats *stats) { return step_impl(c, nsteps, stats, nullptr, nullptr, nullptr); }
+
+int gp_step_timed(gp_ctx *c, long nsteps, gp_stats *stats, double *total_ms, double *ms_phase, double *ms_update) {
+  return step_impl(c, nsteps, stats, total_ms, ms_phase, ms_update);
+}
+
+static int step_impl(gp_ctx *c, long nsteps, gp_stats *stats, double *total_ms, double *ms_phase,
+                     double *ms_update) {
+  if (!c || nsteps < 0) return fail(c, GP_EINVAL, "gp_step: bad argument");
+  const bool timed = total_ms || ms_phase || ms_update;
+  cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+  double t_phase = 0.0, t_update = 0.0;
+  Kern k;
+  pick(c->d.N, c->d.K, c->d.aniso != 0, &k);
+  int rc = bind(c);
+  if (rc) return rc;
+  const gpd::Grid &g = c->g;
+  dim3 gd((g.my + 2 + gpd::TY - 1) / gpd::TY, (g.mx + 2 + gpd::TX - 1) / gpd::TX);
+  dim3 gu((g.my + gpd::TY - 1) / gpd::TY, (g.mx + gpd::TX - 1) / gpd::TX);
+  if (timed) {
+    for (int i = 0; i < 3; i++) CK(cudaEventCreate(&ev[i]));
+  }
+  cudaEvent_t t_start = nullptr, t_end = nullptr;
+  if (total_ms) {
+    CK(cudaEventCreate(&t_start));
+    CK(cudaEventCreate(&t_end));
+    CK(cudaEventRecord(t_start, c->stream));
+  }
+  for (long s = 0; s < nsteps; s++) {
+    gpd::StatBufs st;
+    st.minmax = c->minmax;
+    st.partials = c->partials;
+    st.want_sums = (stats != nullptr && s == nsteps - 1);
+    if (timed) CK(cudaEventRecord(ev[0], c->stream));
+    k.dphi<<<gd, gpd::NT, k.smem_dphi, c->stream>>>(c->phi[c->cur], c->mu[c->cur], c->dphi, g);
+    if (timed) CK(cudaEventRecord(ev[1], c->stream));
+    k.upd<<<gu, gpd::NT, k.smem_upd, c->stream>>>(c->phi[c->cur], c->mu[c->cur], c->dphi, c->phi[c->cur ^ 1],
+                                                   c->mu[c->cur ^ 1], g, st);
+    if (timed) {
+      float a = 0.f, b = 0.f;
+      CK(cudaEventRecord(ev[2], c->stream));
+      CK(cudaEventSynchronize(ev[2]));
+      CK(cudaEventElapsedTime(&a, ev[0], ev[1]));
+      CK(cudaEventElapsedTime(&b, ev[1], ev[2]));
+      t_phase += a;
+      t_update += b;
+    }
+    c->cur ^= 1;
+    c->steps++;
+  }
+  CK(cudaGetLastError());
+  if (total_ms) {
+    float tt = 0.f;
+    CK(cudaEventRecord(t_end, c->stream));
+    CK(cudaEventSynchronize(t_end));
+    CK(cudaEventElapsedTime(&tt, t_start, t_end));
+    *total_ms = tt;
+    cudaEventDestroy(t_start);
+    cudaEventDestroy(t_end);
+  }
+  if (timed) {
+    for (int i = 0; i < 3; i++) cudaEventDestroy(ev[i]);
+    if (ms_phase) *ms_phase = t_phase;
+    if (ms_update) *ms_update = t_update;
+  }
+  if (stats && nsteps > 0) return fill_stats(c, stats);
+  CK(cudaStreamSynchronize(c->stream));
+  return GP_OK;
+}
+
+int gp_get_stats(gp_ctx *c, gp_stats *s) {
+  if (!c || !s) return fail(c, GP_EINVAL, "gp_get_stats: bad argument");
+  *s = c->last;
+  return GP_OK;
+}
+
+int gp_get(gp_ctx *c, double *phi, double *mu) {
+  if (!c || !phi || !mu) return fail(c, GP_EINVAL, "gp_get: NULL argument");
+  int rc = download_state(c, phi, mu, cudaMemcpyDeviceToHost);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(c->stream));
+  return GP_OK;
+}
+
+int gp_set(gp_ctx *c, const double *phi, const double *mu) {
+  if (!c || !phi || !mu) return fail(c, GP_EINVAL, "gp_set: NULL argument");
+  int rc = upload_state(c, phi, mu, cudaMemcpyHostToDevice);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(c->stream));
+  return GP_OK;
+}
+
+int gp_get_dev(gp_ctx *c, double *phi, double *mu) {
+  if (!c || !phi || !mu) return fail(c, GP_EINVAL, "gp_get_dev: NULL argument");
+  int rc = download_state(c, phi, mu, cudaMemcpyDeviceToDevice);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(c->stream));
+  return GP_OK;
+}
+
+int gp_set_dev(gp_ctx *c, const double *phi, const double *mu) {
+  if (!c || !phi || !mu) return fail(c, GP_EINVAL, "gp_set_dev: NULL argument");
+  int rc = upload_state(c, phi, mu, cudaMemcpyDeviceToDevice);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(c->stream));
+  return GP_OK;
+}
+
+void gp_destroy(gp_ctx *c) {
+  if (!c) return;
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  cudaFree(c->phi[0]);
+  cudaFree(c->phi[1]);
+  cudaFree(c->mu[0]);
+  cudaFree(c->mu[1]);
+  cudaFree(c->dphi);
+  cudaFree(c->minmax);
+  cudaFree(c->partials);
+  cudaFree(c->sums);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  if (g_last_ctx == c) g_last_ctx = nullptr;
+  free(c);
+}
+
+}  /* extern "C" */

@@ -1,0 +1,187 @@
+/*
+ * gp.h -- C ABI of libgp, a B200 (sm_100a) implementation of MicroSim's 2D
+ * grand-potential finite-difference time step (serial solver,
+ * Grand_potential_Finite_difference_2D_serial of the reference).
+ *
+ * The reference has no library boundary: main() (microsim_gp.c:41-151) calls
+ * the solver passes directly on global state.  Each entry point below names the
+ * reference routine(s) it replaces.  Conventions:
+ *   - every call returns 0 (GP_OK) or a negative GP_E* code; gp_last_error()
+ *     gives a message for the last failure on a context (or, with NULL, for
+ *     the calling thread's last context-free failure);
+ *   - the caller owns all host buffers; the library owns all device buffers;
+ *   - fields cross the boundary as interior-only planes in the reference's
+ *     order: phi[a][x][y] (a < NUMPHASES), mu[k][x][y] (k < NUMCOMPONENTS-1),
+ *     x < MESH_X, y < MESH_Y, y contiguous (file_writer.h:172-183);
+ *   - one host thread per context; work is ordered on the context's stream and
+ *     every call that returns data synchronises before returning.
+ * Plain C types only: no CUDA or torch types cross this boundary.
+ */
+#ifndef GP_H_
+#define GP_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GP_MAX_PHASES 6   /* parsing limit; the CUDA kernels take N <= 4 */
+#define GP_MAX_COMP   4   /* independent components K = NUMCOMPONENTS-1; kernels take K <= 2 */
+#define GP_NAME_LEN   52
+
+enum {
+  GP_OK = 0,
+  GP_EINVAL = -1,        /* bad argument or unsupported parameter combination */
+  GP_ENOMEM = -2,        /* host or device allocation failed */
+  GP_ECUDA = -3,         /* CUDA runtime error (no device, launch failure, ...) */
+  GP_ETIMEOUT = -4,      /* a bounded device-side wait gave up */
+  GP_ENONFINITE = -5,    /* the state holds non-finite values */
+  GP_EIO = -6,           /* file could not be read or written */
+  GP_EUNSUPPORTED = -7   /* the reference path exists but is not built here */
+};
+
+typedef enum { GP_FP64 = 0, GP_FP32 = 1 } gp_precision;
+
+/* Boundary types as in the reference (utility_functions.h:471-654,
+ * Input.in "0: Free, 1: Neumann, 2: Dirichlet, 3: Periodic"). */
+enum { GP_BC_FREE = 0, GP_BC_NEUMANN = 1, GP_BC_DIRICHLET = 2, GP_BC_PERIODIC = 3 };
+/* Faces, in the reference's boundary[] order: 0 X-, 1 X+, 2 Y+, 3 Y-, 4 Z+, 5 Z-.
+ * Fields: 0 phi, 1 mu, 2 T (assign_buffer_points_conditions, utility_functions.h:471). */
+
+/*
+ * Parameters of one simulation: the reference's globals after
+ * reading_input_parameters() (reading_input_parameters.h:1-307) and
+ * read_boundary_conditions() (read_boundary_conditions.h:4-57).  Field names
+ * follow the Input.in keys.  Arrays are indexed as in the reference:
+ * gamma[a][b], diffusivity[phase][i][j], A[phase][i][j],
+ * ceq/cfill/slopes[phase1][phase2][comp].
+ */
+typedef struct gp_params {
+  int dimension;
+  long mesh_x, mesh_y, mesh_z;
+  double deltax, deltay, deltaz, deltat;
+  int numphases, numcomponents;           /* as in Input.in: K = numcomponents-1 */
+  long ntimesteps, savet, nsmooth, starttime, restart, track_progress;
+  double R, V, T, Teq, Tfill, temperature_scale, tilt_angle, Rtheta;
+  double epsilon, tau;
+  int function_f, function_w, function_anisotropy, anisotropy_type;
+  int obstacle_key;                       /* OBSTACLE key if present (-1 absent) */
+  int isothermal, tempgrady, binary, ternary, dilute;
+  int shift, shiftj, writecomposition, noise_phasefield, ascii;
+  double amp_noise_phase;
+  double tempgrady_v[5];                  /* base, DeltaT, Distance, OFFSET, velocity */
+  double gamma[GP_MAX_PHASES][GP_MAX_PHASES];
+  double tau_ab[GP_MAX_PHASES][GP_MAX_PHASES];
+  double dab[GP_MAX_PHASES][GP_MAX_PHASES];
+  double gamma_abc[GP_MAX_PHASES][GP_MAX_PHASES][GP_MAX_PHASES];
+  double diffusivity[GP_MAX_PHASES][GP_MAX_COMP][GP_MAX_COMP];
+  double A[GP_MAX_PHASES][GP_MAX_COMP][GP_MAX_COMP];
+  double ceq[GP_MAX_PHASES][GP_MAX_PHASES][GP_MAX_COMP];
+  double cfill[GP_MAX_PHASES][GP_MAX_PHASES][GP_MAX_COMP];
+  double slopes[GP_MAX_PHASES][GP_MAX_PHASES][GP_MAX_COMP];
+  /* Rotation_matrix = {p1, p2, theta_x, theta_y, theta_z}: Euler angles in
+   * degrees per unordered phase pair (utility_functions.h:700-774). */
+  double rot_angles[GP_MAX_PHASES][GP_MAX_PHASES][3];
+  int rot_set[GP_MAX_PHASES][GP_MAX_PHASES];
+  int bc_type[3][6];                      /* [field][face]; -1 = no BOUNDARY line */
+  double bc_value[3][6];
+  int bc_value_set[3];                    /* BOUNDARY_VALUE line seen per field */
+  int bc_proxy_type[3][6];                /* type in force when BOUNDARY_VALUE fixed the copy sources */
+  int have_gamma, have_tau_ab, have_dab, have_gamma_abc;
+  char phases[GP_MAX_PHASES][GP_NAME_LEN];
+  char components[GP_MAX_COMP + 1][GP_NAME_LEN];
+} gp_params;
+
+/* Diagnostics after gp_step / gp_smooth.  phi/mu extremes follow the
+ * reference's progress record (calculate_divergence_concentration.h:273-296):
+ * running extremes since gp_init (starting from phi 1/0 and mu 1/1 as in
+ * serialinfo_xy.h:59-66), never reset.  rel_change_* are sum(delta^2) of the
+ * last step (printed as sqrt by microsim_gp.c:139-148).  All sums run over the
+ * interior cells only (the reference also adds ghost cells whose values depend
+ * on stale buffer contents).  phi_sum/comp_sum are FP64 sums of phi_a and of
+ * c_k = sum_a c_a,k(mu) h_a(phi) over the interior after the last step. */
+typedef struct gp_stats {
+  double phi_max[GP_MAX_PHASES], phi_min[GP_MAX_PHASES];
+  double mu_max[GP_MAX_COMP], mu_min[GP_MAX_COMP];
+  double rel_change_phi[GP_MAX_PHASES], rel_change_mu[GP_MAX_COMP];
+  double phi_sum[GP_MAX_PHASES];
+  double comp_sum[GP_MAX_COMP];
+  long long nonfinite;                    /* interior cells with a non-finite field */
+  long long steps_done;                   /* time steps taken since gp_init */
+} gp_stats;
+
+typedef struct gp_ctx gp_ctx;
+
+/* ---- host surface (no GPU needed) ------------------------------------- */
+
+/* Parse Input.in.  Replaces reading_input_parameters (reading_input_parameters.h:1-307)
+ * and read_boundary_conditions (read_boundary_conditions.h:4-41); the echo files
+ * <in>.out/<in>.bd are not written.  Returns GP_EIO if the file cannot be read,
+ * GP_EINVAL if a size/count exceeds GP_MAX_*. */
+int gp_params_load(gp_params *p, const char *input_path);
+
+/* Fill the interior from Filling.in.  Replaces fill_domain (fill_domain.h:4-151)
+ * with fill_phase_cube/cylinder/sphere/ellipse and fill_composition_cube
+ * (filling.h:6-270).  phi: [N][MESH_X][MESH_Y], mu: [K][MESH_X][MESH_Y]. */
+int gp_fill(const gp_params *p, const char *filling_path, double *phi, double *mu);
+
+/* Legacy-VTK writer/reader of the interior.  Replaces writetofile_serial2D[_binary]
+ * and readfromfile_serial2D[_binary] (file_writer.h:23-70,71-416).
+ * ascii=1: "%le" text; ascii=0: big-endian float64. */
+int gp_vtk_write(const gp_params *p, const char *path, const double *phi, const double *mu, int ascii);
+int gp_vtk_read(const gp_params *p, const char *path, double *phi, double *mu, int ascii);
+
+/* ---- device path ------------------------------------------------------- */
+
+/* Create a context on the current CUDA device, upload the interior state and
+ * the derived constants (init_propertymatrices, functionF_01.h:169-230, and
+ * initialize_variables, initialize_variables.h:4-28, evaluated on the host).
+ * Replaces serialinfo_xy (serialinfo_xy.h:1-66) + initialize_functions_solverloop
+ * (initialize_functions_solverloop.h:4-58) + apply_boundary_conditions(0) at
+ * microsim_gp.c:84.  GP_EINVAL for combinations the kernels do not cover
+ * (N>4, K>2, non-isothermal, noise, free/Dirichlet BCs, 3-D). */
+int gp_init(gp_ctx **ctx, const gp_params *p, const double *phi, const double *mu,
+            gp_precision prec);
+
+/* nsteps preconditioning sweeps; replaces the loop
+ * "for(t=1; t<nsmooth; t++) { smooth(); apply_boundary_conditions(0); }"
+ * (microsim_gp.c:97-100, solverloop.h:72-90), i.e. call with nsmooth-1. */
+int gp_smooth(gp_ctx *ctx, long nsteps);
+
+/* nsteps explicit time steps; each replaces solverloop_phasefield +
+ * apply_boundary_conditions + solverloop_concentration + apply_boundary_conditions
+ * (microsim_gp.c:103-106, solverloop.h:21-71, boundary_serial.h:176-203).
+ * stats may be NULL. */
+int gp_step(gp_ctx *ctx, long nsteps, gp_stats *stats);
+
+/* Copy the interior state out / in (host buffers, layouts as above). */
+int gp_get(gp_ctx *ctx, double *phi, double *mu);
+int gp_set(gp_ctx *ctx, const double *phi, const double *mu);
+
+/* Same as gp_get/gp_set with device pointers (FP64, same layouts) on the
+ * context's device; used by the Python integrator to exchange CUDA tensors. */
+int gp_get_dev(gp_ctx *ctx, double *phi_dev, double *mu_dev);
+int gp_set_dev(gp_ctx *ctx, const double *phi_dev, const double *mu_dev);
+
+int gp_get_stats(gp_ctx *ctx, gp_stats *stats);
+
+/* gp_step with CUDA events recorded on the context's stream: total_ms is the
+ * device time of the nsteps steps, ms_phase / ms_update the summed device
+ * times of the phase-field and concentration kernels (each may be NULL).
+ * Measurement entry point for bench.py; results are those of gp_step. */
+int gp_step_timed(gp_ctx *ctx, long nsteps, gp_stats *stats, double *total_ms,
+                  double *ms_phase, double *ms_update);
+
+/* Stream the context's work is ordered on (a cudaStream_t as an opaque pointer). */
+void *gp_stream(gp_ctx *ctx);
+
+void gp_destroy(gp_ctx *ctx);
+const char *gp_last_error(const gp_ctx *ctx);
+const char *gp_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GP_H_ */

@@ -1,0 +1,106 @@
+"""CUDA path (libgp, through the C ABI) against the CPU oracle, bit for bit."""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+import recipes  # noqa: E402
+
+import eshwar_dipan_b200 as gp  # noqa: E402
+from gp_cases import PARITY_CASES, build_case  # noqa: E402
+from oracle_py import Oracle, bits_equal, mismatch_report  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+
+def _both(ip, fp, nsmooth_iters, nsteps, recip_div=1):
+    p = gp.load_params(ip)
+    phi, mu = gp.fill(p, fp)
+    o = Oracle(p, recip_div=recip_div)
+    o.set(phi, mu)
+    o.smooth(nsmooth_iters)
+    sim = gp.Simulation(p, phi, mu)
+    sim.smooth(nsmooth_iters)
+    return p, o, sim
+
+
+@pytest.mark.parametrize("name", sorted(PARITY_CASES))
+def test_step_bitwise(tmp_path, name):
+    """Smoothing sweeps then 25 steps: phi and mu identical bit for bit."""
+    ip, fp = build_case(tmp_path, name)
+    p, o, sim = _both(ip, fp, 9, 0)
+    a_phi, a_mu = sim.get()
+    b_phi, b_mu = o.get()
+    assert bits_equal(a_phi, b_phi), "after smoothing: " + mismatch_report(a_phi, b_phi)
+    assert bits_equal(a_mu, b_mu), "after smoothing: " + mismatch_report(a_mu, b_mu)
+    for chunk in (1, 4, 20):
+        o.step(chunk)
+        st = sim.step(chunk)
+        a_phi, a_mu = sim.get()
+        b_phi, b_mu = o.get()
+        assert bits_equal(a_phi, b_phi), "phi after +%d steps: %s" % (chunk, mismatch_report(a_phi, b_phi))
+        assert bits_equal(a_mu, b_mu), "mu after +%d steps: %s" % (chunk, mismatch_report(a_mu, b_mu))
+    ost = o.stats()
+    for k in ("phi_max", "phi_min", "mu_max", "mu_min"):
+        assert st[k] == ost[k], k
+    for k in ("rel_change_phi", "rel_change_mu", "phi_sum", "comp_sum"):
+        np.testing.assert_allclose(st[k], ost[k], rtol=1e-12, atol=1e-300, err_msg=k)
+    assert st["nonfinite"] == 0 and st["steps_done"] == 25
+
+
+@pytest.mark.parametrize("name", ["bin_iso_antitrap", "ternary3_aniso_periodic"])
+def test_step_from_uploaded_state(tmp_path, name):
+    """gp_set of an arbitrary in-range state, then steps: identical to the oracle."""
+    ip, fp = build_case(tmp_path, name)
+    p = gp.load_params(ip)
+    phi, mu = gp.fill(p, fp)
+    o = Oracle(p, recip_div=1)
+    o.set(phi, mu)
+    o.smooth(9)
+    o.step(7)
+    phi1, mu1 = o.get()
+    sim = gp.Simulation(p, phi, mu)
+    sim.set(phi1, mu1)
+    o2 = Oracle(p, recip_div=1)
+    o2.set(phi1, mu1)
+    o2.step(10)
+    sim.step(10, stats=False)
+    a_phi, a_mu = sim.get()
+    b_phi, b_mu = o2.get()
+    assert bits_equal(a_phi, b_phi), mismatch_report(a_phi, b_phi)
+    assert bits_equal(a_mu, b_mu), mismatch_report(a_mu, b_mu)
+
+
+def test_smoothing_vs_reference_reciprocal(tmp_path):
+    """Against the oracle with the reference's pow(x,-1) reciprocal the
+    smoothing differs only by rounding of the dc/dmu inverse (mu, few ulp)."""
+    ip, fp = build_case(tmp_path, "ternary3_aniso_periodic")
+    p, o, sim = _both(ip, fp, 9, 0, recip_div=0)
+    a_phi, a_mu = sim.get()
+    b_phi, b_mu = o.get()
+    assert bits_equal(a_phi, b_phi)
+    rel = np.abs(a_mu - b_mu) / np.maximum(np.abs(b_mu), 1e-300)
+    assert rel.max() <= 8 * np.finfo(np.float64).eps
+
+
+@pytest.mark.parametrize("key", sorted(recipes.GOLDEN))
+def test_golden_vtk_replay(tmp_path, key):
+    """All twelve result files shipped with the reference, reproduced by the
+    CUDA path at the files' printed precision."""
+    kind, steps, fields = recipes.GOLDEN[key]
+    ip, fp = recipes.write_golden_case(tmp_path, kind)
+    p = gp.load_params(ip)
+    phi, mu = gp.fill(p, fp)
+    sim = gp.Simulation(p, phi, mu)
+    if steps:
+        sim.smooth(9)
+        sim.step(steps, stats=False)
+    phi, mu = sim.get()
+    z = recipes.load_golden()
+    for name, (fk, idx) in fields.items():
+        ours = recipes.as_le((phi if fk == "phi" else mu)[idx])
+        ref = recipes.golden_text(z, key, name)
+        bad = sum(a != b for a, b in zip(ours, ref))
+        assert bad == 0, "%s/%s: %d values differ" % (key, name, bad)
