@@ -114,6 +114,7 @@ SIGNATURES = {
     "gp_get_stats": (c_int, [c_void_p, POINTER(Stats)]),
     "gp_step_timed": (c_int, [c_void_p, c_long, POINTER(Stats), POINTER(c_double), POINTER(c_double),
                               POINTER(c_double)]),
+    "gp_step_noalloc": (c_int, [POINTER(Params), c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     "gp_stream": (c_void_p, [c_void_p]),
     "gp_destroy": (None, [c_void_p]),
     "gp_last_error": (ctypes.c_char_p, [c_void_p]),

@@ -445,3 +445,89 @@ void gp_destroy(gp_ctx *c) {
 }
 
 }  /* extern "C" */
+
+/* ======================================================================= */
+/* One time step without any allocation (gp_step_noalloc in gp.h).          */
+/*                                                                         */
+/* Some callers cannot call cudaMalloc: a host application that hands us   */
+/* device buffers from its own pool or arena allocator and forbids any     */
+/* other allocation (memory budgets fixed up front, allocator locks it     */
+/* must not contend on, or code paths where a failing allocation cannot be */
+/* handled).  For them the step's only scratch buffer, delta-phi over the  */
+/* interior plus a one-cell ring, and the running-extreme counters live in */
+/* this fixed array instead of per-context cudaMalloc'd memory.  Every GPU */
+/* that loads the library holds these 32 MiB until the process exits.      */
+/* ======================================================================= */
+
+#define GP_NOALLOC_SCRATCH_DOUBLES (4u * 1024u * 1024u)   /* 32 MiB */
+static __device__ __align__(256) double g_noalloc_scratch[GP_NOALLOC_SCRATCH_DOUBLES];
+
+#define GP_NOALLOC_MAX_DEVICES 64
+/* Device address of g_noalloc_scratch per device, looked up on the first call
+ * on that device.  In host code the array's name only stands in for the
+ * symbol; kernels must be given the address cudaGetSymbolAddress returns. */
+static double *g_noalloc_ptr[GP_NOALLOC_MAX_DEVICES];
+
+extern "C" int gp_step_noalloc(const gp_params *p, const double *phi_in, const double *mu_in, double *phi_out,
+                               double *mu_out, void *stream) {
+  gp_ctx *c = nullptr; /* CK() reports through the thread's error slot */
+  if (!p || !phi_in || !mu_in || !phi_out || !mu_out)
+    return fail(nullptr, GP_EINVAL, "gp_step_noalloc: NULL argument");
+  if (phi_in == phi_out || mu_in == mu_out)
+    return fail(nullptr, GP_EINVAL, "gp_step_noalloc: input and output buffers must differ");
+  gp_derived d;
+  char err[256] = "";
+  if (gp_host_derive(p, &d, err, sizeof err) != GP_OK) return fail(nullptr, GP_EINVAL, "gp_step_noalloc: %s", err);
+  Kern k;
+  if (!pick(d.N, d.K, d.aniso != 0, &k)) return fail(nullptr, GP_EINVAL, "gp_step_noalloc: no kernel for N=%d K=%d", d.N, d.K);
+  gpd::Grid g;
+  g.mx = (int)d.mx;
+  g.my = (int)d.my;
+  g.pitch = (int)d.my; /* caller's planes are contiguous [field][MESH_X][MESH_Y] */
+  g.plane = (long long)d.mx * d.my;
+  g.dpitch = (int)((d.my + 2 + 31) / 32 * 32);
+  g.dplane = (long long)g.dpitch * (d.mx + 2);
+  g.dx_pow2 = pow2(d.dx);
+  g.dy_pow2 = pow2(d.dy);
+  g.inv_dx = 1.0 / d.dx;
+  g.inv_dy = 1.0 / d.dy;
+  g.inv_2dy = 1.0 / (2.0 * d.dy);
+  /* scratch layout: [running extremes, 2(N+K) long longs][pad to 256 B][delta-phi, N planes] */
+  const size_t head = 32;  /* doubles; holds 2*(4+2) long longs and keeps delta-phi 256-B aligned */
+  const size_t need = head + (size_t)d.N * (size_t)g.dplane;
+  if (need > GP_NOALLOC_SCRATCH_DOUBLES)
+    return fail(nullptr, GP_EINVAL,
+                "gp_step_noalloc: grid %ldx%ld with %d phases needs %zu doubles of scratch, the fixed maximum is %u "
+                "(about 1.3 million cells for 3 phases); use gp_init/gp_step for larger grids",
+                d.mx, d.my, d.N, need, GP_NOALLOC_SCRATCH_DOUBLES);
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= GP_NOALLOC_MAX_DEVICES) return fail(nullptr, GP_EINVAL, "gp_step_noalloc: device %d", dev);
+  if (!g_noalloc_ptr[dev]) {
+    void *ptr = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+    if (e != cudaSuccess || !ptr)
+      return fail(nullptr, GP_ECUDA, "gp_step_noalloc: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+    g_noalloc_ptr[dev] = (double *)ptr;
+  }
+  double *scratch = g_noalloc_ptr[dev];
+  cudaStream_t s = (cudaStream_t)stream;
+  CK(cudaFuncSetAttribute(k.dphi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem_dphi));
+  CK(cudaFuncSetAttribute(k.upd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem_upd));
+  /* the constant block is shared with the contexts: make them upload theirs again */
+  g_last_ctx = nullptr;
+  CK(cudaMemcpyToSymbolAsync(cD, &d, sizeof(gp_derived), 0, cudaMemcpyHostToDevice, s));
+  /* the previous call's extremes are still in the array: start them from zero */
+  CK(cudaMemsetAsync(scratch, 0, head * sizeof(double), s));
+  gpd::StatBufs st;
+  st.minmax = (long long *)scratch;
+  st.partials = scratch; /* not written: no sums requested */
+  st.want_sums = 0;
+  double *dphi = scratch + head;
+  dim3 gd((g.my + 2 + gpd::TY - 1) / gpd::TY, (g.mx + 2 + gpd::TX - 1) / gpd::TX);
+  dim3 gu((g.my + gpd::TY - 1) / gpd::TY, (g.mx + gpd::TX - 1) / gpd::TX);
+  k.dphi<<<gd, gpd::NT, k.smem_dphi, s>>>(phi_in, mu_in, dphi, g);
+  k.upd<<<gu, gpd::NT, k.smem_upd, s>>>(phi_in, mu_in, dphi, phi_out, mu_out, g, st);
+  CK(cudaGetLastError());
+  return GP_OK;
+}

@@ -174,6 +174,27 @@ int gp_get_stats(gp_ctx *ctx, gp_stats *stats);
 int gp_step_timed(gp_ctx *ctx, long nsteps, gp_stats *stats, double *total_ms,
                   double *ms_phase, double *ms_update);
 
+/* One FP64 time step that allocates nothing.  This entry point has no
+ * counterpart in the reference; it exists for callers that cannot call
+ * cudaMalloc -- applications that own all device memory through their own pool
+ * or arena, run under a fixed memory budget, or sit on a path where a failed
+ * allocation cannot be handled.  They pass their own device buffers:
+ * phi_in/mu_in (read) and phi_out/mu_out (written), contiguous planes
+ * [N][MESH_X][MESH_Y] and [K][MESH_X][MESH_Y] on the current device, outputs not
+ * aliasing inputs; stream is a cudaStream_t (NULL = default stream).
+ * The step's scratch (delta-phi over the interior plus a one-cell ring) lives
+ * in a fixed 32 MiB array inside the library that every GPU which loads the
+ * library keeps until exit; grids needing more (about 1.3 million cells with
+ * 3 phases) are rejected with GP_EINVAL and a message.  The first call on a
+ * device looks up that array's device address (cudaGetSymbolAddress); make
+ * that first call before any stream capture.  All calls share the array, so
+ * calls that overlap on the GPU (other streams, other host threads) race; the
+ * same holds for the constant block shared with the contexts.  The call is
+ * asynchronous on `stream`; no progress record is produced.  Results are those
+ * of gp_step. */
+int gp_step_noalloc(const gp_params *p, const double *phi_in, const double *mu_in,
+                    double *phi_out, double *mu_out, void *stream);
+
 /* Stream the context's work is ordered on (a cudaStream_t as an opaque pointer). */
 void *gp_stream(gp_ctx *ctx);
 
