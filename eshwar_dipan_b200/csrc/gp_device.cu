@@ -8,6 +8,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
+#include <climits>
 #include <cstring>
 
 #include "gp_smooth64.cuh"
@@ -25,7 +26,8 @@ struct gp_ctx {
   double *phi[2], *mu[2];       /* ping-pong state planes */
   int cur;
   double *dphi;                 /* delta-phi over the interior plus a ring */
-  long long *minmax;            /* running extremes as ordered integers */
+  long long *ext;               /* per-block running extremes, ordered integers [ublocks][2(N+K)] */
+  long long *ext_red;           /* their fold over blocks [2(N+K)] */
   double *partials;             /* per-block sums of the last stats step */
   double *sums;                 /* reduced sums */
   int ublocks;                  /* blocks of k_update */
@@ -100,13 +102,43 @@ int setup_kernels(gp_ctx *c, const Kern &k) {
   return GP_OK;
 }
 
+/* Fold the per-block sums (one CTA per quantity) in a fixed order: the result
+ * does not depend on scheduling. */
 __global__ void k_reduce_partials(const double *__restrict__ part, int nblocks, int nsum, double *__restrict__ out) {
-  /* one thread per sum, blocks in order: deterministic */
-  int f = blockIdx.x * blockDim.x + threadIdx.x;
-  if (f >= nsum) return;
+  __shared__ double r[256];
+  const int f = blockIdx.x;
   double s = 0.0;
-  for (int b = 0; b < nblocks; b++) s += part[(long long)b * nsum + f];
-  out[f] = s;
+  for (int b = threadIdx.x; b < nblocks; b += 256) s += part[(long long)b * nsum + f];
+  r[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if (threadIdx.x < w) r[threadIdx.x] += r[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[f] = r[0];
+}
+
+/* Fold the per-block running extremes: slot f < nmax is a maximum, else a minimum. */
+__global__ void k_reduce_ext(const long long *__restrict__ ext, int nblocks, int nslot, int N, int K,
+                             long long *__restrict__ out) {
+  __shared__ long long r[256];
+  const int f = blockIdx.x;
+  const bool isMax = f < N || (f >= 2 * N && f < 2 * N + K);
+  long long v = isMax ? LLONG_MIN : LLONG_MAX;
+  for (int b = threadIdx.x; b < nblocks; b += 256) {
+    long long w = ext[(long long)b * nslot + f];
+    v = isMax ? (w > v ? w : v) : (w < v ? w : v);
+  }
+  r[threadIdx.x] = v;
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if (threadIdx.x < w) {
+      long long a = r[threadIdx.x], b = r[threadIdx.x + w];
+      r[threadIdx.x] = isMax ? (a > b ? a : b) : (a < b ? a : b);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[f] = r[0];
 }
 
 double from_ord(long long i) {
@@ -143,13 +175,22 @@ int download_state(gp_ctx *c, double *phi, double *mu, cudaMemcpyKind kind) {
   return GP_OK;
 }
 
+/* Running extremes start where the reference starts them (serialinfo_xy.h:59-66):
+ * phi max 1, min 0; mu max 1, min 1; every block slot holds them. */
 int reset_minmax(gp_ctx *c) {
-  long long h[2 * (GPK_MAXN + GPK_MAXK)];
-  const int N = c->d.N, K = c->d.K;
-  for (int a = 0; a < N; a++) { h[a] = to_ord(1.0); h[N + a] = to_ord(0.0); }
-  for (int k = 0; k < K; k++) { h[2 * N + k] = to_ord(1.0); h[2 * N + K + k] = to_ord(1.0); }
-  CK(cudaMemcpyAsync(c->minmax, h, sizeof(long long) * 2 * (N + K), cudaMemcpyHostToDevice, c->stream));
-  CK(cudaStreamSynchronize(c->stream));
+  const int N = c->d.N, K = c->d.K, ne = 2 * (N + K);
+  long long *h = (long long *)malloc(sizeof(long long) * (size_t)ne * c->ublocks);
+  if (!h) return fail(c, GP_ENOMEM, "gp_init: out of host memory");
+  for (int b = 0; b < c->ublocks; b++) {
+    long long *s = h + (size_t)b * ne;
+    for (int a = 0; a < N; a++) { s[a] = to_ord(1.0); s[N + a] = to_ord(0.0); }
+    for (int k = 0; k < K; k++) { s[2 * N + k] = to_ord(1.0); s[2 * N + K + k] = to_ord(1.0); }
+  }
+  cudaError_t e = cudaMemcpyAsync(c->ext, h, sizeof(long long) * (size_t)ne * c->ublocks, cudaMemcpyHostToDevice,
+                                  c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  free(h);
+  if (e != cudaSuccess) return fail(c, GP_ECUDA, "gp_init: %s", cudaGetErrorString(e));
   return GP_OK;
 }
 
@@ -231,7 +272,8 @@ int gp_init(gp_ctx **out, const gp_params *p, const double *phi, const double *m
   ALLOC(c->mu[0], (size_t)g.plane * d.K * 8);
   ALLOC(c->mu[1], (size_t)g.plane * d.K * 8);
   ALLOC(c->dphi, (size_t)g.dplane * d.N * 8);
-  ALLOC(c->minmax, sizeof(long long) * 2 * (d.N + d.K));
+  ALLOC(c->ext, sizeof(long long) * 2 * (d.N + d.K) * (size_t)ublocks);
+  ALLOC(c->ext_red, sizeof(long long) * 2 * (d.N + d.K));
   ALLOC(c->partials, sizeof(double) * (size_t)ublocks * nsum);
   ALLOC(c->sums, sizeof(double) * nsum);
 #undef ALLOC
@@ -291,9 +333,10 @@ static int fill_stats(gp_ctx *c, gp_stats *s) {
   double sums[2 * GPK_MAXN + 2 * GPK_MAXK + 1];
   gpd::Grid &g = c->g;
   (void)g;
-  k_reduce_partials<<<1, 32, 0, c->stream>>>(c->partials, c->ublocks, nsum, c->sums);
+  k_reduce_partials<<<nsum, 256, 0, c->stream>>>(c->partials, c->ublocks, nsum, c->sums);
+  k_reduce_ext<<<2 * (N + K), 256, 0, c->stream>>>(c->ext, c->ublocks, 2 * (N + K), N, K, c->ext_red);
   CK(cudaGetLastError());
-  CK(cudaMemcpyAsync(mm, c->minmax, sizeof(long long) * 2 * (N + K), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(mm, c->ext_red, sizeof(long long) * 2 * (N + K), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaMemcpyAsync(sums, c->sums, sizeof(double) * nsum, cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   gp_stats r;
@@ -350,7 +393,7 @@ static int step_impl(gp_ctx *c, long nsteps, gp_stats *stats, double *total_ms, 
   }
   for (long s = 0; s < nsteps; s++) {
     gpd::StatBufs st;
-    st.minmax = c->minmax;
+    st.ext = c->ext;
     st.partials = c->partials;
     st.want_sums = (stats != nullptr && s == nsteps - 1);
     if (timed) CK(cudaEventRecord(ev[0], c->stream));
@@ -436,7 +479,8 @@ void gp_destroy(gp_ctx *c) {
   cudaFree(c->mu[0]);
   cudaFree(c->mu[1]);
   cudaFree(c->dphi);
-  cudaFree(c->minmax);
+  cudaFree(c->ext);
+  cudaFree(c->ext_red);
   cudaFree(c->partials);
   cudaFree(c->sums);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -520,7 +564,7 @@ extern "C" int gp_step_noalloc(const gp_params *p, const double *phi_in, const d
   /* the previous call's extremes are still in the array: start them from zero */
   CK(cudaMemsetAsync(scratch, 0, head * sizeof(double), s));
   gpd::StatBufs st;
-  st.minmax = (long long *)scratch;
+  st.ext = nullptr; /* no progress record on this path */
   st.partials = scratch; /* not written: no sums requested */
   st.want_sums = 0;
   double *dphi = scratch + head;

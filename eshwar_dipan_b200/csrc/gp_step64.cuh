@@ -390,10 +390,81 @@ __device__ __forceinline__ long long ord(double v) {
 }
 
 struct StatBufs {
-  long long *minmax;   /* [2*(N+K)]: max phi, min phi, max mu, min mu (ordered ints) */
+  long long *ext;      /* per-block running extremes [blocks][2*(N+K)] (ordered ints), or NULL */
   double *partials;    /* [blocks][2N+2K+1] sums when want_sums */
   int want_sums;
 };
+
+/* Per-block running extremes and (on request) sums of the cells a block owns.
+ * Each block owns its slots, so no atomics are needed and results are
+ * deterministic; gp_step folds the slots when it reports. */
+template <int N, int K>
+__device__ __forceinline__ void block_stats(bool valid, const double *nph, const double *nm, const double *dp,
+                                            const double *dmu, const StatBufs &st) {
+  constexpr int NE = 2 * (N + K), NS = 2 * N + 2 * K + 1, NW = NT / 32;
+  __shared__ double red[NW][NE > NS ? NE : NS];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const long long blk = (long long)blockIdx.y * gridDim.x + blockIdx.x;
+  if (st.ext) {
+#pragma unroll
+    for (int f = 0; f < NE; f++) {
+      const int fld = f >> 1;
+      const bool isMax = !(f & 1);
+      double v = isMax ? -INFINITY : INFINITY;
+      if (valid) {
+        double w = fld < N ? nph[fld] : nm[fld - N];
+        if (w == w) v = w;
+      }
+      v = isMax ? warp_max(v) : warp_min(v);
+      if (lane == 0) red[wid][f] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < NE) {
+      const int f = threadIdx.x, fld = f >> 1;
+      const bool isMax = !(f & 1);
+      double r = red[0][f];
+      for (int w = 1; w < NW; w++) r = isMax ? fmax(r, red[w][f]) : fmin(r, red[w][f]);
+      /* slot layout: max phi[N], min phi[N], max mu[K], min mu[K] */
+      const int slot = fld < N ? (isMax ? fld : N + fld) : (isMax ? 2 * N + (fld - N) : 2 * N + K + (fld - N));
+      long long *p = st.ext + blk * NE + slot;
+      if (isMax && r > -INFINITY && ord(r) > *p) *p = ord(r);
+      if (!isMax && r < INFINITY && ord(r) < *p) *p = ord(r);
+    }
+    __syncthreads();
+  }
+  if (st.want_sums) {
+    for (int f = 0; f < NS; f++) {
+      double v = 0.0;
+      if (valid) {
+        if (f < N) v = dp[f] * dp[f];
+        else if (f < N + K) v = dmu[f - N] * dmu[f - N];
+        else if (f < 2 * N + K) v = nph[f - N - K];
+        else if (f < 2 * N + 2 * K) {
+          int k = f - 2 * N - K;
+          double comp = 0.0;
+#pragma unroll
+          for (int b = 0; b < N; b++) comp += c_mu<K>(nm, b, k) * h<N>(nph, b);
+          v = comp;
+        } else {
+          bool bad = false;
+#pragma unroll
+          for (int a = 0; a < N; a++) bad |= !isfinite(nph[a]);
+#pragma unroll
+          for (int k = 0; k < K; k++) bad |= !isfinite(nm[k]);
+          v = bad ? 1.0 : 0.0;
+        }
+      }
+      v = warp_sum(v);
+      if (lane == 0) red[wid][f] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < NS) {
+      double r = 0.0;
+      for (int w = 0; w < NW; w++) r += red[w][threadIdx.x];
+      st.partials[blk * NS + threadIdx.x] = r;
+    }
+  }
+}
 
 /* mu update and phi commit of the interior
  * (calculate_fluxes_concentration_2D + calculate_divergence_concentration_2D,
@@ -406,69 +477,152 @@ __global__ void __launch_bounds__(NT) k_update(const double *__restrict__ phi, c
   UpdSmem<N, K> &sm = *reinterpret_cast<UpdSmem<N, K> *>(smraw);
   const int x0 = blockIdx.y * TX, y0 = blockIdx.x * TY;
   constexpr int L = N - 1;
+  const double cst = cD.obstacle ? cD.jat_obst : cD.jat_well;
 
-  /* stage phi, mu (remapped) and delta-phi, then per-cell quantities */
+  /* stage phi, mu (remapped) and delta-phi */
   for (int e = threadIdx.x; e < SS; e += NT) {
     int i = e / SW, j = e - i * SW;
     int x = x0 - 1 + i, y = y0 - 1 + j;
-    bool in = x <= g.mx && y <= g.my;
-    double ph[N], m[K];
-    if (in) {
+    if (x <= g.mx && y <= g.my) {
       int sx = remap(x, g.mx, cD.bc_x[0][0], cD.bc_x[0][1]), sy = remap(y, g.my, cD.bc_y[0][0], cD.bc_y[0][1]);
       int tx_ = remap(x, g.mx, cD.bc_x[1][0], cD.bc_x[1][1]), ty_ = remap(y, g.my, cD.bc_y[1][0], cD.bc_y[1][1]);
       long long op = (long long)sx * g.pitch + sy, om = (long long)tx_ * g.pitch + ty_;
       long long od = (long long)(x + 1) * g.dpitch + (y + 1);
 #pragma unroll
       for (int a = 0; a < N; a++) {
-        ph[a] = __ldg(phi + a * g.plane + op);
+        sm.P[a][e] = __ldg(phi + a * g.plane + op);
         sm.DP[a][e] = __ldg(dphi + a * g.dplane + od);
       }
 #pragma unroll
-      for (int k = 0; k < K; k++) m[k] = __ldg(mu + k * g.plane + om);
+      for (int k = 0; k < K; k++) sm.M[k][e] = __ldg(mu + k * g.plane + om);
     } else {
 #pragma unroll
-      for (int a = 0; a < N; a++) { ph[a] = 0.0; sm.DP[a][e] = 0.0; }
+      for (int a = 0; a < N; a++) { sm.P[a][e] = 0.0; sm.DP[a][e] = 0.0; }
 #pragma unroll
-      for (int k = 0; k < K; k++) m[k] = 0.0;
+      for (int k = 0; k < K; k++) sm.M[k][e] = 0.0;
     }
-#pragma unroll
-    for (int a = 0; a < N; a++) sm.P[a][e] = ph[a];
-#pragma unroll
-    for (int k = 0; k < K; k++) sm.M[k][e] = m[k];
+  }
+  __syncthreads();
+
+  /* A tile whose staged cells (in the domain) all hold the same one-hot phi
+   * and no delta-phi has no interface in reach: every anti-trapping current is
+   * 0.0 (all gradients vanish, calculate_fluxes_concentration.h:64,103), every
+   * cell takes the bulk branch, and D is the same everywhere.  The fast path
+   * evaluates exactly the expressions of the general path that remain. */
+  int ref_phase = -1;
+  {
+    const int r = LI(1, 1);
+    int ones = 0, zeros = 0;
 #pragma unroll
     for (int a = 0; a < N; a++) {
-      double hv = h<N>(ph, a);
+      if (sm.P[a][r] == 1.0) { if (ref_phase < 0) ref_phase = a; ones++; }
+      else if (sm.P[a][r] == 0.0) zeros++;
+    }
+    if (!(ones == 1 && zeros == N - 1)) ref_phase = -1;
+  }
+  bool uni = ref_phase >= 0;
+  if (uni) {
+    const int r = LI(1, 1);
+    for (int e = threadIdx.x; e < SS; e += NT) {
+      int i = e / SW, j = e - i * SW;
+      if (x0 - 1 + i > g.mx || y0 - 1 + j > g.my) continue;
+#pragma unroll
+      for (int a = 0; a < N; a++) uni = uni && sm.P[a][e] == sm.P[a][r] && sm.DP[a][e] == 0.0;
+    }
+  }
+  const bool uniform = __syncthreads_and(uni);
+
+  const int tx = threadIdx.x / TY, ty = threadIdx.x - (threadIdx.x / TY) * TY;
+  const int x = x0 + tx, y = y0 + ty, i = tx + 1, j = ty + 1, c = LI(i, j);
+  const bool valid = x < g.mx && y < g.my;
+  double ph[N], m[K], dp[N], nph[N], nm[K], dmu[K];
+
+  if (uniform) {
+    if (valid) {
+#pragma unroll
+      for (int a = 0; a < N; a++) { ph[a] = sm.P[a][c]; dp[a] = sm.DP[a][c]; }
+#pragma unroll
+      for (int k = 0; k < K; k++) m[k] = sm.M[k][c];
+      double Dv[K][K];
+#pragma unroll
+      for (int k = 0; k < K; k++)
+#pragma unroll
+        for (int l = 0; l < K; l++) Dv[k][l] = Dcell<N, K>(ph, k, l);
+      double cn[K];
+#pragma unroll
+      for (int k = 0; k < K; k++) {
+        double divflux = 0.0;
+#pragma unroll
+        for (int l = 0; l < K; l++) {
+          const double *M = sm.M[l];
+          const double dm = (Dv[k][l] + Dv[k][l]) * 0.5;
+          double fx = dm * divx(M[LI(i + 1, j)] - M[c], g), bx = dm * divx(M[c] - M[LI(i - 1, j)], g);
+          double fy = dm * divy(M[LI(i, j + 1)] - M[c], g), by = dm * divy(M[c] - M[LI(i, j - 1)], g);
+          divflux += divx(fx - bx, g);
+          divflux += divy(fy - by, g);
+        }
+        double divjat = divx((0.0 - 0.0) * cst, g);
+        divjat += divy((0.0 - 0.0) * cst, g);
+        cn[k] = c_mu<K>(m, ref_phase, k) + cD.dt * (divflux) - divjat;
+      }
+#pragma unroll
+      for (int k = 0; k < K; k++) {
+        nm[k] = Mu<K>(cn, ref_phase, k);
+        dmu[k] = nm[k] - m[k];
+      }
+#pragma unroll
+      for (int a = 0; a < N; a++) nph[a] = ph[a] + dp[a];
+      const long long o = (long long)x * g.pitch + y;
+#pragma unroll
+      for (int a = 0; a < N; a++) phin[a * g.plane + o] = nph[a];
+#pragma unroll
+      for (int k = 0; k < K; k++) mun[k * g.plane + o] = nm[k];
+    }
+    block_stats<N, K>(valid, nph, nm, dp, dmu, st);
+    return;
+  }
+
+  /* general path: per-cell quantities */
+  for (int e = threadIdx.x; e < SS; e += NT) {
+    double p[N], mm[K];
+#pragma unroll
+    for (int a = 0; a < N; a++) p[a] = sm.P[a][e];
+#pragma unroll
+    for (int k = 0; k < K; k++) mm[k] = sm.M[k][e];
+#pragma unroll
+    for (int a = 0; a < N; a++) {
+      double hv = h<N>(p, a);
       sm.H[a][e] = hv;
 #pragma unroll
-      for (int k = 0; k < K; k++) sm.CM[a][k][e] = c_mu<K>(m, a, k);
+      for (int k = 0; k < K; k++) sm.CM[a][k][e] = c_mu<K>(mm, a, k);
       if (a < L)
-        sm.SP[a][e] = (ph[a] * (1.0 - ph[a]) > 0.0) ? ph[a] * (1.0 - hv) / (sqrt(ph[a] * (1.0 - ph[a]))) : 0.0;
+        sm.SP[a][e] = (p[a] * (1.0 - p[a]) > 0.0) ? p[a] * (1.0 - hv) / (sqrt(p[a] * (1.0 - p[a]))) : 0.0;
     }
 #pragma unroll
     for (int k = 0; k < K; k++)
 #pragma unroll
-      for (int l = 0; l < K; l++) sm.DD[k][l][e] = Dcell<N, K>(ph, k, l);
+      for (int l = 0; l < K; l++) sm.DD[k][l][e] = Dcell<N, K>(p, k, l);
   }
   __syncthreads();
 
   /* faces: anti-trapping current and diffusion flux products */
   for (int e = threadIdx.x; e < NXF + NYF; e += NT) {
     const bool xface = e < NXF;
-    int i, j, i1, j1, fidx;
-    if (xface) { i = e / TY; j = e - i * TY + 1; i1 = i + 1; j1 = j; fidx = e; }
-    else { int f = e - NXF; i = f / (TY + 1) + 1; j = f - (i - 1) * (TY + 1); i1 = i; j1 = j + 1; fidx = f; }
-    const int c = LI(i, j), c1 = LI(i1, j1);
+    int fi, fj, i1, j1, fidx;
+    if (xface) { fi = e / TY; fj = e - fi * TY + 1; i1 = fi + 1; j1 = fj; fidx = e; }
+    else { int f = e - NXF; fi = f / (TY + 1) + 1; fj = f - (fi - 1) * (TY + 1); i1 = fi; j1 = fj + 1; fidx = f; }
+    const int c0 = LI(fi, fj), c1 = LI(i1, j1);
     double gr[N], cn[N];   /* one-sided gradient across the face, mean of the centred tangential gradient */
 #pragma unroll
     for (int a = 0; a < N; a++) {
       const double *S = sm.P[a];
       if (xface) {
-        gr[a] = divx(S[c1] - S[c], g);
-        cn[a] = 0.5 * (div2y(S[LI(i, j + 1)] - S[LI(i, j - 1)], g) + div2y(S[LI(i1, j + 1)] - S[LI(i1, j - 1)], g));
+        gr[a] = divx(S[c1] - S[c0], g);
+        cn[a] = 0.5 * (div2y(S[LI(fi, fj + 1)] - S[LI(fi, fj - 1)], g) + div2y(S[LI(i1, fj + 1)] - S[LI(i1, fj - 1)], g));
       } else {
-        gr[a] = divy(S[c1] - S[c], g);
-        double gc0 = 0.5 * (divx(S[LI(i + 1, j)] - S[c], g) + divx(S[c] - S[LI(i - 1, j)], g));
-        double gc1 = 0.5 * (divx(S[LI(i + 1, j1)] - S[c1], g) + divx(S[c1] - S[LI(i - 1, j1)], g));
+        gr[a] = divy(S[c1] - S[c0], g);
+        double gc0 = 0.5 * (divx(S[LI(fi + 1, fj)] - S[c0], g) + divx(S[c0] - S[LI(fi - 1, fj)], g));
+        double gc1 = 0.5 * (divx(S[LI(fi + 1, j1)] - S[c1], g) + divx(S[c1] - S[LI(fi - 1, j1)], g));
         cn[a] = 0.5 * (gc0 + gc1);
       }
     }
@@ -476,24 +630,27 @@ __global__ void __launch_bounds__(NT) k_update(const double *__restrict__ phi, c
 #pragma unroll
     for (int k = 0; k < K; k++) jat[k] = 0.0;
     /* calculate_fluxes_concentration.h:65: no y-current where gidy is 0 or MESH_Y-2 */
-    const bool yskip = !xface && ((y0 - 1 + j) + 3 == g.my - 2);
-    const double nl = sqrt(cn[L] * cn[L] + gr[L] * gr[L]);
+    const bool yskip = !xface && ((y0 - 1 + fj) + 3 == g.my - 2);
+    double nl = -1.0;   /* |grad phi_liquid| on the face, computed on first use */
 #pragma unroll
     for (int a = 0; a < L; a++) {
-      const double ng = sqrt(cn[a] * cn[a] + gr[a] * gr[a]);
-      if (ng != 0.0 && !yskip) {
+      /* sqrt(s2) != 0 exactly when s2 != 0 (s2 >= 0, or NaN on both sides) */
+      const double s2 = cn[a] * cn[a] + gr[a] * gr[a];
+      if (s2 != 0.0 && !yskip) {
+        const double ng = sqrt(s2);
+        if (nl < 0.0) nl = sqrt(cn[L] * cn[L] + gr[L] * gr[L]);
         double sp = gr[a] * gr[L];
         sp += cn[a] * cn[L];
         if (nl > 0.0) sp /= (nl * ng);
 #pragma unroll
         for (int k = 0; k < K; k++) {
-          double cl1 = sm.CM[L][k][c1], cl0 = sm.CM[L][k][c];
-          double cs1 = sm.CM[a][k][c1], cs0 = sm.CM[a][k][c];
+          double cl1 = sm.CM[L][k][c1], cl0 = sm.CM[L][k][c0];
+          double cs1 = sm.CM[a][k][c1], cs0 = sm.CM[a][k][c0];
           double bracket;
           if (cD.obstacle)
-            bracket = sm.SP[a][c1] * (cl1 - cs1) * sm.DP[a][c1] + sm.SP[a][c] * (cl0 - cs0) * sm.DP[a][c];
+            bracket = sm.SP[a][c1] * (cl1 - cs1) * sm.DP[a][c1] + sm.SP[a][c0] * (cl0 - cs0) * sm.DP[a][c0];
           else
-            bracket = (cl1 - cs1) * sm.DP[a][c1] + (cl0 - cs0) * sm.DP[a][c];
+            bracket = (cl1 - cs1) * sm.DP[a][c1] + (cl0 - cs0) * sm.DP[a][c0];
           jat[k] += cD.atf[a][k] * fabs(sp) * (cD.obstacle ? 0.5 : cD.well_half) * bracket * gr[a] / ng;
         }
       }
@@ -504,8 +661,8 @@ __global__ void __launch_bounds__(NT) k_update(const double *__restrict__ phi, c
       else sm.JY[k][fidx] = jat[k];
 #pragma unroll
       for (int l = 0; l < K; l++) {
-        double dm = (sm.DD[k][l][c1] + sm.DD[k][l][c]) * 0.5;
-        double gm = xface ? divx(sm.M[l][c1] - sm.M[l][c], g) : divy(sm.M[l][c1] - sm.M[l][c], g);
+        double dm = (sm.DD[k][l][c1] + sm.DD[k][l][c0]) * 0.5;
+        double gm = xface ? divx(sm.M[l][c1] - sm.M[l][c0], g) : divy(sm.M[l][c1] - sm.M[l][c0], g);
         if (xface) sm.FX[k][l][fidx] = dm * gm;
         else sm.FY[k][l][fidx] = dm * gm;
       }
@@ -513,29 +670,14 @@ __global__ void __launch_bounds__(NT) k_update(const double *__restrict__ phi, c
   }
   __syncthreads();
 
-  const int tx = threadIdx.x / TY, ty = threadIdx.x - (threadIdx.x / TY) * TY;
-  const int x = x0 + tx, y = y0 + ty, i = tx + 1, j = ty + 1, c = LI(i, j);
-  const bool valid = x < g.mx && y < g.my;
-  double ph[N], m[K], dp[N], nph[N], nm[K], dmu[K];
   if (valid) {
 #pragma unroll
     for (int a = 0; a < N; a++) { ph[a] = sm.P[a][c]; dp[a] = sm.DP[a][c]; }
 #pragma unroll
     for (int k = 0; k < K; k++) m[k] = sm.M[k][c];
-    double sum[K], divflux[K], divjat[K];
-#pragma unroll
-    for (int k = 0; k < K; k++) sum[k] = 0.0;
-#pragma unroll
-    for (int a = 0; a < N; a++) {
-      double sdh = 0.0;
-#pragma unroll
-      for (int b = 0; b < N; b++) sdh += dh<N>(ph, a, b) * dp[b];
-#pragma unroll
-      for (int k = 0; k < K; k++) sum[k] += sm.CM[a][k][c] * sdh;
-    }
+    double divflux[K], divjat[K];
     const int xf = i * TY + (j - 1), xb = (i - 1) * TY + (j - 1);
     const int yr = (i - 1) * (TY + 1) + j, yl = (i - 1) * (TY + 1) + (j - 1);
-    const double cst = cD.obstacle ? cD.jat_obst : cD.jat_well;
 #pragma unroll
     for (int k = 0; k < K; k++) {
       divflux[k] = 0.0;
@@ -561,7 +703,18 @@ __global__ void __launch_bounds__(NT) k_update(const double *__restrict__ phi, c
         dmu[k] = nm[k] - m[k];
       }
     } else {
-      double dc[K], dcdmu[K][K];
+      /* sum_a c_a(mu) sum_b dh_a/dphi_b dphi_b (calculate_divergence_concentration.h:23-31) */
+      double sum[K], dc[K], dcdmu[K][K];
+#pragma unroll
+      for (int k = 0; k < K; k++) sum[k] = 0.0;
+#pragma unroll
+      for (int a = 0; a < N; a++) {
+        double sdh = 0.0;
+#pragma unroll
+        for (int b = 0; b < N; b++) sdh += dh<N>(ph, a, b) * dp[b];
+#pragma unroll
+        for (int k = 0; k < K; k++) sum[k] += sm.CM[a][k][c] * sdh;
+      }
 #pragma unroll
       for (int k = 0; k < K; k++) {
         dc[k] = cD.dt * (divflux[k]) - divjat[k] - sum[k];
@@ -579,12 +732,12 @@ __global__ void __launch_bounds__(NT) k_update(const double *__restrict__ phi, c
         dmu[0] = dc[0] * i00;
         nm[0] += dmu[0];
       } else if (cD.inv_mode == GP_INV_TERNARY && K == 2) {
-        double det = dcdmu[0][0] * dcdmu[1][1] - dcdmu[0][1] * dcdmu[1][0];
-        double iv[2][2];
-        iv[0][0] = dcdmu[1][1] / det;
-        iv[1][1] = dcdmu[0][0] / det;
-        iv[0][1] = -dcdmu[0][1] / det;
-        iv[1][0] = -dcdmu[1][0] / det;
+        double det = dcdmu[0][0] * dcdmu[K - 1][K - 1] - dcdmu[0][K - 1] * dcdmu[K - 1][0];
+        double iv[K][K];
+        iv[0][0] = dcdmu[K - 1][K - 1] / det;
+        iv[K - 1][K - 1] = dcdmu[0][0] / det;
+        iv[0][K - 1] = -dcdmu[0][K - 1] / det;
+        iv[K - 1][0] = -dcdmu[K - 1][0] / det;
 #pragma unroll
         for (int k = 0; k < K; k++) {
           dmu[k] = 0.0;
@@ -622,64 +775,7 @@ __global__ void __launch_bounds__(NT) k_update(const double *__restrict__ phi, c
 #pragma unroll
     for (int k = 0; k < K; k++) mun[k * g.plane + o] = nm[k];
   }
-
-  /* progress record: running extremes every step, sums when asked for */
-  __shared__ double red[NT / 32];
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  for (int f = 0; f < 2 * (N + K); f++) {
-    const int fld = f >> 1;   /* 0..N-1 phi, N.. mu */
-    const bool isMax = !(f & 1);
-    double v = isMax ? -INFINITY : INFINITY;
-    if (valid) {
-      double w = fld < N ? nph[fld] : nm[fld - N];
-      if (w == w) v = w;
-    }
-    v = isMax ? warp_max(v) : warp_min(v);
-    if (lane == 0) red[wid] = v;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double r = red[0];
-      for (int w = 1; w < NT / 32; w++) r = isMax ? fmax(r, red[w]) : fmin(r, red[w]);
-      if (isMax && r > -INFINITY) atomicMax(st.minmax + (fld < N ? fld : 2 * N + (fld - N)), ord(r));
-      if (!isMax && r < INFINITY) atomicMin(st.minmax + (fld < N ? N + fld : 2 * N + K + (fld - N)), ord(r));
-    }
-    __syncthreads();
-  }
-  if (st.want_sums) {
-    const int nsum = 2 * N + 2 * K + 1;
-    const long long blk = (long long)blockIdx.y * gridDim.x + blockIdx.x;
-    for (int f = 0; f < nsum; f++) {
-      double v = 0.0;
-      if (valid) {
-        if (f < N) v = dp[f] * dp[f];
-        else if (f < N + K) v = dmu[f - N] * dmu[f - N];
-        else if (f < 2 * N + K) v = nph[f - N - K];
-        else if (f < 2 * N + 2 * K) {
-          int k = f - 2 * N - K;
-          double comp = 0.0;
-#pragma unroll
-          for (int b = 0; b < N; b++) comp += c_mu<K>(nm, b, k) * h<N>(nph, b);
-          v = comp;
-        } else {
-          bool bad = false;
-#pragma unroll
-          for (int a = 0; a < N; a++) bad |= !isfinite(nph[a]);
-#pragma unroll
-          for (int k = 0; k < K; k++) bad |= !isfinite(nm[k]);
-          v = bad ? 1.0 : 0.0;
-        }
-      }
-      v = warp_sum(v);
-      if (lane == 0) red[wid] = v;
-      __syncthreads();
-      if (threadIdx.x == 0) {
-        double r = 0.0;
-        for (int w = 0; w < NT / 32; w++) r += red[w];
-        st.partials[blk * nsum + f] = r;
-      }
-      __syncthreads();
-    }
-  }
+  block_stats<N, K>(valid, nph, nm, dp, dmu, st);
 }
 
 }  // namespace gpd
