@@ -567,6 +567,16 @@ int gp_host_derive(const gp_params *p, gp_derived *d, char *err, size_t errlen) 
     }
     d->C[a] = C[a];
   }
+  /* D of a pure-phase cell: the same products and sum order as D()
+   * (functionD.h:10-14) with phi_b = 1.0 for b == p and 0.0 otherwise */
+  for (int q = 0; q < N; q++)
+    for (i = 0; i < K; i++)
+      for (j = 0; j < K; j++) {
+        double s = 0.0;
+        for (b = 0; b < N; b++)
+          for (k = 0; k < K; k++) s += d->DC[b][i][j][k] * (b == q ? 1.0 : 0.0);
+        d->Dbulk[q][i][j] = s;
+      }
   d->rot_identity = 1;
   for (a = 0; a < N; a++)
     for (b = 0; b < N; b++) {

@@ -53,6 +53,7 @@ typedef struct gp_derived {
   double C[GPK_MAXN];                     /* C at T  */
   double DC[GPK_MAXN][GPK_MAXK][GPK_MAXK][GPK_MAXK]; /* Diffusivity[b][i][k]*cmu[b][k][j] -> [b][i][j][k] */
   double atf[GPK_MAXN][GPK_MAXK];         /* 1.0 - D[a][k][k]/D[N-1][k][k] */
+  double Dbulk[GPK_MAXN][GPK_MAXK][GPK_MAXK]; /* D_kl of a cell with phi = e_p, summed as functionD.h does */
   /* boundary index maps along x and y: ghosted index -> ghosted index; per field */
   int bc_x[2][2], bc_y[2][2];             /* [field phi/mu][low/high side] type (1 or 3) */
 } gp_derived;

@@ -82,18 +82,35 @@ struct DphiSmem {
 
 /* Load the phi tile whose local (i,j) is interior (x0-1+i, y0-1+j); entries
  * outside [-2, m+1] are not needed by any valid cell and are zeroed. */
+/* Source row offsets and columns of a tile's SH staged rows and SW staged
+ * columns after the boundary remap, one field; -1 where the row/column lies
+ * outside [lo, hi] (not needed by any valid cell).  Filled by threads
+ * 0..SH+SW-1; the caller synchronises before use. */
+struct RemapTab {
+  int row[SH], col[SW];
+};
+__device__ __forceinline__ void remap_tab(RemapTab &t, const Grid &g, int x0, int y0, int field, int lo_x,
+                                          int hi_x, int lo_y, int hi_y) {
+  const int u = threadIdx.x;
+  if (u < SH) {
+    const int x = x0 - 1 + u;
+    t.row[u] = (x >= lo_x && x <= hi_x) ? remap(x, g.mx, cD.bc_x[field][0], cD.bc_x[field][1]) * g.pitch : -1;
+  } else if (u < SH + SW) {
+    const int y = y0 - 1 + (u - SH);
+    t.col[u - SH] = (y >= lo_y && y <= hi_y) ? remap(y, g.my, cD.bc_y[field][0], cD.bc_y[field][1]) : -1;
+  }
+}
+
 template <int NF>
 __device__ __forceinline__ void load_tile(double (*S)[SS], const double *__restrict__ f, const Grid &g,
-                                          int x0, int y0, int field, int lo_x, int hi_x) {
+                                          const RemapTab &t) {
   for (int e = threadIdx.x; e < SS; e += NT) {
-    int i = e / SW, j = e - i * SW;
-    int x = x0 - 1 + i, y = y0 - 1 + j;
-    if (x >= lo_x && x <= hi_x && y >= -2 && y <= g.my + 1) {
-      int sx = remap(x, g.mx, cD.bc_x[field][0], cD.bc_x[field][1]);
-      int sy = remap(y, g.my, cD.bc_y[field][0], cD.bc_y[field][1]);
-      long long o = (long long)sx * g.pitch + sy;
+    const int i = e / SW, j = e - i * SW;
+    const int r = t.row[i], cc = t.col[j];
+    if (r >= 0 && cc >= 0) {
+      const double *src = f + (r + cc);
 #pragma unroll
-      for (int a = 0; a < NF; a++) S[a][e] = __ldg(f + a * g.plane + o);
+      for (int a = 0; a < NF; a++) S[a][e] = __ldg(src + a * g.plane);
     } else {
 #pragma unroll
       for (int a = 0; a < NF; a++) S[a][e] = 0.0;
@@ -166,7 +183,10 @@ __global__ void __launch_bounds__(NT) k_dphi(const double *__restrict__ phi, con
   extern __shared__ __align__(16) unsigned char smraw[];
   DphiSmem<N> &sm = *reinterpret_cast<DphiSmem<N> *>(smraw);
   const int x0 = blockIdx.y * TX - 1, y0 = blockIdx.x * TY - 1;
-  load_tile<N>(sm.S, phi, g, x0, y0, 0, -2, g.mx + 1);
+  __shared__ RemapTab rt;
+  remap_tab(rt, g, x0, y0, 0, -2, g.mx + 1, -2, g.my + 1);
+  __syncthreads();
+  load_tile<N>(sm.S, phi, g, rt);
   __syncthreads();
 
   const int tx = threadIdx.x / TY, ty = threadIdx.x - (threadIdx.x / TY) * TY;
@@ -398,7 +418,9 @@ struct StatBufs {
 /* Per-block running extremes and (on request) sums of the cells a block owns.
  * Each block owns its slots, so no atomics are needed and results are
  * deterministic; gp_step folds the slots when it reports. */
-template <int N, int K>
+/* UNI: every valid cell of the block holds the same phi (uniform tile), so
+ * the phi extremes are thread 0's values and only mu is reduced. */
+template <int N, int K, bool UNI = false>
 __device__ __forceinline__ void block_stats(bool valid, const double *nph, const double *nm, const double *dp,
                                             const double *dmu, const StatBufs &st) {
   constexpr int NE = 2 * (N + K), NS = 2 * N + 2 * K + 1, NW = NT / 32;
@@ -410,6 +432,10 @@ __device__ __forceinline__ void block_stats(bool valid, const double *nph, const
     for (int f = 0; f < NE; f++) {
       const int fld = f >> 1;
       const bool isMax = !(f & 1);
+      if (UNI && fld < N) {
+        if (threadIdx.x == 0) red[0][f] = nph[fld];
+        continue;
+      }
       double v = isMax ? -INFINITY : INFINITY;
       if (valid) {
         double w = fld < N ? nph[fld] : nm[fld - N];
@@ -423,7 +449,8 @@ __device__ __forceinline__ void block_stats(bool valid, const double *nph, const
       const int f = threadIdx.x, fld = f >> 1;
       const bool isMax = !(f & 1);
       double r = red[0][f];
-      for (int w = 1; w < NW; w++) r = isMax ? fmax(r, red[w][f]) : fmin(r, red[w][f]);
+      if (!(UNI && fld < N))
+        for (int w = 1; w < NW; w++) r = isMax ? fmax(r, red[w][f]) : fmin(r, red[w][f]);
       /* slot layout: max phi[N], min phi[N], max mu[K], min mu[K] */
       const int slot = fld < N ? (isMax ? fld : N + fld) : (isMax ? 2 * N + (fld - N) : 2 * N + K + (fld - N));
       long long *p = st.ext + blk * NE + slot;
@@ -479,55 +506,51 @@ __global__ void __launch_bounds__(NT) k_update(const double *__restrict__ phi, c
   constexpr int L = N - 1;
   const double cst = cD.obstacle ? cD.jat_obst : cD.jat_well;
 
-  /* stage phi, mu (remapped) and delta-phi */
+  /* A tile whose staged cells (in the domain) all hold the same one-hot phi
+   * and no delta-phi has no interface in reach: every anti-trapping current is
+   * 0.0 (all gradients vanish, calculate_fluxes_concentration.h:64,103), every
+   * cell takes the bulk branch, and D is the same everywhere.  The fast path
+   * evaluates exactly the expressions of the general path that remain.  The
+   * reference cell is the tile's first cell (x0, y0), always in the domain. */
+  double refp[N];
+  int ref_phase = -1;
+  {
+    int ones = 0, zeros = 0;
+#pragma unroll
+    for (int a = 0; a < N; a++) {
+      refp[a] = __ldg(phi + a * g.plane + (long long)x0 * g.pitch + y0);
+      if (refp[a] == 1.0) { if (ref_phase < 0) ref_phase = a; ones++; }
+      else if (refp[a] == 0.0) zeros++;
+    }
+    if (!(ones == 1 && zeros == N - 1)) ref_phase = -1;
+  }
+
+  /* stage phi, mu (remapped) and delta-phi; check uniformity on the way */
+  __shared__ RemapTab rtp, rtm;
+  remap_tab(rtp, g, x0, y0, 0, -1, g.mx, -1, g.my);
+  remap_tab(rtm, g, x0, y0, 1, -1, g.mx, -1, g.my);
+  __syncthreads();
+  bool uni = ref_phase >= 0;
   for (int e = threadIdx.x; e < SS; e += NT) {
-    int i = e / SW, j = e - i * SW;
-    int x = x0 - 1 + i, y = y0 - 1 + j;
-    if (x <= g.mx && y <= g.my) {
-      int sx = remap(x, g.mx, cD.bc_x[0][0], cD.bc_x[0][1]), sy = remap(y, g.my, cD.bc_y[0][0], cD.bc_y[0][1]);
-      int tx_ = remap(x, g.mx, cD.bc_x[1][0], cD.bc_x[1][1]), ty_ = remap(y, g.my, cD.bc_y[1][0], cD.bc_y[1][1]);
-      long long op = (long long)sx * g.pitch + sy, om = (long long)tx_ * g.pitch + ty_;
-      long long od = (long long)(x + 1) * g.dpitch + (y + 1);
+    const int i = e / SW, j = e - i * SW;
+    const int rp = rtp.row[i], cp = rtp.col[j];
+    if (rp >= 0 && cp >= 0) {
+      const double *sp_ = phi + (rp + cp), *sm_ = mu + (rtm.row[i] + rtm.col[j]);
+      const double *sd_ = dphi + ((long long)(x0 + i) * g.dpitch + (y0 + j));
 #pragma unroll
       for (int a = 0; a < N; a++) {
-        sm.P[a][e] = __ldg(phi + a * g.plane + op);
-        sm.DP[a][e] = __ldg(dphi + a * g.dplane + od);
+        const double pv = __ldg(sp_ + a * g.plane), dv = __ldg(sd_ + a * g.dplane);
+        sm.P[a][e] = pv;
+        sm.DP[a][e] = dv;
+        uni = uni && pv == refp[a] && dv == 0.0;
       }
 #pragma unroll
-      for (int k = 0; k < K; k++) sm.M[k][e] = __ldg(mu + k * g.plane + om);
+      for (int k = 0; k < K; k++) sm.M[k][e] = __ldg(sm_ + k * g.plane);
     } else {
 #pragma unroll
       for (int a = 0; a < N; a++) { sm.P[a][e] = 0.0; sm.DP[a][e] = 0.0; }
 #pragma unroll
       for (int k = 0; k < K; k++) sm.M[k][e] = 0.0;
-    }
-  }
-  __syncthreads();
-
-  /* A tile whose staged cells (in the domain) all hold the same one-hot phi
-   * and no delta-phi has no interface in reach: every anti-trapping current is
-   * 0.0 (all gradients vanish, calculate_fluxes_concentration.h:64,103), every
-   * cell takes the bulk branch, and D is the same everywhere.  The fast path
-   * evaluates exactly the expressions of the general path that remain. */
-  int ref_phase = -1;
-  {
-    const int r = LI(1, 1);
-    int ones = 0, zeros = 0;
-#pragma unroll
-    for (int a = 0; a < N; a++) {
-      if (sm.P[a][r] == 1.0) { if (ref_phase < 0) ref_phase = a; ones++; }
-      else if (sm.P[a][r] == 0.0) zeros++;
-    }
-    if (!(ones == 1 && zeros == N - 1)) ref_phase = -1;
-  }
-  bool uni = ref_phase >= 0;
-  if (uni) {
-    const int r = LI(1, 1);
-    for (int e = threadIdx.x; e < SS; e += NT) {
-      int i = e / SW, j = e - i * SW;
-      if (x0 - 1 + i > g.mx || y0 - 1 + j > g.my) continue;
-#pragma unroll
-      for (int a = 0; a < N; a++) uni = uni && sm.P[a][e] == sm.P[a][r] && sm.DP[a][e] == 0.0;
     }
   }
   const bool uniform = __syncthreads_and(uni);
@@ -547,7 +570,7 @@ __global__ void __launch_bounds__(NT) k_update(const double *__restrict__ phi, c
 #pragma unroll
       for (int k = 0; k < K; k++)
 #pragma unroll
-        for (int l = 0; l < K; l++) Dv[k][l] = Dcell<N, K>(ph, k, l);
+        for (int l = 0; l < K; l++) Dv[k][l] = cD.Dbulk[ref_phase][k][l];   /* == Dcell(ph) */
       double cn[K];
 #pragma unroll
       for (int k = 0; k < K; k++) {
@@ -578,7 +601,7 @@ __global__ void __launch_bounds__(NT) k_update(const double *__restrict__ phi, c
 #pragma unroll
       for (int k = 0; k < K; k++) mun[k * g.plane + o] = nm[k];
     }
-    block_stats<N, K>(valid, nph, nm, dp, dmu, st);
+    block_stats<N, K, true>(valid, nph, nm, dp, dmu, st);
     return;
   }
 
