@@ -2,7 +2,7 @@
 """Benchmark of the grand-potential time step (cell-updates/s) on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload cfg2|cfg1|cfg4]
+                    [--workload cfg2|cfg1|cfg3|cfg4] [--no-fp32]
 
 Default workload (cfg2): the plain FP64 drop-in configuration -- 2048x2048
 grid, 3 phases, ternary alloy (2 chemical potentials), 4-fold anisotropy
@@ -10,6 +10,14 @@ delta=0.02, periodic boundaries, 64 seeds (uniform centres, r ~ U[4,12],
 random solid phase, seed 0), liquid diffusivity diag(1, 0.5), solid 0, FP64.
 Synthetic data: the seed layout comes from a splitmix64 generator, the
 physical constants are fixed in eshwar_dipan_b200/workloads.py.
+
+Beside the FP64 headline the line carries the FP32 storage form on the same
+workload ("fp32": throughput, its own roofline at 4 bytes per field, and its
+max/L2 phi error and solute-mass difference against the FP64 run after the
+same steps).  cfg3 is the batched ensemble: 256 independent binary 2-phase
+simulations of sides log-uniform in [128, 1024] (multiples of 32), c0 ~
+U[0.40, 0.48], delta ~ U[0, 0.05], 1-8 seeds, FP32 storage, stepped by the
+persistent work-queue kernels in 100-step CUDA graphs.
 
 A step is one explicit time step of the whole grid (phase-field pass +
 concentration pass + boundary handling).  Cell-updates count interior cells
@@ -34,7 +42,7 @@ sys.path.insert(0, os.path.join(ROOT, "tests"))
 
 import numpy as np  # noqa: E402
 
-from eshwar_dipan_b200.workloads import filling_text, input_text, random_seeds  # noqa: E402
+from eshwar_dipan_b200.workloads import ensemble, filling_text, input_text, random_seeds  # noqa: E402
 
 HARNESS = os.path.join(ROOT, "oracle", "_ref", "gp_ref_harness")
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
@@ -57,6 +65,12 @@ def workload(name, scale=1):
                   d_solid=0.0, dt=0.02, eps=4.0, T=0.97)
         seeds = random_seeds(nseeds, (m, m), 4.0, 12.0, 2, seed=0)
         desc = "%dx%d ternary 3-phase FP64, isotropic, Neumann, %d seeds" % (m, m, nseeds)
+    elif name == "cfg3":
+        kw, seeds = ensemble(shrink=scale)[0]
+        kw = dict(kw)
+        m = kw["mesh"][0]
+        desc = ("ensemble member 0: %dx%d binary 2-phase, delta %.4f, c0 %.4f, %d seeds"
+                % (m, m, kw["dab"], kw["liquid_c"][0], len(seeds)))
     elif name == "cfg1":
         m = 256 // scale
         kw = dict(N=2, K=1, mesh=(m, m), aniso=False, dab=0.0, d_solid=0.0, d_liquid=[1.0], dt=0.02, eps=4.0,
@@ -192,14 +206,120 @@ def reference_arm(args, rank, world):
     return 0
 
 
+def fp32_form(gp, p, phi0, mu0, args, phi64, st64, local):
+    """The FP32 storage form on the same workload and step count as the FP64
+    run: device-timed throughput and its error against the FP64 result."""
+    s = gp.Simulation(p, phi0, mu0, precision=gp.GP_FP32)
+    s.smooth(p.nsmooth - 1)
+    s.step(args.warmup, stats=False)
+    with ClockSampler(local) as clk:
+        ms, _, _, st = s.step_timed(args.steps, stats=True)
+    phi32, _ = s.get()
+    s.close()
+    err = np.abs(phi32 - phi64)
+    drift = [abs(a - b) / abs(b) for a, b in zip(st["comp_sum"], st64["comp_sum"])]
+    return ms, clk.summary(), float(err.max()), float(np.sqrt((err ** 2).mean())), drift
+
+
+def run_ensemble(args, rank, world, local, dist):
+    """cfg3: the batched ensemble through gp_batch_* (FP32 storage)."""
+    import ctypes
+    import eshwar_dipan_b200 as gp
+    specs = ensemble()
+    work = tempfile.mkdtemp(prefix="gpens")
+    params, fields = [], []
+    for i, (kw, seeds) in enumerate(specs):
+        ip, fp = os.path.join(work, "e%d.in" % i), os.path.join(work, "e%d_fill.in" % i)
+        open(ip, "w").write(input_text(**kw))
+        open(fp, "w").write(filling_text(seeds))
+        p = gp.load_params(ip)
+        params.append(p)
+        fields.append(gp.fill(p, fp))
+    cells = sum(p.mesh_x * p.mesh_y for p in params)
+    N, K = 2, 1
+
+    def barrier():
+        if dist:
+            dist.barrier()
+
+    b = gp.Batch(params, fields, precision=gp.GP_FP32)
+    b.smooth(params[0].nsmooth - 1)
+    b.step(args.warmup, stats=False)
+    barrier()
+    with ClockSampler(local) as clk:
+        tot_ms, st = b.step_timed(args.steps, stats=True)
+    barrier()
+    b.close()
+    if dist:
+        import torch
+        t = torch.tensor([tot_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        tot_ms = float(t.item())
+
+    # end to end: upload of every simulation, smoothing, steps, read-back of all
+    barrier()
+    t0 = time.perf_counter()
+    b = gp.Batch(params, fields, precision=gp.GP_FP32)
+    b.smooth(params[0].nsmooth - 1)
+    b.step(args.warmup + args.steps, stats=False)
+    for i in range(len(params)):
+        b.get(i)
+    t_e2e = time.perf_counter() - t0
+    b.close()
+    barrier()
+    if dist:
+        import torch
+        t = torch.tensor([t_e2e], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_e2e = float(t.item())
+    shutil.rmtree(work, ignore_errors=True)
+    if rank != 0:
+        return 0
+    peaks = measured_peaks()
+    hbm = peaks.get("hbm_gbs") or 6650.0
+    bpc = 2 * (N + K) * 4
+    value = world * cells * args.steps / (tot_ms / 1e3)
+    achieved = bpc * cells * args.steps / (tot_ms / 1e3) / 1e9
+    e2e_steps = args.warmup + args.steps
+    host_bytes = cells * (N + K) * 8
+    nonfinite = sum(x["nonfinite"] for x in st)
+    out = {
+        "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": tot_ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (splitmix64 ensemble, seed 0)",
+        "config": {"workload": "cfg3: 256 binary 2-phase simulations, sides log-uniform [128,1024] x32, "
+                               "c0~U[0.40,0.48], delta~U[0,0.05], 1-8 seeds; FP32 storage, FP64 dc/dmu and sums",
+                   "simulations": len(params), "cells": cells,
+                   "sides": [int(p.mesh_x) for p in params],
+                   "l2": "inputs larger than L2: %.0f MB state per step" % (2 * cells * (N + K) * 4 / 1e6),
+                   "graph_steps": 100, "parallelism": "replicas" if world > 1 else "single"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                     "traffic": None, "bytes_per_cell": bpc,
+                     "peak_source": "measured" if peaks.get("hbm_gbs") else "fallback"},
+        "e2e": {"value": world * cells * e2e_steps / t_e2e, "unit": "cell-updates/s",
+                "h2d_bytes_per_step": host_bytes / e2e_steps, "d2h_bytes_per_step": host_bytes / e2e_steps,
+                "includes": "gp_batch_create upload of 256 simulations, %d smoothing sweeps, %d steps, "
+                            "read-back of every simulation" % (params[0].nsmooth - 1, e2e_steps)},
+        "gpu_launches": 3 * args.steps + 2,
+        "clocks": clk.summary(),
+        "nonfinite": nonfinite,
+    }
+    if not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline("cfg3")
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="cfg2", choices=["cfg1", "cfg2", "cfg4"])
+    ap.add_argument("--workload", default="cfg2", choices=["cfg1", "cfg2", "cfg3", "cfg4"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp32", action="store_true", help="skip the FP32 form beside the FP64 headline")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 
@@ -218,6 +338,12 @@ def main():
 
     if args.impl == "reference":
         rc = reference_arm(args, rank, world)
+        if dist:
+            dist.destroy_process_group()
+        return rc
+
+    if args.workload == "cfg3":
+        rc = run_ensemble(args, rank, world, local, dist)
         if dist:
             dist.destroy_process_group()
         return rc
@@ -253,7 +379,17 @@ def main():
         t = torch.tensor([tot_ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         tot_ms = float(t.item())
+    fp32 = None
+    if not args.no_fp32:
+        phi64, _ = sim.get()
     sim.close()
+    if not args.no_fp32:
+        fp32 = fp32_form(gp, p, phi0, mu0, args, phi64, st, local)
+        if dist:
+            import torch
+            t = torch.tensor([fp32[0]], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            fp32 = (float(t.item()),) + fp32[1:]
 
     # ---- end to end through the C ABI with host buffers ----------------------
     # gp_init uploads the host state, gp_smooth + gp_step run, and every SAVET=50
@@ -322,6 +458,20 @@ def main():
             "clocks": clk.summary(),
             "stats_last_step": st,
         }
+        if fp32:
+            ms32, clk32, emax, el2, drift = fp32
+            v32 = world * cells * args.steps / (ms32 / 1e3)
+            a32 = (N + K) * 2 * 4 * cells * args.steps / (ms32 / 1e3) / 1e9
+            out["fp32"] = {"value": v32, "unit": "cell-updates/s", "ms_per_step": ms32 / args.steps,
+                           "speedup_vs_fp64": v32 / value,
+                           "roofline": {"achieved": a32, "peak": hbm, "unit": "GB/s", "frac": a32 / hbm,
+                                        "bytes_per_cell": (N + K) * 2 * 4},
+                           "error_vs_fp64": {"after_steps": args.warmup + args.steps, "max_abs_dphi": emax,
+                                             "l2_dphi": el2, "mass_rel_diff": drift},
+                           "clocks": clk32,
+                           "form": "fields stored and stepped in FP32, stochastic rounding of each commit; "
+                                   "dc/dmu inversion, bulk dmu/dc and all sums in FP64"}
+            out["gpu_launches"] += 3 * args.steps
         if not args.no_cpu_baseline:
             out["cpu_baseline"] = cpu_baseline(args.workload)
         print(json.dumps(out), flush=True)

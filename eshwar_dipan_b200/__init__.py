@@ -133,3 +133,81 @@ class Simulation:
 
     def __exit__(self, *a):
         self.close()
+
+
+def _bcheck(code, h):
+    if code != 0:
+        m = lib().gp_batch_last_error(h)
+        raise GpError(code, m.decode() if m else "")
+
+
+class Batch:
+    """Many independent simulations stepped together (gp_batch_*): grids of any
+    size and their own parameters; same NUMPHASES, NUMCOMPONENTS and
+    Function_anisotropy.  precision=GP_FP32 stores and steps the fields in
+    float with the dc/dmu inversion and all sums in FP64."""
+
+    def __init__(self, params_list, fields, precision=GP_FP32):
+        n = len(params_list)
+        if n < 1 or len(fields) != n:
+            raise ValueError("need one (phi, mu) pair per parameter set")
+        self.params = list(params_list)
+        arr = (Params * n)(*self.params)
+        self._keep = []
+        phis = (ctypes.c_void_p * n)()
+        mus = (ctypes.c_void_p * n)()
+        for s, ((phi, mu), p) in enumerate(zip(fields, self.params)):
+            sp, sm = _shapes(p)
+            phi = np.ascontiguousarray(phi, dtype=np.float64)
+            mu = np.ascontiguousarray(mu, dtype=np.float64)
+            if phi.shape != sp or mu.shape != sm:
+                raise ValueError("simulation %d: shapes %s/%s, expected %s/%s" % (s, phi.shape, mu.shape, sp, sm))
+            self._keep += [phi, mu]
+            phis[s] = phi.ctypes.data
+            mus[s] = mu.ctypes.data
+        h = ctypes.c_void_p()
+        _bcheck(lib().gp_batch_create(ctypes.byref(h), n, arr, phis, mus, int(precision)), None)
+        self._keep = []
+        self._h = h
+        self.n = n
+        self.N, self.K = self.params[0].numphases, self.params[0].numcomponents - 1
+
+    def smooth(self, n):
+        _bcheck(lib().gp_batch_smooth(self._h, int(n)), self._h)
+
+    def step(self, n, stats=True):
+        if stats:
+            s = (Stats * self.n)()
+            _bcheck(lib().gp_batch_step(self._h, int(n), s), self._h)
+            return [x.as_dict(self.N, self.K) for x in s]
+        _bcheck(lib().gp_batch_step(self._h, int(n), None), self._h)
+        return None
+
+    def step_timed(self, n, stats=False):
+        ms = ctypes.c_double()
+        s = (Stats * self.n)() if stats else None
+        _bcheck(lib().gp_batch_step_timed(self._h, int(n), s, ctypes.byref(ms)), self._h)
+        return ms.value, ([x.as_dict(self.N, self.K) for x in s] if stats else None)
+
+    def get(self, sim):
+        sp, sm = _shapes(self.params[sim])
+        phi = np.zeros(sp, dtype=np.float64)
+        mu = np.zeros(sm, dtype=np.float64)
+        _bcheck(lib().gp_batch_get(self._h, int(sim), _ptr(phi), _ptr(mu)), self._h)
+        return phi, mu
+
+    def set(self, sim, phi, mu):
+        phi = np.ascontiguousarray(phi, dtype=np.float64)
+        mu = np.ascontiguousarray(mu, dtype=np.float64)
+        _bcheck(lib().gp_batch_set(self._h, int(sim), _ptr(phi), _ptr(mu)), self._h)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().gp_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

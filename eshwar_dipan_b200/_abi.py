@@ -115,6 +115,16 @@ SIGNATURES = {
     "gp_step_timed": (c_int, [c_void_p, c_long, POINTER(Stats), POINTER(c_double), POINTER(c_double),
                               POINTER(c_double)]),
     "gp_step_noalloc": (c_int, [POINTER(Params), c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "gp_batch_create": (c_int, [POINTER(c_void_p), c_int, POINTER(Params), POINTER(c_void_p), POINTER(c_void_p),
+                                c_int]),
+    "gp_batch_smooth": (c_int, [c_void_p, c_long]),
+    "gp_batch_step": (c_int, [c_void_p, c_long, POINTER(Stats)]),
+    "gp_batch_step_timed": (c_int, [c_void_p, c_long, POINTER(Stats), POINTER(c_double)]),
+    "gp_batch_get": (c_int, [c_void_p, c_int, c_void_p, c_void_p]),
+    "gp_batch_set": (c_int, [c_void_p, c_int, c_void_p, c_void_p]),
+    "gp_batch_size": (c_int, [c_void_p]),
+    "gp_batch_last_error": (ctypes.c_char_p, [c_void_p]),
+    "gp_batch_destroy": (None, [c_void_p]),
     "gp_stream": (c_void_p, [c_void_p]),
     "gp_destroy": (None, [c_void_p]),
     "gp_last_error": (ctypes.c_char_p, [c_void_p]),

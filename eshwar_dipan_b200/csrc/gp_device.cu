@@ -1,61 +1,39 @@
 /*
  * gp_device.cu -- libgp: the C ABI (include/gp.h) over the sm_100a kernels.
- * Host orchestration only; the kernels are in gp_step64.cuh / gp_smooth64.cuh.
+ * Host orchestration only; the kernels are in gp_tiles.cuh / gp_smooth.cuh.
+ *
+ *  - gp_ctx, FP64: one simulation, kernels k_dphi / k_update (one CTA per
+ *    tile) with the constants in __constant__ memory; bit-identical to the
+ *    reference step.
+ *  - gp_batch: many simulations of different sizes and parameters stepped
+ *    together by persistent kernels pulling (simulation, tile) items from a
+ *    work queue, in FP64 or in the FP32 storage form (gp_batch32.cu); steps
+ *    are replayed as CUDA graphs of GP_GRAPH_STEPS steps.
+ *  - gp_ctx, FP32: a batch of one.
  */
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <climits>
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
-#include <climits>
 #include <cstring>
+#include <vector>
 
-#include "gp_smooth64.cuh"
+#include "gp_batch_impl.cuh"
 
+static __constant__ gpd::Consts<double> cD;
 
 extern "C" const char *gp_host_thread_error(void);
 
-struct gp_ctx {
-  gp_params p;
-  gp_derived d;
-  gp_precision prec;
-  int dev;
-  cudaStream_t stream;
-  gpd::Grid g;
-  double *phi[2], *mu[2];       /* ping-pong state planes */
-  int cur;
-  double *dphi;                 /* delta-phi over the interior plus a ring */
-  long long *ext;               /* per-block running extremes, ordered integers [ublocks][2(N+K)] */
-  long long *ext_red;           /* their fold over blocks [2(N+K)] */
-  double *partials;             /* per-block sums of the last stats step */
-  double *sums;                 /* reduced sums */
-  int ublocks;                  /* blocks of k_update */
-  long long steps;
-  gp_stats last;
-  char err[256];
-};
+#define GP_GRAPH_STEPS 100
+
+/* ======================================================================= */
+/* helpers                                                                 */
+/* ======================================================================= */
 
 namespace {
-
-int fail(gp_ctx *c, int code, const char *fmt, ...) {
-  va_list ap;
-  va_start(ap, fmt);
-  if (c) vsnprintf(c->err, sizeof c->err, fmt, ap);
-  else {
-    char buf[256];
-    vsnprintf(buf, sizeof buf, fmt, ap);
-    gp_set_thread_error("%s", buf);
-  }
-  va_end(ap);
-  return code;
-}
-
-#define CK(call)                                                                        \
-  do {                                                                                  \
-    cudaError_t e_ = (call);                                                            \
-    if (e_ != cudaSuccess) return fail(c, GP_ECUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
-  } while (0)
 
 bool pow2(double v) {
   int e;
@@ -63,70 +41,85 @@ bool pow2(double v) {
   return v != 0.0 && m == 0.5;
 }
 
-/* ---- kernel dispatch over the template parameters -------------------- */
-
-struct Kern {
-  void (*dphi)(const double *, const double *, double *, gpd::Grid);
-  void (*upd)(const double *, const double *, const double *, double *, double *, gpd::Grid, gpd::StatBufs);
-  void (*sdphi)(const double *, double *, gpd::Grid);
-  void (*supd)(const double *, const double *, const double *, double *, double *, gpd::Grid);
-  size_t smem_dphi, smem_upd;
-};
-
-template <int N, int K, bool A>
-Kern make() {
-  Kern k;
-  k.dphi = gpd::k_dphi<N, K, A>;
-  k.upd = gpd::k_update<N, K>;
-  k.sdphi = gpd::k_sdphi<N, A>;
-  k.supd = gpd::k_supdate<N, K>;
-  k.smem_dphi = sizeof(gpd::DphiSmem<N>);
-  k.smem_upd = sizeof(gpd::UpdSmem<N, K>);
-  return k;
-}
-
-bool pick(int N, int K, bool A, Kern *out) {
-#define CASE(n, k)                                   \
-  if (N == n && K == k) {                            \
-    *out = A ? make<n, k, true>() : make<n, k, false>(); \
-    return true;                                     \
+/* Constants of one simulation in the field type.  FP64 divides by dx/dy
+ * unless they are powers of two (x*(1/dx) is then the same correctly rounded
+ * value); the FP32 form always multiplies. */
+template <typename R>
+gpd::Consts<R> make_consts(const gp_derived &d) {
+  gpd::Consts<R> c;
+  memset(&c, 0, sizeof c);
+  const bool f64 = sizeof(R) == 8;
+  c.dx = (R)d.dx; c.dy = (R)d.dy; c.dt = (R)d.dt; c.eps = (R)d.eps; c.inv_eps = (R)d.inv_eps;
+  c.tau = (R)d.tau; c.c16pi2 = (R)d.c16pi2; c.jat_obst = (R)d.jat_obst; c.jat_well = (R)d.jat_well;
+  c.well_half = (R)d.well_half;
+  c.mul_dx = f64 ? pow2(d.dx) : 1;
+  c.mul_dy = f64 ? pow2(d.dy) : 1;
+  c.inv_dx = (R)(1.0 / d.dx);
+  c.inv_dy = (R)(1.0 / d.dy);
+  c.inv_2dy = (R)(1.0 / (2.0 * d.dy));
+  c.obstacle = d.obstacle; c.well = d.well; c.aniso = d.aniso; c.inv_mode = d.inv_mode;
+  c.rot_identity = d.rot_identity;
+  memcpy(c.bc_x, d.bc_x, sizeof c.bc_x);
+  memcpy(c.bc_y, d.bc_y, sizeof c.bc_y);
+  for (int a = 0; a < GPK_MAXN; a++) {
+    for (int b = 0; b < GPK_MAXN; b++) {
+      c.gamma[a][b] = (R)d.gamma[a][b]; c.tau_ab[a][b] = (R)d.tau_ab[a][b];
+      c.dab16[a][b] = (R)d.dab16[a][b]; c.dab[a][b] = (R)d.dab[a][b];
+      for (int e = 0; e < GPK_MAXN; e++) c.gamma_abc[a][b][e] = (R)d.gamma_abc[a][b][e];
+      for (int i = 0; i < 2; i++)
+        for (int j = 0; j < 2; j++) { c.rot[a][b][i][j] = (R)d.rot[a][b][i][j]; c.rinv[a][b][i][j] = (R)d.rinv[a][b][i][j]; }
+    }
+    for (int i = 0; i < GPK_MAXK; i++) {
+      c.E[a][i] = (R)d.E[a][i]; c.twoA[a][i] = (R)d.twoA[a][i]; c.B[a][i] = (R)d.B[a][i]; c.atf[a][i] = (R)d.atf[a][i];
+      for (int j = 0; j < GPK_MAXK; j++) {
+        c.cmu[a][i][j] = (R)d.cmu[a][i][j]; c.cmu64[a][i][j] = d.cmu[a][i][j];
+        c.muc64[a][i][j] = i == j ? d.twoA[a][i] : d.A[a][i][j];
+        c.A[a][i][j] = (R)d.A[a][i][j]; c.Dbulk[a][i][j] = (R)d.Dbulk[a][i][j];
+        for (int k = 0; k < GPK_MAXK; k++) c.DC[a][i][j][k] = (R)d.DC[a][i][j][k];
+      }
+    }
+    c.C[a] = (R)d.C[a];
   }
-  CASE(2, 1) CASE(3, 1) CASE(4, 1) CASE(2, 2) CASE(3, 2) CASE(4, 2)
-#undef CASE
-  return false;
+  return c;
 }
 
-int setup_kernels(gp_ctx *c, const Kern &k) {
-  CK(cudaFuncSetAttribute(k.dphi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem_dphi));
-  CK(cudaFuncSetAttribute(k.upd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem_upd));
-  return GP_OK;
+gpd::Grid make_grid(const gp_derived &d, int pitch_multiple) {
+  gpd::Grid g;
+  g.mx = (int)d.mx;
+  g.my = (int)d.my;
+  g.pitch = (int)((d.my + pitch_multiple - 1) / pitch_multiple * pitch_multiple);
+  g.plane = (long long)g.pitch * d.mx;
+  g.dpitch = (int)((d.my + 2 + 31) / 32 * 32);
+  g.dplane = (long long)g.dpitch * (d.mx + 2);
+  return g;
 }
 
-/* Fold the per-block sums (one CTA per quantity) in a fixed order: the result
- * does not depend on scheduling. */
-__global__ void k_reduce_partials(const double *__restrict__ part, int nblocks, int nsum, double *__restrict__ out) {
+/* Fold per-tile sums of simulation blockIdx.y (tiles [tile0, tile0+ntile))
+ * in a fixed order; one CTA per (quantity, simulation). */
+__global__ void k_reduce_sums(const double *__restrict__ part, const int *__restrict__ tile0,
+                              const int *__restrict__ ntile, int nsum, double *__restrict__ out) {
   __shared__ double r[256];
-  const int f = blockIdx.x;
-  double s = 0.0;
-  for (int b = threadIdx.x; b < nblocks; b += 256) s += part[(long long)b * nsum + f];
-  r[threadIdx.x] = s;
+  const int f = blockIdx.x, s = blockIdx.y, t0 = tile0[s], nt = ntile[s];
+  double v = 0.0;
+  for (int b = threadIdx.x; b < nt; b += 256) v += part[(long long)(t0 + b) * nsum + f];
+  r[threadIdx.x] = v;
   __syncthreads();
   for (int w = 128; w > 0; w >>= 1) {
     if (threadIdx.x < w) r[threadIdx.x] += r[threadIdx.x + w];
     __syncthreads();
   }
-  if (threadIdx.x == 0) out[f] = r[0];
+  if (threadIdx.x == 0) out[(long long)s * nsum + f] = r[0];
 }
 
-/* Fold the per-block running extremes: slot f < nmax is a maximum, else a minimum. */
-__global__ void k_reduce_ext(const long long *__restrict__ ext, int nblocks, int nslot, int N, int K,
-                             long long *__restrict__ out) {
+/* Fold per-tile running extremes: slot f is a maximum for phi/mu maxima. */
+__global__ void k_reduce_ext(const long long *__restrict__ ext, const int *__restrict__ tile0,
+                             const int *__restrict__ ntile, int nslot, int N, int K, long long *__restrict__ out) {
   __shared__ long long r[256];
-  const int f = blockIdx.x;
+  const int f = blockIdx.x, s = blockIdx.y, t0 = tile0[s], nt = ntile[s];
   const bool isMax = f < N || (f >= 2 * N && f < 2 * N + K);
   long long v = isMax ? LLONG_MIN : LLONG_MAX;
-  for (int b = threadIdx.x; b < nblocks; b += 256) {
-    long long w = ext[(long long)b * nslot + f];
+  for (int b = threadIdx.x; b < nt; b += 256) {
+    long long w = ext[(long long)(t0 + b) * nslot + f];
     v = isMax ? (w > v ? w : v) : (w < v ? w : v);
   }
   r[threadIdx.x] = v;
@@ -138,7 +131,7 @@ __global__ void k_reduce_ext(const long long *__restrict__ ext, int nblocks, int
     }
     __syncthreads();
   }
-  if (threadIdx.x == 0) out[f] = r[0];
+  if (threadIdx.x == 0) out[(long long)s * nslot + f] = r[0];
 }
 
 double from_ord(long long i) {
@@ -153,7 +146,157 @@ long long to_ord(double v) {
   return i < 0 ? i ^ 0x7fffffffffffffffLL : i;
 }
 
-int upload_state(gp_ctx *c, const double *phi, const double *mu, cudaMemcpyKind kind) {
+/* running extremes start where the reference starts them (serialinfo_xy.h:59-66):
+ * phi max 1, min 0; mu max 1, min 1 */
+void init_ext(long long *s, int N, int K) {
+  for (int a = 0; a < N; a++) { s[a] = to_ord(1.0); s[N + a] = to_ord(0.0); }
+  for (int k = 0; k < K; k++) { s[2 * N + k] = to_ord(1.0); s[2 * N + K + k] = to_ord(1.0); }
+}
+
+void stats_from(gp_stats *r, const long long *mm, const double *sums, int N, int K, long long steps) {
+  memset(r, 0, sizeof *r);
+  for (int a = 0; a < N; a++) {
+    r->phi_max[a] = from_ord(mm[a]);
+    r->phi_min[a] = from_ord(mm[N + a]);
+    r->rel_change_phi[a] = sums[a];
+    r->phi_sum[a] = sums[N + K + a];
+  }
+  for (int k = 0; k < K; k++) {
+    r->mu_max[k] = from_ord(mm[2 * N + k]);
+    r->mu_min[k] = from_ord(mm[2 * N + K + k]);
+    r->rel_change_mu[k] = sums[N + k];
+    r->comp_sum[k] = sums[2 * N + K + k];
+  }
+  r->nonfinite = (long long)llround(sums[2 * N + 2 * K]);
+  r->steps_done = steps;
+}
+
+}  // namespace
+
+/* ======================================================================= */
+/* single FP64 simulation: one CTA per tile, constants in __constant__     */
+/* ======================================================================= */
+
+namespace gpd {
+
+template <int N, int K, bool A>
+__global__ void __launch_bounds__(NT) k_dphi(const double *__restrict__ phi, const double *__restrict__ mu,
+                                             double *__restrict__ dphi, Grid g) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  dphi_tile<double, N, K, A>(cD, g, phi, mu, dphi, blockIdx.y * TX - 1, blockIdx.x * TY - 1,
+                             *reinterpret_cast<DphiSmem<double, N> *>(smraw));
+}
+
+template <int N, int K>
+__global__ void __launch_bounds__(NT) k_update(const double *__restrict__ phi, const double *__restrict__ mu,
+                                               const double *__restrict__ dphi, double *__restrict__ phin,
+                                               double *__restrict__ mun, Grid g, StatBufs st) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  update_tile<double, N, K>(cD, g, phi, mu, dphi, phin, mun, blockIdx.y * TX, blockIdx.x * TY, st,
+                            (long long)blockIdx.y * gridDim.x + blockIdx.x,
+                            *reinterpret_cast<UpdSmem<double, N, K> *>(smraw));
+}
+
+}  // namespace gpd
+
+namespace {
+
+struct Kern {
+  void (*dphi)(const double *, const double *, double *, gpd::Grid);
+  void (*upd)(const double *, const double *, const double *, double *, double *, gpd::Grid, gpd::StatBufs);
+  gpd::BatchLaunch b;   /* smoothing kernels */
+  size_t smem_dphi, smem_upd;
+};
+
+template <int N, int K, bool A>
+Kern make() {
+  Kern k;
+  k.dphi = gpd::k_dphi<N, K, A>;
+  k.upd = gpd::k_update<N, K>;
+  k.b = gpd::BatchKernels<double, N, K, A>::table();
+  k.smem_dphi = sizeof(gpd::DphiSmem<double, N>);
+  k.smem_upd = sizeof(gpd::UpdSmem<double, N, K>);
+  return k;
+}
+
+bool pick(int N, int K, bool A, Kern *out) {
+#define CASE(n, k)                                       \
+  if (N == n && K == k) {                                \
+    *out = A ? make<n, k, true>() : make<n, k, false>(); \
+    return true;                                         \
+  }
+  CASE(2, 1) CASE(3, 1) CASE(4, 1) CASE(2, 2) CASE(3, 2) CASE(4, 2)
+#undef CASE
+  return false;
+}
+
+}  // namespace
+
+bool gp_batch_launch_f64(int N, int K, bool aniso, gpd::BatchLaunch *out) {
+  return gpd::batch_launch_table<double>(N, K, aniso, out);
+}
+
+struct gp_batch;
+
+struct gp_ctx {
+  gp_params p;
+  gp_derived d;
+  gp_precision prec;
+  gp_batch *b;                  /* FP32 contexts are a batch of one */
+  int dev;
+  cudaStream_t stream;
+  gpd::Grid g;
+  gpd::Consts<double> consts;
+  gpd::Consts<double> *dconsts; /* device copy for the smoothing kernels */
+  double *phi[2], *mu[2];       /* ping-pong state planes */
+  int cur;
+  double *dphi;                 /* delta-phi over the interior plus a ring */
+  long long *ext;               /* per-tile running extremes [ublocks][2(N+K)] */
+  long long *ext_red;
+  double *partials;             /* per-tile sums of the last stats step */
+  double *sums;
+  int *seg;                     /* {0, ublocks} for the per-simulation folds */
+  int ublocks;
+  long long steps;
+  gp_stats last;
+  char err[256];
+};
+
+static int fail(gp_ctx *c, int code, const char *fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  if (c) vsnprintf(c->err, sizeof c->err, fmt, ap);
+  else {
+    char buf[256];
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    gp_set_thread_error("%s", buf);
+  }
+  va_end(ap);
+  return code;
+}
+
+#define CK(call)                                                                                \
+  do {                                                                                          \
+    cudaError_t e_ = (call);                                                                    \
+    if (e_ != cudaSuccess) return fail(c, GP_ECUDA, "%s: %s", #call, cudaGetErrorString(e_));  \
+  } while (0)
+
+/* The constant block is per module and device; a context re-uploads it when
+ * another context (or gp_step_noalloc) used it last.  Contexts are not meant to
+ * be driven from several host threads at once. */
+static const gp_ctx *g_last_ctx = nullptr;
+
+static int bind(gp_ctx *c) {
+  if (g_last_ctx != c) {
+    /* another context's kernels may still read the constant block */
+    CK(cudaDeviceSynchronize());
+    CK(cudaMemcpyToSymbol(cD, &c->consts, sizeof(c->consts)));
+    g_last_ctx = c;
+  }
+  return GP_OK;
+}
+
+static int upload_state(gp_ctx *c, const double *phi, const double *mu, cudaMemcpyKind kind) {
   const gp_derived &d = c->d;
   for (int a = 0; a < d.N; a++)
     CK(cudaMemcpy2DAsync(c->phi[c->cur] + a * c->g.plane, (size_t)c->g.pitch * 8, phi + (size_t)a * d.mx * d.my,
@@ -164,7 +307,7 @@ int upload_state(gp_ctx *c, const double *phi, const double *mu, cudaMemcpyKind 
   return GP_OK;
 }
 
-int download_state(gp_ctx *c, double *phi, double *mu, cudaMemcpyKind kind) {
+static int download_state(gp_ctx *c, double *phi, double *mu, cudaMemcpyKind kind) {
   const gp_derived &d = c->d;
   for (int a = 0; a < d.N; a++)
     CK(cudaMemcpy2DAsync(phi + (size_t)a * d.mx * d.my, (size_t)d.my * 8, c->phi[c->cur] + a * c->g.plane,
@@ -175,49 +318,443 @@ int download_state(gp_ctx *c, double *phi, double *mu, cudaMemcpyKind kind) {
   return GP_OK;
 }
 
-/* Running extremes start where the reference starts them (serialinfo_xy.h:59-66):
- * phi max 1, min 0; mu max 1, min 1; every block slot holds them. */
-int reset_minmax(gp_ctx *c) {
-  const int N = c->d.N, K = c->d.K, ne = 2 * (N + K);
-  long long *h = (long long *)malloc(sizeof(long long) * (size_t)ne * c->ublocks);
-  if (!h) return fail(c, GP_ENOMEM, "gp_init: out of host memory");
-  for (int b = 0; b < c->ublocks; b++) {
-    long long *s = h + (size_t)b * ne;
-    for (int a = 0; a < N; a++) { s[a] = to_ord(1.0); s[N + a] = to_ord(0.0); }
-    for (int k = 0; k < K; k++) { s[2 * N + k] = to_ord(1.0); s[2 * N + K + k] = to_ord(1.0); }
-  }
-  cudaError_t e = cudaMemcpyAsync(c->ext, h, sizeof(long long) * (size_t)ne * c->ublocks, cudaMemcpyHostToDevice,
-                                  c->stream);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
-  free(h);
-  if (e != cudaSuccess) return fail(c, GP_ECUDA, "gp_init: %s", cudaGetErrorString(e));
+/* ======================================================================= */
+/* batches                                                                 */
+/* ======================================================================= */
+
+struct gp_batch {
+  int nsims, N, K, aniso;
+  gp_precision prec;
+  size_t elem;
+  gpd::BatchLaunch L;
+  std::vector<gp_params> params;
+  std::vector<gp_derived> derived;
+  std::vector<gpd::SimDesc> desc;
+  int dev, nsm, grid_d, grid_u;
+  int ntiles_u, ntiles_d;
+  cudaStream_t stream;
+  gpd::SimDesc *d_desc;
+  void *d_consts;
+  size_t consts_bytes;
+  int *d_tsim_u, *d_tsim_d, *d_seg0, *d_segn;
+  void *state[2];
+  void *dphi;
+  int cur;
+  long long *ext, *ext_sim;
+  double *partials, *sums_sim;
+  int *counters;
+  cudaGraphExec_t graph[2];
+  long long steps;
+  std::vector<gp_stats> last;
+  char err[256];
+};
+
+static int bfail(gp_batch *b, int code, const char *fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  char buf[256];
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  if (b) snprintf(b->err, sizeof b->err, "%s", buf);
+  gp_set_thread_error("%s", buf);
+  return code;
+}
+
+#define BK(call)                                                                                 \
+  do {                                                                                           \
+    cudaError_t e_ = (call);                                                                     \
+    if (e_ != cudaSuccess) return bfail(b, GP_ECUDA, "%s: %s", #call, cudaGetErrorString(e_));  \
+  } while (0)
+
+/* Start of a batched step: empty both work queues and advance the step counter
+ * that keys the FP32 rounding stream (a kernel, so that graph replays advance it). */
+__global__ void k_step_begin(int *counters) {
+  counters[0] = 0;
+  counters[1] = 0;
+  counters[2] = (int)((unsigned)counters[2] + 1u);
+}
+
+static int batch_step_once(gp_batch *b, int want_sums) {
+  gpd::StatBufs st = {};
+  st.ext = b->ext;
+  st.partials = b->partials;
+  st.want_sums = want_sums;
+  st.round_step = (const unsigned *)(b->counters + 2);
+  k_step_begin<<<1, 1, 0, b->stream>>>(b->counters);
+  BK(cudaGetLastError());
+  BK(b->L.dphi(b->grid_d, b->stream, b->d_desc, b->d_consts, b->d_tsim_d, b->ntiles_d, b->counters,
+               b->state[b->cur], b->dphi));
+  BK(b->L.update(b->grid_u, b->stream, b->d_desc, b->d_consts, b->d_tsim_u, b->ntiles_u, b->counters + 1,
+                 b->state[b->cur], b->dphi, b->state[b->cur ^ 1], st));
+  b->cur ^= 1;
+  b->steps++;
   return GP_OK;
 }
 
-}  // namespace
+static int batch_fold_stats(gp_batch *b, gp_stats *out) {
+  const int N = b->N, K = b->K, ne = 2 * (N + K), ns = 2 * N + 2 * K + 1;
+  k_reduce_sums<<<dim3(ns, b->nsims), 256, 0, b->stream>>>(b->partials, b->d_seg0, b->d_segn, ns, b->sums_sim);
+  k_reduce_ext<<<dim3(ne, b->nsims), 256, 0, b->stream>>>(b->ext, b->d_seg0, b->d_segn, ne, N, K, b->ext_sim);
+  BK(cudaGetLastError());
+  std::vector<long long> mm((size_t)ne * b->nsims);
+  std::vector<double> sums((size_t)ns * b->nsims);
+  BK(cudaMemcpyAsync(mm.data(), b->ext_sim, mm.size() * 8, cudaMemcpyDeviceToHost, b->stream));
+  BK(cudaMemcpyAsync(sums.data(), b->sums_sim, sums.size() * 8, cudaMemcpyDeviceToHost, b->stream));
+  BK(cudaStreamSynchronize(b->stream));
+  for (int s = 0; s < b->nsims; s++) {
+    stats_from(&b->last[s], &mm[(size_t)s * ne], &sums[(size_t)s * ns], N, K, b->steps);
+    if (out) out[s] = b->last[s];
+  }
+  return GP_OK;
+}
 
-/* ======================================================================= */
+static int batch_step_impl(gp_batch *b, long nsteps, gp_stats *stats, double *total_ms) {
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (total_ms) {
+    BK(cudaEventCreate(&e0));
+    BK(cudaEventCreate(&e1));
+    BK(cudaEventRecord(e0, b->stream));
+  }
+  long s = 0;
+  /* whole chunks as CUDA graphs (an even number of steps returns the ping-pong
+   * parity to where it started, so one graph per starting parity suffices);
+   * the last step runs outside so that it can produce the sums */
+  while (nsteps - s > GP_GRAPH_STEPS) {
+    const int p = b->cur;
+    if (!b->graph[p]) {
+      cudaGraph_t gr;
+      BK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+      int rc = GP_OK;
+      for (int i = 0; i < GP_GRAPH_STEPS && rc == GP_OK; i++) rc = batch_step_once(b, 0);
+      b->steps -= GP_GRAPH_STEPS; /* captured, not run */
+      cudaError_t ec = cudaStreamEndCapture(b->stream, &gr);
+      if (rc != GP_OK) return rc;
+      if (ec != cudaSuccess) return bfail(b, GP_ECUDA, "graph capture: %s", cudaGetErrorString(ec));
+      ec = cudaGraphInstantiate(&b->graph[p], gr, 0);
+      cudaGraphDestroy(gr);
+      if (ec != cudaSuccess) return bfail(b, GP_ECUDA, "graph instantiate: %s", cudaGetErrorString(ec));
+    }
+    BK(cudaGraphLaunch(b->graph[p], b->stream));
+    b->steps += GP_GRAPH_STEPS;
+    s += GP_GRAPH_STEPS;
+  }
+  for (; s < nsteps; s++) {
+    int rc = batch_step_once(b, stats != nullptr && s == nsteps - 1);
+    if (rc != GP_OK) return rc;
+  }
+  if (total_ms) {
+    float ms = 0.f;
+    BK(cudaEventRecord(e1, b->stream));
+    BK(cudaEventSynchronize(e1));
+    BK(cudaEventElapsedTime(&ms, e0, e1));
+    *total_ms = ms;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+  }
+  if (stats && nsteps > 0) return batch_fold_stats(b, stats);
+  BK(cudaStreamSynchronize(b->stream));
+  if (stats)
+    for (int i = 0; i < b->nsims; i++) stats[i] = b->last[i];
+  return GP_OK;
+}
 
-/* The constant block is per module and device; a context re-uploads it when
- * another context was used last.  Contexts are not meant to be driven from
- * several host threads at once. */
-static const gp_ctx *g_last_ctx = nullptr;
+static int batch_copy(gp_batch *b, int s, const double *phi, const double *mu, double *ophi, double *omu) {
+  /* host <-> device for one simulation; FP32 converts through a staging buffer */
+  const gpd::SimDesc &sd = b->desc[s];
+  const int N = b->N, K = b->K;
+  const size_t mx = sd.g.mx, my = sd.g.my;
+  char *base = (char *)b->state[b->cur] + (size_t)sd.off_state * b->elem;
+  for (int f = 0; f < N + K; f++) {
+    char *plane = base + (size_t)f * sd.g.plane * b->elem;
+    if (b->elem == 8) {
+      if (phi) {
+        const double *src = f < N ? phi + (size_t)f * mx * my : mu + (size_t)(f - N) * mx * my;
+        BK(cudaMemcpy2DAsync(plane, (size_t)sd.g.pitch * 8, src, my * 8, my * 8, mx, cudaMemcpyHostToDevice, b->stream));
+      } else {
+        double *dst = f < N ? ophi + (size_t)f * mx * my : omu + (size_t)(f - N) * mx * my;
+        BK(cudaMemcpy2DAsync(dst, my * 8, plane, (size_t)sd.g.pitch * 8, my * 8, mx, cudaMemcpyDeviceToHost, b->stream));
+      }
+    } else {
+      std::vector<float> tmp(mx * my);
+      if (phi) {
+        const double *src = f < N ? phi + (size_t)f * mx * my : mu + (size_t)(f - N) * mx * my;
+        for (size_t i = 0; i < mx * my; i++) tmp[i] = (float)src[i];
+        BK(cudaMemcpy2DAsync(plane, (size_t)sd.g.pitch * 4, tmp.data(), my * 4, my * 4, mx, cudaMemcpyHostToDevice, b->stream));
+        BK(cudaStreamSynchronize(b->stream));
+      } else {
+        BK(cudaMemcpy2DAsync(tmp.data(), my * 4, plane, (size_t)sd.g.pitch * 4, my * 4, mx, cudaMemcpyDeviceToHost, b->stream));
+        BK(cudaStreamSynchronize(b->stream));
+        double *dst = f < N ? ophi + (size_t)f * mx * my : omu + (size_t)(f - N) * mx * my;
+        for (size_t i = 0; i < mx * my; i++) dst[i] = (double)tmp[i];
+      }
+    }
+  }
+  BK(cudaStreamSynchronize(b->stream));
+  return GP_OK;
+}
 
 extern "C" {
 
-const char *gp_version(void) { return "libgp 0.1 (sm_100a, FP64 plain step)"; }
+void gp_batch_destroy(gp_batch *b) {
+  if (!b) return;
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  for (int p = 0; p < 2; p++) {
+    if (b->graph[p]) cudaGraphExecDestroy(b->graph[p]);
+    cudaFree(b->state[p]);
+  }
+  cudaFree(b->dphi);
+  cudaFree(b->d_desc);
+  cudaFree(b->d_consts);
+  cudaFree(b->d_tsim_u);
+  cudaFree(b->d_tsim_d);
+  cudaFree(b->d_seg0);
+  cudaFree(b->d_segn);
+  cudaFree(b->ext);
+  cudaFree(b->ext_sim);
+  cudaFree(b->partials);
+  cudaFree(b->sums_sim);
+  cudaFree(b->counters);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+}
+
+const char *gp_batch_last_error(const gp_batch *b) { return b ? b->err : gp_host_thread_error(); }
+
+int gp_batch_create(gp_batch **out, int nsims, const gp_params *params, const double *const *phi,
+                    const double *const *mu, gp_precision prec) {
+  gp_batch *b = nullptr;
+  if (!out || nsims < 1 || !params || !phi || !mu) return bfail(nullptr, GP_EINVAL, "gp_batch_create: bad argument");
+  *out = nullptr;
+  if (prec != GP_FP64 && prec != GP_FP32) return bfail(nullptr, GP_EINVAL, "gp_batch_create: precision");
+  b = new gp_batch();
+  b->nsims = nsims;
+  b->prec = prec;
+  b->params.assign(params, params + nsims);
+  b->derived.resize(nsims);
+  b->last.resize(nsims);
+  for (int s = 0; s < nsims; s++) {
+    char err[256] = "";
+    if (gp_host_derive(&params[s], &b->derived[s], err, sizeof err) != GP_OK) {
+      int r = bfail(nullptr, GP_EINVAL, "gp_batch_create: simulation %d: %s", s, err);
+      delete b;
+      return r;
+    }
+    const gp_derived &d = b->derived[s];
+    if (s == 0) { b->N = d.N; b->K = d.K; b->aniso = d.aniso; }
+    else if (d.N != b->N || d.K != b->K || d.aniso != b->aniso) {
+      delete b;
+      return bfail(nullptr, GP_EINVAL, "gp_batch_create: simulation %d differs in NUMPHASES, NUMCOMPONENTS or "
+                                       "Function_anisotropy from simulation 0", s);
+    }
+  }
+  bool ok = prec == GP_FP64 ? gp_batch_launch_f64(b->N, b->K, b->aniso != 0, &b->L)
+                            : gp_batch_launch_f32(b->N, b->K, b->aniso != 0, &b->L);
+  if (!ok) {
+    delete b;
+    return bfail(nullptr, GP_EINVAL, "gp_batch_create: no kernel for N=%d K=%d", b->N, b->K);
+  }
+  b->elem = b->L.elem;
+  int rc = GP_OK;
+  cudaError_t e = cudaGetDevice(&b->dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&b->nsm, cudaDevAttrMultiProcessorCount, b->dev);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    rc = bfail(b, GP_ECUDA, "gp_batch_create: %s", cudaGetErrorString(e));
+    gp_set_thread_error("%s", b->err);
+    gp_batch_destroy(b);
+    return rc;
+  }
+  /* layout: every simulation's N+K planes back to back, pitch a multiple of 32 */
+  const int N = b->N, K = b->K, ne = 2 * (N + K), ns = 2 * N + 2 * K + 1;
+  long long off = 0, offd = 0;
+  int tu = 0, td = 0;
+  std::vector<int> tsim_u, tsim_d, seg0, segn;
+  std::vector<char> consts;
+  const size_t csz = b->elem == 8 ? sizeof(gpd::Consts<double>) : sizeof(gpd::Consts<float>);
+  b->consts_bytes = csz;
+  consts.resize(csz * nsims);
+  for (int s = 0; s < nsims; s++) {
+    const gp_derived &d = b->derived[s];
+    gpd::SimDesc sd;
+    sd.g = make_grid(d, 32);
+    sd.off_state = off;
+    sd.off_dphi = offd;
+    sd.tiles_x = (sd.g.my + gpd::TY - 1) / gpd::TY;
+    const int tiles_y = (sd.g.mx + gpd::TX - 1) / gpd::TX;
+    sd.tile0 = tu;
+    sd.dtiles_x = (sd.g.my + 2 + gpd::TY - 1) / gpd::TY;
+    const int dtiles_y = (sd.g.mx + 2 + gpd::TX - 1) / gpd::TX;
+    sd.dtile0 = td;
+    seg0.push_back(tu);
+    segn.push_back(sd.tiles_x * tiles_y);
+    for (int t = 0; t < sd.tiles_x * tiles_y; t++) tsim_u.push_back(s);
+    for (int t = 0; t < sd.dtiles_x * dtiles_y; t++) tsim_d.push_back(s);
+    tu += sd.tiles_x * tiles_y;
+    td += sd.dtiles_x * dtiles_y;
+    off += (long long)(N + K) * sd.g.plane;
+    offd += (long long)N * sd.g.dplane;
+    b->desc.push_back(sd);
+    if (b->elem == 8) {
+      gpd::Consts<double> c = make_consts<double>(d);
+      memcpy(&consts[csz * s], &c, csz);
+    } else {
+      gpd::Consts<float> c = make_consts<float>(d);
+      memcpy(&consts[csz * s], &c, csz);
+    }
+  }
+  b->ntiles_u = tu;
+  b->ntiles_d = td;
+  int bpd = 1, bpu = 1;
+  e = b->L.prepare(&bpd, &bpu);
+  if (e != cudaSuccess) {
+    rc = bfail(b, GP_ECUDA, "gp_batch_create: %s", cudaGetErrorString(e));
+    gp_batch_destroy(b);
+    return rc;
+  }
+  b->grid_d = std::min(td, b->nsm * std::max(1, bpd));
+  b->grid_u = std::min(tu, b->nsm * std::max(1, bpu));
+#define BALLOC(ptr, bytes)                                                                        \
+  do {                                                                                            \
+    if (cudaMalloc((void **)&(ptr), (bytes)) != cudaSuccess) {                                     \
+      rc = bfail(b, GP_ENOMEM, "gp_batch_create: cudaMalloc of %zu bytes failed", (size_t)(bytes)); \
+      gp_batch_destroy(b);                                                                        \
+      return rc;                                                                                  \
+    }                                                                                             \
+  } while (0)
+  BALLOC(b->state[0], (size_t)off * b->elem);
+  BALLOC(b->state[1], (size_t)off * b->elem);
+  BALLOC(b->dphi, (size_t)offd * b->elem);
+  BALLOC(b->d_desc, sizeof(gpd::SimDesc) * nsims);
+  BALLOC(b->d_consts, csz * nsims);
+  BALLOC(b->d_tsim_u, sizeof(int) * tu);
+  BALLOC(b->d_tsim_d, sizeof(int) * td);
+  BALLOC(b->d_seg0, sizeof(int) * nsims);
+  BALLOC(b->d_segn, sizeof(int) * nsims);
+  BALLOC(b->ext, sizeof(long long) * (size_t)ne * tu);
+  BALLOC(b->ext_sim, sizeof(long long) * (size_t)ne * nsims);
+  BALLOC(b->partials, sizeof(double) * (size_t)ns * tu);
+  BALLOC(b->sums_sim, sizeof(double) * (size_t)ns * nsims);
+  BALLOC(b->counters, 4 * sizeof(int));   /* dphi queue, update queue, step, pad */
+#undef BALLOC
+  std::vector<long long> ext((size_t)ne * tu);
+  for (int t = 0; t < tu; t++) init_ext(&ext[(size_t)t * ne], N, K);
+#define BUP(dst, src, bytes)                                                                       \
+  do {                                                                                             \
+    if (cudaMemcpyAsync((dst), (src), (bytes), cudaMemcpyHostToDevice, b->stream) != cudaSuccess) { \
+      rc = bfail(b, GP_ECUDA, "gp_batch_create: upload failed");                                   \
+      gp_batch_destroy(b);                                                                         \
+      return rc;                                                                                   \
+    }                                                                                              \
+  } while (0)
+  BUP(b->d_desc, b->desc.data(), sizeof(gpd::SimDesc) * nsims);
+  BUP(b->d_consts, consts.data(), csz * nsims);
+  BUP(b->d_tsim_u, tsim_u.data(), sizeof(int) * tu);
+  BUP(b->d_tsim_d, tsim_d.data(), sizeof(int) * td);
+  BUP(b->d_seg0, seg0.data(), sizeof(int) * nsims);
+  BUP(b->d_segn, segn.data(), sizeof(int) * nsims);
+  BUP(b->ext, ext.data(), sizeof(long long) * ext.size());
+#undef BUP
+  if (cudaMemsetAsync(b->dphi, 0, (size_t)offd * b->elem, b->stream) != cudaSuccess ||
+      cudaMemsetAsync(b->counters, 0, 4 * sizeof(int), b->stream) != cudaSuccess) {
+    rc = bfail(b, GP_ECUDA, "gp_batch_create: memset failed");
+    gp_batch_destroy(b);
+    return rc;
+  }
+  for (int s = 0; s < nsims; s++) {
+    if ((rc = batch_copy(b, s, phi[s], mu[s], nullptr, nullptr)) != GP_OK) {
+      gp_batch_destroy(b);
+      return rc;
+    }
+  }
+  *out = b;
+  return GP_OK;
+}
+
+int gp_batch_smooth(gp_batch *b, long nsteps) {
+  if (!b || nsteps < 0) return bfail(b, GP_EINVAL, "gp_batch_smooth: bad argument");
+  const size_t csz = b->consts_bytes;
+  for (long t = 0; t < nsteps; t++) {
+    for (int s = 0; s < b->nsims; s++) {
+      const gpd::SimDesc &sd = b->desc[s];
+      const char *cs = (const char *)b->d_consts + csz * s;
+      const char *st = (const char *)b->state[b->cur] + (size_t)sd.off_state * b->elem;
+      char *nx = (char *)b->state[b->cur ^ 1] + (size_t)sd.off_state * b->elem;
+      char *dp = (char *)b->dphi + (size_t)sd.off_dphi * b->elem;
+      const size_t mu_off = (size_t)b->N * sd.g.plane * b->elem;
+      BK(b->L.sdphi(b->stream, cs, st, dp, sd.g));
+      BK(b->L.supd(b->stream, cs, st, st + mu_off, dp, nx, nx + mu_off, sd.g));
+    }
+    b->cur ^= 1;
+  }
+  BK(cudaStreamSynchronize(b->stream));
+  return GP_OK;
+}
+
+int gp_batch_step(gp_batch *b, long nsteps, gp_stats *stats) {
+  if (!b || nsteps < 0) return bfail(b, GP_EINVAL, "gp_batch_step: bad argument");
+  return batch_step_impl(b, nsteps, stats, nullptr);
+}
+
+int gp_batch_step_timed(gp_batch *b, long nsteps, gp_stats *stats, double *total_ms) {
+  if (!b || nsteps < 0) return bfail(b, GP_EINVAL, "gp_batch_step_timed: bad argument");
+  return batch_step_impl(b, nsteps, stats, total_ms);
+}
+
+int gp_batch_get(gp_batch *b, int sim, double *phi, double *mu) {
+  if (!b || sim < 0 || sim >= b->nsims || !phi || !mu) return bfail(b, GP_EINVAL, "gp_batch_get: bad argument");
+  return batch_copy(b, sim, nullptr, nullptr, phi, mu);
+}
+
+int gp_batch_set(gp_batch *b, int sim, const double *phi, const double *mu) {
+  if (!b || sim < 0 || sim >= b->nsims || !phi || !mu) return bfail(b, GP_EINVAL, "gp_batch_set: bad argument");
+  return batch_copy(b, sim, phi, mu, nullptr, nullptr);
+}
+
+int gp_batch_size(const gp_batch *b) { return b ? b->nsims : 0; }
+
+/* ======================================================================= */
+/* single-simulation API                                                   */
+/* ======================================================================= */
+
+const char *gp_version(void) { return "libgp 0.2 (sm_100a; FP64 plain step, batched FP64/FP32)"; }
 
 size_t gp_params_size(void) { return sizeof(gp_params); }
 
-const char *gp_last_error(const gp_ctx *ctx) { return ctx ? ctx->err : gp_host_thread_error(); }
+const char *gp_last_error(const gp_ctx *ctx) {
+  if (ctx && ctx->b) return ctx->b->err[0] ? ctx->b->err : ctx->err;
+  return ctx ? ctx->err : gp_host_thread_error();
+}
 
-void *gp_stream(gp_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
+void *gp_stream(gp_ctx *ctx) {
+  if (!ctx) return nullptr;
+  return ctx->b ? (void *)ctx->b->stream : (void *)ctx->stream;
+}
+
+void gp_destroy(gp_ctx *c) {
+  if (!c) return;
+  if (c->b) gp_batch_destroy(c->b);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  cudaFree(c->phi[0]);
+  cudaFree(c->phi[1]);
+  cudaFree(c->mu[0]);
+  cudaFree(c->mu[1]);
+  cudaFree(c->dphi);
+  cudaFree(c->ext);
+  cudaFree(c->ext_red);
+  cudaFree(c->partials);
+  cudaFree(c->sums);
+  cudaFree(c->seg);
+  cudaFree(c->dconsts);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  if (g_last_ctx == c) g_last_ctx = nullptr;
+  free(c);
+}
 
 int gp_init(gp_ctx **out, const gp_params *p, const double *phi, const double *mu, gp_precision prec) {
   gp_ctx *c = nullptr;
   if (!out || !p || !phi || !mu) return fail(nullptr, GP_EINVAL, "gp_init: NULL argument");
   *out = nullptr;
-  if (prec != GP_FP64) return fail(nullptr, GP_EUNSUPPORTED, "gp_init: only GP_FP64 is built in this context type");
+  if (prec != GP_FP64 && prec != GP_FP32) return fail(nullptr, GP_EINVAL, "gp_init: unknown precision %d", (int)prec);
   c = (gp_ctx *)calloc(1, sizeof(gp_ctx));
   if (!c) return fail(nullptr, GP_ENOMEM, "gp_init: out of host memory");
   c->p = *p;
@@ -227,6 +764,16 @@ int gp_init(gp_ctx **out, const gp_params *p, const double *phi, const double *m
     int r = fail(nullptr, GP_EINVAL, "gp_init: %s", err);
     free(c);
     return r;
+  }
+  if (prec == GP_FP32) {
+    const double *ph[1] = {phi}, *m[1] = {mu};
+    int r = gp_batch_create(&c->b, 1, p, ph, m, GP_FP32);
+    if (r != GP_OK) {
+      free(c);
+      return r;
+    }
+    *out = c;
+    return GP_OK;
   }
   Kern k;
   if (!pick(c->d.N, c->d.K, c->d.aniso != 0, &k)) {
@@ -245,51 +792,54 @@ int gp_init(gp_ctx **out, const gp_params *p, const double *phi, const double *m
     return fail(nullptr, GP_ECUDA, "gp_init: %s", cudaGetErrorString(e));
   }
   const gp_derived &d = c->d;
-  gpd::Grid &g = c->g;
-  g.mx = (int)d.mx;
-  g.my = (int)d.my;
-  g.pitch = (int)((d.my + 31) / 32 * 32);
-  g.plane = (long long)g.pitch * d.mx;
-  g.dpitch = (int)((d.my + 2 + 31) / 32 * 32);
-  g.dplane = (long long)g.dpitch * (d.mx + 2);
-  g.dx_pow2 = pow2(d.dx);
-  g.dy_pow2 = pow2(d.dy);
-  g.inv_dx = 1.0 / d.dx;
-  g.inv_dy = 1.0 / d.dy;
-  g.inv_2dy = 1.0 / (2.0 * d.dy);
+  c->g = make_grid(d, 32);
+  c->consts = make_consts<double>(d);
+  const gpd::Grid &g = c->g;
   const int ublocks = (int)(((d.my + gpd::TY - 1) / gpd::TY) * ((d.mx + gpd::TX - 1) / gpd::TX));
   c->ublocks = ublocks;
-  const int nsum = 2 * d.N + 2 * d.K + 1;
-#define ALLOC(ptr, bytes)                                                           \
-  do {                                                                              \
-    if (cudaMalloc((void **)&(ptr), (bytes)) != cudaSuccess) {                       \
-      rc = fail(c, GP_ENOMEM, "gp_init: cudaMalloc of %zu bytes failed", (size_t)(bytes)); \
-      goto bad;                                                                     \
-    }                                                                               \
+  const int nsum = 2 * d.N + 2 * d.K + 1, ne = 2 * (d.N + d.K);
+#define ALLOC(ptr, bytes)                                                                           \
+  do {                                                                                              \
+    if (cudaMalloc((void **)&(ptr), (bytes)) != cudaSuccess) {                                       \
+      rc = fail(c, GP_ENOMEM, "gp_init: cudaMalloc of %zu bytes failed", (size_t)(bytes));          \
+      goto bad;                                                                                     \
+    }                                                                                               \
   } while (0)
   ALLOC(c->phi[0], (size_t)g.plane * d.N * 8);
   ALLOC(c->phi[1], (size_t)g.plane * d.N * 8);
   ALLOC(c->mu[0], (size_t)g.plane * d.K * 8);
   ALLOC(c->mu[1], (size_t)g.plane * d.K * 8);
   ALLOC(c->dphi, (size_t)g.dplane * d.N * 8);
-  ALLOC(c->ext, sizeof(long long) * 2 * (d.N + d.K) * (size_t)ublocks);
-  ALLOC(c->ext_red, sizeof(long long) * 2 * (d.N + d.K));
+  ALLOC(c->ext, sizeof(long long) * ne * (size_t)ublocks);
+  ALLOC(c->ext_red, sizeof(long long) * ne);
   ALLOC(c->partials, sizeof(double) * (size_t)ublocks * nsum);
   ALLOC(c->sums, sizeof(double) * nsum);
+  ALLOC(c->seg, sizeof(int) * 2);
+  ALLOC(c->dconsts, sizeof(gpd::Consts<double>));
 #undef ALLOC
-  if (cudaDeviceSynchronize() != cudaSuccess ||
-      cudaMemcpyToSymbol(cD, &c->d, sizeof(gp_derived)) != cudaSuccess) {
-    rc = fail(c, GP_ECUDA, "gp_init: constant upload failed");
+  {
+    int seg[2] = {0, ublocks};
+    std::vector<long long> ext((size_t)ne * ublocks);
+    for (int t = 0; t < ublocks; t++) init_ext(&ext[(size_t)t * ne], d.N, d.K);
+    if (cudaMemcpy(c->seg, seg, sizeof seg, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(c->ext, ext.data(), ext.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(c->dconsts, &c->consts, sizeof(c->consts), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemset(c->dphi, 0, (size_t)g.dplane * d.N * 8) != cudaSuccess) {
+      rc = fail(c, GP_ECUDA, "gp_init: upload failed");
+      goto bad;
+    }
+  }
+  if (cudaFuncSetAttribute(k.dphi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem_dphi) != cudaSuccess ||
+      cudaFuncSetAttribute(k.upd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem_upd) != cudaSuccess) {
+    rc = fail(c, GP_ECUDA, "gp_init: kernel attributes");
     goto bad;
   }
-  g_last_ctx = c;
-  if ((rc = setup_kernels(c, k)) != GP_OK) goto bad;
-  if (cudaMemsetAsync(c->dphi, 0, (size_t)g.dplane * d.N * 8, c->stream) != cudaSuccess) {
-    rc = fail(c, GP_ECUDA, "gp_init: memset failed");
-    goto bad;
-  }
+  if ((rc = bind(c)) != GP_OK) goto bad;
   if ((rc = upload_state(c, phi, mu, cudaMemcpyHostToDevice)) != GP_OK) goto bad;
-  if ((rc = reset_minmax(c)) != GP_OK) goto bad;
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess) {
+    rc = fail(c, GP_ECUDA, "gp_init: upload failed");
+    goto bad;
+  }
   *out = c;
   return GP_OK;
 bad:
@@ -298,80 +848,44 @@ bad:
   return rc;
 }
 
-
-static int bind(gp_ctx *c) {
-  if (g_last_ctx != c) {
-    /* another context's kernels may still read the constant block */
-    CK(cudaDeviceSynchronize());
-    CK(cudaMemcpyToSymbol(cD, &c->d, sizeof(gp_derived)));
-    g_last_ctx = c;
-  }
-  return GP_OK;
-}
-
 int gp_smooth(gp_ctx *c, long nsteps) {
   if (!c || nsteps < 0) return fail(c, GP_EINVAL, "gp_smooth: bad argument");
+  if (c->b) return gp_batch_smooth(c->b, nsteps);
   Kern k;
   pick(c->d.N, c->d.K, c->d.aniso != 0, &k);
-  int rc = bind(c);
-  if (rc) return rc;
   const gpd::Grid &g = c->g;
-  dim3 grid((g.my + 127) / 128, g.mx);
   for (long s = 0; s < nsteps; s++) {
-    k.sdphi<<<grid, 128, 0, c->stream>>>(c->phi[c->cur], c->dphi, g);
-    k.supd<<<grid, 128, 0, c->stream>>>(c->phi[c->cur], c->mu[c->cur], c->dphi, c->phi[c->cur ^ 1], c->mu[c->cur ^ 1], g);
+    CK(k.b.sdphi(c->stream, c->dconsts, c->phi[c->cur], c->dphi, g));
+    CK(k.b.supd(c->stream, c->dconsts, c->phi[c->cur], c->mu[c->cur], c->dphi, c->phi[c->cur ^ 1], c->mu[c->cur ^ 1], g));
     c->cur ^= 1;
   }
-  CK(cudaGetLastError());
   CK(cudaStreamSynchronize(c->stream));
   return GP_OK;
 }
 
 static int fill_stats(gp_ctx *c, gp_stats *s) {
-  const int N = c->d.N, K = c->d.K, nsum = 2 * N + 2 * K + 1;
+  const int N = c->d.N, K = c->d.K, nsum = 2 * N + 2 * K + 1, ne = 2 * (N + K);
   long long mm[2 * (GPK_MAXN + GPK_MAXK)];
   double sums[2 * GPK_MAXN + 2 * GPK_MAXK + 1];
-  gpd::Grid &g = c->g;
-  (void)g;
-  k_reduce_partials<<<nsum, 256, 0, c->stream>>>(c->partials, c->ublocks, nsum, c->sums);
-  k_reduce_ext<<<2 * (N + K), 256, 0, c->stream>>>(c->ext, c->ublocks, 2 * (N + K), N, K, c->ext_red);
+  k_reduce_sums<<<dim3(nsum, 1), 256, 0, c->stream>>>(c->partials, c->seg, c->seg + 1, nsum, c->sums);
+  k_reduce_ext<<<dim3(ne, 1), 256, 0, c->stream>>>(c->ext, c->seg, c->seg + 1, ne, N, K, c->ext_red);
   CK(cudaGetLastError());
-  CK(cudaMemcpyAsync(mm, c->ext_red, sizeof(long long) * 2 * (N + K), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(mm, c->ext_red, sizeof(long long) * ne, cudaMemcpyDeviceToHost, c->stream));
   CK(cudaMemcpyAsync(sums, c->sums, sizeof(double) * nsum, cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
-  gp_stats r;
-  memset(&r, 0, sizeof r);
-  for (int a = 0; a < N; a++) {
-    r.phi_max[a] = from_ord(mm[a]);
-    r.phi_min[a] = from_ord(mm[N + a]);
-    r.rel_change_phi[a] = sums[a];
-    r.phi_sum[a] = sums[N + K + a];
-  }
-  for (int k = 0; k < K; k++) {
-    r.mu_max[k] = from_ord(mm[2 * N + k]);
-    r.mu_min[k] = from_ord(mm[2 * N + K + k]);
-    r.rel_change_mu[k] = sums[N + k];
-    r.comp_sum[k] = sums[2 * N + K + k];
-  }
-  r.nonfinite = (long long)llround(sums[2 * N + 2 * K]);
-  r.steps_done = c->steps;
-  c->last = r;
-  if (s) *s = r;
+  stats_from(&c->last, mm, sums, N, K, c->steps);
+  if (s) *s = c->last;
   return GP_OK;
-}
-
-static int step_impl(gp_ctx *c, long nsteps, gp_stats *stats, double *total_ms, double *ms_phase,
-                     double *ms_update);
-
-int gp_step(gp_ctx *c, long nsteps, gp_stats *stats) { return step_impl(c, nsteps, stats, nullptr, nullptr, nullptr); }
-
-int gp_step_timed(gp_ctx *c, long nsteps, gp_stats *stats, double *total_ms, double *ms_phase, double *ms_update) {
-  return step_impl(c, nsteps, stats, total_ms, ms_phase, ms_update);
 }
 
 static int step_impl(gp_ctx *c, long nsteps, gp_stats *stats, double *total_ms, double *ms_phase,
                      double *ms_update) {
   if (!c || nsteps < 0) return fail(c, GP_EINVAL, "gp_step: bad argument");
+  if (c->b) {
+    if (ms_phase) *ms_phase = 0.0;
+    if (ms_update) *ms_update = 0.0;
+    return batch_step_impl(c->b, nsteps, stats, total_ms);
+  }
   const bool timed = total_ms || ms_phase || ms_update;
   cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
   double t_phase = 0.0, t_update = 0.0;
@@ -392,7 +906,7 @@ static int step_impl(gp_ctx *c, long nsteps, gp_stats *stats, double *total_ms, 
     CK(cudaEventRecord(t_start, c->stream));
   }
   for (long s = 0; s < nsteps; s++) {
-    gpd::StatBufs st;
+    gpd::StatBufs st = {};
     st.ext = c->ext;
     st.partials = c->partials;
     st.want_sums = (stats != nullptr && s == nsteps - 1);
@@ -402,13 +916,13 @@ static int step_impl(gp_ctx *c, long nsteps, gp_stats *stats, double *total_ms, 
     k.upd<<<gu, gpd::NT, k.smem_upd, c->stream>>>(c->phi[c->cur], c->mu[c->cur], c->dphi, c->phi[c->cur ^ 1],
                                                    c->mu[c->cur ^ 1], g, st);
     if (timed) {
-      float a = 0.f, b = 0.f;
+      float a = 0.f, bb = 0.f;
       CK(cudaEventRecord(ev[2], c->stream));
       CK(cudaEventSynchronize(ev[2]));
       CK(cudaEventElapsedTime(&a, ev[0], ev[1]));
-      CK(cudaEventElapsedTime(&b, ev[1], ev[2]));
+      CK(cudaEventElapsedTime(&bb, ev[1], ev[2]));
       t_phase += a;
-      t_update += b;
+      t_update += bb;
     }
     c->cur ^= 1;
     c->steps++;
@@ -433,14 +947,21 @@ static int step_impl(gp_ctx *c, long nsteps, gp_stats *stats, double *total_ms, 
   return GP_OK;
 }
 
+int gp_step(gp_ctx *c, long nsteps, gp_stats *stats) { return step_impl(c, nsteps, stats, nullptr, nullptr, nullptr); }
+
+int gp_step_timed(gp_ctx *c, long nsteps, gp_stats *stats, double *total_ms, double *ms_phase, double *ms_update) {
+  return step_impl(c, nsteps, stats, total_ms, ms_phase, ms_update);
+}
+
 int gp_get_stats(gp_ctx *c, gp_stats *s) {
   if (!c || !s) return fail(c, GP_EINVAL, "gp_get_stats: bad argument");
-  *s = c->last;
+  *s = c->b ? c->b->last[0] : c->last;
   return GP_OK;
 }
 
 int gp_get(gp_ctx *c, double *phi, double *mu) {
   if (!c || !phi || !mu) return fail(c, GP_EINVAL, "gp_get: NULL argument");
+  if (c->b) return gp_batch_get(c->b, 0, phi, mu);
   int rc = download_state(c, phi, mu, cudaMemcpyDeviceToHost);
   if (rc) return rc;
   CK(cudaStreamSynchronize(c->stream));
@@ -449,6 +970,7 @@ int gp_get(gp_ctx *c, double *phi, double *mu) {
 
 int gp_set(gp_ctx *c, const double *phi, const double *mu) {
   if (!c || !phi || !mu) return fail(c, GP_EINVAL, "gp_set: NULL argument");
+  if (c->b) return gp_batch_set(c->b, 0, phi, mu);
   int rc = upload_state(c, phi, mu, cudaMemcpyHostToDevice);
   if (rc) return rc;
   CK(cudaStreamSynchronize(c->stream));
@@ -457,6 +979,7 @@ int gp_set(gp_ctx *c, const double *phi, const double *mu) {
 
 int gp_get_dev(gp_ctx *c, double *phi, double *mu) {
   if (!c || !phi || !mu) return fail(c, GP_EINVAL, "gp_get_dev: NULL argument");
+  if (c->b) return fail(c, GP_EUNSUPPORTED, "gp_get_dev: FP32 contexts exchange host buffers only");
   int rc = download_state(c, phi, mu, cudaMemcpyDeviceToDevice);
   if (rc) return rc;
   CK(cudaStreamSynchronize(c->stream));
@@ -465,27 +988,11 @@ int gp_get_dev(gp_ctx *c, double *phi, double *mu) {
 
 int gp_set_dev(gp_ctx *c, const double *phi, const double *mu) {
   if (!c || !phi || !mu) return fail(c, GP_EINVAL, "gp_set_dev: NULL argument");
+  if (c->b) return fail(c, GP_EUNSUPPORTED, "gp_set_dev: FP32 contexts exchange host buffers only");
   int rc = upload_state(c, phi, mu, cudaMemcpyDeviceToDevice);
   if (rc) return rc;
   CK(cudaStreamSynchronize(c->stream));
   return GP_OK;
-}
-
-void gp_destroy(gp_ctx *c) {
-  if (!c) return;
-  if (c->stream) cudaStreamSynchronize(c->stream);
-  cudaFree(c->phi[0]);
-  cudaFree(c->phi[1]);
-  cudaFree(c->mu[0]);
-  cudaFree(c->mu[1]);
-  cudaFree(c->dphi);
-  cudaFree(c->ext);
-  cudaFree(c->ext_red);
-  cudaFree(c->partials);
-  cudaFree(c->sums);
-  if (c->stream) cudaStreamDestroy(c->stream);
-  if (g_last_ctx == c) g_last_ctx = nullptr;
-  free(c);
 }
 
 }  /* extern "C" */
@@ -501,7 +1008,7 @@ void gp_destroy(gp_ctx *c) {
 /* interior plus a one-cell ring, and the running-extreme counters live in */
 /* this fixed array instead of per-context cudaMalloc'd memory.  Every GPU */
 /* that loads the library holds these 32 MiB until the process exits.      */
-/* ======================================================================= */
+
 
 #define GP_NOALLOC_SCRATCH_DOUBLES (4u * 1024u * 1024u)   /* 32 MiB */
 static __device__ __align__(256) double g_noalloc_scratch[GP_NOALLOC_SCRATCH_DOUBLES];
@@ -524,18 +1031,8 @@ extern "C" int gp_step_noalloc(const gp_params *p, const double *phi_in, const d
   if (gp_host_derive(p, &d, err, sizeof err) != GP_OK) return fail(nullptr, GP_EINVAL, "gp_step_noalloc: %s", err);
   Kern k;
   if (!pick(d.N, d.K, d.aniso != 0, &k)) return fail(nullptr, GP_EINVAL, "gp_step_noalloc: no kernel for N=%d K=%d", d.N, d.K);
-  gpd::Grid g;
-  g.mx = (int)d.mx;
-  g.my = (int)d.my;
-  g.pitch = (int)d.my; /* caller's planes are contiguous [field][MESH_X][MESH_Y] */
-  g.plane = (long long)d.mx * d.my;
-  g.dpitch = (int)((d.my + 2 + 31) / 32 * 32);
-  g.dplane = (long long)g.dpitch * (d.mx + 2);
-  g.dx_pow2 = pow2(d.dx);
-  g.dy_pow2 = pow2(d.dy);
-  g.inv_dx = 1.0 / d.dx;
-  g.inv_dy = 1.0 / d.dy;
-  g.inv_2dy = 1.0 / (2.0 * d.dy);
+  gpd::Grid g = make_grid(d, 1); /* caller's planes are contiguous [field][MESH_X][MESH_Y] */
+  gpd::Consts<double> cs = make_consts<double>(d);
   /* scratch layout: [running extremes, 2(N+K) long longs][pad to 256 B][delta-phi, N planes] */
   const size_t head = 32;  /* doubles; holds 2*(4+2) long longs and keeps delta-phi 256-B aligned */
   const size_t need = head + (size_t)d.N * (size_t)g.dplane;
@@ -560,10 +1057,10 @@ extern "C" int gp_step_noalloc(const gp_params *p, const double *phi_in, const d
   CK(cudaFuncSetAttribute(k.upd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem_upd));
   /* the constant block is shared with the contexts: make them upload theirs again */
   g_last_ctx = nullptr;
-  CK(cudaMemcpyToSymbolAsync(cD, &d, sizeof(gp_derived), 0, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyToSymbolAsync(cD, &cs, sizeof(cs), 0, cudaMemcpyHostToDevice, s));
   /* the previous call's extremes are still in the array: start them from zero */
   CK(cudaMemsetAsync(scratch, 0, head * sizeof(double), s));
-  gpd::StatBufs st;
+  gpd::StatBufs st = {};
   st.ext = nullptr; /* no progress record on this path */
   st.partials = scratch; /* not written: no sums requested */
   st.want_sums = 0;

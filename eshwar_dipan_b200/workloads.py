@@ -181,3 +181,24 @@ def random_seeds(n, mesh, rmin, rmax, nsolid, seed=0):
         ph = int(rng.uniform() * nsolid) % nsolid
         out.append((ph, x, y, r))
     return out
+
+
+def ensemble(n=256, seed=0, side_min=128, side_max=1024, shrink=1):
+    """Batched-ensemble decks: n independent binary 2-phase simulations, side
+    32*round(logU[side_min, side_max]/32) (divided by shrink, at least 32),
+    liquid composition c0 ~ U[0.40, 0.48], anisotropy strength delta ~ U[0, 0.05],
+    1..8 solid seeds with uniform centres and r ~ U[4, 12].  Returns a list of
+    (input kwargs, seeds)."""
+    rng = SplitMix64(seed)
+    out = []
+    lo, hi = math.log(side_min), math.log(side_max)
+    for s in range(n):
+        side = 32 * int(round(math.exp(lo + (hi - lo) * rng.uniform()) / 32.0))
+        side = max(32, side // shrink // 32 * 32 if shrink > 1 else side)
+        c0 = round(0.40 + 0.08 * rng.uniform(), 6)
+        delta = round(0.05 * rng.uniform(), 6)
+        nseeds = 1 + int(8 * rng.uniform()) % 8
+        kw = dict(N=2, K=1, mesh=(side, side), aniso=True, dab=delta, d_solid=0.0, d_liquid=[1.0], dt=0.02,
+                  eps=4.0, T=1.0, liquid_c=[c0])
+        out.append((kw, random_seeds(nseeds, (side, side), 4.0, 12.0, 1, seed=seed * 1000003 + s + 1)))
+    return out

@@ -174,6 +174,31 @@ int gp_get_stats(gp_ctx *ctx, gp_stats *stats);
 int gp_step_timed(gp_ctx *ctx, long nsteps, gp_stats *stats, double *total_ms,
                   double *ms_phase, double *ms_update);
 
+/* ---- batches of simulations ------------------------------------------- */
+
+/* Many independent simulations stepped together: grids of different sizes,
+ * different physical parameters, one launch per pass over all of them
+ * (persistent CTAs pulling (simulation, tile) items from a work queue), steps
+ * replayed as CUDA graphs of 100 steps.  All simulations share NUMPHASES,
+ * NUMCOMPONENTS and Function_anisotropy.  The reference runs one simulation
+ * per process (microsim_gp.c); there is no batch call to replace.
+ * prec = GP_FP64: each simulation is bit-identical to gp_step on its own.
+ * prec = GP_FP32: fields stored and stepped in float; the dc/dmu inversion and
+ * every reduction in FP64.
+ * params: nsims structs; phi[s], mu[s]: host interior planes of simulation s. */
+typedef struct gp_batch gp_batch;
+int gp_batch_create(gp_batch **b, int nsims, const gp_params *params, const double *const *phi,
+                    const double *const *mu, gp_precision prec);
+int gp_batch_smooth(gp_batch *b, long nsteps);
+/* stats: NULL or nsims records, in simulation order */
+int gp_batch_step(gp_batch *b, long nsteps, gp_stats *stats);
+int gp_batch_step_timed(gp_batch *b, long nsteps, gp_stats *stats, double *total_ms);
+int gp_batch_get(gp_batch *b, int sim, double *phi, double *mu);
+int gp_batch_set(gp_batch *b, int sim, const double *phi, const double *mu);
+int gp_batch_size(const gp_batch *b);
+const char *gp_batch_last_error(const gp_batch *b);
+void gp_batch_destroy(gp_batch *b);
+
 /* One FP64 time step that allocates nothing.  This entry point has no
  * counterpart in the reference; it exists for callers that cannot call
  * cudaMalloc -- applications that own all device memory through their own pool
