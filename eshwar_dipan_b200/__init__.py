@@ -19,7 +19,7 @@ import numpy as np
 
 from ._abi import (GP_FP32, GP_FP64, GpError, Params, Stats, check, lib)
 
-__all__ = ["Params", "Stats", "GpError", "Simulation", "load_params", "fill", "vtk_write", "vtk_read",
+__all__ = ["Params", "Stats", "GpError", "Simulation", "Batch", "load_params", "fill", "vtk_write", "vtk_read",
            "GP_FP64", "GP_FP32", "version"]
 
 
@@ -97,13 +97,17 @@ class Simulation:
         check(lib().gp_step(self._h, int(n), None), self._h)
         return None
 
-    def step_timed(self, n, stats=False):
-        """Steps with device timing: (total_ms, phase_kernel_ms, update_kernel_ms, stats)."""
+    def step_timed(self, n, stats=False, split=False):
+        """Steps with device timing: (total_ms, bulk_kernel_ms, interface_kernel_ms, stats).
+        The per-kernel times are measured only with split=True (the steps then
+        run one by one instead of as CUDA graphs) and are None otherwise."""
         tot, a, b = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
         s = Stats() if stats else None
         check(lib().gp_step_timed(self._h, int(n), ctypes.byref(s) if stats else None, ctypes.byref(tot),
-                                  ctypes.byref(a), ctypes.byref(b)), self._h)
-        return tot.value, a.value, b.value, (s.as_dict(self.N, self.K) if stats else None)
+                                  ctypes.byref(a) if split else None, ctypes.byref(b) if split else None),
+              self._h)
+        return (tot.value, a.value if split else None, b.value if split else None,
+                s.as_dict(self.N, self.K) if stats else None)
 
     def get(self):
         sp, sm = _shapes(self.params)

@@ -7,16 +7,23 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include "gp_fused.cuh"
 #include "gp_smooth.cuh"
 
 namespace gpd {
 
 struct BatchLaunch {
-  cudaError_t (*prepare)(int *blocks_per_sm_dphi, int *blocks_per_sm_upd);
-  cudaError_t (*dphi)(int grid, cudaStream_t s, const SimDesc *sims, const void *consts, const int *tsim,
-                      int ntiles, int *counter, const void *state, void *dphi);
-  cudaError_t (*update)(int grid, cudaStream_t s, const SimDesc *sims, const void *consts, const int *tsim,
-                        int ntiles, int *counter, const void *state, const void *dphi, void *next, StatBufs st);
+  /* occupancy of the interface kernel (blocks per SM) */
+  cudaError_t (*prepare)(int *blocks_per_sm_general);
+  /* one step: bulk tiles + interface list, then the interface tiles */
+  cudaError_t (*bulk)(int ntiles, cudaStream_t s, const SimDesc *sims, const void *consts, const int *tsim,
+                      const void *state, void *next, const signed char *flag_in, signed char *flag_out, int *glist,
+                      int *ctr, StatBufs st);
+  cudaError_t (*general)(int grid, cudaStream_t s, const SimDesc *sims, const void *consts, const int *tsim,
+                         const void *state, void *next, signed char *flag_out, const int *glist, int *ctr,
+                         StatBufs st);
+  cudaError_t (*flags)(int ntiles, cudaStream_t s, const SimDesc *sims, const int *tsim, const void *state,
+                       signed char *flags);
   cudaError_t (*sdphi)(cudaStream_t s, const void *consts, const void *phi, void *dphi, Grid g);
   cudaError_t (*supd)(cudaStream_t s, const void *consts, const void *phi, const void *mu, const void *dphi,
                       void *phin, void *mun, Grid g);
@@ -25,27 +32,29 @@ struct BatchLaunch {
 
 template <typename R, int N, int K, bool A>
 struct BatchKernels {
-  static cudaError_t prepare(int *bd, int *bu) {
-    cudaError_t e = cudaFuncSetAttribute(kb_dphi<R, N, K, A>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)sizeof(DphiSmem<R, N>));
+  static cudaError_t prepare(int *bg) {
+    cudaError_t e = cudaFuncSetAttribute(kf_general<R, N, K, A>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)sizeof(GenSmem<R, N, K>));
     if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(kb_update<R, N, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)sizeof(UpdSmem<R, N, K>));
-    if (e != cudaSuccess) return e;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(bd, kb_dphi<R, N, K, A>, NT, sizeof(DphiSmem<R, N>));
-    if (e != cudaSuccess) return e;
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bu, kb_update<R, N, K>, NT, sizeof(UpdSmem<R, N, K>));
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bg, kf_general<R, N, K, A>, NT, sizeof(GenSmem<R, N, K>));
   }
-  static cudaError_t dphi(int grid, cudaStream_t s, const SimDesc *sims, const void *consts, const int *tsim,
-                          int ntiles, int *counter, const void *state, void *dphi) {
-    kb_dphi<R, N, K, A><<<grid, NT, sizeof(DphiSmem<R, N>), s>>>(
-        sims, (const Consts<R> *)consts, tsim, ntiles, counter, (const R *)state, (R *)dphi);
+  static cudaError_t bulk(int ntiles, cudaStream_t s, const SimDesc *sims, const void *consts, const int *tsim,
+                          const void *state, void *next, const signed char *flag_in, signed char *flag_out,
+                          int *glist, int *ctr, StatBufs st) {
+    kf_bulk<R, N, K><<<ntiles, NT, 0, s>>>(sims, (const Consts<R> *)consts, tsim, (const R *)state, (R *)next,
+                                           flag_in, flag_out, glist, ctr, st);
     return cudaGetLastError();
   }
-  static cudaError_t update(int grid, cudaStream_t s, const SimDesc *sims, const void *consts, const int *tsim,
-                            int ntiles, int *counter, const void *state, const void *dphi, void *next, StatBufs st) {
-    kb_update<R, N, K><<<grid, NT, sizeof(UpdSmem<R, N, K>), s>>>(
-        sims, (const Consts<R> *)consts, tsim, ntiles, counter, (const R *)state, (const R *)dphi, (R *)next, st);
+  static cudaError_t general(int grid, cudaStream_t s, const SimDesc *sims, const void *consts, const int *tsim,
+                             const void *state, void *next, signed char *flag_out, const int *glist, int *ctr,
+                             StatBufs st) {
+    kf_general<R, N, K, A><<<grid, NT, sizeof(GenSmem<R, N, K>), s>>>(
+        sims, (const Consts<R> *)consts, tsim, (const R *)state, (R *)next, flag_out, glist, ctr, st);
+    return cudaGetLastError();
+  }
+  static cudaError_t flags(int ntiles, cudaStream_t s, const SimDesc *sims, const int *tsim, const void *state,
+                           signed char *fl) {
+    kf_flags<R, N><<<ntiles, NT, 0, s>>>(sims, tsim, (const R *)state, fl);
     return cudaGetLastError();
   }
   static cudaError_t sdphi(cudaStream_t s, const void *consts, const void *phi, void *dphi, Grid g) {
@@ -63,8 +72,9 @@ struct BatchKernels {
   static BatchLaunch table() {
     BatchLaunch t;
     t.prepare = prepare;
-    t.dphi = dphi;
-    t.update = update;
+    t.bulk = bulk;
+    t.general = general;
+    t.flags = flags;
     t.sdphi = sdphi;
     t.supd = supd;
     t.elem = sizeof(R);

@@ -1,15 +1,17 @@
 /*
  * gp_device.cu -- libgp: the C ABI (include/gp.h) over the sm_100a kernels.
- * Host orchestration only; the kernels are in gp_tiles.cuh / gp_smooth.cuh.
+ * Host orchestration only; the kernels are in gp_fused.cuh (the stepping
+ * engine), gp_tiles.cuh (shared tile code and the two-pass kernels of
+ * gp_step_noalloc) and gp_smooth.cuh (the smoothing sweeps).
  *
- *  - gp_ctx, FP64: one simulation, kernels k_dphi / k_update (one CTA per
- *    tile) with the constants in __constant__ memory; bit-identical to the
- *    reference step.
- *  - gp_batch: many simulations of different sizes and parameters stepped
- *    together by persistent kernels pulling (simulation, tile) items from a
- *    work queue, in FP64 or in the FP32 storage form (gp_batch32.cu); steps
- *    are replayed as CUDA graphs of GP_GRAPH_STEPS steps.
- *  - gp_ctx, FP32: a batch of one.
+ *  - gp_batch: simulations of different sizes and parameters stepped together
+ *    by two kernels per step (bulk tiles, then interface tiles from a device
+ *    work list), in FP64 (bit-identical to the reference step) or in the FP32
+ *    storage form (gp_batch32.cu); steps are replayed as CUDA graphs of
+ *    GP_GRAPH_STEPS steps.
+ *  - gp_ctx: one simulation, a batch of one.
+ *  - gp_step_noalloc: one FP64 step on caller-owned buffers, two-pass kernels
+ *    with constants in __constant__ memory and a fixed scratch array.
  */
 #include <cuda_runtime.h>
 
@@ -174,7 +176,8 @@ void stats_from(gp_stats *r, const long long *mm, const double *sums, int N, int
 }  // namespace
 
 /* ======================================================================= */
-/* single FP64 simulation: one CTA per tile, constants in __constant__     */
+/* two-pass FP64 kernels of gp_step_noalloc: one CTA per tile, constants   */
+/* in __constant__ memory                                                  */
 /* ======================================================================= */
 
 namespace gpd {
@@ -204,7 +207,6 @@ namespace {
 struct Kern {
   void (*dphi)(const double *, const double *, double *, gpd::Grid);
   void (*upd)(const double *, const double *, const double *, double *, double *, gpd::Grid, gpd::StatBufs);
-  gpd::BatchLaunch b;   /* smoothing kernels */
   size_t smem_dphi, smem_upd;
 };
 
@@ -213,7 +215,6 @@ Kern make() {
   Kern k;
   k.dphi = gpd::k_dphi<N, K, A>;
   k.upd = gpd::k_update<N, K>;
-  k.b = gpd::BatchKernels<double, N, K, A>::table();
   k.smem_dphi = sizeof(gpd::DphiSmem<double, N>);
   k.smem_upd = sizeof(gpd::UpdSmem<double, N, K>);
   return k;
@@ -236,29 +237,12 @@ bool gp_batch_launch_f64(int N, int K, bool aniso, gpd::BatchLaunch *out) {
   return gpd::batch_launch_table<double>(N, K, aniso, out);
 }
 
+
 struct gp_batch;
 
+/* A single simulation is a batch of one. */
 struct gp_ctx {
-  gp_params p;
-  gp_derived d;
-  gp_precision prec;
-  gp_batch *b;                  /* FP32 contexts are a batch of one */
-  int dev;
-  cudaStream_t stream;
-  gpd::Grid g;
-  gpd::Consts<double> consts;
-  gpd::Consts<double> *dconsts; /* device copy for the smoothing kernels */
-  double *phi[2], *mu[2];       /* ping-pong state planes */
-  int cur;
-  double *dphi;                 /* delta-phi over the interior plus a ring */
-  long long *ext;               /* per-tile running extremes [ublocks][2(N+K)] */
-  long long *ext_red;
-  double *partials;             /* per-tile sums of the last stats step */
-  double *sums;
-  int *seg;                     /* {0, ublocks} for the per-simulation folds */
-  int ublocks;
-  long long steps;
-  gp_stats last;
+  gp_batch *b;
   char err[256];
 };
 
@@ -281,43 +265,6 @@ static int fail(gp_ctx *c, int code, const char *fmt, ...) {
     if (e_ != cudaSuccess) return fail(c, GP_ECUDA, "%s: %s", #call, cudaGetErrorString(e_));  \
   } while (0)
 
-/* The constant block is per module and device; a context re-uploads it when
- * another context (or gp_step_noalloc) used it last.  Contexts are not meant to
- * be driven from several host threads at once. */
-static const gp_ctx *g_last_ctx = nullptr;
-
-static int bind(gp_ctx *c) {
-  if (g_last_ctx != c) {
-    /* another context's kernels may still read the constant block */
-    CK(cudaDeviceSynchronize());
-    CK(cudaMemcpyToSymbol(cD, &c->consts, sizeof(c->consts)));
-    g_last_ctx = c;
-  }
-  return GP_OK;
-}
-
-static int upload_state(gp_ctx *c, const double *phi, const double *mu, cudaMemcpyKind kind) {
-  const gp_derived &d = c->d;
-  for (int a = 0; a < d.N; a++)
-    CK(cudaMemcpy2DAsync(c->phi[c->cur] + a * c->g.plane, (size_t)c->g.pitch * 8, phi + (size_t)a * d.mx * d.my,
-                         (size_t)d.my * 8, (size_t)d.my * 8, (size_t)d.mx, kind, c->stream));
-  for (int k = 0; k < d.K; k++)
-    CK(cudaMemcpy2DAsync(c->mu[c->cur] + k * c->g.plane, (size_t)c->g.pitch * 8, mu + (size_t)k * d.mx * d.my,
-                         (size_t)d.my * 8, (size_t)d.my * 8, (size_t)d.mx, kind, c->stream));
-  return GP_OK;
-}
-
-static int download_state(gp_ctx *c, double *phi, double *mu, cudaMemcpyKind kind) {
-  const gp_derived &d = c->d;
-  for (int a = 0; a < d.N; a++)
-    CK(cudaMemcpy2DAsync(phi + (size_t)a * d.mx * d.my, (size_t)d.my * 8, c->phi[c->cur] + a * c->g.plane,
-                         (size_t)c->g.pitch * 8, (size_t)d.my * 8, (size_t)d.mx, kind, c->stream));
-  for (int k = 0; k < d.K; k++)
-    CK(cudaMemcpy2DAsync(mu + (size_t)k * d.mx * d.my, (size_t)d.my * 8, c->mu[c->cur] + k * c->g.plane,
-                         (size_t)c->g.pitch * 8, (size_t)d.my * 8, (size_t)d.mx, kind, c->stream));
-  return GP_OK;
-}
-
 /* ======================================================================= */
 /* batches                                                                 */
 /* ======================================================================= */
@@ -330,20 +277,23 @@ struct gp_batch {
   std::vector<gp_params> params;
   std::vector<gp_derived> derived;
   std::vector<gpd::SimDesc> desc;
-  int dev, nsm, grid_d, grid_u;
-  int ntiles_u, ntiles_d;
+  int dev, nsm, grid_g;
+  int ntiles;                   /* TX x TY tiles over all simulations */
   cudaStream_t stream;
   gpd::SimDesc *d_desc;
   void *d_consts;
   size_t consts_bytes;
-  int *d_tsim_u, *d_tsim_d, *d_seg0, *d_segn;
-  void *state[2];
-  void *dphi;
+  int *d_tsim, *d_seg0, *d_segn;
+  void *state[2];               /* ping-pong: every simulation's N phi then K mu planes */
+  void *dphi;                   /* delta-phi planes of the smoothing sweeps */
+  signed char *flags[2];        /* per tile and state buffer: one-hot phase, or mixed/unknown */
+  int *glist;                   /* interface tiles of the current step */
+  int *counters;                /* gpd::CTR_* */
   int cur;
   long long *ext, *ext_sim;
   double *partials, *sums_sim;
-  int *counters;
   cudaGraphExec_t graph[2];
+  cudaEvent_t ev[4];
   long long steps;
   std::vector<gp_stats> last;
   char err[256];
@@ -366,28 +316,32 @@ static int bfail(gp_batch *b, int code, const char *fmt, ...) {
     if (e_ != cudaSuccess) return bfail(b, GP_ECUDA, "%s: %s", #call, cudaGetErrorString(e_));  \
   } while (0)
 
-/* Start of a batched step: empty both work queues and advance the step counter
- * that keys the FP32 rounding stream (a kernel, so that graph replays advance it). */
-__global__ void k_step_begin(int *counters) {
-  counters[0] = 0;
-  counters[1] = 0;
-  counters[2] = (int)((unsigned)counters[2] + 1u);
-}
-
-static int batch_step_once(gp_batch *b, int want_sums) {
+/* One step: bulk tiles (and the interface list), then the interface tiles.
+ * ev: optional events around the two kernels. */
+static int batch_step_once(gp_batch *b, int want_sums, cudaEvent_t *ev) {
   gpd::StatBufs st = {};
   st.ext = b->ext;
   st.partials = b->partials;
   st.want_sums = want_sums;
-  st.round_step = (const unsigned *)(b->counters + 2);
-  k_step_begin<<<1, 1, 0, b->stream>>>(b->counters);
-  BK(cudaGetLastError());
-  BK(b->L.dphi(b->grid_d, b->stream, b->d_desc, b->d_consts, b->d_tsim_d, b->ntiles_d, b->counters,
-               b->state[b->cur], b->dphi));
-  BK(b->L.update(b->grid_u, b->stream, b->d_desc, b->d_consts, b->d_tsim_u, b->ntiles_u, b->counters + 1,
-                 b->state[b->cur], b->dphi, b->state[b->cur ^ 1], st));
-  b->cur ^= 1;
+  st.round_step = (const unsigned *)(b->counters + gpd::CTR_STEP);
+  const int in = b->cur, out = b->cur ^ 1;
+  if (ev) BK(cudaEventRecord(ev[0], b->stream));
+  BK(b->L.bulk(b->ntiles, b->stream, b->d_desc, b->d_consts, b->d_tsim, b->state[in], b->state[out], b->flags[in],
+               b->flags[out], b->glist, b->counters, st));
+  if (ev) BK(cudaEventRecord(ev[1], b->stream));
+  BK(b->L.general(b->grid_g, b->stream, b->d_desc, b->d_consts, b->d_tsim, b->state[in], b->state[out],
+                  b->flags[out], b->glist, b->counters, st));
+  if (ev) BK(cudaEventRecord(ev[2], b->stream));
+  b->cur = out;
   b->steps++;
+  return GP_OK;
+}
+
+/* Flags of the current buffer from its contents; the other buffer's are
+ * unknown (it is rewritten in full by the next step). */
+static int batch_reflag(gp_batch *b, bool other_unknown) {
+  BK(b->L.flags(b->ntiles, b->stream, b->d_desc, b->d_tsim, b->state[b->cur], b->flags[b->cur]));
+  if (other_unknown) BK(cudaMemsetAsync(b->flags[b->cur ^ 1], 0xfe, (size_t)b->ntiles, b->stream));
   return GP_OK;
 }
 
@@ -408,24 +362,24 @@ static int batch_fold_stats(gp_batch *b, gp_stats *out) {
   return GP_OK;
 }
 
-static int batch_step_impl(gp_batch *b, long nsteps, gp_stats *stats, double *total_ms) {
-  cudaEvent_t e0 = nullptr, e1 = nullptr;
-  if (total_ms) {
-    BK(cudaEventCreate(&e0));
-    BK(cudaEventCreate(&e1));
-    BK(cudaEventRecord(e0, b->stream));
-  }
+/* nsteps steps.  Whole chunks of GP_GRAPH_STEPS steps are replayed as CUDA
+ * graphs (an even number of steps returns the ping-pong parity to where it
+ * started, so one graph per starting parity suffices); the last step runs
+ * outside so that it can produce the sums.  With ms_bulk/ms_iface every step
+ * runs outside graphs with events around the two kernels. */
+static int batch_step_impl(gp_batch *b, long nsteps, gp_stats *stats, double *total_ms, double *ms_bulk,
+                           double *ms_iface) {
+  const bool split = ms_bulk || ms_iface;
+  double tb = 0.0, ti = 0.0;
+  if (total_ms) BK(cudaEventRecord(b->ev[3], b->stream));
   long s = 0;
-  /* whole chunks as CUDA graphs (an even number of steps returns the ping-pong
-   * parity to where it started, so one graph per starting parity suffices);
-   * the last step runs outside so that it can produce the sums */
-  while (nsteps - s > GP_GRAPH_STEPS) {
+  while (!split && nsteps - s > GP_GRAPH_STEPS) {
     const int p = b->cur;
     if (!b->graph[p]) {
       cudaGraph_t gr;
       BK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
       int rc = GP_OK;
-      for (int i = 0; i < GP_GRAPH_STEPS && rc == GP_OK; i++) rc = batch_step_once(b, 0);
+      for (int i = 0; i < GP_GRAPH_STEPS && rc == GP_OK; i++) rc = batch_step_once(b, 0, nullptr);
       b->steps -= GP_GRAPH_STEPS; /* captured, not run */
       cudaError_t ec = cudaStreamEndCapture(b->stream, &gr);
       if (rc != GP_OK) return rc;
@@ -439,18 +393,26 @@ static int batch_step_impl(gp_batch *b, long nsteps, gp_stats *stats, double *to
     s += GP_GRAPH_STEPS;
   }
   for (; s < nsteps; s++) {
-    int rc = batch_step_once(b, stats != nullptr && s == nsteps - 1);
+    int rc = batch_step_once(b, stats != nullptr && s == nsteps - 1, split ? b->ev : nullptr);
     if (rc != GP_OK) return rc;
+    if (split) {
+      float x = 0.f, y = 0.f;
+      BK(cudaEventSynchronize(b->ev[2]));
+      BK(cudaEventElapsedTime(&x, b->ev[0], b->ev[1]));
+      BK(cudaEventElapsedTime(&y, b->ev[1], b->ev[2]));
+      tb += x;
+      ti += y;
+    }
   }
   if (total_ms) {
     float ms = 0.f;
-    BK(cudaEventRecord(e1, b->stream));
-    BK(cudaEventSynchronize(e1));
-    BK(cudaEventElapsedTime(&ms, e0, e1));
+    BK(cudaEventRecord(b->ev[2], b->stream));
+    BK(cudaEventSynchronize(b->ev[2]));
+    BK(cudaEventElapsedTime(&ms, b->ev[3], b->ev[2]));
     *total_ms = ms;
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
   }
+  if (ms_bulk) *ms_bulk = tb;
+  if (ms_iface) *ms_iface = ti;
   if (stats && nsteps > 0) return batch_fold_stats(b, stats);
   BK(cudaStreamSynchronize(b->stream));
   if (stats)
@@ -458,31 +420,36 @@ static int batch_step_impl(gp_batch *b, long nsteps, gp_stats *stats, double *to
   return GP_OK;
 }
 
-static int batch_copy(gp_batch *b, int s, const double *phi, const double *mu, double *ophi, double *omu) {
-  /* host <-> device for one simulation; FP32 converts through a staging buffer */
+/* host <-> state of one simulation (kind: H2D, D2H, D2D).  FP32 converts
+ * through a host staging buffer and exchanges host buffers only. */
+static int batch_copy(gp_batch *b, int s, const double *phi, const double *mu, double *ophi, double *omu,
+                      cudaMemcpyKind kind) {
   const gpd::SimDesc &sd = b->desc[s];
   const int N = b->N, K = b->K;
   const size_t mx = sd.g.mx, my = sd.g.my;
   char *base = (char *)b->state[b->cur] + (size_t)sd.off_state * b->elem;
+  const bool up = phi != nullptr;
   for (int f = 0; f < N + K; f++) {
     char *plane = base + (size_t)f * sd.g.plane * b->elem;
     if (b->elem == 8) {
-      if (phi) {
+      if (up) {
         const double *src = f < N ? phi + (size_t)f * mx * my : mu + (size_t)(f - N) * mx * my;
-        BK(cudaMemcpy2DAsync(plane, (size_t)sd.g.pitch * 8, src, my * 8, my * 8, mx, cudaMemcpyHostToDevice, b->stream));
+        BK(cudaMemcpy2DAsync(plane, (size_t)sd.g.pitch * 8, src, my * 8, my * 8, mx, kind, b->stream));
       } else {
         double *dst = f < N ? ophi + (size_t)f * mx * my : omu + (size_t)(f - N) * mx * my;
-        BK(cudaMemcpy2DAsync(dst, my * 8, plane, (size_t)sd.g.pitch * 8, my * 8, mx, cudaMemcpyDeviceToHost, b->stream));
+        BK(cudaMemcpy2DAsync(dst, my * 8, plane, (size_t)sd.g.pitch * 8, my * 8, mx, kind, b->stream));
       }
     } else {
       std::vector<float> tmp(mx * my);
-      if (phi) {
+      if (up) {
         const double *src = f < N ? phi + (size_t)f * mx * my : mu + (size_t)(f - N) * mx * my;
         for (size_t i = 0; i < mx * my; i++) tmp[i] = (float)src[i];
-        BK(cudaMemcpy2DAsync(plane, (size_t)sd.g.pitch * 4, tmp.data(), my * 4, my * 4, mx, cudaMemcpyHostToDevice, b->stream));
+        BK(cudaMemcpy2DAsync(plane, (size_t)sd.g.pitch * 4, tmp.data(), my * 4, my * 4, mx, cudaMemcpyHostToDevice,
+                             b->stream));
         BK(cudaStreamSynchronize(b->stream));
       } else {
-        BK(cudaMemcpy2DAsync(tmp.data(), my * 4, plane, (size_t)sd.g.pitch * 4, my * 4, mx, cudaMemcpyDeviceToHost, b->stream));
+        BK(cudaMemcpy2DAsync(tmp.data(), my * 4, plane, (size_t)sd.g.pitch * 4, my * 4, mx, cudaMemcpyDeviceToHost,
+                             b->stream));
         BK(cudaStreamSynchronize(b->stream));
         double *dst = f < N ? ophi + (size_t)f * mx * my : omu + (size_t)(f - N) * mx * my;
         for (size_t i = 0; i < mx * my; i++) dst[i] = (double)tmp[i];
@@ -502,11 +469,14 @@ void gp_batch_destroy(gp_batch *b) {
     if (b->graph[p]) cudaGraphExecDestroy(b->graph[p]);
     cudaFree(b->state[p]);
   }
+  for (int i = 0; i < 4; i++)
+    if (b->ev[i]) cudaEventDestroy(b->ev[i]);
   cudaFree(b->dphi);
+  cudaFree(b->flags[0]);   /* flags[1] is part of the same allocation */
+  cudaFree(b->glist);
   cudaFree(b->d_desc);
   cudaFree(b->d_consts);
-  cudaFree(b->d_tsim_u);
-  cudaFree(b->d_tsim_d);
+  cudaFree(b->d_tsim);
   cudaFree(b->d_seg0);
   cudaFree(b->d_segn);
   cudaFree(b->ext);
@@ -558,17 +528,17 @@ int gp_batch_create(gp_batch **out, int nsims, const gp_params *params, const do
   cudaError_t e = cudaGetDevice(&b->dev);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&b->nsm, cudaDevAttrMultiProcessorCount, b->dev);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+  for (int i = 0; i < 4 && e == cudaSuccess; i++) e = cudaEventCreate(&b->ev[i]);
   if (e != cudaSuccess) {
     rc = bfail(b, GP_ECUDA, "gp_batch_create: %s", cudaGetErrorString(e));
-    gp_set_thread_error("%s", b->err);
     gp_batch_destroy(b);
     return rc;
   }
   /* layout: every simulation's N+K planes back to back, pitch a multiple of 32 */
   const int N = b->N, K = b->K, ne = 2 * (N + K), ns = 2 * N + 2 * K + 1;
   long long off = 0, offd = 0;
-  int tu = 0, td = 0;
-  std::vector<int> tsim_u, tsim_d, seg0, segn;
+  int nt = 0;
+  std::vector<int> tsim, seg0, segn;
   std::vector<char> consts;
   const size_t csz = b->elem == 8 ? sizeof(gpd::Consts<double>) : sizeof(gpd::Consts<float>);
   b->consts_bytes = csz;
@@ -576,21 +546,17 @@ int gp_batch_create(gp_batch **out, int nsims, const gp_params *params, const do
   for (int s = 0; s < nsims; s++) {
     const gp_derived &d = b->derived[s];
     gpd::SimDesc sd;
+    memset(&sd, 0, sizeof sd);
     sd.g = make_grid(d, 32);
     sd.off_state = off;
     sd.off_dphi = offd;
     sd.tiles_x = (sd.g.my + gpd::TY - 1) / gpd::TY;
     const int tiles_y = (sd.g.mx + gpd::TX - 1) / gpd::TX;
-    sd.tile0 = tu;
-    sd.dtiles_x = (sd.g.my + 2 + gpd::TY - 1) / gpd::TY;
-    const int dtiles_y = (sd.g.mx + 2 + gpd::TX - 1) / gpd::TX;
-    sd.dtile0 = td;
-    seg0.push_back(tu);
+    sd.tile0 = nt;
+    seg0.push_back(nt);
     segn.push_back(sd.tiles_x * tiles_y);
-    for (int t = 0; t < sd.tiles_x * tiles_y; t++) tsim_u.push_back(s);
-    for (int t = 0; t < sd.dtiles_x * dtiles_y; t++) tsim_d.push_back(s);
-    tu += sd.tiles_x * tiles_y;
-    td += sd.dtiles_x * dtiles_y;
+    for (int t = 0; t < sd.tiles_x * tiles_y; t++) tsim.push_back(s);
+    nt += sd.tiles_x * tiles_y;
     off += (long long)(N + K) * sd.g.plane;
     offd += (long long)N * sd.g.dplane;
     b->desc.push_back(sd);
@@ -602,17 +568,15 @@ int gp_batch_create(gp_batch **out, int nsims, const gp_params *params, const do
       memcpy(&consts[csz * s], &c, csz);
     }
   }
-  b->ntiles_u = tu;
-  b->ntiles_d = td;
-  int bpd = 1, bpu = 1;
-  e = b->L.prepare(&bpd, &bpu);
+  b->ntiles = nt;
+  int bpg = 1;
+  e = b->L.prepare(&bpg);
   if (e != cudaSuccess) {
     rc = bfail(b, GP_ECUDA, "gp_batch_create: %s", cudaGetErrorString(e));
     gp_batch_destroy(b);
     return rc;
   }
-  b->grid_d = std::min(td, b->nsm * std::max(1, bpd));
-  b->grid_u = std::min(tu, b->nsm * std::max(1, bpu));
+  b->grid_g = b->nsm * std::max(1, bpg);
 #define BALLOC(ptr, bytes)                                                                        \
   do {                                                                                            \
     if (cudaMalloc((void **)&(ptr), (bytes)) != cudaSuccess) {                                     \
@@ -624,20 +588,22 @@ int gp_batch_create(gp_batch **out, int nsims, const gp_params *params, const do
   BALLOC(b->state[0], (size_t)off * b->elem);
   BALLOC(b->state[1], (size_t)off * b->elem);
   BALLOC(b->dphi, (size_t)offd * b->elem);
+  BALLOC(b->flags[0], 2 * (size_t)nt);
+  b->flags[1] = b->flags[0] + nt;
+  BALLOC(b->glist, sizeof(int) * (size_t)nt);
   BALLOC(b->d_desc, sizeof(gpd::SimDesc) * nsims);
   BALLOC(b->d_consts, csz * nsims);
-  BALLOC(b->d_tsim_u, sizeof(int) * tu);
-  BALLOC(b->d_tsim_d, sizeof(int) * td);
+  BALLOC(b->d_tsim, sizeof(int) * (size_t)nt);
   BALLOC(b->d_seg0, sizeof(int) * nsims);
   BALLOC(b->d_segn, sizeof(int) * nsims);
-  BALLOC(b->ext, sizeof(long long) * (size_t)ne * tu);
+  BALLOC(b->ext, sizeof(long long) * (size_t)ne * nt);
   BALLOC(b->ext_sim, sizeof(long long) * (size_t)ne * nsims);
-  BALLOC(b->partials, sizeof(double) * (size_t)ns * tu);
+  BALLOC(b->partials, sizeof(double) * (size_t)ns * nt);
   BALLOC(b->sums_sim, sizeof(double) * (size_t)ns * nsims);
-  BALLOC(b->counters, 4 * sizeof(int));   /* dphi queue, update queue, step, pad */
+  BALLOC(b->counters, 4 * sizeof(int));
 #undef BALLOC
-  std::vector<long long> ext((size_t)ne * tu);
-  for (int t = 0; t < tu; t++) init_ext(&ext[(size_t)t * ne], N, K);
+  std::vector<long long> ext((size_t)ne * nt);
+  for (int t = 0; t < nt; t++) init_ext(&ext[(size_t)t * ne], N, K);
 #define BUP(dst, src, bytes)                                                                       \
   do {                                                                                             \
     if (cudaMemcpyAsync((dst), (src), (bytes), cudaMemcpyHostToDevice, b->stream) != cudaSuccess) { \
@@ -648,8 +614,7 @@ int gp_batch_create(gp_batch **out, int nsims, const gp_params *params, const do
   } while (0)
   BUP(b->d_desc, b->desc.data(), sizeof(gpd::SimDesc) * nsims);
   BUP(b->d_consts, consts.data(), csz * nsims);
-  BUP(b->d_tsim_u, tsim_u.data(), sizeof(int) * tu);
-  BUP(b->d_tsim_d, tsim_d.data(), sizeof(int) * td);
+  BUP(b->d_tsim, tsim.data(), sizeof(int) * (size_t)nt);
   BUP(b->d_seg0, seg0.data(), sizeof(int) * nsims);
   BUP(b->d_segn, segn.data(), sizeof(int) * nsims);
   BUP(b->ext, ext.data(), sizeof(long long) * ext.size());
@@ -661,10 +626,14 @@ int gp_batch_create(gp_batch **out, int nsims, const gp_params *params, const do
     return rc;
   }
   for (int s = 0; s < nsims; s++) {
-    if ((rc = batch_copy(b, s, phi[s], mu[s], nullptr, nullptr)) != GP_OK) {
+    if ((rc = batch_copy(b, s, phi[s], mu[s], nullptr, nullptr, cudaMemcpyHostToDevice)) != GP_OK) {
       gp_batch_destroy(b);
       return rc;
     }
+  }
+  if ((rc = batch_reflag(b, true)) != GP_OK) {
+    gp_batch_destroy(b);
+    return rc;
   }
   *out = b;
   return GP_OK;
@@ -686,316 +655,138 @@ int gp_batch_smooth(gp_batch *b, long nsteps) {
     }
     b->cur ^= 1;
   }
+  if (nsteps > 0) {
+    int rc = batch_reflag(b, true);
+    if (rc != GP_OK) return rc;
+  }
   BK(cudaStreamSynchronize(b->stream));
   return GP_OK;
 }
 
 int gp_batch_step(gp_batch *b, long nsteps, gp_stats *stats) {
   if (!b || nsteps < 0) return bfail(b, GP_EINVAL, "gp_batch_step: bad argument");
-  return batch_step_impl(b, nsteps, stats, nullptr);
+  return batch_step_impl(b, nsteps, stats, nullptr, nullptr, nullptr);
 }
 
 int gp_batch_step_timed(gp_batch *b, long nsteps, gp_stats *stats, double *total_ms) {
   if (!b || nsteps < 0) return bfail(b, GP_EINVAL, "gp_batch_step_timed: bad argument");
-  return batch_step_impl(b, nsteps, stats, total_ms);
+  return batch_step_impl(b, nsteps, stats, total_ms, nullptr, nullptr);
 }
 
 int gp_batch_get(gp_batch *b, int sim, double *phi, double *mu) {
   if (!b || sim < 0 || sim >= b->nsims || !phi || !mu) return bfail(b, GP_EINVAL, "gp_batch_get: bad argument");
-  return batch_copy(b, sim, nullptr, nullptr, phi, mu);
+  return batch_copy(b, sim, nullptr, nullptr, phi, mu, cudaMemcpyDeviceToHost);
 }
 
 int gp_batch_set(gp_batch *b, int sim, const double *phi, const double *mu) {
   if (!b || sim < 0 || sim >= b->nsims || !phi || !mu) return bfail(b, GP_EINVAL, "gp_batch_set: bad argument");
-  return batch_copy(b, sim, phi, mu, nullptr, nullptr);
+  int rc = batch_copy(b, sim, phi, mu, nullptr, nullptr, cudaMemcpyHostToDevice);
+  if (rc != GP_OK) return rc;
+  /* the other buffer still holds what its flags say */
+  rc = batch_reflag(b, false);
+  if (rc != GP_OK) return rc;
+  BK(cudaStreamSynchronize(b->stream));
+  return GP_OK;
 }
 
 int gp_batch_size(const gp_batch *b) { return b ? b->nsims : 0; }
 
 /* ======================================================================= */
-/* single-simulation API                                                   */
+/* single-simulation API: a batch of one                                   */
 /* ======================================================================= */
 
-const char *gp_version(void) { return "libgp 0.2 (sm_100a; FP64 plain step, batched FP64/FP32)"; }
+const char *gp_version(void) { return "libgp 0.3 (sm_100a; bulk/interface tile engine, FP64 and FP32)"; }
 
 size_t gp_params_size(void) { return sizeof(gp_params); }
 
 const char *gp_last_error(const gp_ctx *ctx) {
-  if (ctx && ctx->b) return ctx->b->err[0] ? ctx->b->err : ctx->err;
-  return ctx ? ctx->err : gp_host_thread_error();
+  if (!ctx) return gp_host_thread_error();
+  if (ctx->err[0]) return ctx->err;
+  return ctx->b ? ctx->b->err : "";
 }
 
-void *gp_stream(gp_ctx *ctx) {
-  if (!ctx) return nullptr;
-  return ctx->b ? (void *)ctx->b->stream : (void *)ctx->stream;
-}
+void *gp_stream(gp_ctx *ctx) { return ctx && ctx->b ? (void *)ctx->b->stream : nullptr; }
 
 void gp_destroy(gp_ctx *c) {
   if (!c) return;
-  if (c->b) gp_batch_destroy(c->b);
-  if (c->stream) cudaStreamSynchronize(c->stream);
-  cudaFree(c->phi[0]);
-  cudaFree(c->phi[1]);
-  cudaFree(c->mu[0]);
-  cudaFree(c->mu[1]);
-  cudaFree(c->dphi);
-  cudaFree(c->ext);
-  cudaFree(c->ext_red);
-  cudaFree(c->partials);
-  cudaFree(c->sums);
-  cudaFree(c->seg);
-  cudaFree(c->dconsts);
-  if (c->stream) cudaStreamDestroy(c->stream);
-  if (g_last_ctx == c) g_last_ctx = nullptr;
+  gp_batch_destroy(c->b);
   free(c);
 }
 
 int gp_init(gp_ctx **out, const gp_params *p, const double *phi, const double *mu, gp_precision prec) {
-  gp_ctx *c = nullptr;
   if (!out || !p || !phi || !mu) return fail(nullptr, GP_EINVAL, "gp_init: NULL argument");
   *out = nullptr;
   if (prec != GP_FP64 && prec != GP_FP32) return fail(nullptr, GP_EINVAL, "gp_init: unknown precision %d", (int)prec);
-  c = (gp_ctx *)calloc(1, sizeof(gp_ctx));
+  gp_ctx *c = (gp_ctx *)calloc(1, sizeof(gp_ctx));
   if (!c) return fail(nullptr, GP_ENOMEM, "gp_init: out of host memory");
-  c->p = *p;
-  c->prec = prec;
-  char err[256] = "";
-  if (gp_host_derive(p, &c->d, err, sizeof err) != GP_OK) {
-    int r = fail(nullptr, GP_EINVAL, "gp_init: %s", err);
+  const double *ph[1] = {phi}, *m[1] = {mu};
+  int r = gp_batch_create(&c->b, 1, p, ph, m, prec);
+  if (r != GP_OK) {
     free(c);
-    return r;
-  }
-  if (prec == GP_FP32) {
-    const double *ph[1] = {phi}, *m[1] = {mu};
-    int r = gp_batch_create(&c->b, 1, p, ph, m, GP_FP32);
-    if (r != GP_OK) {
-      free(c);
-      return r;
-    }
-    *out = c;
-    return GP_OK;
-  }
-  Kern k;
-  if (!pick(c->d.N, c->d.K, c->d.aniso != 0, &k)) {
-    free(c);
-    return fail(nullptr, GP_EINVAL, "gp_init: no kernel for N=%d K=%d", c->d.N, c->d.K);
-  }
-  int rc;
-  cudaError_t e = cudaGetDevice(&c->dev);
-  if (e != cudaSuccess) {
-    free(c);
-    return fail(nullptr, GP_ECUDA, "gp_init: no CUDA device: %s", cudaGetErrorString(e));
-  }
-  e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
-  if (e != cudaSuccess) {
-    free(c);
-    return fail(nullptr, GP_ECUDA, "gp_init: %s", cudaGetErrorString(e));
-  }
-  const gp_derived &d = c->d;
-  c->g = make_grid(d, 32);
-  c->consts = make_consts<double>(d);
-  const gpd::Grid &g = c->g;
-  const int ublocks = (int)(((d.my + gpd::TY - 1) / gpd::TY) * ((d.mx + gpd::TX - 1) / gpd::TX));
-  c->ublocks = ublocks;
-  const int nsum = 2 * d.N + 2 * d.K + 1, ne = 2 * (d.N + d.K);
-#define ALLOC(ptr, bytes)                                                                           \
-  do {                                                                                              \
-    if (cudaMalloc((void **)&(ptr), (bytes)) != cudaSuccess) {                                       \
-      rc = fail(c, GP_ENOMEM, "gp_init: cudaMalloc of %zu bytes failed", (size_t)(bytes));          \
-      goto bad;                                                                                     \
-    }                                                                                               \
-  } while (0)
-  ALLOC(c->phi[0], (size_t)g.plane * d.N * 8);
-  ALLOC(c->phi[1], (size_t)g.plane * d.N * 8);
-  ALLOC(c->mu[0], (size_t)g.plane * d.K * 8);
-  ALLOC(c->mu[1], (size_t)g.plane * d.K * 8);
-  ALLOC(c->dphi, (size_t)g.dplane * d.N * 8);
-  ALLOC(c->ext, sizeof(long long) * ne * (size_t)ublocks);
-  ALLOC(c->ext_red, sizeof(long long) * ne);
-  ALLOC(c->partials, sizeof(double) * (size_t)ublocks * nsum);
-  ALLOC(c->sums, sizeof(double) * nsum);
-  ALLOC(c->seg, sizeof(int) * 2);
-  ALLOC(c->dconsts, sizeof(gpd::Consts<double>));
-#undef ALLOC
-  {
-    int seg[2] = {0, ublocks};
-    std::vector<long long> ext((size_t)ne * ublocks);
-    for (int t = 0; t < ublocks; t++) init_ext(&ext[(size_t)t * ne], d.N, d.K);
-    if (cudaMemcpy(c->seg, seg, sizeof seg, cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(c->ext, ext.data(), ext.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(c->dconsts, &c->consts, sizeof(c->consts), cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemset(c->dphi, 0, (size_t)g.dplane * d.N * 8) != cudaSuccess) {
-      rc = fail(c, GP_ECUDA, "gp_init: upload failed");
-      goto bad;
-    }
-  }
-  if (cudaFuncSetAttribute(k.dphi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem_dphi) != cudaSuccess ||
-      cudaFuncSetAttribute(k.upd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem_upd) != cudaSuccess) {
-    rc = fail(c, GP_ECUDA, "gp_init: kernel attributes");
-    goto bad;
-  }
-  if ((rc = bind(c)) != GP_OK) goto bad;
-  if ((rc = upload_state(c, phi, mu, cudaMemcpyHostToDevice)) != GP_OK) goto bad;
-  if (cudaStreamSynchronize(c->stream) != cudaSuccess) {
-    rc = fail(c, GP_ECUDA, "gp_init: upload failed");
-    goto bad;
+    return r;   /* the message is in the thread's error slot */
   }
   *out = c;
   return GP_OK;
-bad:
-  gp_set_thread_error("%s", c->err);
-  gp_destroy(c);
-  return rc;
 }
 
 int gp_smooth(gp_ctx *c, long nsteps) {
   if (!c || nsteps < 0) return fail(c, GP_EINVAL, "gp_smooth: bad argument");
-  if (c->b) return gp_batch_smooth(c->b, nsteps);
-  Kern k;
-  pick(c->d.N, c->d.K, c->d.aniso != 0, &k);
-  const gpd::Grid &g = c->g;
-  for (long s = 0; s < nsteps; s++) {
-    CK(k.b.sdphi(c->stream, c->dconsts, c->phi[c->cur], c->dphi, g));
-    CK(k.b.supd(c->stream, c->dconsts, c->phi[c->cur], c->mu[c->cur], c->dphi, c->phi[c->cur ^ 1], c->mu[c->cur ^ 1], g));
-    c->cur ^= 1;
-  }
-  CK(cudaStreamSynchronize(c->stream));
-  return GP_OK;
+  c->err[0] = 0;
+  return gp_batch_smooth(c->b, nsteps);
 }
 
-static int fill_stats(gp_ctx *c, gp_stats *s) {
-  const int N = c->d.N, K = c->d.K, nsum = 2 * N + 2 * K + 1, ne = 2 * (N + K);
-  long long mm[2 * (GPK_MAXN + GPK_MAXK)];
-  double sums[2 * GPK_MAXN + 2 * GPK_MAXK + 1];
-  k_reduce_sums<<<dim3(nsum, 1), 256, 0, c->stream>>>(c->partials, c->seg, c->seg + 1, nsum, c->sums);
-  k_reduce_ext<<<dim3(ne, 1), 256, 0, c->stream>>>(c->ext, c->seg, c->seg + 1, ne, N, K, c->ext_red);
-  CK(cudaGetLastError());
-  CK(cudaMemcpyAsync(mm, c->ext_red, sizeof(long long) * ne, cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaMemcpyAsync(sums, c->sums, sizeof(double) * nsum, cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaStreamSynchronize(c->stream));
-  stats_from(&c->last, mm, sums, N, K, c->steps);
-  if (s) *s = c->last;
-  return GP_OK;
-}
-
-static int step_impl(gp_ctx *c, long nsteps, gp_stats *stats, double *total_ms, double *ms_phase,
-                     double *ms_update) {
+int gp_step(gp_ctx *c, long nsteps, gp_stats *stats) {
   if (!c || nsteps < 0) return fail(c, GP_EINVAL, "gp_step: bad argument");
-  if (c->b) {
-    if (ms_phase) *ms_phase = 0.0;
-    if (ms_update) *ms_update = 0.0;
-    return batch_step_impl(c->b, nsteps, stats, total_ms);
-  }
-  const bool timed = total_ms || ms_phase || ms_update;
-  cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
-  double t_phase = 0.0, t_update = 0.0;
-  Kern k;
-  pick(c->d.N, c->d.K, c->d.aniso != 0, &k);
-  int rc = bind(c);
-  if (rc) return rc;
-  const gpd::Grid &g = c->g;
-  dim3 gd((g.my + 2 + gpd::TY - 1) / gpd::TY, (g.mx + 2 + gpd::TX - 1) / gpd::TX);
-  dim3 gu((g.my + gpd::TY - 1) / gpd::TY, (g.mx + gpd::TX - 1) / gpd::TX);
-  if (timed) {
-    for (int i = 0; i < 3; i++) CK(cudaEventCreate(&ev[i]));
-  }
-  cudaEvent_t t_start = nullptr, t_end = nullptr;
-  if (total_ms) {
-    CK(cudaEventCreate(&t_start));
-    CK(cudaEventCreate(&t_end));
-    CK(cudaEventRecord(t_start, c->stream));
-  }
-  for (long s = 0; s < nsteps; s++) {
-    gpd::StatBufs st = {};
-    st.ext = c->ext;
-    st.partials = c->partials;
-    st.want_sums = (stats != nullptr && s == nsteps - 1);
-    if (timed) CK(cudaEventRecord(ev[0], c->stream));
-    k.dphi<<<gd, gpd::NT, k.smem_dphi, c->stream>>>(c->phi[c->cur], c->mu[c->cur], c->dphi, g);
-    if (timed) CK(cudaEventRecord(ev[1], c->stream));
-    k.upd<<<gu, gpd::NT, k.smem_upd, c->stream>>>(c->phi[c->cur], c->mu[c->cur], c->dphi, c->phi[c->cur ^ 1],
-                                                   c->mu[c->cur ^ 1], g, st);
-    if (timed) {
-      float a = 0.f, bb = 0.f;
-      CK(cudaEventRecord(ev[2], c->stream));
-      CK(cudaEventSynchronize(ev[2]));
-      CK(cudaEventElapsedTime(&a, ev[0], ev[1]));
-      CK(cudaEventElapsedTime(&bb, ev[1], ev[2]));
-      t_phase += a;
-      t_update += bb;
-    }
-    c->cur ^= 1;
-    c->steps++;
-  }
-  CK(cudaGetLastError());
-  if (total_ms) {
-    float tt = 0.f;
-    CK(cudaEventRecord(t_end, c->stream));
-    CK(cudaEventSynchronize(t_end));
-    CK(cudaEventElapsedTime(&tt, t_start, t_end));
-    *total_ms = tt;
-    cudaEventDestroy(t_start);
-    cudaEventDestroy(t_end);
-  }
-  if (timed) {
-    for (int i = 0; i < 3; i++) cudaEventDestroy(ev[i]);
-    if (ms_phase) *ms_phase = t_phase;
-    if (ms_update) *ms_update = t_update;
-  }
-  if (stats && nsteps > 0) return fill_stats(c, stats);
-  CK(cudaStreamSynchronize(c->stream));
-  return GP_OK;
+  c->err[0] = 0;
+  return batch_step_impl(c->b, nsteps, stats, nullptr, nullptr, nullptr);
 }
 
-int gp_step(gp_ctx *c, long nsteps, gp_stats *stats) { return step_impl(c, nsteps, stats, nullptr, nullptr, nullptr); }
-
-int gp_step_timed(gp_ctx *c, long nsteps, gp_stats *stats, double *total_ms, double *ms_phase, double *ms_update) {
-  return step_impl(c, nsteps, stats, total_ms, ms_phase, ms_update);
+int gp_step_timed(gp_ctx *c, long nsteps, gp_stats *stats, double *total_ms, double *ms_bulk, double *ms_iface) {
+  if (!c || nsteps < 0) return fail(c, GP_EINVAL, "gp_step_timed: bad argument");
+  c->err[0] = 0;
+  return batch_step_impl(c->b, nsteps, stats, total_ms, ms_bulk, ms_iface);
 }
 
 int gp_get_stats(gp_ctx *c, gp_stats *s) {
   if (!c || !s) return fail(c, GP_EINVAL, "gp_get_stats: bad argument");
-  *s = c->b ? c->b->last[0] : c->last;
+  *s = c->b->last[0];
   return GP_OK;
 }
 
 int gp_get(gp_ctx *c, double *phi, double *mu) {
   if (!c || !phi || !mu) return fail(c, GP_EINVAL, "gp_get: NULL argument");
-  if (c->b) return gp_batch_get(c->b, 0, phi, mu);
-  int rc = download_state(c, phi, mu, cudaMemcpyDeviceToHost);
-  if (rc) return rc;
-  CK(cudaStreamSynchronize(c->stream));
-  return GP_OK;
+  c->err[0] = 0;
+  return gp_batch_get(c->b, 0, phi, mu);
 }
 
 int gp_set(gp_ctx *c, const double *phi, const double *mu) {
   if (!c || !phi || !mu) return fail(c, GP_EINVAL, "gp_set: NULL argument");
-  if (c->b) return gp_batch_set(c->b, 0, phi, mu);
-  int rc = upload_state(c, phi, mu, cudaMemcpyHostToDevice);
-  if (rc) return rc;
-  CK(cudaStreamSynchronize(c->stream));
-  return GP_OK;
+  c->err[0] = 0;
+  return gp_batch_set(c->b, 0, phi, mu);
 }
 
 int gp_get_dev(gp_ctx *c, double *phi, double *mu) {
   if (!c || !phi || !mu) return fail(c, GP_EINVAL, "gp_get_dev: NULL argument");
-  if (c->b) return fail(c, GP_EUNSUPPORTED, "gp_get_dev: FP32 contexts exchange host buffers only");
-  int rc = download_state(c, phi, mu, cudaMemcpyDeviceToDevice);
-  if (rc) return rc;
-  CK(cudaStreamSynchronize(c->stream));
-  return GP_OK;
+  if (c->b->elem != 8) return fail(c, GP_EUNSUPPORTED, "gp_get_dev: FP32 contexts exchange host buffers only");
+  c->err[0] = 0;
+  return batch_copy(c->b, 0, nullptr, nullptr, phi, mu, cudaMemcpyDeviceToDevice);
 }
 
 int gp_set_dev(gp_ctx *c, const double *phi, const double *mu) {
   if (!c || !phi || !mu) return fail(c, GP_EINVAL, "gp_set_dev: NULL argument");
-  if (c->b) return fail(c, GP_EUNSUPPORTED, "gp_set_dev: FP32 contexts exchange host buffers only");
-  int rc = upload_state(c, phi, mu, cudaMemcpyDeviceToDevice);
-  if (rc) return rc;
-  CK(cudaStreamSynchronize(c->stream));
+  if (c->b->elem != 8) return fail(c, GP_EUNSUPPORTED, "gp_set_dev: FP32 contexts exchange host buffers only");
+  c->err[0] = 0;
+  gp_batch *b = c->b;
+  int rc = batch_copy(b, 0, phi, mu, nullptr, nullptr, cudaMemcpyDeviceToDevice);
+  if (rc != GP_OK) return rc;
+  rc = batch_reflag(b, false);
+  if (rc != GP_OK) return rc;
+  BK(cudaStreamSynchronize(b->stream));
   return GP_OK;
 }
 
 }  /* extern "C" */
+
 
 /* ======================================================================= */
 /* One time step without any allocation (gp_step_noalloc in gp.h).          */
@@ -1055,8 +846,6 @@ extern "C" int gp_step_noalloc(const gp_params *p, const double *phi_in, const d
   cudaStream_t s = (cudaStream_t)stream;
   CK(cudaFuncSetAttribute(k.dphi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem_dphi));
   CK(cudaFuncSetAttribute(k.upd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem_upd));
-  /* the constant block is shared with the contexts: make them upload theirs again */
-  g_last_ctx = nullptr;
   CK(cudaMemcpyToSymbolAsync(cD, &cs, sizeof(cs), 0, cudaMemcpyHostToDevice, s));
   /* the previous call's extremes are still in the array: start them from zero */
   CK(cudaMemsetAsync(scratch, 0, head * sizeof(double), s));

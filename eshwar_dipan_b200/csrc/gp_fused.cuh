@@ -1,0 +1,760 @@
+/*
+ * gp_fused.cuh -- the time step as two kernels over classified tiles.
+ *
+ * Every TX x TY tile of every simulation carries a phase flag per state
+ * buffer: p >= 0 when each of its cells holds exactly the one-hot phi of phase
+ * p (bits of 1.0 and +0.0), -1 otherwise, -2 when not known.  A tile whose own
+ * flag and the flags of every tile its two-cell phi halo reaches (through the
+ * boundary copy tables) are the same p >= 0 is a bulk tile: no phase is
+ * active anywhere on its delta-phi ring (every Laplacian is 0.0), so delta-phi
+ * is +0.0 there, no anti-trapping current flows, every cell takes the bulk
+ * branch of the mu update with the pure-phase D, and phi stays as it is
+ * (calculate_divergence_phasefield.h:19-22, calculate_fluxes_concentration.h:64,
+ * calculate_divergence_concentration.h:43-57).
+ *
+ *  kf_bulk     one CTA per tile.  Classifies the tile; bulk tiles read and
+ *              write mu only (phi is rewritten only when the output buffer does
+ *              not already hold the same one-hot tile); other tiles are put on
+ *              the interface list.
+ *  kf_general  persistent CTAs over the interface list.  Stages phi with a
+ *              two-cell halo and mu with one, computes delta-phi on the tile
+ *              plus its one-cell ring in shared memory (the ring is recomputed
+ *              by each neighbour instead of going through HBM), then the mu
+ *              update and the phi commit, and the tile's new flag.
+ *
+ * The arithmetic of each cell is the reference's, in its order (FP64 results
+ * are bit-identical to the reference step); the FP32 form differs only where
+ * gp_tiles.cuh says.
+ */
+#pragma once
+#include <climits>
+
+#include "gp_tiles.cuh"
+
+namespace gpd {
+
+constexpr int W2 = TY + 4, H2 = TX + 4, S2 = W2 * H2;   /* phi with a two-cell halo */
+constexpr int RXF = (TX + 3) * (TY + 2);                 /* x-faces around the ring cells */
+constexpr int RYF = (TX + 2) * (TY + 3);                 /* y-faces around the ring cells */
+#define L2I(i, j) ((i) * W2 + (j))
+
+constexpr signed char FLAG_MIXED = -1, FLAG_UNKNOWN = -2;
+
+struct RemapTab2 {
+  int row[H2], col[W2];
+};
+
+/* rows/columns of the two-cell phi halo (origin x0-2, y0-2) after the remap;
+ * -1 outside [-2, m+1] (not needed by any delta-phi ring cell). */
+template <typename R>
+__device__ __forceinline__ void remap_tab2(RemapTab2 &t, const Consts<R> &D, const Grid &g, int x0, int y0) {
+  const int u = threadIdx.x;
+  if (u < H2) {
+    const int x = x0 - 2 + u;
+    t.row[u] = (x >= -2 && x <= g.mx + 1) ? remap(x, g.mx, D.bc_x[0][0], D.bc_x[0][1]) * g.pitch : -1;
+  } else if (u < H2 + W2) {
+    const int y = y0 - 2 + (u - H2);
+    t.col[u - H2] = (y >= -2 && y <= g.my + 1) ? remap(y, g.my, D.bc_y[0][0], D.bc_y[0][1]) : -1;
+  }
+}
+
+/* one-hot test on exact bits: phase index, or -1 */
+template <typename R, int N>
+__device__ __forceinline__ int one_hot(const R *ph) {
+  int p = -1, ones = 0, zeros = 0;
+#pragma unroll
+  for (int a = 0; a < N; a++) {
+    if (sizeof(R) == 8) {
+      const long long b = __double_as_longlong((double)ph[a]);
+      if (b == 0x3ff0000000000000LL) { p = a; ones++; }
+      else if (b == 0) zeros++;
+    } else {
+      const unsigned b = __float_as_uint((float)ph[a]);
+      if (b == 0x3f800000u) { p = a; ones++; }
+      else if (b == 0u) zeros++;
+    }
+  }
+  return (ones == 1 && zeros == N - 1) ? p : -1;
+}
+
+/* Flag of a tile from its new phi, one value per thread (valid cells only):
+ * the same phase everywhere or FLAG_MIXED.  Call with all threads. */
+__device__ __forceinline__ signed char tile_flag(bool valid, int p) {
+  __shared__ int s_p[NT / 32], s_bad[NT / 32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  /* a valid cell with p < 0 spoils the tile; valid cells must agree */
+  int mine = valid ? p : INT_MAX;
+  int lo = mine, hi = valid ? p : INT_MIN;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+    hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+  }
+  if (lane == 0) { s_p[wid] = lo; s_bad[wid] = hi; }
+  __syncthreads();
+  int l2 = INT_MAX, h2 = INT_MIN;
+#pragma unroll
+  for (int w = 0; w < NT / 32; w++) { l2 = min(l2, s_p[w]); h2 = max(h2, s_bad[w]); }
+  __syncthreads();
+  return (l2 >= 0 && l2 == h2) ? (signed char)l2 : FLAG_MIXED;
+}
+
+/* Bulk test of tile (tile rows by, columns bx) of a simulation: its flag and
+ * the flags of the tiles holding every cell of its two-cell phi halo agree on
+ * a phase.  Evaluated by one warp; returns the phase or -1. */
+template <typename R>
+__device__ __forceinline__ int bulk_phase(const Consts<R> &D, const Grid &g, const signed char *__restrict__ flags,
+                                          int tile0, int tiles_x, int by, int bx) {
+  const int lane = threadIdx.x & 31;
+  const int x0 = by * TX, y0 = bx * TY;
+  const int xl = min(x0 + TX, g.mx) - 1, yl = min(y0 + TY, g.my) - 1;
+  /* candidate tile rows: own, and the tiles of rows x0-2, x0-1, xl+1, xl+2 */
+  int rows[5], cols[5];
+  {
+    const int xs[4] = {x0 - 2, x0 - 1, xl + 1, xl + 2};
+    const int ys[4] = {y0 - 2, y0 - 1, yl + 1, yl + 2};
+    rows[0] = by;
+    cols[0] = bx;
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      int x = xs[q], y = ys[q];
+      if (x < 0 || x >= g.mx) x = remap(x, g.mx, D.bc_x[0][0], D.bc_x[0][1]);
+      if (y < 0 || y >= g.my) y = remap(y, g.my, D.bc_y[0][0], D.bc_y[0][1]);
+      rows[q + 1] = x / TX;
+      cols[q + 1] = y / TY;
+    }
+  }
+  int f = 0x7f;
+  if (lane < 25) {
+    const int r = lane / 5, c = lane - r * 5;
+    f = flags[tile0 + rows[r] * tiles_x + cols[c]];
+  }
+  const int own = __shfl_sync(0xffffffffu, f, 0);
+  const bool ok = lane >= 25 || f == own;
+  return (__all_sync(0xffffffffu, ok) && own >= 0) ? own : -1;
+}
+
+
+/* ------------------------------------------------------------------ */
+/* interface tiles                                                     */
+/* ------------------------------------------------------------------ */
+
+template <typename R, int N, int K>
+struct GenSmem {
+  R P[N][S2];              /* phi, two-cell halo, origin (x0-2, y0-2) */
+  R M[K][SS];              /* mu, one-cell halo, origin (x0-1, y0-1)  */
+  R DP[N][SS];             /* delta-phi of the ring region (same origin as M) */
+  unsigned char ACT[SS];   /* active phases of each ring cell (bit a) */
+  union {
+    R T[NP<N>::v][4][RXF + RYF];   /* anisotropy face terms of the ring region */
+    struct {
+      R CM[N][K][SS];      /* c_a,k(mu) per cell */
+      R H[N][SS];          /* h_a(phi) per cell */
+      R SP[N][SS];         /* s_phi of the obstacle anti-trapping (solid phases) */
+      R DD[K][K][SS];      /* D_kl per cell */
+      R JX[K][NXF], JY[K][NYF];
+      R FX[K][K][NXF], FY[K][K][NYF];
+    } u;
+  } w;
+  RemapTab2 rtp;
+  RemapTab rtm;
+};
+
+/* Anisotropy terms of one face of the ring region for all pairs: the same
+ * arithmetic as face_terms (function_A_01.h:163-215 through functionQ.h and
+ * anisotropy_01.h) on the two-cell-halo layout.  xface: face between P rows
+ * i and i+1 at column j; else between columns j and j+1 of row i. */
+template <typename R, int N>
+__device__ __forceinline__ void ring_face_terms(const Consts<R> &D, const R (*P)[S2], R (*T)[4][RXF + RYF],
+                                                bool xface, int i, int j, int fidx) {
+  R s[N], gr[N], c0[N], c1[N];
+#pragma unroll
+  for (int a = 0; a < N; a++) {
+    const R *S = P[a];
+    if (xface) {
+      R p0 = S[L2I(i, j)], p1 = S[L2I(i + 1, j)];
+      s[a] = R(0.5) * (p1 + p0);
+      gr[a] = divx(p1 - p0, D);
+      c0[a] = div2y(S[L2I(i, j + 1)] - S[L2I(i, j - 1)], D);
+      c1[a] = div2y(S[L2I(i + 1, j + 1)] - S[L2I(i + 1, j - 1)], D);
+    } else {
+      R p0 = S[L2I(i, j)], p1 = S[L2I(i, j + 1)];
+      s[a] = R(0.5) * (p1 + p0);
+      gr[a] = divy(p1 - p0, D);
+      c0[a] = R(0.5) * (divx(S[L2I(i + 1, j)] - S[L2I(i, j)], D) + divx(S[L2I(i, j)] - S[L2I(i - 1, j)], D));
+      c1[a] = R(0.5) * (divx(S[L2I(i + 1, j + 1)] - S[L2I(i, j + 1)], D) +
+                        divx(S[L2I(i, j + 1)] - S[L2I(i - 1, j + 1)], D));
+    }
+  }
+#pragma unroll
+  for (int a = 0; a < N; a++)
+#pragma unroll
+    for (int b = a + 1; b < N; b++) {
+      const int p = pidx<N>(a, b);
+      R Pab = s[a] * gr[b] - s[b] * gr[a];
+      R Pba = s[b] * gr[a] - s[a] * gr[b];
+      R tq = R(0.5) * (s[a] * (c0[b] + c1[b]) - s[b] * (c0[a] + c1[a]));
+      R q0, q1;
+      if (xface) rot2(D, D.rot[a][b], Pab, tq, q0, q1);
+      else rot2(D, D.rot[a][b], tq, Pab, q0, q1);
+      R acv = ac(q0, q1, D.dab[a][b]);
+      QPow<R> qp = qpow(q0, q1);
+      R rd;
+      if (D.rot_identity) {
+        rd = (xface ? dadq_c(q0, qp, D.dab16[a][b]) : dadq_c(q1, qp, D.dab16[a][b])) + R(0.0);
+      } else {
+        R d0 = dadq_c(q0, qp, D.dab16[a][b]), d1 = dadq_c(q1, qp, D.dab16[a][b]);
+        R r0, r1;
+        rot2(D, D.rinv[a][b], d0, d1, r0, r1);
+        rd = xface ? r0 : r1;
+      }
+      R ac2 = acv * acv, acq = acv * qp.q2;
+      T[p][0][fidx] = ac2 * Pab * (-s[b]);
+      T[p][1][fidx] = ac2 * Pba * (-s[a]);
+      T[p][2][fidx] = acq * rd * (-s[b]);
+      T[p][3][fidx] = acq * (R(0.0) - rd) * (-s[a]);
+    }
+}
+
+/* delta-phi of one ring cell (ring coordinates ri, rj; its phi at P row ri+1,
+ * column rj+1) from the staged tile: calculate_divergence_phasefield_2D
+ * (calculate_divergence_phasefield.h:4-62) in the same arithmetic as dphi_tile. */
+template <typename R, int N, int K, bool ANISO>
+__device__ __forceinline__ void ring_dphi(const Consts<R> &D, const GenSmem<R, N, K> &sm, int ri, int rj,
+                                          unsigned mask, R *d) {
+  const int i = ri + 1, j = rj + 1, e = LI(ri, rj);
+  R ph[N];
+  bool act[N];
+#pragma unroll
+  for (int a = 0; a < N; a++) {
+    ph[a] = sm.P[a][L2I(i, j)];
+    act[a] = (mask >> a) & 1u;
+  }
+  if (!mask) {
+#pragma unroll
+    for (int a = 0; a < N; a++) {
+      d[a] = R(0.0);
+      if ((ph[a] + d[a]) < R(0.0)) d[a] += fabs(d[a] + ph[a]);
+    }
+    return;
+  }
+  R m[K];
+#pragma unroll
+  for (int k = 0; k < K; k++) m[k] = sm.M[k][e];
+  R gcx[N], gcy[N];
+#pragma unroll
+  for (int a = 0; a < N; a++) {
+    const R *S = sm.P[a];
+    gcx[a] = R(0.5) * (divx(S[L2I(i + 1, j)] - S[L2I(i, j)], D) + divx(S[L2I(i, j)] - S[L2I(i - 1, j)], D));
+    gcy[a] = div2y(S[L2I(i, j + 1)] - S[L2I(i, j - 1)], D);
+  }
+  R psi[N];
+#pragma unroll
+  for (int b = 0; b < N; b++) {
+    R c[K], ps = R(0.0);
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      c[k] = c_mu<R, K>(D, m, b, k);
+      ps -= m[k] * c[k];
+    }
+    ps += fe<R, K>(D, c, b);
+    psi[b] = ps;
+  }
+  R cq0[NP<N>::v], cq1[NP<N>::v], cd0[NP<N>::v], cd1[NP<N>::v], cac[NP<N>::v], cq2[NP<N>::v];
+  if (ANISO) {
+#pragma unroll
+    for (int a = 0; a < N; a++)
+#pragma unroll
+      for (int b = a + 1; b < N; b++) {
+        const int p = pidx<N>(a, b);
+        R q0, q1;
+        rot2(D, D.rot[a][b], (ph[a] * gcx[b] - ph[b] * gcx[a]), (ph[a] * gcy[b] - ph[b] * gcy[a]), q0, q1);
+        QPow<R> qp = qpow(q0, q1);
+        cq0[p] = q0;
+        cq1[p] = q1;
+        cd0[p] = dadq_c(q0, qp, D.dab16[a][b]);
+        cd1[p] = dadq_c(q1, qp, D.dab16[a][b]);
+        cq2[p] = (q0 * q0 + q1 * q1 + R(0.0) * R(0.0));
+        cac[p] = ac(q0, q1, D.dab[a][b]);
+      }
+  }
+  const R tau = tau_of<R, N>(D, ph);
+  R lam[N], sl = R(0.0);
+  long nact = 0;
+  /* face indices of this cell in the ring face cache */
+  const int xf = i * (TY + 2) + (j - 1), xb = (i - 1) * (TY + 2) + (j - 1);
+  const int yr = RXF + (i - 1) * (TY + 3) + j, yl = RXF + (i - 1) * (TY + 3) + (j - 1);
+#pragma unroll
+  for (int a = 0; a < N; a++) {
+    if (!act[a]) continue;
+    R dA, div;
+    if (ANISO) {
+      R s1 = R(0.0), s2 = R(0.0), t1 = R(0.0), t2 = R(0.0);
+#pragma unroll
+      for (int b = 0; b < N; b++) {
+        if (b == a) continue;
+        const int p = a < b ? pidx<N>(a, b) : pidx<N>(b, a);
+        const R sg = R(0.0);
+        R q0 = a < b ? cq0[p] : sg - cq0[p], q1 = a < b ? cq1[p] : sg - cq1[p];
+        R d0 = a < b ? cd0[p] : sg - cd0[p], d1 = a < b ? cd1[p] : sg - cd1[p];
+        R w0, w1;
+        rot2(D, D.rot[a][b], gcx[b], gcy[b], w0, w1);
+        R sp1 = R(0.0), sp2 = R(0.0);
+        sp1 += q0 * w0;
+        sp1 += q1 * w1;
+        sp2 += (d0) * w0;
+        sp2 += (d1) * w1;
+        sp1 *= D.gamma[a][b] * (cac[p] * cac[p]);
+        sp2 *= D.gamma[a][b] * cac[p] * cq2[p];
+        s1 += sp1;
+        s2 += sp2;
+        const int o = a < b ? 0 : 1;
+        const R(*T)[RXF + RYF] = sm.w.T[p];
+        R d1v = divx((T[o][xf]) - (T[o][xb]), D);
+        d1v += divy((T[o][yr]) - (T[o][yl]), D);
+        d1v *= D.gamma[a][b];
+        t1 += d1v;
+        R d2v = divx(T[2 + o][xf] - T[2 + o][xb], D);
+        d2v += divy(T[2 + o][yr] - T[2 + o][yl], D);
+        d2v *= D.gamma[a][b];
+        t2 += d2v;
+      }
+      dA = R(2.0) * (s1 + s2);
+      div = (R(2.0) * (t1 + t2) + R(0.0));
+    } else {
+      R s = R(0.0), t = R(0.0);
+      const R *Sa = sm.P[a];
+#pragma unroll
+      for (int b = 0; b < N; b++) {
+        if (b == a) continue;
+        const R *Sb = sm.P[b];
+        R sp = R(0.0);
+        sp += (ph[a] * gcx[b] - ph[b] * gcx[a]) * gcx[b];
+        sp += (ph[a] * gcy[b] - ph[b] * gcy[a]) * gcy[b];
+        sp *= D.gamma[a][b];
+        s += sp;
+        R pa = Sa[L2I(i, j)], pb = Sb[L2I(i, j)];
+        R sxa = R(0.5) * (Sa[L2I(i + 1, j)] + pa), sxb = R(0.5) * (Sb[L2I(i + 1, j)] + pb);
+        R gxa = divx(Sa[L2I(i + 1, j)] - pa, D), gxb = divx(Sb[L2I(i + 1, j)] - pb, D);
+        R bxa = R(0.5) * (pa + Sa[L2I(i - 1, j)]), bxb = R(0.5) * (pb + Sb[L2I(i - 1, j)]);
+        R hxa = divx(pa - Sa[L2I(i - 1, j)], D), hxb = divx(pb - Sb[L2I(i - 1, j)], D);
+        R sya = R(0.5) * (Sa[L2I(i, j + 1)] + pa), syb = R(0.5) * (Sb[L2I(i, j + 1)] + pb);
+        R gya = divy(Sa[L2I(i, j + 1)] - pa, D), gyb = divy(Sb[L2I(i, j + 1)] - pb, D);
+        R lya = R(0.5) * (pa + Sa[L2I(i, j - 1)]), lyb = R(0.5) * (pb + Sb[L2I(i, j - 1)]);
+        R hya = divy(pa - Sa[L2I(i, j - 1)], D), hyb = divy(pb - Sb[L2I(i, j - 1)], D);
+        R dvg = divx((sxa * gxb - sxb * gxa) * (-sxb) - ((bxa * hxb - bxb * hxa) * (-bxb)), D);
+        dvg += divy((sya * gyb - syb * gya) * (-syb) - ((lya * hyb - lyb * hya) * (-lyb)), D);
+        dvg *= D.gamma[a][b];
+        t += dvg;
+      }
+      dA = R(2.0) * s;
+      div = R(2.0) * t;
+    }
+    R dpsi = R(0.0);
+#pragma unroll
+    for (int b = 0; b < N; b++) dpsi += psi[b] * dh<R, N>(ph, b, a);
+    lam[a] = D.eps * (-dA + div) - D.inv_eps * dwdphi<R, N>(D, ph, act, a, false) - dpsi;
+    sl += lam[a];
+    nact++;
+  }
+  if (nact) sl /= (R)nact;
+#pragma unroll
+  for (int a = 0; a < N; a++) d[a] = act[a] ? D.dt * (lam[a] - sl) / (tau * D.eps) : R(0.0);
+  project<R, N>(ph, act, d);
+}
+
+/* One interface tile (cells (x0+tx, y0+ty)): delta-phi on the tile and its
+ * ring, then the concentration pass (calculate_fluxes_concentration_2D +
+ * calculate_divergence_concentration_2D, calculate_fluxes_concentration.h:4-145,
+ * calculate_divergence_concentration.h:4-153) and the phi commit, in the
+ * arithmetic of update_tile's general path.  Returns the tile's new flag
+ * (valid in thread 0). */
+template <typename R, int N, int K, bool ANISO>
+__device__ __forceinline__ signed char general_tile(const Consts<R> &D, const Grid &g, const R *__restrict__ phi,
+                                                    const R *__restrict__ mu, R *__restrict__ phin,
+                                                    R *__restrict__ mun, int x0, int y0, const StatBufs &st,
+                                                    long long slot, GenSmem<R, N, K> &sm) {
+  constexpr int L = N - 1;
+  const R cst = D.obstacle ? D.jat_obst : D.jat_well;
+
+  /* ---- stage phi (two-cell halo) and mu (one-cell halo) through the copy tables */
+  remap_tab2(sm.rtp, D, g, x0, y0);
+  remap_tab(sm.rtm, D, g, x0, y0, 1, -1, g.mx, -1, g.my);
+  __syncthreads();
+  for (int e = threadIdx.x; e < S2; e += NT) {
+    const int i = e / W2, j = e - i * W2;
+    const int r = sm.rtp.row[i], c = sm.rtp.col[j];
+    if (r >= 0 && c >= 0) {
+      const R *src = phi + (r + c);
+#pragma unroll
+      for (int a = 0; a < N; a++) sm.P[a][e] = __ldg(src + a * g.plane);
+    } else {
+#pragma unroll
+      for (int a = 0; a < N; a++) sm.P[a][e] = R(0.0);
+    }
+  }
+  for (int e = threadIdx.x; e < SS; e += NT) {
+    const int i = e / SW, j = e - i * SW;
+    const int r = sm.rtm.row[i], c = sm.rtm.col[j];
+    if (r >= 0 && c >= 0) {
+      const R *src = mu + (r + c);
+#pragma unroll
+      for (int k = 0; k < K; k++) sm.M[k][e] = __ldg(src + k * g.plane);
+    } else {
+#pragma unroll
+      for (int k = 0; k < K; k++) sm.M[k][e] = R(0.0);
+    }
+  }
+  __syncthreads();
+
+  /* ---- active phases of the ring cells (interior plus ring: x <= mx, y <= my) */
+  bool any = false;
+  for (int e = threadIdx.x; e < SS; e += NT) {
+    const int ri = e / SW, rj = e - ri * SW, i = ri + 1, j = rj + 1;
+    const bool vd = (x0 - 1 + ri <= g.mx) && (y0 - 1 + rj <= g.my);
+    unsigned mask = 0;
+#pragma unroll
+    for (int a = 0; a < N; a++) {
+      const R *S = sm.P[a];
+      R gxf = divx(S[L2I(i + 1, j)] - S[L2I(i, j)], D), gxb = divx(S[L2I(i, j)] - S[L2I(i - 1, j)], D);
+      R gyr = divy(S[L2I(i, j + 1)] - S[L2I(i, j)], D), gyl = divy(S[L2I(i, j)] - S[L2I(i, j - 1)], D);
+      R dv = divx(gxf - gxb, D);
+      dv += divy(gyr - gyl, D);
+      if (fabs(dv) > R(0.0)) mask |= 1u << a;
+    }
+    if (!vd) mask = 0;
+    sm.ACT[e] = (unsigned char)mask;
+    any |= mask != 0;
+  }
+  const bool blockact = __syncthreads_or(any);
+  if (ANISO && blockact) {
+    for (int e = threadIdx.x; e < RXF + RYF; e += NT) {
+      if (e < RXF) {
+        const int fi = e / (TY + 2), fj = e - fi * (TY + 2) + 1;
+        ring_face_terms<R, N>(D, sm.P, sm.w.T, true, fi, fj, e);
+      } else {
+        const int f = e - RXF, fi = f / (TY + 3) + 1, fj = f - (fi - 1) * (TY + 3);
+        ring_face_terms<R, N>(D, sm.P, sm.w.T, false, fi, fj, e);
+      }
+    }
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < SS; e += NT) {
+    const int ri = e / SW, rj = e - ri * SW;
+    const bool vd = (x0 - 1 + ri <= g.mx) && (y0 - 1 + rj <= g.my);
+    R d[N];
+    if (vd) {
+      ring_dphi<R, N, K, ANISO>(D, sm, ri, rj, sm.ACT[e], d);
+    } else {
+#pragma unroll
+      for (int a = 0; a < N; a++) d[a] = R(0.0);
+    }
+#pragma unroll
+    for (int a = 0; a < N; a++) sm.DP[a][e] = d[a];
+  }
+  __syncthreads();   /* the face-term cache is dead from here: its space holds the update's arrays */
+
+#define PR(a, e) sm.P[a][L2I((e) / SW + 1, (e) % SW + 1)]
+  /* ---- per-cell quantities of the ring region */
+  for (int e = threadIdx.x; e < SS; e += NT) {
+    R p[N], mm[K];
+#pragma unroll
+    for (int a = 0; a < N; a++) p[a] = PR(a, e);
+#pragma unroll
+    for (int k = 0; k < K; k++) mm[k] = sm.M[k][e];
+#pragma unroll
+    for (int a = 0; a < N; a++) {
+      R hv = h<R, N>(p, a);
+      sm.w.u.H[a][e] = hv;
+#pragma unroll
+      for (int k = 0; k < K; k++) sm.w.u.CM[a][k][e] = c_mu<R, K>(D, mm, a, k);
+      if (a < L)
+        sm.w.u.SP[a][e] =
+            (p[a] * (R(1.0) - p[a]) > R(0.0)) ? p[a] * (R(1.0) - hv) / (sqrt(p[a] * (R(1.0) - p[a]))) : R(0.0);
+    }
+#pragma unroll
+    for (int k = 0; k < K; k++)
+#pragma unroll
+      for (int l = 0; l < K; l++) sm.w.u.DD[k][l][e] = Dcell<R, N, K>(D, p, k, l);
+  }
+  __syncthreads();
+
+#define PRIJ(a, i, j) sm.P[a][L2I((i) + 1, (j) + 1)]
+  /* ---- faces of the tile: anti-trapping current and diffusion flux products */
+  for (int e = threadIdx.x; e < NXF + NYF; e += NT) {
+    const bool xface = e < NXF;
+    int fi, fj, i1, j1, fidx;
+    if (xface) { fi = e / TY; fj = e - fi * TY + 1; i1 = fi + 1; j1 = fj; fidx = e; }
+    else { int f = e - NXF; fi = f / (TY + 1) + 1; fj = f - (fi - 1) * (TY + 1); i1 = fi; j1 = fj + 1; fidx = f; }
+    const int c0 = LI(fi, fj), c1 = LI(i1, j1);
+    R gr[N], cn[N];
+#pragma unroll
+    for (int a = 0; a < N; a++) {
+      if (xface) {
+        gr[a] = divx(PRIJ(a, i1, j1) - PRIJ(a, fi, fj), D);
+        cn[a] = R(0.5) * (div2y(PRIJ(a, fi, fj + 1) - PRIJ(a, fi, fj - 1), D) +
+                          div2y(PRIJ(a, i1, fj + 1) - PRIJ(a, i1, fj - 1), D));
+      } else {
+        gr[a] = divy(PRIJ(a, i1, j1) - PRIJ(a, fi, fj), D);
+        R gc0 = R(0.5) * (divx(PRIJ(a, fi + 1, fj) - PRIJ(a, fi, fj), D) + divx(PRIJ(a, fi, fj) - PRIJ(a, fi - 1, fj), D));
+        R gc1 = R(0.5) * (divx(PRIJ(a, fi + 1, j1) - PRIJ(a, i1, j1), D) + divx(PRIJ(a, i1, j1) - PRIJ(a, fi - 1, j1), D));
+        cn[a] = R(0.5) * (gc0 + gc1);
+      }
+    }
+    R jat[K];
+#pragma unroll
+    for (int k = 0; k < K; k++) jat[k] = R(0.0);
+    /* calculate_fluxes_concentration.h:65: no y-current where gidy is 0 or MESH_Y-2 */
+    const bool yskip = !xface && ((y0 - 1 + fj) + 3 == g.my - 2);
+    R nl = R(-1.0);
+#pragma unroll
+    for (int a = 0; a < L; a++) {
+      const R s2 = cn[a] * cn[a] + gr[a] * gr[a];
+      if (s2 != R(0.0) && !yskip) {
+        const R ng = sqrt(s2);
+        if (nl < R(0.0)) nl = sqrt(cn[L] * cn[L] + gr[L] * gr[L]);
+        R sp = gr[a] * gr[L];
+        sp += cn[a] * cn[L];
+        if (nl > R(0.0)) sp /= (nl * ng);
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+          R cl1 = sm.w.u.CM[L][k][c1], cl0 = sm.w.u.CM[L][k][c0];
+          R cs1 = sm.w.u.CM[a][k][c1], cs0 = sm.w.u.CM[a][k][c0];
+          R bracket;
+          if (D.obstacle)
+            bracket = sm.w.u.SP[a][c1] * (cl1 - cs1) * sm.DP[a][c1] + sm.w.u.SP[a][c0] * (cl0 - cs0) * sm.DP[a][c0];
+          else
+            bracket = (cl1 - cs1) * sm.DP[a][c1] + (cl0 - cs0) * sm.DP[a][c0];
+          jat[k] += D.atf[a][k] * fabs(sp) * (D.obstacle ? R(0.5) : D.well_half) * bracket * gr[a] / ng;
+        }
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      if (xface) sm.w.u.JX[k][fidx] = jat[k];
+      else sm.w.u.JY[k][fidx] = jat[k];
+#pragma unroll
+      for (int l = 0; l < K; l++) {
+        R dm = (sm.w.u.DD[k][l][c1] + sm.w.u.DD[k][l][c0]) * R(0.5);
+        R gm = xface ? divx(sm.M[l][c1] - sm.M[l][c0], D) : divy(sm.M[l][c1] - sm.M[l][c0], D);
+        if (xface) sm.w.u.FX[k][l][fidx] = dm * gm;
+        else sm.w.u.FY[k][l][fidx] = dm * gm;
+      }
+    }
+  }
+  __syncthreads();
+
+  /* ---- per cell: mu update, phi commit */
+  const int tx = threadIdx.x / TY, ty = threadIdx.x - (threadIdx.x / TY) * TY;
+  const int x = x0 + tx, y = y0 + ty, i = tx + 1, j = ty + 1, c = LI(i, j);
+  const bool valid = (x < g.mx) && (y < g.my);
+  R ph[N], dp[N], m[K], nph[N], nm[K];
+  double dmu[K];
+  int oh = -1;
+  if (valid) {
+#pragma unroll
+    for (int a = 0; a < N; a++) { ph[a] = PRIJ(a, i, j); dp[a] = sm.DP[a][c]; }
+#pragma unroll
+    for (int k = 0; k < K; k++) m[k] = sm.M[k][c];
+    commit_cell<R, N, K>(D, sm.w.u.FX, sm.w.u.FY, sm.w.u.JX, sm.w.u.JY, sm.w.u.CM, sm.w.u.H, i, j, x, y, ph, dp, m,
+                         nph, nm, dmu, st);
+    const long long o = (long long)x * g.pitch + y;
+#pragma unroll
+    for (int a = 0; a < N; a++) phin[a * g.plane + o] = nph[a];
+#pragma unroll
+    for (int k = 0; k < K; k++) mun[k * g.plane + o] = nm[k];
+    oh = one_hot<R, N>(nph);
+  }
+#undef PRIJ
+#undef PR
+  block_stats<R, N, K>(D, valid, nph, nm, dp, dmu, st, slot);
+  return tile_flag(valid, oh);
+}
+
+/* ------------------------------------------------------------------ */
+/* kernels                                                             */
+/* ------------------------------------------------------------------ */
+
+/* Work-list counters of a batch: [0] interface tiles listed by kf_bulk,
+ * [1] next list entry to take, [2] kf_general CTAs finished, [3] step number
+ * (keys the FP32 rounding stream).  kf_general's last CTA resets [0..2] and
+ * advances [3], so a step is exactly these two launches. */
+enum { CTR_LIST = 0, CTR_HEAD = 1, CTR_DONE = 2, CTR_STEP = 3 };
+
+/* One CTA per tile of every simulation: bulk tiles are stepped here, the
+ * others go on the interface list. */
+template <typename R, int N, int K>
+__global__ void __launch_bounds__(NT, 4) kf_bulk(const SimDesc *__restrict__ sims, const Consts<R> *__restrict__ consts,
+                                              const int *__restrict__ tsim, const R *__restrict__ state,
+                                              R *__restrict__ next, const signed char *__restrict__ flag_in,
+                                              signed char *__restrict__ flag_out, int *__restrict__ glist,
+                                              int *__restrict__ ctr, StatBufs st) {
+  __shared__ R M[K][SS];
+  __shared__ RemapTab rtm;
+  __shared__ int s_phase, s_have;
+  const int t = blockIdx.x;
+  const int s = __ldg(tsim + t);
+  const SimDesc sd = sims[s];
+  const Consts<R> &D = consts[s];
+  const Grid &g = sd.g;
+  const int lt = t - sd.tile0, by = lt / sd.tiles_x, bx = lt - by * sd.tiles_x;
+  const int x0 = by * TX, y0 = bx * TY;
+  if (threadIdx.x < 32) {
+    const int p = bulk_phase<R>(D, g, flag_in, sd.tile0, sd.tiles_x, by, bx);
+    if (threadIdx.x == 0) {
+      s_phase = p;
+      s_have = flag_out[t];
+      if (p < 0) glist[atomicAdd(ctr + CTR_LIST, 1)] = t;
+    }
+  }
+  __syncthreads();
+  const int p = s_phase;
+  if (p < 0) return;
+
+  const R *mu = state + sd.off_state + (long long)N * g.plane;
+  R *phin = next + sd.off_state;
+  R *mun = phin + (long long)N * g.plane;
+  remap_tab(rtm, D, g, x0, y0, 1, -1, g.mx, -1, g.my);
+  __syncthreads();
+  for (int e = threadIdx.x; e < SS; e += NT) {
+    const int i = e / SW, j = e - i * SW;
+    const int r = rtm.row[i], c = rtm.col[j];
+    if (r >= 0 && c >= 0) {
+#pragma unroll
+      for (int k = 0; k < K; k++) M[k][e] = __ldg(mu + (r + c) + k * g.plane);
+    } else {
+#pragma unroll
+      for (int k = 0; k < K; k++) M[k][e] = R(0.0);
+    }
+  }
+  __syncthreads();
+
+  const int tx = threadIdx.x / TY, ty = threadIdx.x - (threadIdx.x / TY) * TY;
+  const int x = x0 + tx, y = y0 + ty, i = tx + 1, j = ty + 1, c = LI(i, j);
+  const bool valid = (x < g.mx) && (y < g.my);
+  const R cst = D.obstacle ? D.jat_obst : D.jat_well;
+  R ph[N], dp[N], m[K], nph[N], nm[K];
+  double dmu[K];
+#pragma unroll
+  for (int a = 0; a < N; a++) { ph[a] = a == p ? R(1.0) : R(0.0); dp[a] = R(0.0); nph[a] = ph[a]; }
+#pragma unroll
+  for (int k = 0; k < K; k++) { nm[k] = R(0.0); dmu[k] = 0.0; }
+  if (valid) {
+#pragma unroll
+    for (int k = 0; k < K; k++) m[k] = M[k][c];
+    /* the bulk expressions of the general path (update_tile's uniform path) */
+    R cn[K];
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      R divflux = R(0.0);
+#pragma unroll
+      for (int l = 0; l < K; l++) {
+        const R *Ml = M[l];
+        const R Dv = D.Dbulk[p][k][l];
+        const R dm = (Dv + Dv) * R(0.5);
+        R fx = dm * divx(Ml[LI(i + 1, j)] - Ml[c], D), bx_ = dm * divx(Ml[c] - Ml[LI(i - 1, j)], D);
+        R fy = dm * divy(Ml[LI(i, j + 1)] - Ml[c], D), by_ = dm * divy(Ml[c] - Ml[LI(i, j - 1)], D);
+        divflux += divx(fx - bx_, D);
+        divflux += divy(fy - by_, D);
+      }
+      R divjat = divx((R(0.0) - R(0.0)) * cst, D);
+      divjat += divy((R(0.0) - R(0.0)) * cst, D);
+      if constexpr (sizeof(R) == 8) cn[k] = c_mu<R, K>(D, m, p, k) + D.dt * (divflux) - divjat;
+      else cn[k] = D.dt * divflux - divjat;
+    }
+    if constexpr (sizeof(R) == 8) {
+#pragma unroll
+      for (int k = 0; k < K; k++) {
+        nm[k] = Mu<R, K>(D, cn, p, k);
+        dmu[k] = (double)nm[k] - (double)m[k];
+      }
+#pragma unroll
+      for (int a = 0; a < N; a++) nph[a] = ph[a] + dp[a];
+    } else {
+      bulk_commit_f32<R, N, K>(D, p, cn, ph, dp, m, nph, nm, dmu, round_key(__ldg(st.round_step), x, y));
+    }
+    const long long o = (long long)x * g.pitch + y;
+#pragma unroll
+    for (int k = 0; k < K; k++) mun[k * g.plane + o] = nm[k];
+    if (s_have != p) {
+#pragma unroll
+      for (int a = 0; a < N; a++) phin[a * g.plane + o] = nph[a];
+    }
+  }
+  block_stats<R, N, K, true>(D, valid, nph, nm, dp, dmu, st, t);
+  if (threadIdx.x == 0) flag_out[t] = (signed char)p;
+}
+
+/* Persistent CTAs over the interface list.  Each simulation's constants are
+ * copied into shared memory when a CTA moves to it. */
+template <typename R, int N, int K, bool ANISO>
+__global__ void __launch_bounds__(NT, (N <= 3 ? 2 : 1)) kf_general(const SimDesc *__restrict__ sims,
+                                                 const Consts<R> *__restrict__ consts, const int *__restrict__ tsim,
+                                                 const R *__restrict__ state, R *__restrict__ next,
+                                                 signed char *__restrict__ flag_out, const int *__restrict__ glist,
+                                                 int *__restrict__ ctr, StatBufs st) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  GenSmem<R, N, K> &sm = *reinterpret_cast<GenSmem<R, N, K> *>(smraw);
+  __shared__ Consts<R> sc;
+  __shared__ int s_item, s_last;
+  const int nlist = *(volatile int *)(ctr + CTR_LIST);
+  int cur_sim = -1;
+  for (;;) {
+    if (threadIdx.x == 0) s_item = atomicAdd(ctr + CTR_HEAD, 1);
+    __syncthreads();
+    const int item = s_item;
+    if (item >= nlist) break;
+    const int t = __ldg(glist + item);
+    const int s = __ldg(tsim + t);
+    if (s != cur_sim) {
+      load_consts(sc, consts + s);
+      cur_sim = s;
+      __syncthreads();
+    }
+    const SimDesc sd = sims[s];
+    const int lt = t - sd.tile0, by = lt / sd.tiles_x, bx = lt - by * sd.tiles_x;
+    const R *ph = state + sd.off_state;
+    R *nx = next + sd.off_state;
+    const signed char f = general_tile<R, N, K, ANISO>(sc, sd.g, ph, ph + (long long)N * sd.g.plane, nx,
+                                                       nx + (long long)N * sd.g.plane, by * TX, bx * TY, st, t, sm);
+    if (threadIdx.x == 0) flag_out[t] = f;
+    __syncthreads();
+  }
+  /* the last CTA to finish empties the list for the next step */
+  if (threadIdx.x == 0) {
+    __threadfence();
+    s_last = atomicAdd(ctr + CTR_DONE, 1) == (int)gridDim.x - 1;
+  }
+  __syncthreads();
+  if (s_last && threadIdx.x == 0) {
+    ctr[CTR_LIST] = 0;
+    ctr[CTR_HEAD] = 0;
+    ctr[CTR_DONE] = 0;
+    ctr[CTR_STEP] = (int)((unsigned)ctr[CTR_STEP] + 1u);
+    __threadfence();
+  }
+}
+
+/* Flags of every tile of a state buffer from its phi (after an upload,
+ * smoothing or gp_batch_set). */
+template <typename R, int N>
+__global__ void __launch_bounds__(NT) kf_flags(const SimDesc *__restrict__ sims, const int *__restrict__ tsim,
+                                               const R *__restrict__ state, signed char *__restrict__ flags) {
+  const int t = blockIdx.x;
+  const SimDesc sd = sims[__ldg(tsim + t)];
+  const int lt = t - sd.tile0, by = lt / sd.tiles_x, bx = lt - by * sd.tiles_x;
+  const int tx = threadIdx.x / TY, ty = threadIdx.x - (threadIdx.x / TY) * TY;
+  const int x = by * TX + tx, y = bx * TY + ty;
+  const bool valid = (x < sd.g.mx) && (y < sd.g.my);
+  int oh = -1;
+  if (valid) {
+    R ph[N];
+#pragma unroll
+    for (int a = 0; a < N; a++) ph[a] = __ldg(state + sd.off_state + a * sd.g.plane + (long long)x * sd.g.pitch + y);
+    oh = one_hot<R, N>(ph);
+  }
+  const signed char f = tile_flag(valid, oh);
+  if (threadIdx.x == 0) flags[t] = f;
+}
+
+}  // namespace gpd

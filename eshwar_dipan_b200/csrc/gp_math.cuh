@@ -262,13 +262,19 @@ __device__ __forceinline__ void rot2(const Consts<R> &D, const R (&M)[2][2], R q
   }
 }
 
+/* Anisotropy functions.  They are evaluated in FP64 for both field types: in
+ * float, |q|^6 of a gradient just above the reference's |q|^2 > 1e-15 guard is
+ * about 1e-45 and underflows, which turns dA/dq into inf or NaN.  For FP64
+ * fields the expressions are exactly the reference's. */
+
 /* anisotropy_01_function_ac (anisotropy_01.h:30-48), q_z = 0 */
 template <typename R>
-__device__ __forceinline__ R ac(R qx, R qy, R dab) {
-  R qx2 = qx * qx, qx4 = qx2 * qx2, qy2 = qy * qy, qy4 = qy2 * qy2;
-  R qz2 = R(0.0) * R(0.0), qz4 = qz2 * qz2;
-  R q2 = qx2 + qy2 + qz2;
-  if (fabs(q2) > R(1.0e-15)) return R(1.0) - dab * (R(3.0) - R(4.0) * (qx4 + qy4 + qz4) / (q2 * q2));
+__device__ __forceinline__ R ac(R qx_, R qy_, R dab) {
+  const double qx = qx_, qy = qy_;
+  double qx2 = qx * qx, qx4 = qx2 * qx2, qy2 = qy * qy, qy4 = qy2 * qy2;
+  double qz2 = 0.0 * 0.0, qz4 = qz2 * qz2;
+  double q2 = qx2 + qy2 + qz2;
+  if (fabs(q2) > 1.0e-15) return (R)(1.0 - (double)dab * (3.0 - 4.0 * (qx4 + qy4 + qz4) / (q2 * q2)));
   return R(1.0);
 }
 
@@ -276,21 +282,23 @@ __device__ __forceinline__ R ac(R qx, R qy, R dab) {
  * 16*dab*(q_i^3/|q|^4 - q_i*sum q^4/|q|^6) */
 template <typename R>
 struct QPow {
-  R q2, q22, q23, q4;
+  double q2, q22, q23, q4;
 };
 template <typename R>
-__device__ __forceinline__ QPow<R> qpow(R qx, R qy) {
+__device__ __forceinline__ QPow<R> qpow(R qx_, R qy_) {
+  const double qx = qx_, qy = qy_;
   QPow<R> r;
-  R qx3 = qx * qx * qx, qy3 = qy * qy * qy, qz3 = R(0.0);
-  r.q2 = qx * qx + qy * qy + R(0.0) * R(0.0);
+  double qx3 = qx * qx * qx, qy3 = qy * qy * qy, qz3 = 0.0;
+  r.q2 = qx * qx + qy * qy + 0.0 * 0.0;
   r.q22 = r.q2 * r.q2;
   r.q23 = r.q2 * r.q2 * r.q2;
-  r.q4 = qx3 * qx + qy3 * qy + qz3 * R(0.0);
+  r.q4 = qx3 * qx + qy3 * qy + qz3 * 0.0;
   return r;
 }
 template <typename R>
-__device__ __forceinline__ R dadq_c(R qi, const QPow<R> &p, R dab16) {
-  if (fabs(p.q2) > R(1.0e-15)) return dab16 * (qi * qi * qi / p.q22 - qi * p.q4 / p.q23);
+__device__ __forceinline__ R dadq_c(R qi_, const QPow<R> &p, R dab16) {
+  const double qi = qi_;
+  if (fabs(p.q2) > 1.0e-15) return (R)((double)dab16 * (qi * qi * qi / p.q22 - qi * p.q4 / p.q23));
   return R(0.0);
 }
 

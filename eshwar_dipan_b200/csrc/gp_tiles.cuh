@@ -18,12 +18,11 @@
  * (b,a) reuses the work of pair (a,b): its rotated q and dA/dq are 0.0 minus
  * those of (a,b) bit for bit (rotation results are never -0, negation is exact).
  *
- * The tile functions are driven by two kinds of kernels: k_dphi / k_update,
- * one CTA per tile of one simulation with its constants in __constant__
- * memory (the plain FP64 form), and kb_dphi / kb_update, persistent CTAs that
- * pull (simulation, tile) items from a work queue over a batch of simulations
- * of different sizes and parameters, each simulation's constants copied into
- * shared memory when a CTA moves to it.
+ * dphi_tile / update_tile drive k_dphi / k_update (gp_device.cu), one CTA
+ * per tile of one simulation with its constants in __constant__ memory: the
+ * two-pass step of gp_step_noalloc.  The stepping engine of gp_ctx and
+ * gp_batch is in gp_fused.cuh and shares this file's staging, face, commit
+ * and statistics code.
  */
 #pragma once
 #include "gp_math.cuh"
@@ -546,6 +545,134 @@ __device__ __forceinline__ void block_stats(const Consts<R> &D, bool valid, cons
   }
 }
 
+/* mu update and phi commit of one tile cell from the tile's face fluxes
+ * (calculate_divergence_concentration.h:24-140): divergences, then the bulk
+ * branch (mu = Mu_a(c_a(mu) + dc)) or the interface branch (dmu = (dc/dmu)^-1 dc,
+ * inverted in FP64), then phi += delta-phi.  i, j: the cell's position in the
+ * one-cell-halo tile layout; x, y: its interior coordinates. */
+template <typename R, int N, int K>
+__device__ __forceinline__ void commit_cell(const Consts<R> &D, const R (&FX)[K][K][NXF], const R (&FY)[K][K][NYF],
+                                            const R (&JX)[K][NXF], const R (&JY)[K][NYF], const R (&CM)[N][K][SS],
+                                            const R (&H)[N][SS], int i, int j, int x, int y, const R *ph,
+                                            const R *dp, const R *m, R *nph, R *nm, double *dmu,
+                                            const StatBufs &st) {
+  const R cst = D.obstacle ? D.jat_obst : D.jat_well;
+  const int c = LI(i, j);
+  R divflux[K], divjat[K];
+  const int xf = i * TY + (j - 1), xb = (i - 1) * TY + (j - 1);
+  const int yr = (i - 1) * (TY + 1) + j, yl = (i - 1) * (TY + 1) + (j - 1);
+#pragma unroll
+  for (int k = 0; k < K; k++) {
+    divflux[k] = R(0.0);
+#pragma unroll
+    for (int l = 0; l < K; l++) {
+      divflux[k] += divx(FX[k][l][xf] - FX[k][l][xb], D);
+      divflux[k] += divy(FY[k][l][yr] - FY[k][l][yl], D);
+    }
+    divjat[k] = divx((JX[k][xf] - JX[k][xb]) * cst, D);
+    divjat[k] += divy((JY[k][yr] - JY[k][yl]) * cst, D);
+  }
+  int bulk = -1;
+#pragma unroll
+  for (int a = 0; a < N; a++)
+    if (bulk < 0 && ph[a] == R(1.0)) bulk = a;
+  if (bulk >= 0 && sizeof(R) == 4) {
+    R cn[K];
+#pragma unroll
+    for (int k = 0; k < K; k++) cn[k] = D.dt * (divflux[k]) - divjat[k];
+    bulk_commit_f32<R, N, K>(D, bulk, cn, ph, dp, m, nph, nm, dmu, round_key(__ldg(st.round_step), x, y));
+  } else if (bulk >= 0) {
+    R cn[K];
+#pragma unroll
+    for (int k = 0; k < K; k++) cn[k] = CM[bulk][k][c] + D.dt * (divflux[k]) - divjat[k];
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      nm[k] = Mu<R, K>(D, cn, bulk, k);
+      dmu[k] = (double)nm[k] - (double)m[k];
+    }
+#pragma unroll
+    for (int a = 0; a < N; a++) nph[a] = ph[a] + dp[a];
+  } else {
+    /* sum_a c_a(mu) sum_b dh_a/dphi_b dphi_b (calculate_divergence_concentration.h:23-31) */
+    R sum[K];
+    double dc[K], dcdmu[K][K];
+#pragma unroll
+    for (int k = 0; k < K; k++) sum[k] = R(0.0);
+#pragma unroll
+    for (int a = 0; a < N; a++) {
+      R sdh = R(0.0);
+#pragma unroll
+      for (int b = 0; b < N; b++) sdh += dh<R, N>(ph, a, b) * dp[b];
+#pragma unroll
+      for (int k = 0; k < K; k++) sum[k] += CM[a][k][c] * sdh;
+    }
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      dc[k] = (double)(D.dt * (divflux[k]) - divjat[k] - sum[k]);
+#pragma unroll
+      for (int l = 0; l < K; l++) {
+        dcdmu[k][l] = 0.0;
+#pragma unroll
+        for (int a = 0; a < N; a++) dcdmu[k][l] += D.cmu64[a][k][l] * (double)H[a][c];
+      }
+    }
+    double m64[K];
+#pragma unroll
+    for (int k = 0; k < K; k++) { m64[k] = (double)m[k]; dmu[k] = 0.0; }
+    if (D.inv_mode == GP_INV_BINARY) {
+      double i00 = 1.0 / dcdmu[0][0];
+      dmu[0] = dc[0] * i00;
+      m64[0] += dmu[0];
+    } else if (D.inv_mode == GP_INV_TERNARY && K == 2) {
+      double det = dcdmu[0][0] * dcdmu[K - 1][K - 1] - dcdmu[0][K - 1] * dcdmu[K - 1][0];
+      double iv[K][K];
+      iv[0][0] = dcdmu[K - 1][K - 1] / det;
+      iv[K - 1][K - 1] = dcdmu[0][0] / det;
+      iv[0][K - 1] = -dcdmu[0][K - 1] / det;
+      iv[K - 1][0] = -dcdmu[K - 1][0] / det;
+#pragma unroll
+      for (int k = 0; k < K; k++) {
+        dmu[k] = 0.0;
+#pragma unroll
+        for (int l = 0; l < K; l++) dmu[k] += iv[k][l] * dc[l];
+      }
+#pragma unroll
+      for (int k = 0; k < K; k++) m64[k] = dmu[k] + m64[k];
+    } else if (D.inv_mode == GP_INV_DILUTE) {
+#pragma unroll
+      for (int k = 0; k < K; k++) {
+        double ikk = 1.0 / dcdmu[k][k];
+        dmu[k] = dc[k] * ikk;
+        m64[k] += dmu[k];
+      }
+    } else {
+      double iv[K][K];
+      matinv_div<double, K>(dcdmu, iv);
+#pragma unroll
+      for (int k = 0; k < K; k++) {
+        double s = 0;
+#pragma unroll
+        for (int l = 0; l < K; l++) s = s + iv[k][l] * dc[l];
+        dmu[k] = s;
+      }
+#pragma unroll
+      for (int k = 0; k < K; k++) m64[k] = dmu[k] + m64[k];
+    }
+    if constexpr (sizeof(R) == 8) {
+#pragma unroll
+      for (int k = 0; k < K; k++) nm[k] = (R)m64[k];
+#pragma unroll
+      for (int a = 0; a < N; a++) nph[a] = ph[a] + dp[a];
+    } else {
+      const unsigned key = round_key(__ldg(st.round_step), x, y);
+#pragma unroll
+      for (int k = 0; k < K; k++) nm[k] = round_stochastic(m64[k], key, N + k);
+#pragma unroll
+      for (int a = 0; a < N; a++) nph[a] = round_stochastic((double)ph[a] + (double)dp[a], key, a);
+    }
+  }
+}
+
 /* mu update and phi commit of one interior tile
  * (calculate_fluxes_concentration_2D + calculate_divergence_concentration_2D,
  * calculate_fluxes_concentration.h:4-145, calculate_divergence_concentration.h:4-153).
@@ -754,119 +881,7 @@ __device__ __forceinline__ void update_tile(const Consts<R> &D, const Grid &g, c
     for (int a = 0; a < N; a++) { ph[a] = sm.P[a][c]; dp[a] = sm.DP[a][c]; }
 #pragma unroll
     for (int k = 0; k < K; k++) m[k] = sm.M[k][c];
-    R divflux[K], divjat[K];
-    const int xf = i * TY + (j - 1), xb = (i - 1) * TY + (j - 1);
-    const int yr = (i - 1) * (TY + 1) + j, yl = (i - 1) * (TY + 1) + (j - 1);
-#pragma unroll
-    for (int k = 0; k < K; k++) {
-      divflux[k] = R(0.0);
-#pragma unroll
-      for (int l = 0; l < K; l++) {
-        divflux[k] += divx(sm.FX[k][l][xf] - sm.FX[k][l][xb], D);
-        divflux[k] += divy(sm.FY[k][l][yr] - sm.FY[k][l][yl], D);
-      }
-      divjat[k] = divx((sm.JX[k][xf] - sm.JX[k][xb]) * cst, D);
-      divjat[k] += divy((sm.JY[k][yr] - sm.JY[k][yl]) * cst, D);
-    }
-    int bulk = -1;
-#pragma unroll
-    for (int a = 0; a < N; a++)
-      if (bulk < 0 && ph[a] == R(1.0)) bulk = a;
-    if (bulk >= 0 && sizeof(R) == 4) {
-      R cn[K];
-#pragma unroll
-      for (int k = 0; k < K; k++) cn[k] = D.dt * (divflux[k]) - divjat[k];
-      bulk_commit_f32<R, N, K>(D, bulk, cn, ph, dp, m, nph, nm, dmu, round_key(__ldg(st.round_step), x, y));
-    } else if (bulk >= 0) {
-      R cn[K];
-#pragma unroll
-      for (int k = 0; k < K; k++) cn[k] = sm.CM[bulk][k][c] + D.dt * (divflux[k]) - divjat[k];
-#pragma unroll
-      for (int k = 0; k < K; k++) {
-        nm[k] = Mu<R, K>(D, cn, bulk, k);
-        dmu[k] = (double)nm[k] - (double)m[k];
-      }
-#pragma unroll
-      for (int a = 0; a < N; a++) nph[a] = ph[a] + dp[a];
-    } else {
-      /* sum_a c_a(mu) sum_b dh_a/dphi_b dphi_b (calculate_divergence_concentration.h:23-31) */
-      R sum[K];
-      double dc[K], dcdmu[K][K];
-#pragma unroll
-      for (int k = 0; k < K; k++) sum[k] = R(0.0);
-#pragma unroll
-      for (int a = 0; a < N; a++) {
-        R sdh = R(0.0);
-#pragma unroll
-        for (int b = 0; b < N; b++) sdh += dh<R, N>(ph, a, b) * dp[b];
-#pragma unroll
-        for (int k = 0; k < K; k++) sum[k] += sm.CM[a][k][c] * sdh;
-      }
-#pragma unroll
-      for (int k = 0; k < K; k++) {
-        dc[k] = (double)(D.dt * (divflux[k]) - divjat[k] - sum[k]);
-#pragma unroll
-        for (int l = 0; l < K; l++) {
-          dcdmu[k][l] = 0.0;
-#pragma unroll
-          for (int a = 0; a < N; a++) dcdmu[k][l] += D.cmu64[a][k][l] * (double)sm.H[a][c];
-        }
-      }
-      double m64[K];
-#pragma unroll
-      for (int k = 0; k < K; k++) { m64[k] = (double)m[k]; dmu[k] = 0.0; }
-      if (D.inv_mode == GP_INV_BINARY) {
-        double i00 = 1.0 / dcdmu[0][0];
-        dmu[0] = dc[0] * i00;
-        m64[0] += dmu[0];
-      } else if (D.inv_mode == GP_INV_TERNARY && K == 2) {
-        double det = dcdmu[0][0] * dcdmu[K - 1][K - 1] - dcdmu[0][K - 1] * dcdmu[K - 1][0];
-        double iv[K][K];
-        iv[0][0] = dcdmu[K - 1][K - 1] / det;
-        iv[K - 1][K - 1] = dcdmu[0][0] / det;
-        iv[0][K - 1] = -dcdmu[0][K - 1] / det;
-        iv[K - 1][0] = -dcdmu[K - 1][0] / det;
-#pragma unroll
-        for (int k = 0; k < K; k++) {
-          dmu[k] = 0.0;
-#pragma unroll
-          for (int l = 0; l < K; l++) dmu[k] += iv[k][l] * dc[l];
-        }
-#pragma unroll
-        for (int k = 0; k < K; k++) m64[k] = dmu[k] + m64[k];
-      } else if (D.inv_mode == GP_INV_DILUTE) {
-#pragma unroll
-        for (int k = 0; k < K; k++) {
-          double ikk = 1.0 / dcdmu[k][k];
-          dmu[k] = dc[k] * ikk;
-          m64[k] += dmu[k];
-        }
-      } else {
-        double iv[K][K];
-        matinv_div<double, K>(dcdmu, iv);
-#pragma unroll
-        for (int k = 0; k < K; k++) {
-          double s = 0;
-#pragma unroll
-          for (int l = 0; l < K; l++) s = s + iv[k][l] * dc[l];
-          dmu[k] = s;
-        }
-#pragma unroll
-        for (int k = 0; k < K; k++) m64[k] = dmu[k] + m64[k];
-      }
-      if constexpr (sizeof(R) == 8) {
-#pragma unroll
-        for (int k = 0; k < K; k++) nm[k] = (R)m64[k];
-#pragma unroll
-        for (int a = 0; a < N; a++) nph[a] = ph[a] + dp[a];
-      } else {
-        const unsigned key = round_key(__ldg(st.round_step), x, y);
-#pragma unroll
-        for (int k = 0; k < K; k++) nm[k] = round_stochastic(m64[k], key, N + k);
-#pragma unroll
-        for (int a = 0; a < N; a++) nph[a] = round_stochastic((double)ph[a] + (double)dp[a], key, a);
-      }
-    }
+    commit_cell<R, N, K>(D, sm.FX, sm.FY, sm.JX, sm.JY, sm.CM, sm.H, i, j, x, y, ph, dp, m, nph, nm, dmu, st);
     const long long o = (long long)x * g.pitch + y;
 #pragma unroll
     for (int a = 0; a < N; a++) phin[a * g.plane + o] = nph[a];
@@ -881,13 +896,12 @@ __device__ __forceinline__ void update_tile(const Consts<R> &D, const Grid &g, c
 /* ------------------------------------------------------------------ */
 
 /* One simulation of a batch: its geometry, where its planes start in the
- * pooled buffers, and its tiles in the two work lists. */
+ * pooled buffers, and its tiles in the batch's tile numbering. */
 struct SimDesc {
   Grid g;
   long long off_state;   /* N phi planes then K mu planes */
-  long long off_dphi;    /* N delta-phi planes */
-  int tiles_x, tile0;    /* update tiles per row, first update tile */
-  int dtiles_x, dtile0;  /* delta-phi tiles per row, first delta-phi tile */
+  long long off_dphi;    /* N delta-phi planes (smoothing sweeps) */
+  int tiles_x, tile0;    /* tiles per row, first tile */
 };
 
 template <typename R>
@@ -895,68 +909,6 @@ __device__ __forceinline__ void load_consts(Consts<R> &dst, const Consts<R> *__r
   const int *s = reinterpret_cast<const int *>(src);
   int *d = reinterpret_cast<int *>(&dst);
   for (int w = threadIdx.x; w < (int)(sizeof(Consts<R>) / sizeof(int)); w += NT) d[w] = __ldg(s + w);
-}
-
-/* Persistent CTAs over the delta-phi work list of all simulations. */
-template <typename R, int N, int K, bool ANISO>
-__global__ void __launch_bounds__(NT) kb_dphi(const SimDesc *__restrict__ sims, const Consts<R> *__restrict__ consts,
-                                              const int *__restrict__ tsim, int ntiles, int *counter,
-                                              const R *__restrict__ state, R *__restrict__ dphi) {
-  extern __shared__ __align__(16) unsigned char smraw[];
-  DphiSmem<R, N> &sm = *reinterpret_cast<DphiSmem<R, N> *>(smraw);
-  __shared__ Consts<R> sc;
-  __shared__ int s_tile;
-  int cur_sim = -1;
-  for (;;) {
-    if (threadIdx.x == 0) s_tile = atomicAdd(counter, 1);
-    __syncthreads();
-    const int t = s_tile;
-    if (t >= ntiles) break;
-    const int s = __ldg(tsim + t);
-    if (s != cur_sim) {
-      load_consts(sc, consts + s);
-      cur_sim = s;
-      __syncthreads();
-    }
-    const SimDesc sd = sims[s];
-    const int lt = t - sd.dtile0, by = lt / sd.dtiles_x, bx = lt - by * sd.dtiles_x;
-    const R *ph = state + sd.off_state;
-    dphi_tile<R, N, K, ANISO>(sc, sd.g, ph, ph + N * sd.g.plane, dphi + sd.off_dphi, by * TX - 1, bx * TY - 1, sm);
-    __syncthreads();
-  }
-}
-
-/* Persistent CTAs over the update work list of all simulations; the tile
- * index is the slot of its progress record. */
-template <typename R, int N, int K>
-__global__ void __launch_bounds__(NT) kb_update(const SimDesc *__restrict__ sims, const Consts<R> *__restrict__ consts,
-                                                const int *__restrict__ tsim, int ntiles, int *counter,
-                                                const R *__restrict__ state, const R *__restrict__ dphi,
-                                                R *__restrict__ next, StatBufs st) {
-  extern __shared__ __align__(16) unsigned char smraw[];
-  UpdSmem<R, N, K> &sm = *reinterpret_cast<UpdSmem<R, N, K> *>(smraw);
-  __shared__ Consts<R> sc;
-  __shared__ int s_tile;
-  int cur_sim = -1;
-  for (;;) {
-    if (threadIdx.x == 0) s_tile = atomicAdd(counter, 1);
-    __syncthreads();
-    const int t = s_tile;
-    if (t >= ntiles) break;
-    const int s = __ldg(tsim + t);
-    if (s != cur_sim) {
-      load_consts(sc, consts + s);
-      cur_sim = s;
-      __syncthreads();
-    }
-    const SimDesc sd = sims[s];
-    const int lt = t - sd.tile0, by = lt / sd.tiles_x, bx = lt - by * sd.tiles_x;
-    const R *ph = state + sd.off_state;
-    R *nx = next + sd.off_state;
-    update_tile<R, N, K>(sc, sd.g, ph, ph + N * sd.g.plane, dphi + sd.off_dphi, nx, nx + N * sd.g.plane, by * TX,
-                         bx * TY, st, t, sm);
-    __syncthreads();
-  }
 }
 
 }  // namespace gpd

@@ -168,11 +168,14 @@ int gp_set_dev(gp_ctx *ctx, const double *phi_dev, const double *mu_dev);
 int gp_get_stats(gp_ctx *ctx, gp_stats *stats);
 
 /* gp_step with CUDA events recorded on the context's stream: total_ms is the
- * device time of the nsteps steps, ms_phase / ms_update the summed device
- * times of the phase-field and concentration kernels (each may be NULL).
- * Measurement entry point for bench.py; results are those of gp_step. */
+ * device time of the nsteps steps.  A step is two kernels: the bulk-tile
+ * kernel (tiles with one pure phase everywhere within reach of their stencil,
+ * which only move mu) and the interface-tile kernel (everything else);
+ * ms_bulk / ms_iface, when not NULL, receive their summed device times, and
+ * the steps then run one by one instead of as CUDA graphs.  Each may be NULL.
+ * Measurement entry point; results are those of gp_step. */
 int gp_step_timed(gp_ctx *ctx, long nsteps, gp_stats *stats, double *total_ms,
-                  double *ms_phase, double *ms_update);
+                  double *ms_bulk, double *ms_iface);
 
 /* ---- batches of simulations ------------------------------------------- */
 
