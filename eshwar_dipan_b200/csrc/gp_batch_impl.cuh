@@ -13,12 +13,13 @@
 namespace gpd {
 
 struct BatchLaunch {
-  /* occupancy of the interface kernel (blocks per SM) */
-  cudaError_t (*prepare)(int *blocks_per_sm_general);
+  /* occupancy of the bulk and interface kernels (blocks per SM) */
+  cudaError_t (*prepare)(int *blocks_per_sm_bulk, int *blocks_per_sm_general);
   /* one step: bulk tiles + interface list, then the interface tiles */
-  cudaError_t (*bulk)(int ntiles, cudaStream_t s, const SimDesc *sims, const void *consts, const int *tsim,
-                      const void *state, void *next, const signed char *flag_in, signed char *flag_out, int *glist,
-                      int *ctr, StatBufs st);
+  /* mul: every simulation's spacings are powers of two (x/dx == x*(1/dx)) */
+  cudaError_t (*bulk)(int grid, int ntiles, bool mul, cudaStream_t s, const SimDesc *sims, const void *consts,
+                      const int *tsim, const void *state, void *next, const signed char *flag_in,
+                      signed char *flag_out, int *glist, int *ctr, StatBufs st);
   cudaError_t (*general)(int grid, cudaStream_t s, const SimDesc *sims, const void *consts, const int *tsim,
                          const void *state, void *next, signed char *flag_out, const int *glist, int *ctr,
                          StatBufs st);
@@ -32,17 +33,39 @@ struct BatchLaunch {
 
 template <typename R, int N, int K, bool A>
 struct BatchKernels {
-  static cudaError_t prepare(int *bg) {
+  static constexpr size_t bulk_smem = (NT / 32) * sizeof(BulkWarpStage<R, N, K>);
+  template <bool SUMS, bool MUL>
+  static cudaError_t bulk_attr() {
+    return cudaFuncSetAttribute(kf_bulk<R, N, K, SUMS, MUL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)bulk_smem);
+  }
+  static cudaError_t prepare(int *bb, int *bg) {
     cudaError_t e = cudaFuncSetAttribute(kf_general<R, N, K, A>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)sizeof(GenSmem<R, N, K>));
+    if (e == cudaSuccess) e = bulk_attr<false, false>();
+    if (e == cudaSuccess) e = bulk_attr<false, true>();
+    if (e == cudaSuccess) e = bulk_attr<true, false>();
+    if (e == cudaSuccess) e = bulk_attr<true, true>();
+    if (e != cudaSuccess) return e;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(bb, kf_bulk<R, N, K, false, true>, NT, bulk_smem);
     if (e != cudaSuccess) return e;
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bg, kf_general<R, N, K, A>, NT, sizeof(GenSmem<R, N, K>));
   }
-  static cudaError_t bulk(int ntiles, cudaStream_t s, const SimDesc *sims, const void *consts, const int *tsim,
-                          const void *state, void *next, const signed char *flag_in, signed char *flag_out,
-                          int *glist, int *ctr, StatBufs st) {
-    kf_bulk<R, N, K><<<ntiles, NT, 0, s>>>(sims, (const Consts<R> *)consts, tsim, (const R *)state, (R *)next,
-                                           flag_in, flag_out, glist, ctr, st);
+  static cudaError_t bulk(int grid, int ntiles, bool mul, cudaStream_t s, const SimDesc *sims, const void *consts,
+                          const int *tsim, const void *state, void *next, const signed char *flag_in,
+                          signed char *flag_out, int *glist, int *ctr, StatBufs st) {
+#define GP_BULK(SUMS, MUL)                                                                                       \
+  kf_bulk<R, N, K, SUMS, MUL><<<grid, NT, bulk_smem, s>>>(sims, (const Consts<R> *)consts, tsim, ntiles,         \
+                                                          (const R *)state, (R *)next, flag_in, flag_out, glist, \
+                                                          ctr, st)
+    if (st.want_sums) {
+      if (mul) GP_BULK(true, true);
+      else GP_BULK(true, false);
+    } else {
+      if (mul) GP_BULK(false, true);
+      else GP_BULK(false, false);
+    }
+#undef GP_BULK
     return cudaGetLastError();
   }
   static cudaError_t general(int grid, cudaStream_t s, const SimDesc *sims, const void *consts, const int *tsim,

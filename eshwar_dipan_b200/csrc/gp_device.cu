@@ -113,29 +113,6 @@ __global__ void k_reduce_sums(const double *__restrict__ part, const int *__rest
   if (threadIdx.x == 0) out[(long long)s * nsum + f] = r[0];
 }
 
-/* Fold per-tile running extremes: slot f is a maximum for phi/mu maxima. */
-__global__ void k_reduce_ext(const long long *__restrict__ ext, const int *__restrict__ tile0,
-                             const int *__restrict__ ntile, int nslot, int N, int K, long long *__restrict__ out) {
-  __shared__ long long r[256];
-  const int f = blockIdx.x, s = blockIdx.y, t0 = tile0[s], nt = ntile[s];
-  const bool isMax = f < N || (f >= 2 * N && f < 2 * N + K);
-  long long v = isMax ? LLONG_MIN : LLONG_MAX;
-  for (int b = threadIdx.x; b < nt; b += 256) {
-    long long w = ext[(long long)(t0 + b) * nslot + f];
-    v = isMax ? (w > v ? w : v) : (w < v ? w : v);
-  }
-  r[threadIdx.x] = v;
-  __syncthreads();
-  for (int w = 128; w > 0; w >>= 1) {
-    if (threadIdx.x < w) {
-      long long a = r[threadIdx.x], b = r[threadIdx.x + w];
-      r[threadIdx.x] = isMax ? (a > b ? a : b) : (a < b ? a : b);
-    }
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) out[(long long)s * nslot + f] = r[0];
-}
-
 double from_ord(long long i) {
   if (i < 0) i ^= 0x7fffffffffffffffLL;
   double v;
@@ -277,7 +254,8 @@ struct gp_batch {
   std::vector<gp_params> params;
   std::vector<gp_derived> derived;
   std::vector<gpd::SimDesc> desc;
-  int dev, nsm, grid_g;
+  int dev, nsm, grid_b, grid_g;
+  bool mul;                     /* every simulation's dx and dy are powers of two (or FP32) */
   int ntiles;                   /* TX x TY tiles over all simulations */
   cudaStream_t stream;
   gpd::SimDesc *d_desc;
@@ -290,7 +268,7 @@ struct gp_batch {
   int *glist;                   /* interface tiles of the current step */
   int *counters;                /* gpd::CTR_* */
   int cur;
-  long long *ext, *ext_sim;
+  long long *ext;               /* running extremes per simulation [nsims][2(N+K)] */
   double *partials, *sums_sim;
   cudaGraphExec_t graph[2];
   cudaEvent_t ev[4];
@@ -326,8 +304,8 @@ static int batch_step_once(gp_batch *b, int want_sums, cudaEvent_t *ev) {
   st.round_step = (const unsigned *)(b->counters + gpd::CTR_STEP);
   const int in = b->cur, out = b->cur ^ 1;
   if (ev) BK(cudaEventRecord(ev[0], b->stream));
-  BK(b->L.bulk(b->ntiles, b->stream, b->d_desc, b->d_consts, b->d_tsim, b->state[in], b->state[out], b->flags[in],
-               b->flags[out], b->glist, b->counters, st));
+  BK(b->L.bulk(b->grid_b, b->ntiles, b->mul, b->stream, b->d_desc, b->d_consts, b->d_tsim, b->state[in],
+               b->state[out], b->flags[in], b->flags[out], b->glist, b->counters, st));
   if (ev) BK(cudaEventRecord(ev[1], b->stream));
   BK(b->L.general(b->grid_g, b->stream, b->d_desc, b->d_consts, b->d_tsim, b->state[in], b->state[out],
                   b->flags[out], b->glist, b->counters, st));
@@ -348,11 +326,10 @@ static int batch_reflag(gp_batch *b, bool other_unknown) {
 static int batch_fold_stats(gp_batch *b, gp_stats *out) {
   const int N = b->N, K = b->K, ne = 2 * (N + K), ns = 2 * N + 2 * K + 1;
   k_reduce_sums<<<dim3(ns, b->nsims), 256, 0, b->stream>>>(b->partials, b->d_seg0, b->d_segn, ns, b->sums_sim);
-  k_reduce_ext<<<dim3(ne, b->nsims), 256, 0, b->stream>>>(b->ext, b->d_seg0, b->d_segn, ne, N, K, b->ext_sim);
   BK(cudaGetLastError());
   std::vector<long long> mm((size_t)ne * b->nsims);
   std::vector<double> sums((size_t)ns * b->nsims);
-  BK(cudaMemcpyAsync(mm.data(), b->ext_sim, mm.size() * 8, cudaMemcpyDeviceToHost, b->stream));
+  BK(cudaMemcpyAsync(mm.data(), b->ext, mm.size() * 8, cudaMemcpyDeviceToHost, b->stream));
   BK(cudaMemcpyAsync(sums.data(), b->sums_sim, sums.size() * 8, cudaMemcpyDeviceToHost, b->stream));
   BK(cudaStreamSynchronize(b->stream));
   for (int s = 0; s < b->nsims; s++) {
@@ -480,7 +457,6 @@ void gp_batch_destroy(gp_batch *b) {
   cudaFree(b->d_seg0);
   cudaFree(b->d_segn);
   cudaFree(b->ext);
-  cudaFree(b->ext_sim);
   cudaFree(b->partials);
   cudaFree(b->sums_sim);
   cudaFree(b->counters);
@@ -569,13 +545,17 @@ int gp_batch_create(gp_batch **out, int nsims, const gp_params *params, const do
     }
   }
   b->ntiles = nt;
-  int bpg = 1;
-  e = b->L.prepare(&bpg);
+  b->mul = true;
+  for (int s = 0; s < nsims; s++)
+    if (b->elem == 8 && !(pow2(b->derived[s].dx) && pow2(b->derived[s].dy))) b->mul = false;
+  int bpb = 1, bpg = 1;
+  e = b->L.prepare(&bpb, &bpg);
   if (e != cudaSuccess) {
     rc = bfail(b, GP_ECUDA, "gp_batch_create: %s", cudaGetErrorString(e));
     gp_batch_destroy(b);
     return rc;
   }
+  b->grid_b = std::min(nt, b->nsm * std::max(1, bpb));
   b->grid_g = b->nsm * std::max(1, bpg);
 #define BALLOC(ptr, bytes)                                                                        \
   do {                                                                                            \
@@ -596,14 +576,13 @@ int gp_batch_create(gp_batch **out, int nsims, const gp_params *params, const do
   BALLOC(b->d_tsim, sizeof(int) * (size_t)nt);
   BALLOC(b->d_seg0, sizeof(int) * nsims);
   BALLOC(b->d_segn, sizeof(int) * nsims);
-  BALLOC(b->ext, sizeof(long long) * (size_t)ne * nt);
-  BALLOC(b->ext_sim, sizeof(long long) * (size_t)ne * nsims);
+  BALLOC(b->ext, sizeof(long long) * (size_t)ne * nsims);
   BALLOC(b->partials, sizeof(double) * (size_t)ns * nt);
   BALLOC(b->sums_sim, sizeof(double) * (size_t)ns * nsims);
   BALLOC(b->counters, 4 * sizeof(int));
 #undef BALLOC
-  std::vector<long long> ext((size_t)ne * nt);
-  for (int t = 0; t < nt; t++) init_ext(&ext[(size_t)t * ne], N, K);
+  std::vector<long long> ext((size_t)ne * nsims);
+  for (int t = 0; t < nsims; t++) init_ext(&ext[(size_t)t * ne], N, K);
 #define BUP(dst, src, bytes)                                                                       \
   do {                                                                                             \
     if (cudaMemcpyAsync((dst), (src), (bytes), cudaMemcpyHostToDevice, b->stream) != cudaSuccess) { \

@@ -12,10 +12,12 @@
  * (calculate_divergence_phasefield.h:19-22, calculate_fluxes_concentration.h:64,
  * calculate_divergence_concentration.h:43-57).
  *
- *  kf_bulk     one CTA per tile.  Classifies the tile; bulk tiles read and
- *              write mu only (phi is rewritten only when the output buffer does
- *              not already hold the same one-hot tile); other tiles are put on
- *              the interface list.
+ *  kf_bulk     persistent warps, one tile at a time over contiguous tile
+ *              ranges, the next bulk tile's mu in flight (cp.async) while one
+ *              is stepped.  Classifies each tile; bulk tiles read and write mu only
+ *              (phi is rewritten only when the output buffer does not already
+ *              hold the same one-hot tile); other tiles are put on the
+ *              interface list.
  *  kf_general  persistent CTAs over the interface list.  Stages phi with a
  *              two-cell halo and mu with one, computes delta-phi on the tile
  *              plus its one-cell ring in shared memory (the ring is recomputed
@@ -373,7 +375,7 @@ template <typename R, int N, int K, bool ANISO>
 __device__ __forceinline__ signed char general_tile(const Consts<R> &D, const Grid &g, const R *__restrict__ phi,
                                                     const R *__restrict__ mu, R *__restrict__ phin,
                                                     R *__restrict__ mun, int x0, int y0, const StatBufs &st,
-                                                    long long slot, GenSmem<R, N, K> &sm) {
+                                                    long long ext_slot, long long slot, GenSmem<R, N, K> &sm) {
   constexpr int L = N - 1;
   const R cst = D.obstacle ? D.jat_obst : D.jat_well;
 
@@ -567,7 +569,7 @@ __device__ __forceinline__ signed char general_tile(const Consts<R> &D, const Gr
   }
 #undef PRIJ
 #undef PR
-  block_stats<R, N, K>(D, valid, nph, nm, dp, dmu, st, slot);
+  block_stats<R, N, K>(D, valid, nph, nm, dp, dmu, st, ext_slot, slot);
   return tile_flag(valid, oh);
 }
 
@@ -581,108 +583,274 @@ __device__ __forceinline__ signed char general_tile(const Consts<R> &D, const Gr
  * advances [3], so a step is exactly these two launches. */
 enum { CTR_LIST = 0, CTR_HEAD = 1, CTR_DONE = 2, CTR_STEP = 3 };
 
-/* One CTA per tile of every simulation: bulk tiles are stepped here, the
- * others go on the interface list. */
+/* cp.async of one 4- or 8-byte element, global -> shared (completion tracked
+ * by the issuing thread's commit/wait groups) */
+template <typename R>
+__device__ __forceinline__ void cp_async_elem(R *dst, const R *src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  if (sizeof(R) == 8) asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+  else asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int NPEND>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(NPEND) : "memory"); }
+
+/* x/dx and y/dy of the bulk kernel: a multiplication by the reciprocal when
+ * the spacing is a power of two (MUL, chosen at launch), else the division */
+template <bool MUL, typename R>
+__device__ __forceinline__ R bdiv(R v, R inv, R d) {
+  if constexpr (MUL) return v * inv;
+  else return v / d;
+}
+
+/* Bulk tiles, one warp per tile.  Warps take contiguous tile ranges; each
+ * classifies its tiles in order and puts the ones that are not bulk on the
+ * interface list.  The mu of a bulk tile with its one-cell halo is copied
+ * into the warp's shared-memory stage by cp.async while the warp steps the
+ * previous bulk tile from the other stage; lane j then steps column y0+j row
+ * by row.  No block-wide barrier anywhere.  The running mu extremes of the
+ * cells a warp steps stay in registers and are merged into the simulation's
+ * slots (atomic max/min) when the warp moves to another simulation or
+ * finishes; bulk tiles cannot move the phi extremes (their phi is 0 or 1,
+ * inside the initial [0, 1]). */
 template <typename R, int N, int K>
-__global__ void __launch_bounds__(NT, 4) kf_bulk(const SimDesc *__restrict__ sims, const Consts<R> *__restrict__ consts,
-                                              const int *__restrict__ tsim, const R *__restrict__ state,
-                                              R *__restrict__ next, const signed char *__restrict__ flag_in,
-                                              signed char *__restrict__ flag_out, int *__restrict__ glist,
-                                              int *__restrict__ ctr, StatBufs st) {
-  __shared__ R M[K][SS];
-  __shared__ RemapTab rtm;
-  __shared__ int s_phase, s_have;
-  const int t = blockIdx.x;
-  const int s = __ldg(tsim + t);
-  const SimDesc sd = sims[s];
-  const Consts<R> &D = consts[s];
-  const Grid &g = sd.g;
-  const int lt = t - sd.tile0, by = lt / sd.tiles_x, bx = lt - by * sd.tiles_x;
-  const int x0 = by * TX, y0 = bx * TY;
-  if (threadIdx.x < 32) {
-    const int p = bulk_phase<R>(D, g, flag_in, sd.tile0, sd.tiles_x, by, bx);
-    if (threadIdx.x == 0) {
-      s_phase = p;
-      s_have = flag_out[t];
-      if (p < 0) glist[atomicAdd(ctr + CTR_LIST, 1)] = t;
-    }
-  }
-  __syncthreads();
-  const int p = s_phase;
-  if (p < 0) return;
+struct BulkWarpStage {
+  R M[2][K][SH][SW];   /* two stages of mu with a one-cell halo */
+};
 
-  const R *mu = state + sd.off_state + (long long)N * g.plane;
-  R *phin = next + sd.off_state;
-  R *mun = phin + (long long)N * g.plane;
-  remap_tab(rtm, D, g, x0, y0, 1, -1, g.mx, -1, g.my);
-  __syncthreads();
-  for (int e = threadIdx.x; e < SS; e += NT) {
-    const int i = e / SW, j = e - i * SW;
-    const int r = rtm.row[i], c = rtm.col[j];
-    if (r >= 0 && c >= 0) {
-#pragma unroll
-      for (int k = 0; k < K; k++) M[k][e] = __ldg(mu + (r + c) + k * g.plane);
-    } else {
-#pragma unroll
-      for (int k = 0; k < K; k++) M[k][e] = R(0.0);
-    }
-  }
-  __syncthreads();
+template <typename R, int N, int K, bool SUMS, bool MUL>
+__global__ void __launch_bounds__(NT, 2) kf_bulk(const SimDesc *__restrict__ sims, const Consts<R> *__restrict__ consts,
+                                                 const int *__restrict__ tsim, int ntiles, const R *__restrict__ state,
+                                                 R *__restrict__ next, const signed char *__restrict__ flag_in,
+                                                 signed char *__restrict__ flag_out, int *__restrict__ glist,
+                                                 int *__restrict__ ctr, StatBufs st) {
+  constexpr int NW = NT / 32, NS = 2 * N + 2 * K + 1;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  BulkWarpStage<R, N, K> &stg = reinterpret_cast<BulkWarpStage<R, N, K> *>(smraw)[threadIdx.x >> 5];
+  const int lane = threadIdx.x & 31;
+  const int gw = blockIdx.x * NW + (threadIdx.x >> 5), nwarps = gridDim.x * NW;
+  const int per = (ntiles + nwarps - 1) / nwarps;
+  const int t0 = gw * per, t1 = min(ntiles, t0 + per);
 
-  const int tx = threadIdx.x / TY, ty = threadIdx.x - (threadIdx.x / TY) * TY;
-  const int x = x0 + tx, y = y0 + ty, i = tx + 1, j = ty + 1, c = LI(i, j);
-  const bool valid = (x < g.mx) && (y < g.my);
-  const R cst = D.obstacle ? D.jat_obst : D.jat_well;
-  R ph[N], dp[N], m[K], nph[N], nm[K];
-  double dmu[K];
+  double emax[K], emin[K];
 #pragma unroll
-  for (int a = 0; a < N; a++) { ph[a] = a == p ? R(1.0) : R(0.0); dp[a] = R(0.0); nph[a] = ph[a]; }
-#pragma unroll
-  for (int k = 0; k < K; k++) { nm[k] = R(0.0); dmu[k] = 0.0; }
-  if (valid) {
-#pragma unroll
-    for (int k = 0; k < K; k++) m[k] = M[k][c];
-    /* the bulk expressions of the general path (update_tile's uniform path) */
-    R cn[K];
+  for (int k = 0; k < K; k++) { emax[k] = -INFINITY; emin[k] = INFINITY; }
+  int cur_sim = -1;
+  auto flush = [&](int s) {
 #pragma unroll
     for (int k = 0; k < K; k++) {
-      R divflux = R(0.0);
+      const double a = warp_max(emax[k]), c = warp_min(emin[k]);
+      if (lane == 0 && st.ext) {
+        long long *slot = st.ext + (long long)s * (2 * (N + K));
+        if (a > -INFINITY) atomicMax(slot + 2 * N + k, ord(a));
+        if (c < INFINITY) atomicMin(slot + 2 * N + K + k, ord(c));
+      }
+      emax[k] = -INFINITY;
+      emin[k] = INFINITY;
+    }
+  };
+
+  /* next bulk tile of the range (the others go on the interface list) */
+  int tn = t0;
+  auto advance = [&](int &phase) -> int {
+    while (tn < t1) {
+      const int t = tn++;
+      const int s = __ldg(tsim + t);
+      const SimDesc &sd = sims[s];
+      const int lt = t - sd.tile0, by = lt / sd.tiles_x, bx = lt - by * sd.tiles_x;
+      const int p = bulk_phase<R>(consts[s], sd.g, flag_in, sd.tile0, sd.tiles_x, by, bx);
+      if (p >= 0) {
+        phase = p;
+        return t;
+      }
+      if (lane == 0) glist[atomicAdd(ctr + CTR_LIST, 1)] = t;
+    }
+    return -1;
+  };
+  /* start copying tile t's mu with its halo into stage b */
+  auto issue = [&](int t, int b) {
+    const int s = __ldg(tsim + t);
+    const SimDesc &sd = sims[s];
+    const Consts<R> &D = consts[s];
+    const Grid g = sd.g;
+    const int lt = t - sd.tile0, by = lt / sd.tiles_x, bx = lt - by * sd.tiles_x;
+    const int x0 = by * TX, y0 = bx * TY;
+    const R *mu = state + sd.off_state + (long long)N * g.plane;
+    const int bx0 = D.bc_x[1][0], bx1 = D.bc_x[1][1], by0 = D.bc_y[1][0], by1 = D.bc_y[1][1];
+    for (int e = lane; e < SH * SW; e += 32) {
+      const int i = e / SW, j = e - i * SW;
+      int x = x0 - 1 + i, y = y0 - 1 + j;
+      if (x <= g.mx && y <= g.my) {
+        if (x < 0 || x >= g.mx) x = remap(x, g.mx, bx0, bx1);
+        if (y < 0 || y >= g.my) y = remap(y, g.my, by0, by1);
+        const R *src = mu + (long long)x * g.pitch + y;
+#pragma unroll
+        for (int k = 0; k < K; k++) cp_async_elem(&stg.M[b][k][i][j], src + (long long)k * g.plane);
+      } else {
+#pragma unroll
+        for (int k = 0; k < K; k++) stg.M[b][k][i][j] = R(0.0);
+      }
+    }
+    cp_async_commit();
+  };
+
+  int pc = -1, pn = -1;
+  int tc = advance(pc);
+  if (tc >= 0) issue(tc, 0);
+  int b = 0;
+  while (tc >= 0) {
+    const int tnx = advance(pn);
+    if (tnx >= 0) {
+      issue(tnx, b ^ 1);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncwarp();
+
+    /* ---- step bulk tile tc (phase pc) from stage b */
+    const int t = tc, p = pc;
+    const int s = __ldg(tsim + t);
+    if (s != cur_sim) {
+      if (cur_sim >= 0) flush(cur_sim);
+      cur_sim = s;
+    }
+    const SimDesc &sd = sims[s];
+    const Consts<R> &D = consts[s];
+    const Grid g = sd.g;
+    const int lt = t - sd.tile0, by = lt / sd.tiles_x, bx = lt - by * sd.tiles_x;
+    const int x0 = by * TX, y0 = bx * TY;
+    const int have = flag_out[t];
+    const R idx = D.inv_dx, idy = D.inv_dy, ddx = D.dx, ddy = D.dy, dt = D.dt;
+    const R cst = D.obstacle ? D.jat_obst : D.jat_well;
+    R dmf[K][K];
+#pragma unroll
+    for (int k = 0; k < K; k++)
 #pragma unroll
       for (int l = 0; l < K; l++) {
-        const R *Ml = M[l];
         const R Dv = D.Dbulk[p][k][l];
-        const R dm = (Dv + Dv) * R(0.5);
-        R fx = dm * divx(Ml[LI(i + 1, j)] - Ml[c], D), bx_ = dm * divx(Ml[c] - Ml[LI(i - 1, j)], D);
-        R fy = dm * divy(Ml[LI(i, j + 1)] - Ml[c], D), by_ = dm * divy(Ml[c] - Ml[LI(i, j - 1)], D);
-        divflux += divx(fx - bx_, D);
-        divflux += divy(fy - by_, D);
+        dmf[k][l] = (Dv + Dv) * R(0.5);
       }
-      R divjat = divx((R(0.0) - R(0.0)) * cst, D);
-      divjat += divy((R(0.0) - R(0.0)) * cst, D);
-      if constexpr (sizeof(R) == 8) cn[k] = c_mu<R, K>(D, m, p, k) + D.dt * (divflux) - divjat;
-      else cn[k] = D.dt * divflux - divjat;
-    }
-    if constexpr (sizeof(R) == 8) {
+    /* constants of c_mu / Mu of phase p (FP64 update) */
+    R cmu[K][K], E[K], twoA[K], Aoff[K][K];
+    double muc[K][K];
 #pragma unroll
-      for (int k = 0; k < K; k++) {
-        nm[k] = Mu<R, K>(D, cn, p, k);
-        dmu[k] = (double)nm[k] - (double)m[k];
+    for (int k = 0; k < K; k++) {
+      E[k] = D.E[p][k];
+      twoA[k] = D.twoA[p][k];
+#pragma unroll
+      for (int l = 0; l < K; l++) { cmu[k][l] = D.cmu[p][k][l]; Aoff[k][l] = D.A[p][k][l]; muc[k][l] = D.muc64[p][k][l]; }
+    }
+    const unsigned rkey = sizeof(R) == 4 ? __ldg(st.round_step) : 0u;
+    R *phin = next + sd.off_state;
+    R *mun = phin + (long long)N * g.plane;
+    const int y = y0 + lane, j = lane + 1;
+    const bool yvalid = y < g.my;
+    const int rows = min(TX, g.mx - x0);
+    double acc[SUMS ? NS : 1];
+#pragma unroll
+    for (int f = 0; f < (SUMS ? NS : 1); f++) acc[f] = 0.0;
+    if (yvalid) {
+#pragma unroll 1
+      for (int i = 1; i <= rows; i++) {
+        const int x = x0 + i - 1;
+        R m[K], cn[K], nm[K];
+        double dmu[K];
+#pragma unroll
+        for (int k = 0; k < K; k++) m[k] = stg.M[b][k][i][j];
+        /* the bulk expressions of the general path (update_tile's uniform path) */
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+          R divflux = R(0.0);
+#pragma unroll
+          for (int l = 0; l < K; l++) {
+            const R dm = dmf[k][l], c = stg.M[b][l][i][j];
+            R fx = dm * bdiv<MUL>(stg.M[b][l][i + 1][j] - c, idx, ddx);
+            R bx_ = dm * bdiv<MUL>(c - stg.M[b][l][i - 1][j], idx, ddx);
+            R fy = dm * bdiv<MUL>(stg.M[b][l][i][j + 1] - c, idy, ddy);
+            R by_ = dm * bdiv<MUL>(c - stg.M[b][l][i][j - 1], idy, ddy);
+            divflux += bdiv<MUL>(fx - bx_, idx, ddx);
+            divflux += bdiv<MUL>(fy - by_, idy, ddy);
+          }
+          R divjat = bdiv<MUL>((R(0.0) - R(0.0)) * cst, idx, ddx);
+          divjat += bdiv<MUL>((R(0.0) - R(0.0)) * cst, idy, ddy);
+          if constexpr (sizeof(R) == 8) {
+            R cm = R(0.0);   /* c_mu (functionF_01.h:30-37) */
+#pragma unroll
+            for (int l = 0; l < K; l++) cm += cmu[k][l] * (m[l] - E[l]);
+            cn[k] = cm + dt * (divflux) - divjat;
+          } else {
+            cn[k] = dt * divflux - divjat;
+          }
+        }
+        const long long o = (long long)x * g.pitch + y;
+        if constexpr (sizeof(R) == 8) {
+#pragma unroll
+          for (int k = 0; k < K; k++) {
+            R sm = twoA[k] * cn[k] + E[k];   /* Mu (functionF_01.h:19-29) */
+#pragma unroll
+            for (int l = 0; l < K; l++)
+              if (k != l) sm += Aoff[k][l] * cn[l];
+            nm[k] = sm;
+            dmu[k] = (double)nm[k] - (double)m[k];
+          }
+        } else {
+          const unsigned key = round_key(rkey, x, y);
+#pragma unroll
+          for (int k = 0; k < K; k++) {
+            double sdm = 0.0;
+#pragma unroll
+            for (int l = 0; l < K; l++) sdm += muc[k][l] * (double)cn[l];
+            dmu[k] = sdm;
+            nm[k] = (R)round_stochastic((double)m[k] + sdm, key, N + k);
+          }
+        }
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+          mun[k * g.plane + o] = nm[k];
+          const double w = (double)nm[k];
+          if (w == w) { emax[k] = fmax(emax[k], w); emin[k] = fmin(emin[k], w); }
+        }
+        if (have != p) {
+#pragma unroll
+          for (int a = 0; a < N; a++) phin[a * g.plane + o] = a == p ? R(1.0) : R(0.0);
+        }
+        if constexpr (SUMS) {
+          R nph[N];
+#pragma unroll
+          for (int a = 0; a < N; a++) nph[a] = a == p ? R(1.0) : R(0.0);
+#pragma unroll
+          for (int k = 0; k < K; k++) acc[N + k] += dmu[k] * dmu[k];
+#pragma unroll
+          for (int a = 0; a < N; a++) acc[N + K + a] += (double)nph[a];
+#pragma unroll
+          for (int k = 0; k < K; k++) {
+            R comp = R(0.0);
+#pragma unroll
+            for (int b2 = 0; b2 < N; b2++) comp += c_mu<R, K>(D, nm, b2, k) * h<R, N>(nph, b2);
+            acc[2 * N + K + k] += (double)comp;
+          }
+          bool bad = false;
+#pragma unroll
+          for (int k = 0; k < K; k++) bad |= !isfinite(nm[k]);
+          acc[NS - 1] += bad ? 1.0 : 0.0;
+        }
       }
-#pragma unroll
-      for (int a = 0; a < N; a++) nph[a] = ph[a] + dp[a];
-    } else {
-      bulk_commit_f32<R, N, K>(D, p, cn, ph, dp, m, nph, nm, dmu, round_key(__ldg(st.round_step), x, y));
     }
-    const long long o = (long long)x * g.pitch + y;
+    if constexpr (SUMS) {
 #pragma unroll
-    for (int k = 0; k < K; k++) mun[k * g.plane + o] = nm[k];
-    if (s_have != p) {
-#pragma unroll
-      for (int a = 0; a < N; a++) phin[a * g.plane + o] = nph[a];
+      for (int f = 0; f < NS; f++) {
+        const double r = warp_sum(acc[f]);
+        if (lane == 0) st.partials[(long long)t * NS + f] = r;
+      }
     }
+    if (lane == 0) flag_out[t] = (signed char)p;
+    __syncwarp();   /* stage b is refilled by the next issue */
+    tc = tnx;
+    pc = pn;
+    b ^= 1;
   }
-  block_stats<R, N, K, true>(D, valid, nph, nm, dp, dmu, st, t);
-  if (threadIdx.x == 0) flag_out[t] = (signed char)p;
+  if (cur_sim >= 0) flush(cur_sim);
 }
 
 /* Persistent CTAs over the interface list.  Each simulation's constants are
@@ -716,7 +884,8 @@ __global__ void __launch_bounds__(NT, (N <= 3 ? 2 : 1)) kf_general(const SimDesc
     const R *ph = state + sd.off_state;
     R *nx = next + sd.off_state;
     const signed char f = general_tile<R, N, K, ANISO>(sc, sd.g, ph, ph + (long long)N * sd.g.plane, nx,
-                                                       nx + (long long)N * sd.g.plane, by * TX, bx * TY, st, t, sm);
+                                                       nx + (long long)N * sd.g.plane, by * TX, bx * TY, st, s, t,
+                                                       sm);
     if (threadIdx.x == 0) flag_out[t] = f;
     __syncthreads();
   }

@@ -410,7 +410,7 @@ __device__ __forceinline__ long long ord(double v) {
 }
 
 struct StatBufs {
-  long long *ext;      /* per-tile running extremes [tiles][2*(N+K)] (ordered ints), or NULL */
+  long long *ext;      /* running extremes [simulations][2*(N+K)] (ordered ints, atomic max/min), or NULL */
   double *partials;    /* [tiles][2N+2K+1] sums when want_sums */
   int want_sums;
   const unsigned *round_step;  /* FP32 form: device step counter keying the rounding stream */
@@ -467,14 +467,16 @@ __device__ __forceinline__ void bulk_commit_f32(const Consts<R> &D, int a, const
   for (int a2 = 0; a2 < N; a2++) nph[a2] = (R)round_stochastic((double)ph[a2] + (double)dp[a2], key, a2);
 }
 
-/* Per-tile running extremes and (on request) FP64 sums of the cells a tile
- * owns.  Each tile owns its slots, so no atomics are needed and results are
- * deterministic; the host folds the slots when it reports.  UNI: every valid
- * cell of the tile holds the same phi (uniform tile), so the phi extremes are
- * thread 0's values and only mu is reduced. */
+/* Running extremes and (on request) FP64 sums of the cells a tile owns.
+ * Extremes go to the simulation's slots (ext_slot) by atomic max/min on the
+ * ordered integer image (exact and order-free, so deterministic); the sums go
+ * to the tile's own slot (sum_slot) and the host folds the slots in a fixed
+ * order.  UNI: every valid cell of the tile holds the same phi (uniform tile),
+ * so the phi extremes are thread 0's values and only mu is reduced. */
 template <typename R, int N, int K, bool UNI = false>
 __device__ __forceinline__ void block_stats(const Consts<R> &D, bool valid, const R *nph, const R *nm, const R *dp,
-                                            const double *dmu, const StatBufs &st, long long slot) {
+                                            const double *dmu, const StatBufs &st, long long ext_slot,
+                                            long long sum_slot) {
   constexpr int NE = 2 * (N + K), NS = 2 * N + 2 * K + 1, NW = NT / 32;
   __shared__ double red[NW][NE > NS ? NE : NS];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -504,9 +506,9 @@ __device__ __forceinline__ void block_stats(const Consts<R> &D, bool valid, cons
         for (int w = 1; w < NW; w++) r = isMax ? fmax(r, red[w][f]) : fmin(r, red[w][f]);
       /* slot layout: max phi[N], min phi[N], max mu[K], min mu[K] */
       const int sl = fld < N ? (isMax ? fld : N + fld) : (isMax ? 2 * N + (fld - N) : 2 * N + K + (fld - N));
-      long long *p = st.ext + slot * NE + sl;
-      if (isMax && r > -INFINITY && ord(r) > *p) *p = ord(r);
-      if (!isMax && r < INFINITY && ord(r) < *p) *p = ord(r);
+      long long *p = st.ext + ext_slot * NE + sl;
+      if (isMax && r > -INFINITY) atomicMax(p, ord(r));
+      if (!isMax && r < INFINITY) atomicMin(p, ord(r));
     }
     __syncthreads();
   }
@@ -539,7 +541,7 @@ __device__ __forceinline__ void block_stats(const Consts<R> &D, bool valid, cons
     if (threadIdx.x < NS) {
       double r = 0.0;
       for (int w = 0; w < NW; w++) r += red[w][threadIdx.x];
-      st.partials[slot * NS + threadIdx.x] = r;
+      st.partials[sum_slot * NS + threadIdx.x] = r;
     }
     __syncthreads();
   }
@@ -784,7 +786,7 @@ __device__ __forceinline__ void update_tile(const Consts<R> &D, const Grid &g, c
 #pragma unroll
       for (int k = 0; k < K; k++) mun[k * g.plane + o] = nm[k];
     }
-    block_stats<R, N, K, true>(D, valid, nph, nm, dp, dmu, st, slot);
+    block_stats<R, N, K, true>(D, valid, nph, nm, dp, dmu, st, 0, slot);
     return;
   }
 
@@ -888,7 +890,7 @@ __device__ __forceinline__ void update_tile(const Consts<R> &D, const Grid &g, c
 #pragma unroll
     for (int k = 0; k < K; k++) mun[k * g.plane + o] = nm[k];
   }
-  block_stats<R, N, K>(D, valid, nph, nm, dp, dmu, st, slot);
+  block_stats<R, N, K>(D, valid, nph, nm, dp, dmu, st, 0, slot);
 }
 
 /* ------------------------------------------------------------------ */
