@@ -18,13 +18,13 @@ struct BatchLaunch {
   /* one step: bulk tiles + interface list, then the interface tiles */
   /* mul: every simulation's spacings are powers of two (x/dx == x*(1/dx)) */
   cudaError_t (*bulk)(int grid, int ntiles, bool mul, cudaStream_t s, const SimDesc *sims, const void *consts,
-                      const int *tsim, const void *state, void *next, const signed char *flag_in,
-                      signed char *flag_out, int *glist, int *ctr, StatBufs st);
+                      const int *tsim, const void *state, void *next, const TileFlags *flag_in,
+                      TileFlags *flag_out, int *glist, int *ctr, StatBufs st);
   cudaError_t (*general)(int grid, cudaStream_t s, const SimDesc *sims, const void *consts, const int *tsim,
-                         const void *state, void *next, signed char *flag_out, const int *glist, int *ctr,
+                         const void *state, void *next, TileFlags *flag_out, const int *glist, int *ctr,
                          StatBufs st);
   cudaError_t (*flags)(int ntiles, cudaStream_t s, const SimDesc *sims, const int *tsim, const void *state,
-                       signed char *flags);
+                       TileFlags *flags);
   cudaError_t (*sdphi)(cudaStream_t s, const void *consts, const void *phi, void *dphi, Grid g);
   cudaError_t (*supd)(cudaStream_t s, const void *consts, const void *phi, const void *mu, const void *dphi,
                       void *phin, void *mun, Grid g);
@@ -52,8 +52,8 @@ struct BatchKernels {
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bg, kf_general<R, N, K, A>, NT, sizeof(GenSmem<R, N, K>));
   }
   static cudaError_t bulk(int grid, int ntiles, bool mul, cudaStream_t s, const SimDesc *sims, const void *consts,
-                          const int *tsim, const void *state, void *next, const signed char *flag_in,
-                          signed char *flag_out, int *glist, int *ctr, StatBufs st) {
+                          const int *tsim, const void *state, void *next, const TileFlags *flag_in,
+                          TileFlags *flag_out, int *glist, int *ctr, StatBufs st) {
 #define GP_BULK(SUMS, MUL)                                                                                       \
   kf_bulk<R, N, K, SUMS, MUL><<<grid, NT, bulk_smem, s>>>(sims, (const Consts<R> *)consts, tsim, ntiles,         \
                                                           (const R *)state, (R *)next, flag_in, flag_out, glist, \
@@ -69,14 +69,14 @@ struct BatchKernels {
     return cudaGetLastError();
   }
   static cudaError_t general(int grid, cudaStream_t s, const SimDesc *sims, const void *consts, const int *tsim,
-                             const void *state, void *next, signed char *flag_out, const int *glist, int *ctr,
+                             const void *state, void *next, TileFlags *flag_out, const int *glist, int *ctr,
                              StatBufs st) {
     kf_general<R, N, K, A><<<grid, NT, sizeof(GenSmem<R, N, K>), s>>>(
         sims, (const Consts<R> *)consts, tsim, (const R *)state, (R *)next, flag_out, glist, ctr, st);
     return cudaGetLastError();
   }
   static cudaError_t flags(int ntiles, cudaStream_t s, const SimDesc *sims, const int *tsim, const void *state,
-                           signed char *fl) {
+                           TileFlags *fl) {
     kf_flags<R, N><<<ntiles, NT, 0, s>>>(sims, tsim, (const R *)state, fl);
     return cudaGetLastError();
   }

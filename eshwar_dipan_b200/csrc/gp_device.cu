@@ -264,7 +264,7 @@ struct gp_batch {
   int *d_tsim, *d_seg0, *d_segn;
   void *state[2];               /* ping-pong: every simulation's N phi then K mu planes */
   void *dphi;                   /* delta-phi planes of the smoothing sweeps */
-  signed char *flags[2];        /* per tile and state buffer: one-hot phase, or mixed/unknown */
+  gpd::TileFlags *flags[2];     /* per tile and state buffer: one-hot phase of the tile and its edge bands */
   int *glist;                   /* interface tiles of the current step */
   int *counters;                /* gpd::CTR_* */
   int cur;
@@ -319,7 +319,8 @@ static int batch_step_once(gp_batch *b, int want_sums, cudaEvent_t *ev) {
  * unknown (it is rewritten in full by the next step). */
 static int batch_reflag(gp_batch *b, bool other_unknown) {
   BK(b->L.flags(b->ntiles, b->stream, b->d_desc, b->d_tsim, b->state[b->cur], b->flags[b->cur]));
-  if (other_unknown) BK(cudaMemsetAsync(b->flags[b->cur ^ 1], 0xfe, (size_t)b->ntiles, b->stream));
+  if (other_unknown)
+    BK(cudaMemsetAsync(b->flags[b->cur ^ 1], 0xfe, sizeof(gpd::TileFlags) * (size_t)b->ntiles, b->stream));
   return GP_OK;
 }
 
@@ -568,7 +569,7 @@ int gp_batch_create(gp_batch **out, int nsims, const gp_params *params, const do
   BALLOC(b->state[0], (size_t)off * b->elem);
   BALLOC(b->state[1], (size_t)off * b->elem);
   BALLOC(b->dphi, (size_t)offd * b->elem);
-  BALLOC(b->flags[0], 2 * (size_t)nt);
+  BALLOC(b->flags[0], 2 * sizeof(gpd::TileFlags) * (size_t)nt);
   b->flags[1] = b->flags[0] + nt;
   BALLOC(b->glist, sizeof(int) * (size_t)nt);
   BALLOC(b->d_desc, sizeof(gpd::SimDesc) * nsims);

@@ -42,6 +42,15 @@ constexpr int RYF = (TX + 2) * (TY + 3);                 /* y-faces around the r
 
 constexpr signed char FLAG_MIXED = -1, FLAG_UNKNOWN = -2;
 
+/* Phase flags of one tile in one state buffer: for the whole tile and for its
+ * four two-cell-deep edge bands (top = first two rows, bot = last two rows,
+ * left/right = first/last two columns, over the tile's cells inside the
+ * domain): the phase p whose exact one-hot phi every cell of the region holds,
+ * FLAG_MIXED, or FLAG_UNKNOWN.  8 bytes, read as one word. */
+struct __align__(8) TileFlags {
+  signed char whole, top, bot, left, right, pad0, pad1, pad2;
+};
+
 struct RemapTab2 {
   int row[H2], col[W2];
 };
@@ -79,37 +88,82 @@ __device__ __forceinline__ int one_hot(const R *ph) {
   return (ones == 1 && zeros == N - 1) ? p : -1;
 }
 
-/* Flag of a tile from its new phi, one value per thread (valid cells only):
- * the same phase everywhere or FLAG_MIXED.  Call with all threads. */
-__device__ __forceinline__ signed char tile_flag(bool valid, int p) {
-  __shared__ int s_p[NT / 32], s_bad[NT / 32];
+/* Flags of a tile from its new phi, one one-hot phase (or -1) per thread
+ * (cell (tx, ty) of the tile, valid cells only; rows x cols cells are in the
+ * domain).  Call with all threads; the result is valid in every thread. */
+__device__ __forceinline__ TileFlags tile_flags(bool valid, int p, int tx, int ty, int rows, int cols) {
+  __shared__ int s_lo[NT / 32][5], s_hi[NT / 32][5];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  /* a valid cell with p < 0 spoils the tile; valid cells must agree */
-  int mine = valid ? p : INT_MAX;
-  int lo = mine, hi = valid ? p : INT_MIN;
+  const bool in[5] = {true, tx < 2, tx >= rows - 2, ty < 2, ty >= cols - 2};
+  int lo[5], hi[5];
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
-    hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+  for (int r = 0; r < 5; r++) {
+    lo[r] = (valid && in[r]) ? p : INT_MAX;
+    hi[r] = (valid && in[r]) ? p : INT_MIN;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      lo[r] = min(lo[r], __shfl_xor_sync(0xffffffffu, lo[r], o));
+      hi[r] = max(hi[r], __shfl_xor_sync(0xffffffffu, hi[r], o));
+    }
   }
-  if (lane == 0) { s_p[wid] = lo; s_bad[wid] = hi; }
-  __syncthreads();
-  int l2 = INT_MAX, h2 = INT_MIN;
+  if (lane == 0) {
 #pragma unroll
-  for (int w = 0; w < NT / 32; w++) { l2 = min(l2, s_p[w]); h2 = max(h2, s_bad[w]); }
+    for (int r = 0; r < 5; r++) { s_lo[wid][r] = lo[r]; s_hi[wid][r] = hi[r]; }
+  }
   __syncthreads();
-  return (l2 >= 0 && l2 == h2) ? (signed char)l2 : FLAG_MIXED;
+  signed char f[5];
+#pragma unroll
+  for (int r = 0; r < 5; r++) {
+    int l2 = INT_MAX, h2 = INT_MIN;
+#pragma unroll
+    for (int w = 0; w < NT / 32; w++) { l2 = min(l2, s_lo[w][r]); h2 = max(h2, s_hi[w][r]); }
+    f[r] = (l2 >= 0 && l2 == h2) ? (signed char)l2 : FLAG_MIXED;
+  }
+  __syncthreads();
+  TileFlags t;
+  t.whole = f[0]; t.top = f[1]; t.bot = f[2]; t.left = f[3]; t.right = f[4];
+  t.pad0 = t.pad1 = t.pad2 = 0;
+  return t;
 }
 
-/* Bulk test of tile (tile rows by, columns bx) of a simulation: its flag and
- * the flags of the tiles holding every cell of its two-cell phi halo agree on
- * a phase.  Evaluated by one warp; returns the phase or -1. */
+__device__ __forceinline__ TileFlags uniform_flags(int p) {
+  TileFlags t;
+  t.whole = t.top = t.bot = t.left = t.right = (signed char)p;
+  t.pad0 = t.pad1 = t.pad2 = 0;
+  return t;
+}
+
+/* Bulk test of tile (tile rows by, columns bx) of a simulation: every cell
+ * of the tile and of its two-cell phi halo holds the exact one-hot phi of one
+ * phase.  Evaluated by one warp; returns the phase or -1.  When the halo stays
+ * inside the domain it is covered by the facing edge bands of the eight
+ * neighbour tiles (a corner by either band that contains it); otherwise the
+ * whole-tile flags of the tiles that hold the halo cells after the boundary
+ * remap are used. */
 template <typename R>
-__device__ __forceinline__ int bulk_phase(const Consts<R> &D, const Grid &g, const signed char *__restrict__ flags,
+__device__ __forceinline__ int bulk_phase(const Consts<R> &D, const Grid &g, const TileFlags *__restrict__ flags,
                                           int tile0, int tiles_x, int by, int bx) {
   const int lane = threadIdx.x & 31;
   const int x0 = by * TX, y0 = bx * TY;
   const int xl = min(x0 + TX, g.mx) - 1, yl = min(y0 + TY, g.my) - 1;
+  if (x0 >= 2 && xl + 2 < g.mx && y0 >= 2 && yl + 2 < g.my) {
+    TileFlags F = uniform_flags(0);
+    if (lane < 9) F = flags[tile0 + (by + lane / 3 - 1) * tiles_x + (bx + lane % 3 - 1)];
+    const int own = __shfl_sync(0xffffffffu, (int)F.whole, 4);
+    bool ok = true;
+    switch (lane) {
+      case 0: ok = F.bot == own || F.right == own; break;   /* up-left */
+      case 1: ok = F.bot == own; break;                     /* up */
+      case 2: ok = F.bot == own || F.left == own; break;    /* up-right */
+      case 3: ok = F.right == own; break;                   /* left */
+      case 5: ok = F.left == own; break;                    /* right */
+      case 6: ok = F.top == own || F.right == own; break;   /* down-left */
+      case 7: ok = F.top == own; break;                     /* down */
+      case 8: ok = F.top == own || F.left == own; break;    /* down-right */
+      default: break;
+    }
+    return (__all_sync(0xffffffffu, ok) && own >= 0) ? own : -1;
+  }
   /* candidate tile rows: own, and the tiles of rows x0-2, x0-1, xl+1, xl+2 */
   int rows[5], cols[5];
   {
@@ -129,7 +183,7 @@ __device__ __forceinline__ int bulk_phase(const Consts<R> &D, const Grid &g, con
   int f = 0x7f;
   if (lane < 25) {
     const int r = lane / 5, c = lane - r * 5;
-    f = flags[tile0 + rows[r] * tiles_x + cols[c]];
+    f = flags[tile0 + rows[r] * tiles_x + cols[c]].whole;
   }
   const int own = __shfl_sync(0xffffffffu, f, 0);
   const bool ok = lane >= 25 || f == own;
@@ -369,10 +423,9 @@ __device__ __forceinline__ void ring_dphi(const Consts<R> &D, const GenSmem<R, N
  * ring, then the concentration pass (calculate_fluxes_concentration_2D +
  * calculate_divergence_concentration_2D, calculate_fluxes_concentration.h:4-145,
  * calculate_divergence_concentration.h:4-153) and the phi commit, in the
- * arithmetic of update_tile's general path.  Returns the tile's new flag
- * (valid in thread 0). */
+ * arithmetic of update_tile's general path.  Returns the tile's new flags. */
 template <typename R, int N, int K, bool ANISO>
-__device__ __forceinline__ signed char general_tile(const Consts<R> &D, const Grid &g, const R *__restrict__ phi,
+__device__ __forceinline__ TileFlags general_tile(const Consts<R> &D, const Grid &g, const R *__restrict__ phi,
                                                     const R *__restrict__ mu, R *__restrict__ phin,
                                                     R *__restrict__ mun, int x0, int y0, const StatBufs &st,
                                                     long long ext_slot, long long slot, GenSmem<R, N, K> &sm) {
@@ -570,7 +623,7 @@ __device__ __forceinline__ signed char general_tile(const Consts<R> &D, const Gr
 #undef PRIJ
 #undef PR
   block_stats<R, N, K>(D, valid, nph, nm, dp, dmu, st, ext_slot, slot);
-  return tile_flag(valid, oh);
+  return tile_flags(valid, oh, tx, ty, min(TX, g.mx - x0), min(TY, g.my - y0));
 }
 
 /* ------------------------------------------------------------------ */
@@ -621,8 +674,8 @@ struct BulkWarpStage {
 template <typename R, int N, int K, bool SUMS, bool MUL>
 __global__ void __launch_bounds__(NT, 2) kf_bulk(const SimDesc *__restrict__ sims, const Consts<R> *__restrict__ consts,
                                                  const int *__restrict__ tsim, int ntiles, const R *__restrict__ state,
-                                                 R *__restrict__ next, const signed char *__restrict__ flag_in,
-                                                 signed char *__restrict__ flag_out, int *__restrict__ glist,
+                                                 R *__restrict__ next, const TileFlags *__restrict__ flag_in,
+                                                 TileFlags *__restrict__ flag_out, int *__restrict__ glist,
                                                  int *__restrict__ ctr, StatBufs st) {
   constexpr int NW = NT / 32, NS = 2 * N + 2 * K + 1;
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -720,7 +773,7 @@ __global__ void __launch_bounds__(NT, 2) kf_bulk(const SimDesc *__restrict__ sim
     const Grid g = sd.g;
     const int lt = t - sd.tile0, by = lt / sd.tiles_x, bx = lt - by * sd.tiles_x;
     const int x0 = by * TX, y0 = bx * TY;
-    const int have = flag_out[t];
+    const int have = flag_out[t].whole;
     const R idx = D.inv_dx, idy = D.inv_dy, ddx = D.dx, ddy = D.dy, dt = D.dt;
     const R cst = D.obstacle ? D.jat_obst : D.jat_well;
     R dmf[K][K];
@@ -844,7 +897,7 @@ __global__ void __launch_bounds__(NT, 2) kf_bulk(const SimDesc *__restrict__ sim
         if (lane == 0) st.partials[(long long)t * NS + f] = r;
       }
     }
-    if (lane == 0) flag_out[t] = (signed char)p;
+    if (lane == 0) flag_out[t] = uniform_flags(p);
     __syncwarp();   /* stage b is refilled by the next issue */
     tc = tnx;
     pc = pn;
@@ -859,7 +912,7 @@ template <typename R, int N, int K, bool ANISO>
 __global__ void __launch_bounds__(NT, (N <= 3 ? 2 : 1)) kf_general(const SimDesc *__restrict__ sims,
                                                  const Consts<R> *__restrict__ consts, const int *__restrict__ tsim,
                                                  const R *__restrict__ state, R *__restrict__ next,
-                                                 signed char *__restrict__ flag_out, const int *__restrict__ glist,
+                                                 TileFlags *__restrict__ flag_out, const int *__restrict__ glist,
                                                  int *__restrict__ ctr, StatBufs st) {
   extern __shared__ __align__(16) unsigned char smraw[];
   GenSmem<R, N, K> &sm = *reinterpret_cast<GenSmem<R, N, K> *>(smraw);
@@ -883,7 +936,7 @@ __global__ void __launch_bounds__(NT, (N <= 3 ? 2 : 1)) kf_general(const SimDesc
     const int lt = t - sd.tile0, by = lt / sd.tiles_x, bx = lt - by * sd.tiles_x;
     const R *ph = state + sd.off_state;
     R *nx = next + sd.off_state;
-    const signed char f = general_tile<R, N, K, ANISO>(sc, sd.g, ph, ph + (long long)N * sd.g.plane, nx,
+    const TileFlags f = general_tile<R, N, K, ANISO>(sc, sd.g, ph, ph + (long long)N * sd.g.plane, nx,
                                                        nx + (long long)N * sd.g.plane, by * TX, bx * TY, st, s, t,
                                                        sm);
     if (threadIdx.x == 0) flag_out[t] = f;
@@ -908,7 +961,7 @@ __global__ void __launch_bounds__(NT, (N <= 3 ? 2 : 1)) kf_general(const SimDesc
  * smoothing or gp_batch_set). */
 template <typename R, int N>
 __global__ void __launch_bounds__(NT) kf_flags(const SimDesc *__restrict__ sims, const int *__restrict__ tsim,
-                                               const R *__restrict__ state, signed char *__restrict__ flags) {
+                                               const R *__restrict__ state, TileFlags *__restrict__ flags) {
   const int t = blockIdx.x;
   const SimDesc sd = sims[__ldg(tsim + t)];
   const int lt = t - sd.tile0, by = lt / sd.tiles_x, bx = lt - by * sd.tiles_x;
@@ -922,7 +975,7 @@ __global__ void __launch_bounds__(NT) kf_flags(const SimDesc *__restrict__ sims,
     for (int a = 0; a < N; a++) ph[a] = __ldg(state + sd.off_state + a * sd.g.plane + (long long)x * sd.g.pitch + y);
     oh = one_hot<R, N>(ph);
   }
-  const signed char f = tile_flag(valid, oh);
+  const TileFlags f = tile_flags(valid, oh, tx, ty, min(TX, sd.g.mx - by * TX), min(TY, sd.g.my - bx * TY));
   if (threadIdx.x == 0) flags[t] = f;
 }
 
