@@ -20,7 +20,7 @@ struct BatchLaunch {
   cudaError_t (*bulk)(int grid, int ntiles, bool mul, cudaStream_t s, const SimDesc *sims, const void *consts,
                       const int *tsim, const void *state, void *next, const TileFlags *flag_in,
                       TileFlags *flag_out, int *glist, int *ctr, StatBufs st);
-  cudaError_t (*general)(int grid, cudaStream_t s, const SimDesc *sims, const void *consts, const int *tsim,
+  cudaError_t (*general)(int grid, bool mul, cudaStream_t s, const SimDesc *sims, const void *consts, const int *tsim,
                          const void *state, void *next, TileFlags *flag_out, const int *glist, int *ctr,
                          StatBufs st);
   cudaError_t (*flags)(int ntiles, cudaStream_t s, const SimDesc *sims, const int *tsim, const void *state,
@@ -40,8 +40,11 @@ struct BatchKernels {
                                 (int)bulk_smem);
   }
   static cudaError_t prepare(int *bb, int *bg) {
-    cudaError_t e = cudaFuncSetAttribute(kf_general<R, N, K, A>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t e = cudaFuncSetAttribute(kf_general<R, N, K, A, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)sizeof(GenSmem<R, N, K>));
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(kf_general<R, N, K, A, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)sizeof(GenSmem<R, N, K>));
     if (e == cudaSuccess) e = bulk_attr<false, false>();
     if (e == cudaSuccess) e = bulk_attr<false, true>();
     if (e == cudaSuccess) e = bulk_attr<true, false>();
@@ -49,7 +52,8 @@ struct BatchKernels {
     if (e != cudaSuccess) return e;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(bb, kf_bulk<R, N, K, false, true>, NT, bulk_smem);
     if (e != cudaSuccess) return e;
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bg, kf_general<R, N, K, A>, NT, sizeof(GenSmem<R, N, K>));
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bg, kf_general<R, N, K, A, true>, NT,
+                                                         sizeof(GenSmem<R, N, K>));
   }
   static cudaError_t bulk(int grid, int ntiles, bool mul, cudaStream_t s, const SimDesc *sims, const void *consts,
                           const int *tsim, const void *state, void *next, const TileFlags *flag_in,
@@ -68,11 +72,15 @@ struct BatchKernels {
 #undef GP_BULK
     return cudaGetLastError();
   }
-  static cudaError_t general(int grid, cudaStream_t s, const SimDesc *sims, const void *consts, const int *tsim,
-                             const void *state, void *next, TileFlags *flag_out, const int *glist, int *ctr,
-                             StatBufs st) {
-    kf_general<R, N, K, A><<<grid, NT, sizeof(GenSmem<R, N, K>), s>>>(
-        sims, (const Consts<R> *)consts, tsim, (const R *)state, (R *)next, flag_out, glist, ctr, st);
+  static cudaError_t general(int grid, bool mul, cudaStream_t s, const SimDesc *sims, const void *consts,
+                             const int *tsim, const void *state, void *next, TileFlags *flag_out, const int *glist,
+                             int *ctr, StatBufs st) {
+    if (mul)
+      kf_general<R, N, K, A, true><<<grid, NT, sizeof(GenSmem<R, N, K>), s>>>(
+          sims, (const Consts<R> *)consts, tsim, (const R *)state, (R *)next, flag_out, glist, ctr, st);
+    else
+      kf_general<R, N, K, A, false><<<grid, NT, sizeof(GenSmem<R, N, K>), s>>>(
+          sims, (const Consts<R> *)consts, tsim, (const R *)state, (R *)next, flag_out, glist, ctr, st);
     return cudaGetLastError();
   }
   static cudaError_t flags(int ntiles, cudaStream_t s, const SimDesc *sims, const int *tsim, const void *state,

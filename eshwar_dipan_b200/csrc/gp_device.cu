@@ -307,7 +307,7 @@ static int batch_step_once(gp_batch *b, int want_sums, cudaEvent_t *ev) {
   BK(b->L.bulk(b->grid_b, b->ntiles, b->mul, b->stream, b->d_desc, b->d_consts, b->d_tsim, b->state[in],
                b->state[out], b->flags[in], b->flags[out], b->glist, b->counters, st));
   if (ev) BK(cudaEventRecord(ev[1], b->stream));
-  BK(b->L.general(b->grid_g, b->stream, b->d_desc, b->d_consts, b->d_tsim, b->state[in], b->state[out],
+  BK(b->L.general(b->grid_g, b->mul, b->stream, b->d_desc, b->d_consts, b->d_tsim, b->state[in], b->state[out],
                   b->flags[out], b->glist, b->counters, st));
   if (ev) BK(cudaEventRecord(ev[2], b->stream));
   b->cur = out;

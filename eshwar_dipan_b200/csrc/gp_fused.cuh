@@ -30,6 +30,7 @@
  */
 #pragma once
 #include <climits>
+#include <type_traits>
 
 #include "gp_tiles.cuh"
 
@@ -220,8 +221,8 @@ struct GenSmem {
  * arithmetic as face_terms (function_A_01.h:163-215 through functionQ.h and
  * anisotropy_01.h) on the two-cell-halo layout.  xface: face between P rows
  * i and i+1 at column j; else between columns j and j+1 of row i. */
-template <typename R, int N>
-__device__ __forceinline__ void ring_face_terms(const Consts<R> &D, const R (*P)[S2], R (*T)[4][RXF + RYF],
+template <typename R, int N, typename CT>
+__device__ __forceinline__ void ring_face_terms(const CT &D, const R (*P)[S2], R (*T)[4][RXF + RYF],
                                                 bool xface, int i, int j, int fidx) {
   R s[N], gr[N], c0[N], c1[N];
 #pragma unroll
@@ -275,8 +276,8 @@ __device__ __forceinline__ void ring_face_terms(const Consts<R> &D, const R (*P)
 /* delta-phi of one ring cell (ring coordinates ri, rj; its phi at P row ri+1,
  * column rj+1) from the staged tile: calculate_divergence_phasefield_2D
  * (calculate_divergence_phasefield.h:4-62) in the same arithmetic as dphi_tile. */
-template <typename R, int N, int K, bool ANISO>
-__device__ __forceinline__ void ring_dphi(const Consts<R> &D, const GenSmem<R, N, K> &sm, int ri, int rj,
+template <typename R, int N, int K, bool ANISO, typename CT>
+__device__ __forceinline__ void ring_dphi(const CT &D, const GenSmem<R, N, K> &sm, int ri, int rj,
                                           unsigned mask, R *d) {
   const int i = ri + 1, j = rj + 1, e = LI(ri, rj);
   R ph[N];
@@ -424,8 +425,8 @@ __device__ __forceinline__ void ring_dphi(const Consts<R> &D, const GenSmem<R, N
  * calculate_divergence_concentration_2D, calculate_fluxes_concentration.h:4-145,
  * calculate_divergence_concentration.h:4-153) and the phi commit, in the
  * arithmetic of update_tile's general path.  Returns the tile's new flags. */
-template <typename R, int N, int K, bool ANISO>
-__device__ __forceinline__ TileFlags general_tile(const Consts<R> &D, const Grid &g, const R *__restrict__ phi,
+template <typename R, int N, int K, bool ANISO, typename CT>
+__device__ __forceinline__ TileFlags general_tile(const CT &D, const Grid &g, const R *__restrict__ phi,
                                                     const R *__restrict__ mu, R *__restrict__ phin,
                                                     R *__restrict__ mun, int x0, int y0, const StatBufs &st,
                                                     long long ext_slot, long long slot, GenSmem<R, N, K> &sm) {
@@ -908,7 +909,7 @@ __global__ void __launch_bounds__(NT, 2) kf_bulk(const SimDesc *__restrict__ sim
 
 /* Persistent CTAs over the interface list.  Each simulation's constants are
  * copied into shared memory when a CTA moves to it. */
-template <typename R, int N, int K, bool ANISO>
+template <typename R, int N, int K, bool ANISO, bool MUL>
 __global__ void __launch_bounds__(NT, (N <= 3 ? 2 : 1)) kf_general(const SimDesc *__restrict__ sims,
                                                  const Consts<R> *__restrict__ consts, const int *__restrict__ tsim,
                                                  const R *__restrict__ state, R *__restrict__ next,
@@ -936,7 +937,8 @@ __global__ void __launch_bounds__(NT, (N <= 3 ? 2 : 1)) kf_general(const SimDesc
     const int lt = t - sd.tile0, by = lt / sd.tiles_x, bx = lt - by * sd.tiles_x;
     const R *ph = state + sd.off_state;
     R *nx = next + sd.off_state;
-    const TileFlags f = general_tile<R, N, K, ANISO>(sc, sd.g, ph, ph + (long long)N * sd.g.plane, nx,
+    using CT = typename std::conditional<MUL, ConstsMul<R>, Consts<R>>::type;
+    const TileFlags f = general_tile<R, N, K, ANISO>(static_cast<const CT &>(sc), sd.g, ph, ph + (long long)N * sd.g.plane, nx,
                                                        nx + (long long)N * sd.g.plane, by * TX, bx * TY, st, s, t,
                                                        sm);
     if (threadIdx.x == 0) flag_out[t] = f;

@@ -67,6 +67,19 @@ __device__ __forceinline__ R divy(R v, const Consts<R> &D) { return D.mul_dy ? v
 template <typename R>
 __device__ __forceinline__ R div2y(R v, const Consts<R> &D) { return D.mul_dy ? v * D.inv_2dy : v / (R(2.0) * D.dy); }
 
+/* The same constants when every spacing is known to be a power of two (or
+ * the field type is float): the divisions are multiplications by the exact
+ * reciprocals and no division code is emitted.  Kernels view their Consts
+ * through this type when the launch says so. */
+template <typename R>
+struct ConstsMul : Consts<R> {};
+template <typename R>
+__device__ __forceinline__ R divx(R v, const ConstsMul<R> &D) { return v * D.inv_dx; }
+template <typename R>
+__device__ __forceinline__ R divy(R v, const ConstsMul<R> &D) { return v * D.inv_dy; }
+template <typename R>
+__device__ __forceinline__ R div2y(R v, const ConstsMul<R> &D) { return v * D.inv_2dy; }
+
 /* pair index of a<b among N phases */
 template <int N>
 __device__ __forceinline__ constexpr int pidx(int a, int b) {
@@ -552,8 +565,8 @@ __device__ __forceinline__ void block_stats(const Consts<R> &D, bool valid, cons
  * branch (mu = Mu_a(c_a(mu) + dc)) or the interface branch (dmu = (dc/dmu)^-1 dc,
  * inverted in FP64), then phi += delta-phi.  i, j: the cell's position in the
  * one-cell-halo tile layout; x, y: its interior coordinates. */
-template <typename R, int N, int K>
-__device__ __forceinline__ void commit_cell(const Consts<R> &D, const R (&FX)[K][K][NXF], const R (&FY)[K][K][NYF],
+template <typename R, int N, int K, typename CT>
+__device__ __forceinline__ void commit_cell(const CT &D, const R (&FX)[K][K][NXF], const R (&FY)[K][K][NYF],
                                             const R (&JX)[K][NXF], const R (&JY)[K][NYF], const R (&CM)[N][K][SS],
                                             const R (&H)[N][SS], int i, int j, int x, int y, const R *ph,
                                             const R *dp, const R *m, R *nph, R *nm, double *dmu,
