@@ -7,6 +7,7 @@ The CUDA sources are compiled for sm_100a only, with FMA contraction off
 (--fmad=false) so that the FP64 step is bit-identical to the reference's
 C arithmetic; the host C files likewise use -ffp-contract=off.
 """
+import concurrent.futures
 import os
 import shlex
 import subprocess
@@ -56,6 +57,7 @@ def build(verbose=False, ptxas_info=False):
             _run([CC, "-O2", "-ffp-contract=off", "-fno-fast-math", "-fPIC", "-std=gnu11", "-Wall",
                   "-Wno-unused-function", *INC, "-c", src, "-o", obj], verbose)
         objs.append(obj)
+    jobs = []
     for f, flags in CUDA:
         src, obj = os.path.join(CSRC, f), os.path.join(BUILD, f + ".o")
         if _stale(obj, [src] + headers) or ptxas_info:
@@ -63,10 +65,13 @@ def build(verbose=False, ptxas_info=False):
                    "-Xcompiler", "-ffp-contract=off", *INC, "-c", src, "-o", obj]
             if ptxas_info:
                 cmd.insert(1, "-Xptxas=-v")
-            r = _run(cmd, verbose)
+            jobs.append(cmd)
+        objs.append(obj)
+    # the CUDA translation units are independent: compile them side by side
+    with concurrent.futures.ThreadPoolExecutor(max_workers=max(1, len(jobs))) as pool:
+        for r in pool.map(lambda c: _run(c, verbose), jobs):
             if ptxas_info and r.stderr:
                 sys.stderr.write(r.stderr)
-        objs.append(obj)
     lib = os.path.join(HERE, "libgp.so")
     if _stale(lib, objs):
         _run([NVCC, *ARCH, "-shared", "-cudart", "static", "-o", lib, *objs, "-lm"], verbose)

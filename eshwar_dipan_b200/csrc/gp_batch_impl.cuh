@@ -16,10 +16,12 @@ struct BatchLaunch {
   /* occupancy of the bulk and interface kernels (blocks per SM) */
   cudaError_t (*prepare)(int *blocks_per_sm_bulk, int *blocks_per_sm_general);
   /* one step: bulk tiles + interface list, then the interface tiles */
+  cudaError_t (*classify)(int ntiles, cudaStream_t s, const SimDesc *sims, const void *consts, const int *tsim,
+                          const TileFlags *flag_in, int *glist, int *blist, int *ctr);
   /* mul: every simulation's spacings are powers of two (x/dx == x*(1/dx)) */
-  cudaError_t (*bulk)(int grid, int ntiles, bool mul, cudaStream_t s, const SimDesc *sims, const void *consts,
-                      const int *tsim, const void *state, void *next, const TileFlags *flag_in,
-                      TileFlags *flag_out, int *glist, int *ctr, StatBufs st);
+  cudaError_t (*bulk)(int grid, bool mul, cudaStream_t s, const SimDesc *sims, const void *consts, const int *tsim,
+                      const int *blist, const void *state, void *next, TileFlags *flag_out, const int *ctr,
+                      StatBufs st);
   cudaError_t (*general)(int grid, bool mul, cudaStream_t s, const SimDesc *sims, const void *consts, const int *tsim,
                          const void *state, void *next, TileFlags *flag_out, const int *glist, int *ctr,
                          StatBufs st);
@@ -55,13 +57,18 @@ struct BatchKernels {
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bg, kf_general<R, N, K, A, true>, NT,
                                                          sizeof(GenSmem<R, N, K>));
   }
-  static cudaError_t bulk(int grid, int ntiles, bool mul, cudaStream_t s, const SimDesc *sims, const void *consts,
-                          const int *tsim, const void *state, void *next, const TileFlags *flag_in,
-                          TileFlags *flag_out, int *glist, int *ctr, StatBufs st) {
-#define GP_BULK(SUMS, MUL)                                                                                       \
-  kf_bulk<R, N, K, SUMS, MUL><<<grid, NT, bulk_smem, s>>>(sims, (const Consts<R> *)consts, tsim, ntiles,         \
-                                                          (const R *)state, (R *)next, flag_in, flag_out, glist, \
-                                                          ctr, st)
+  static cudaError_t classify(int ntiles, cudaStream_t s, const SimDesc *sims, const void *consts,
+                              const int *tsim, const TileFlags *flag_in, int *glist, int *blist, int *ctr) {
+    kf_classify<R><<<(ntiles + NT - 1) / NT, NT, 0, s>>>(sims, (const Consts<R> *)consts, tsim, ntiles, flag_in, glist,
+                                                         blist, ctr);
+    return cudaGetLastError();
+  }
+  static cudaError_t bulk(int grid, bool mul, cudaStream_t s, const SimDesc *sims, const void *consts,
+                          const int *tsim, const int *blist, const void *state, void *next, TileFlags *flag_out,
+                          const int *ctr, StatBufs st) {
+#define GP_BULK(SUMS, MUL)                                                                                     \
+  kf_bulk<R, N, K, SUMS, MUL><<<grid, NT, bulk_smem, s>>>(sims, (const Consts<R> *)consts, tsim, blist,         \
+                                                          (const R *)state, (R *)next, flag_out, ctr, st)
     if (st.want_sums) {
       if (mul) GP_BULK(true, true);
       else GP_BULK(true, false);
@@ -103,6 +110,7 @@ struct BatchKernels {
   static BatchLaunch table() {
     BatchLaunch t;
     t.prepare = prepare;
+    t.classify = classify;
     t.bulk = bulk;
     t.general = general;
     t.flags = flags;

@@ -266,6 +266,7 @@ struct gp_batch {
   void *dphi;                   /* delta-phi planes of the smoothing sweeps */
   gpd::TileFlags *flags[2];     /* per tile and state buffer: one-hot phase of the tile and its edge bands */
   int *glist;                   /* interface tiles of the current step */
+  int *blist;                   /* bulk tiles of the current step (tile | phase << 28) */
   int *counters;                /* gpd::CTR_* */
   int cur;
   long long *ext;               /* running extremes per simulation [nsims][2(N+K)] */
@@ -304,8 +305,10 @@ static int batch_step_once(gp_batch *b, int want_sums, cudaEvent_t *ev) {
   st.round_step = (const unsigned *)(b->counters + gpd::CTR_STEP);
   const int in = b->cur, out = b->cur ^ 1;
   if (ev) BK(cudaEventRecord(ev[0], b->stream));
-  BK(b->L.bulk(b->grid_b, b->ntiles, b->mul, b->stream, b->d_desc, b->d_consts, b->d_tsim, b->state[in],
-               b->state[out], b->flags[in], b->flags[out], b->glist, b->counters, st));
+  BK(b->L.classify(b->ntiles, b->stream, b->d_desc, b->d_consts, b->d_tsim, b->flags[in], b->glist, b->blist,
+                   b->counters));
+  BK(b->L.bulk(b->grid_b, b->mul, b->stream, b->d_desc, b->d_consts, b->d_tsim, b->blist, b->state[in],
+               b->state[out], b->flags[out], b->counters, st));
   if (ev) BK(cudaEventRecord(ev[1], b->stream));
   BK(b->L.general(b->grid_g, b->mul, b->stream, b->d_desc, b->d_consts, b->d_tsim, b->state[in], b->state[out],
                   b->flags[out], b->glist, b->counters, st));
@@ -452,6 +455,7 @@ void gp_batch_destroy(gp_batch *b) {
   cudaFree(b->dphi);
   cudaFree(b->flags[0]);   /* flags[1] is part of the same allocation */
   cudaFree(b->glist);
+  cudaFree(b->blist);
   cudaFree(b->d_desc);
   cudaFree(b->d_consts);
   cudaFree(b->d_tsim);
@@ -546,6 +550,11 @@ int gp_batch_create(gp_batch **out, int nsims, const gp_params *params, const do
     }
   }
   b->ntiles = nt;
+  if (nt >= (1 << 28)) {
+    rc = bfail(b, GP_EINVAL, "gp_batch_create: %d tiles of %dx%d cells, at most 2^28", nt, gpd::TX, gpd::TY);
+    gp_batch_destroy(b);
+    return rc;
+  }
   b->mul = true;
   for (int s = 0; s < nsims; s++)
     if (b->elem == 8 && !(pow2(b->derived[s].dx) && pow2(b->derived[s].dy))) b->mul = false;
@@ -572,6 +581,7 @@ int gp_batch_create(gp_batch **out, int nsims, const gp_params *params, const do
   BALLOC(b->flags[0], 2 * sizeof(gpd::TileFlags) * (size_t)nt);
   b->flags[1] = b->flags[0] + nt;
   BALLOC(b->glist, sizeof(int) * (size_t)nt);
+  BALLOC(b->blist, sizeof(int) * (size_t)nt);
   BALLOC(b->d_desc, sizeof(gpd::SimDesc) * nsims);
   BALLOC(b->d_consts, csz * nsims);
   BALLOC(b->d_tsim, sizeof(int) * (size_t)nt);
@@ -580,7 +590,7 @@ int gp_batch_create(gp_batch **out, int nsims, const gp_params *params, const do
   BALLOC(b->ext, sizeof(long long) * (size_t)ne * nsims);
   BALLOC(b->partials, sizeof(double) * (size_t)ns * nt);
   BALLOC(b->sums_sim, sizeof(double) * (size_t)ns * nsims);
-  BALLOC(b->counters, 4 * sizeof(int));
+  BALLOC(b->counters, gpd::CTR_COUNT * sizeof(int));
 #undef BALLOC
   std::vector<long long> ext((size_t)ne * nsims);
   for (int t = 0; t < nsims; t++) init_ext(&ext[(size_t)t * ne], N, K);
@@ -600,7 +610,7 @@ int gp_batch_create(gp_batch **out, int nsims, const gp_params *params, const do
   BUP(b->ext, ext.data(), sizeof(long long) * ext.size());
 #undef BUP
   if (cudaMemsetAsync(b->dphi, 0, (size_t)offd * b->elem, b->stream) != cudaSuccess ||
-      cudaMemsetAsync(b->counters, 0, 4 * sizeof(int), b->stream) != cudaSuccess) {
+      cudaMemsetAsync(b->counters, 0, gpd::CTR_COUNT * sizeof(int), b->stream) != cudaSuccess) {
     rc = bfail(b, GP_ECUDA, "gp_batch_create: memset failed");
     gp_batch_destroy(b);
     return rc;

@@ -12,12 +12,11 @@
  * (calculate_divergence_phasefield.h:19-22, calculate_fluxes_concentration.h:64,
  * calculate_divergence_concentration.h:43-57).
  *
- *  kf_bulk     persistent warps, one tile at a time over contiguous tile
- *              ranges, the next bulk tile's mu in flight (cp.async) while one
- *              is stepped.  Classifies each tile; bulk tiles read and write mu only
- *              (phi is rewritten only when the output buffer does not already
- *              hold the same one-hot tile); other tiles are put on the
- *              interface list.
+ *  kf_classify one thread per tile: the bulk test; bulk and interface lists.
+ *  kf_bulk     persistent warps over contiguous ranges of the bulk list, the
+ *              next tile's mu in flight (cp.async) while one is stepped.  Bulk
+ *              tiles read and write mu only (phi is rewritten only when the
+ *              output buffer does not already hold the same one-hot tile).
  *  kf_general  persistent CTAs over the interface list.  Stages phi with a
  *              two-cell halo and mu with one, computes delta-phi on the tile
  *              plus its one-cell ring in shared memory (the ring is recomputed
@@ -134,38 +133,30 @@ __device__ __forceinline__ TileFlags uniform_flags(int p) {
   return t;
 }
 
-/* Bulk test of tile (tile rows by, columns bx) of a simulation: every cell
- * of the tile and of its two-cell phi halo holds the exact one-hot phi of one
- * phase.  Evaluated by one warp; returns the phase or -1.  When the halo stays
+/* Bulk test of tile (tile rows by, columns bx) of a simulation, by one
+ * thread: every cell of the tile and of its two-cell phi halo holds the exact
+ * one-hot phi of one phase.  Returns the phase or -1.  When the halo stays
  * inside the domain it is covered by the facing edge bands of the eight
- * neighbour tiles (a corner by either band that contains it); otherwise the
+ * neighbour tiles (a corner by either band that contains it); otherwise by the
  * whole-tile flags of the tiles that hold the halo cells after the boundary
- * remap are used. */
+ * remap. */
 template <typename R>
 __device__ __forceinline__ int bulk_phase(const Consts<R> &D, const Grid &g, const TileFlags *__restrict__ flags,
                                           int tile0, int tiles_x, int by, int bx) {
-  const int lane = threadIdx.x & 31;
   const int x0 = by * TX, y0 = bx * TY;
   const int xl = min(x0 + TX, g.mx) - 1, yl = min(y0 + TY, g.my) - 1;
   if (x0 >= 2 && xl + 2 < g.mx && y0 >= 2 && yl + 2 < g.my) {
-    TileFlags F = uniform_flags(0);
-    if (lane < 9) F = flags[tile0 + (by + lane / 3 - 1) * tiles_x + (bx + lane % 3 - 1)];
-    const int own = __shfl_sync(0xffffffffu, (int)F.whole, 4);
-    bool ok = true;
-    switch (lane) {
-      case 0: ok = F.bot == own || F.right == own; break;   /* up-left */
-      case 1: ok = F.bot == own; break;                     /* up */
-      case 2: ok = F.bot == own || F.left == own; break;    /* up-right */
-      case 3: ok = F.right == own; break;                   /* left */
-      case 5: ok = F.left == own; break;                    /* right */
-      case 6: ok = F.top == own || F.right == own; break;   /* down-left */
-      case 7: ok = F.top == own; break;                     /* down */
-      case 8: ok = F.top == own || F.left == own; break;    /* down-right */
-      default: break;
-    }
-    return (__all_sync(0xffffffffu, ok) && own >= 0) ? own : -1;
+    const TileFlags *f = flags + tile0 + by * tiles_x + bx;
+    const TileFlags ul = f[-tiles_x - 1], u = f[-tiles_x], ur = f[-tiles_x + 1];
+    const TileFlags l = f[-1], c = f[0], r = f[1];
+    const TileFlags dl = f[tiles_x - 1], d = f[tiles_x], dr = f[tiles_x + 1];
+    const int p = c.whole;
+    const bool ok = p >= 0 && u.bot == p && d.top == p && l.right == p && r.left == p &&
+                    (ul.bot == p || ul.right == p) && (ur.bot == p || ur.left == p) &&
+                    (dl.top == p || dl.right == p) && (dr.top == p || dr.left == p);
+    return ok ? p : -1;
   }
-  /* candidate tile rows: own, and the tiles of rows x0-2, x0-1, xl+1, xl+2 */
+  /* the tiles of rows x0-2, x0-1, xl+1, xl+2 and columns y0-2, y0-1, yl+1, yl+2 */
   int rows[5], cols[5];
   {
     const int xs[4] = {x0 - 2, x0 - 1, xl + 1, xl + 2};
@@ -181,14 +172,11 @@ __device__ __forceinline__ int bulk_phase(const Consts<R> &D, const Grid &g, con
       cols[q + 1] = y / TY;
     }
   }
-  int f = 0x7f;
-  if (lane < 25) {
-    const int r = lane / 5, c = lane - r * 5;
-    f = flags[tile0 + rows[r] * tiles_x + cols[c]].whole;
-  }
-  const int own = __shfl_sync(0xffffffffu, f, 0);
-  const bool ok = lane >= 25 || f == own;
-  return (__all_sync(0xffffffffu, ok) && own >= 0) ? own : -1;
+  const int p = flags[tile0 + by * tiles_x + bx].whole;
+  bool ok = p >= 0;
+#pragma unroll
+  for (int q = 0; q < 25; q++) ok = ok && flags[tile0 + rows[q / 5] * tiles_x + cols[q % 5]].whole == p;
+  return ok ? p : -1;
 }
 
 
@@ -631,11 +619,45 @@ __device__ __forceinline__ TileFlags general_tile(const CT &D, const Grid &g, co
 /* kernels                                                             */
 /* ------------------------------------------------------------------ */
 
-/* Work-list counters of a batch: [0] interface tiles listed by kf_bulk,
- * [1] next list entry to take, [2] kf_general CTAs finished, [3] step number
- * (keys the FP32 rounding stream).  kf_general's last CTA resets [0..2] and
- * advances [3], so a step is exactly these two launches. */
-enum { CTR_LIST = 0, CTR_HEAD = 1, CTR_DONE = 2, CTR_STEP = 3 };
+/* Work-list counters of a batch: [0] interface tiles listed by kf_classify,
+ * [1] next interface entry to take, [2] kf_general CTAs finished, [3] step
+ * number (keys the FP32 rounding stream), [4] bulk tiles listed.  kf_general's
+ * last CTA resets [0..2] and [4] and advances [3], so a step is exactly the
+ * three launches kf_classify, kf_bulk, kf_general. */
+enum { CTR_LIST = 0, CTR_HEAD = 1, CTR_DONE = 2, CTR_STEP = 3, CTR_BULK = 4, CTR_COUNT = 8 };
+
+/* One thread per tile: the bulk test, then the tile goes on the bulk list
+ * (entry t | phase << 28) or the interface list; one atomic per warp and
+ * list. */
+template <typename R>
+__global__ void __launch_bounds__(NT) kf_classify(const SimDesc *__restrict__ sims,
+                                                  const Consts<R> *__restrict__ consts, const int *__restrict__ tsim,
+                                                  int ntiles, const TileFlags *__restrict__ flag_in,
+                                                  int *__restrict__ glist, int *__restrict__ blist,
+                                                  int *__restrict__ ctr) {
+  const int t = blockIdx.x * NT + threadIdx.x, lane = threadIdx.x & 31;
+  int p = -1;
+  if (t < ntiles) {
+    const int s = __ldg(tsim + t);
+    const SimDesc &sd = sims[s];
+    const int lt = t - sd.tile0, by = lt / sd.tiles_x, bx = lt - by * sd.tiles_x;
+    p = bulk_phase<R>(consts[s], sd.g, flag_in, sd.tile0, sd.tiles_x, by, bx);
+  }
+  const unsigned mb = __ballot_sync(0xffffffffu, t < ntiles && p >= 0);
+  const unsigned mg = __ballot_sync(0xffffffffu, t < ntiles && p < 0);
+  int bb = 0, bg = 0;
+  if (lane == 0) {
+    if (mb) bb = atomicAdd(ctr + CTR_BULK, __popc(mb));
+    if (mg) bg = atomicAdd(ctr + CTR_LIST, __popc(mg));
+  }
+  bb = __shfl_sync(0xffffffffu, bb, 0);
+  bg = __shfl_sync(0xffffffffu, bg, 0);
+  const unsigned below = (1u << lane) - 1u;
+  if (t < ntiles) {
+    if (p >= 0) blist[bb + __popc(mb & below)] = t | (p << 28);
+    else glist[bg + __popc(mg & below)] = t;
+  }
+}
 
 /* cp.async of one 4- or 8-byte element, global -> shared (completion tracked
  * by the issuing thread's commit/wait groups) */
@@ -657,11 +679,10 @@ __device__ __forceinline__ R bdiv(R v, R inv, R d) {
   else return v / d;
 }
 
-/* Bulk tiles, one warp per tile.  Warps take contiguous tile ranges; each
- * classifies its tiles in order and puts the ones that are not bulk on the
- * interface list.  The mu of a bulk tile with its one-cell halo is copied
- * into the warp's shared-memory stage by cp.async while the warp steps the
- * previous bulk tile from the other stage; lane j then steps column y0+j row
+/* Bulk tiles, one warp per tile.  Warps take contiguous ranges of the bulk
+ * list.  The mu of a bulk tile with its one-cell halo is copied into the
+ * warp's shared-memory stage by cp.async while the warp steps the previous
+ * bulk tile from the other stage; lane j then steps column y0+j row
  * by row.  No block-wide barrier anywhere.  The running mu extremes of the
  * cells a warp steps stay in registers and are merged into the simulation's
  * slots (atomic max/min) when the warp moves to another simulation or
@@ -674,17 +695,18 @@ struct BulkWarpStage {
 
 template <typename R, int N, int K, bool SUMS, bool MUL>
 __global__ void __launch_bounds__(NT, 2) kf_bulk(const SimDesc *__restrict__ sims, const Consts<R> *__restrict__ consts,
-                                                 const int *__restrict__ tsim, int ntiles, const R *__restrict__ state,
-                                                 R *__restrict__ next, const TileFlags *__restrict__ flag_in,
-                                                 TileFlags *__restrict__ flag_out, int *__restrict__ glist,
-                                                 int *__restrict__ ctr, StatBufs st) {
+                                                 const int *__restrict__ tsim, const int *__restrict__ blist,
+                                                 const R *__restrict__ state, R *__restrict__ next,
+                                                 TileFlags *__restrict__ flag_out, const int *__restrict__ ctr,
+                                                 StatBufs st) {
   constexpr int NW = NT / 32, NS = 2 * N + 2 * K + 1;
   extern __shared__ __align__(16) unsigned char smraw[];
   BulkWarpStage<R, N, K> &stg = reinterpret_cast<BulkWarpStage<R, N, K> *>(smraw)[threadIdx.x >> 5];
   const int lane = threadIdx.x & 31;
   const int gw = blockIdx.x * NW + (threadIdx.x >> 5), nwarps = gridDim.x * NW;
-  const int per = (ntiles + nwarps - 1) / nwarps;
-  const int t0 = gw * per, t1 = min(ntiles, t0 + per);
+  const int nbulk = *(const volatile int *)(ctr + CTR_BULK);
+  const int per = (nbulk + nwarps - 1) / nwarps;
+  const int i0 = gw * per, i1 = min(nbulk, i0 + per);
 
   double emax[K], emin[K];
 #pragma unroll
@@ -704,23 +726,6 @@ __global__ void __launch_bounds__(NT, 2) kf_bulk(const SimDesc *__restrict__ sim
     }
   };
 
-  /* next bulk tile of the range (the others go on the interface list) */
-  int tn = t0;
-  auto advance = [&](int &phase) -> int {
-    while (tn < t1) {
-      const int t = tn++;
-      const int s = __ldg(tsim + t);
-      const SimDesc &sd = sims[s];
-      const int lt = t - sd.tile0, by = lt / sd.tiles_x, bx = lt - by * sd.tiles_x;
-      const int p = bulk_phase<R>(consts[s], sd.g, flag_in, sd.tile0, sd.tiles_x, by, bx);
-      if (p >= 0) {
-        phase = p;
-        return t;
-      }
-      if (lane == 0) glist[atomicAdd(ctr + CTR_LIST, 1)] = t;
-    }
-    return -1;
-  };
   /* start copying tile t's mu with its halo into stage b */
   auto issue = [&](int t, int b) {
     const int s = __ldg(tsim + t);
@@ -748,22 +753,21 @@ __global__ void __launch_bounds__(NT, 2) kf_bulk(const SimDesc *__restrict__ sim
     cp_async_commit();
   };
 
-  int pc = -1, pn = -1;
-  int tc = advance(pc);
-  if (tc >= 0) issue(tc, 0);
+  int item = i0 < i1 ? __ldg(blist + i0) : 0;
+  if (i0 < i1) issue(item & 0x0fffffff, 0);
   int b = 0;
-  while (tc >= 0) {
-    const int tnx = advance(pn);
-    if (tnx >= 0) {
-      issue(tnx, b ^ 1);
+  for (int i = i0; i < i1; i++) {
+    const int nitem = i + 1 < i1 ? __ldg(blist + i + 1) : 0;
+    if (i + 1 < i1) {
+      issue(nitem & 0x0fffffff, b ^ 1);
       cp_async_wait<1>();
     } else {
       cp_async_wait<0>();
     }
     __syncwarp();
 
-    /* ---- step bulk tile tc (phase pc) from stage b */
-    const int t = tc, p = pc;
+    /* ---- step bulk tile t (phase p) from stage b */
+    const int t = item & 0x0fffffff, p = item >> 28;
     const int s = __ldg(tsim + t);
     if (s != cur_sim) {
       if (cur_sim >= 0) flush(cur_sim);
@@ -900,8 +904,7 @@ __global__ void __launch_bounds__(NT, 2) kf_bulk(const SimDesc *__restrict__ sim
     }
     if (lane == 0) flag_out[t] = uniform_flags(p);
     __syncwarp();   /* stage b is refilled by the next issue */
-    tc = tnx;
-    pc = pn;
+    item = nitem;
     b ^= 1;
   }
   if (cur_sim >= 0) flush(cur_sim);
@@ -954,6 +957,7 @@ __global__ void __launch_bounds__(NT, (N <= 3 ? 2 : 1)) kf_general(const SimDesc
     ctr[CTR_LIST] = 0;
     ctr[CTR_HEAD] = 0;
     ctr[CTR_DONE] = 0;
+    ctr[CTR_BULK] = 0;
     ctr[CTR_STEP] = (int)((unsigned)ctr[CTR_STEP] + 1u);
     __threadfence();
   }
