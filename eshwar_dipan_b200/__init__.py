@@ -17,7 +17,7 @@ import ctypes
 
 import numpy as np
 
-from ._abi import (GP_FP32, GP_FP64, GpError, Params, Stats, check, lib)
+from ._abi import (GP_FP32, GP_FP64, AdjOut, AdjReq, GpError, Params, Stats, check, lib)
 
 __all__ = ["Params", "Stats", "GpError", "Simulation", "Batch", "load_params", "fill", "vtk_write", "vtk_read",
            "GP_FP64", "GP_FP32", "version"]
@@ -115,6 +115,49 @@ class Simulation:
         mu = np.zeros(sm, dtype=np.float64)
         check(lib().gp_get(self._h, _ptr(phi), _ptr(mu)), self._h)
         return phi, mu
+
+    def adjoint(self, nsteps, target_phi=None, phi_bar=None, mu_bar=None, checkpoint_every=0):
+        """gp_adjoint: run nsteps from the current state (the simulation ends at
+        the final state) and return a dict with the loss (with target_phi), the
+        parameter gradients d_tau, d_dab, d_epsilon, d_gamma (phase pair 0,1),
+        phi0_bar / mu0_bar (gradient with respect to the start state) and the
+        device times of the two passes."""
+        sp, sm = _shapes(self.params)
+        req = AdjReq()
+        req.nsteps = int(nsteps)
+        req.checkpoint_every = int(checkpoint_every)
+        keep = []
+        if phi_bar is not None:
+            a = np.ascontiguousarray(phi_bar, dtype=np.float64)
+            keep.append(a)
+            req.phi_bar = a.ctypes.data
+            if mu_bar is not None:
+                m = np.ascontiguousarray(mu_bar, dtype=np.float64)
+                keep.append(m)
+                req.mu_bar = m.ctypes.data
+        elif target_phi is not None:
+            t = np.ascontiguousarray(target_phi, dtype=np.float64)
+            keep.append(t)
+            req.target_phi = t.ctypes.data
+        else:
+            raise ValueError("give target_phi or phi_bar")
+        out = AdjOut()
+        g_phi = np.zeros(sp, dtype=np.float64)
+        g_mu = np.zeros(sm, dtype=np.float64)
+        out.phi0_bar = g_phi.ctypes.data
+        out.mu0_bar = g_mu.ctypes.data
+        check(lib().gp_adjoint(self._h, ctypes.byref(req), ctypes.byref(out)), self._h)
+        return {"loss": out.loss, "d_tau": out.d_tau, "d_dab": out.d_dab, "d_epsilon": out.d_epsilon,
+                "d_gamma": out.d_gamma, "phi0_bar": g_phi, "mu0_bar": g_mu,
+                "ms_forward": out.ms_forward, "ms_reverse": out.ms_reverse}
+
+    def adjoint_replay(self, nsteps):
+        """gp_adjoint_replay: (max |difference|, number of differing values)
+        between the adjoint's cell functions and the step kernels over nsteps."""
+        d = ctypes.c_double()
+        n = ctypes.c_longlong()
+        check(lib().gp_adjoint_replay(self._h, int(nsteps), ctypes.byref(d), ctypes.byref(n)), self._h)
+        return d.value, n.value
 
     def set(self, phi, mu):
         phi = np.ascontiguousarray(phi, dtype=np.float64)

@@ -98,6 +98,19 @@ class Stats(ctypes.Structure):
         return d
 
 
+class AdjReq(ctypes.Structure):
+    """gp_adj_req (include/gp.h)."""
+    _fields_ = [("nsteps", c_long), ("phi_bar", c_void_p), ("mu_bar", c_void_p), ("target_phi", c_void_p),
+                ("checkpoint_every", c_long)]
+
+
+class AdjOut(ctypes.Structure):
+    """gp_adj_out (include/gp.h)."""
+    _fields_ = [("loss", c_double), ("d_tau", c_double), ("d_dab", c_double), ("d_epsilon", c_double),
+                ("d_gamma", c_double), ("phi0_bar", c_void_p), ("mu0_bar", c_void_p),
+                ("ms_forward", c_double), ("ms_reverse", c_double)]
+
+
 # Every entry point declared in include/gp.h, with its ctypes signature.
 SIGNATURES = {
     "gp_params_load": (c_int, [POINTER(Params), ctypes.c_char_p]),
@@ -125,6 +138,8 @@ SIGNATURES = {
     "gp_batch_size": (c_int, [c_void_p]),
     "gp_batch_last_error": (ctypes.c_char_p, [c_void_p]),
     "gp_batch_destroy": (None, [c_void_p]),
+    "gp_adjoint": (c_int, [c_void_p, POINTER(AdjReq), POINTER(AdjOut)]),
+    "gp_adjoint_replay": (c_int, [c_void_p, c_long, POINTER(c_double), POINTER(c_longlong)]),
     "gp_stream": (c_void_p, [c_void_p]),
     "gp_destroy": (None, [c_void_p]),
     "gp_last_error": (ctypes.c_char_p, [c_void_p]),

@@ -25,7 +25,8 @@ INC = ["-I" + os.path.join(ROOT, "include"), "-I" + CSRC]
 HOST_C = ["gp_host.c", "gp_host_io.c"]
 # (file, extra nvcc flags): the FP64 unit stays without FMA contraction so the
 # plain step is bit-identical to the reference; the FP32 storage form may fuse.
-CUDA = [("gp_device.cu", ["--fmad=false"]), ("gp_batch32.cu", ["--fmad=true"])]
+CUDA = [("gp_device.cu", ["--fmad=false"]), ("gp_batch32.cu", ["--fmad=true"]),
+        ("gp_adjoint.cu", ["--fmad=false"])]
 
 
 def _run(cmd, verbose):

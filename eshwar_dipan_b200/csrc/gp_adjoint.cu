@@ -1,0 +1,331 @@
+/*
+ * gp_adjoint.cu -- kernels of the adjoint of the FP64 step (gp_adjoint).
+ * Compiled without FMA contraction, like the FP64 step, so that the cell
+ * functions of gp_adjoint.cuh evaluated in double reproduce it bit for bit.
+ *
+ * One reverse step maps the adjoint of the state after a step (ybar) to the
+ * adjoint of the state before it (xbar):
+ *   ka_rev_update  for every interior cell, the transposed local Jacobian of
+ *                  update_cell applied to the cell's ybar, scattered onto the
+ *                  phi / mu of its stencil (through the boundary copy tables:
+ *                  a ghost cell is a copy of an interior cell, so its adjoint
+ *                  belongs to that cell), onto the delta-phi of its 5-point
+ *                  stencil (dphibar, interior plus ring) and onto the four
+ *                  parameters;
+ *   ka_rev_dphi    for every interior or ring cell, the transposed local
+ *                  Jacobian of dphi_cell applied to its dphibar, scattered the
+ *                  same way.
+ * The local Jacobians are exact: the cell functions are evaluated on
+ * Dual<ADJ_W> numbers seeded on ADJ_W of the stencil inputs at a time.
+ * Scatter-adds are atomic (FP64), so the last bits of a gradient may differ
+ * between runs; values are exact derivatives up to summation order.
+ */
+#include <cuda_runtime.h>
+
+#include "gp_adjoint.cuh"
+#include "gp_adjoint_launch.h"
+
+namespace gpd {
+
+constexpr int ADJ_W = 8;
+constexpr int AB = 128;   /* threads per block along y */
+
+__device__ __forceinline__ int rmx(int x, const Grid &g, const Consts<double> *c, int f) {
+  return (x < 0 || x >= g.mx) ? remap(x, g.mx, c->bc_x[f][0], c->bc_x[f][1]) : x;
+}
+__device__ __forceinline__ int rmy(int y, const Grid &g, const Consts<double> *c, int f) {
+  return (y < 0 || y >= g.my) ? remap(y, g.my, c->bc_y[f][0], c->bc_y[f][1]) : y;
+}
+
+/* phi of the 3x3 window around (x, y) and mu of its 5-point stencil (corners
+ * of the mu window are filled too; update_cell does not read them) */
+template <int N, int K>
+__device__ __forceinline__ void gather(const Consts<double> *c, const Grid &g, const double *st, int x, int y,
+                                       double (&S)[N][3][3], double (&M)[K][3][3]) {
+#pragma unroll
+  for (int di = 0; di < 3; di++) {
+    const int xp = rmx(x + di - 1, g, c, 0), xm = rmx(x + di - 1, g, c, 1);
+#pragma unroll
+    for (int dj = 0; dj < 3; dj++) {
+      const int yp = rmy(y + dj - 1, g, c, 0), ym = rmy(y + dj - 1, g, c, 1);
+#pragma unroll
+      for (int a = 0; a < N; a++) S[a][di][dj] = st[a * g.plane + (long long)xp * g.pitch + yp];
+#pragma unroll
+      for (int k = 0; k < K; k++) M[k][di][dj] = st[(N + k) * g.plane + (long long)xm * g.pitch + ym];
+    }
+  }
+}
+
+__device__ __forceinline__ long long didx(const Grid &g, int a, int x, int y) {
+  return a * g.dplane + (long long)(x + 1) * g.dpitch + (y + 1);
+}
+
+/* ---- forward ------------------------------------------------------------ */
+
+template <int N, int K, bool A>
+__global__ void __launch_bounds__(AB) ka_dphi(const Consts<double> *__restrict__ c, AdjParams prm, Grid g,
+                                              const double *__restrict__ st, double *__restrict__ dphi) {
+  const int y = blockIdx.x * AB + threadIdx.x - 1, x = (int)blockIdx.y - 1;
+  if (y > g.my) return;
+  double S[N][3][3], M[K][3][3];
+  gather<N, K>(c, g, st, x, y, S, M);
+  double p[ADJ_NPARAM];
+#pragma unroll
+  for (int j = 0; j < ADJ_NPARAM; j++) p[j] = prm.v[j];
+  const AK<double> D = make_ak<double>(c, p);
+  double m[K], d[N];
+#pragma unroll
+  for (int k = 0; k < K; k++) m[k] = M[k][1][1];
+  dphi_cell<double, N, K, A>(D, S, m, d);
+#pragma unroll
+  for (int a = 0; a < N; a++) dphi[didx(g, a, x, y)] = d[a];
+}
+
+template <int N, int K>
+__global__ void __launch_bounds__(AB) ka_update(const Consts<double> *__restrict__ c, AdjParams prm, Grid g,
+                                                const double *__restrict__ st, const double *__restrict__ dphi,
+                                                double *__restrict__ next) {
+  const int y = blockIdx.x * AB + threadIdx.x, x = blockIdx.y;
+  if (y >= g.my) return;
+  double S[N][3][3], M[K][3][3], DP[N][3][3];
+  gather<N, K>(c, g, st, x, y, S, M);
+#pragma unroll
+  for (int a = 0; a < N; a++)
+#pragma unroll
+    for (int di = 0; di < 3; di++)
+#pragma unroll
+      for (int dj = 0; dj < 3; dj++) DP[a][di][dj] = dphi[didx(g, a, x + di - 1, y + dj - 1)];
+  double p[ADJ_NPARAM];
+#pragma unroll
+  for (int j = 0; j < ADJ_NPARAM; j++) p[j] = prm.v[j];
+  const AK<double> D = make_ak<double>(c, p);
+  double nph[N], nm[K];
+  update_cell<double, N, K>(D, S, M, DP, y, g.my, nph, nm);
+  const long long o = (long long)x * g.pitch + y;
+#pragma unroll
+  for (int a = 0; a < N; a++) next[a * g.plane + o] = nph[a];
+#pragma unroll
+  for (int k = 0; k < K; k++) next[(N + k) * g.plane + o] = nm[k];
+}
+
+/* ---- reverse ------------------------------------------------------------ */
+
+/* parameter adjoints: one atomic per warp */
+__device__ __forceinline__ void flush_params(double (&pacc)[ADJ_NPARAM], double *pbar) {
+#pragma unroll
+  for (int j = 0; j < ADJ_NPARAM; j++) {
+    double v = pacc[j];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0 && v != 0.0) atomicAdd(pbar + j, v);
+  }
+}
+
+template <int N, int K>
+__global__ void __launch_bounds__(AB) ka_rev_update(const Consts<double> *__restrict__ c, AdjParams prm, Grid g,
+                                                    const double *__restrict__ st, const double *__restrict__ dphi,
+                                                    const double *__restrict__ ybar, double *__restrict__ xbar,
+                                                    double *__restrict__ dphibar, double *__restrict__ pbar) {
+  using DT = Dual<ADJ_W>;
+  constexpr int NPHI = 9 * N, NMU = 5 * K, NDP = 5 * N, NIN = NPHI + NMU + NDP + ADJ_NPARAM;
+  const int y = blockIdx.x * AB + threadIdx.x, x = blockIdx.y;
+  double pacc[ADJ_NPARAM] = {};
+  const bool live = y < g.my;
+  double yb[N + K];
+  bool any = false;
+  if (live) {
+    const long long o = (long long)x * g.pitch + y;
+#pragma unroll
+    for (int f = 0; f < N + K; f++) {
+      yb[f] = ybar[f * g.plane + o];
+      any |= yb[f] != 0.0;
+    }
+  }
+  if (live && any) {
+    double S[N][3][3], M[K][3][3], DP[N][3][3];
+    gather<N, K>(c, g, st, x, y, S, M);
+#pragma unroll
+    for (int a = 0; a < N; a++)
+#pragma unroll
+      for (int di = 0; di < 3; di++)
+#pragma unroll
+        for (int dj = 0; dj < 3; dj++) DP[a][di][dj] = dphi[didx(g, a, x + di - 1, y + dj - 1)];
+    const int pi[5] = {1, 0, 2, 1, 1}, pj[5] = {1, 1, 1, 0, 2};
+    for (int base = 0; base < NIN; base += ADJ_W) {
+      DT Sd[N][3][3], Md[K][3][3], DPd[N][3][3], pd[ADJ_NPARAM];
+#pragma unroll
+      for (int a = 0; a < N; a++)
+#pragma unroll
+        for (int di = 0; di < 3; di++)
+#pragma unroll
+          for (int dj = 0; dj < 3; dj++) {
+            Sd[a][di][dj] = DT(S[a][di][dj]);
+            DPd[a][di][dj] = DT(DP[a][di][dj]);
+          }
+#pragma unroll
+      for (int k = 0; k < K; k++)
+#pragma unroll
+        for (int di = 0; di < 3; di++)
+#pragma unroll
+          for (int dj = 0; dj < 3; dj++) Md[k][di][dj] = DT(M[k][di][dj]);
+#pragma unroll
+      for (int j = 0; j < ADJ_NPARAM; j++) pd[j] = DT(prm.v[j]);
+      /* seed inputs base .. base+W-1 */
+      for (int w = 0; w < ADJ_W; w++) {
+        const int id = base + w;
+        if (id < NPHI) {
+          const int a = id / 9, r = id % 9;
+          Sd[a][r / 3][r % 3].d[w] = 1.0;
+        } else if (id < NPHI + NMU) {
+          const int k = (id - NPHI) / 5, r = (id - NPHI) % 5;
+          Md[k][pi[r]][pj[r]].d[w] = 1.0;
+        } else if (id < NPHI + NMU + NDP) {
+          const int a = (id - NPHI - NMU) / 5, r = (id - NPHI - NMU) % 5;
+          DPd[a][pi[r]][pj[r]].d[w] = 1.0;
+        } else if (id < NIN) {
+          pd[id - NPHI - NMU - NDP].d[w] = 1.0;
+        }
+      }
+      const AK<DT> D = make_ak<DT>(c, pd);
+      DT nph[N], nm[K];
+      update_cell<DT, N, K>(D, Sd, Md, DPd, y, g.my, nph, nm);
+      for (int w = 0; w < ADJ_W; w++) {
+        const int id = base + w;
+        if (id >= NIN) break;
+        double gsum = 0.0;
+#pragma unroll
+        for (int a = 0; a < N; a++) gsum += yb[a] * nph[a].d[w];
+#pragma unroll
+        for (int k = 0; k < K; k++) gsum += yb[N + k] * nm[k].d[w];
+        if (gsum == 0.0) continue;
+        if (id < NPHI) {
+          const int a = id / 9, r = id % 9;
+          const int xs = rmx(x + r / 3 - 1, g, c, 0), ys = rmy(y + r % 3 - 1, g, c, 0);
+          atomicAdd(xbar + a * g.plane + (long long)xs * g.pitch + ys, gsum);
+        } else if (id < NPHI + NMU) {
+          const int k = (id - NPHI) / 5, r = (id - NPHI) % 5;
+          const int xs = rmx(x + pi[r] - 1, g, c, 1), ys = rmy(y + pj[r] - 1, g, c, 1);
+          atomicAdd(xbar + (N + k) * g.plane + (long long)xs * g.pitch + ys, gsum);
+        } else if (id < NPHI + NMU + NDP) {
+          const int a = (id - NPHI - NMU) / 5, r = (id - NPHI - NMU) % 5;
+          atomicAdd(dphibar + didx(g, a, x + pi[r] - 1, y + pj[r] - 1), gsum);
+        } else {
+          pacc[id - NPHI - NMU - NDP] += gsum;
+        }
+      }
+    }
+  }
+  flush_params(pacc, pbar);
+}
+
+template <int N, int K, bool A>
+__global__ void __launch_bounds__(AB) ka_rev_dphi(const Consts<double> *__restrict__ c, AdjParams prm, Grid g,
+                                                  const double *__restrict__ st, const double *__restrict__ dphibar,
+                                                  double *__restrict__ xbar, double *__restrict__ pbar) {
+  using DT = Dual<ADJ_W>;
+  constexpr int NPHI = 9 * N, NIN = NPHI + K + ADJ_NPARAM;
+  const int y = blockIdx.x * AB + threadIdx.x - 1, x = (int)blockIdx.y - 1;
+  double pacc[ADJ_NPARAM] = {};
+  const bool live = y <= g.my;
+  double db[N];
+  bool any = false;
+  if (live) {
+#pragma unroll
+    for (int a = 0; a < N; a++) {
+      db[a] = dphibar[didx(g, a, x, y)];
+      any |= db[a] != 0.0;
+    }
+  }
+  if (live && any) {
+    double S[N][3][3], M[K][3][3];
+    gather<N, K>(c, g, st, x, y, S, M);
+    for (int base = 0; base < NIN; base += ADJ_W) {
+      DT Sd[N][3][3], md[K], pd[ADJ_NPARAM];
+#pragma unroll
+      for (int a = 0; a < N; a++)
+#pragma unroll
+        for (int di = 0; di < 3; di++)
+#pragma unroll
+          for (int dj = 0; dj < 3; dj++) Sd[a][di][dj] = DT(S[a][di][dj]);
+#pragma unroll
+      for (int k = 0; k < K; k++) md[k] = DT(M[k][1][1]);
+#pragma unroll
+      for (int j = 0; j < ADJ_NPARAM; j++) pd[j] = DT(prm.v[j]);
+      for (int w = 0; w < ADJ_W; w++) {
+        const int id = base + w;
+        if (id < NPHI) Sd[id / 9][(id % 9) / 3][id % 3].d[w] = 1.0;
+        else if (id < NPHI + K) md[id - NPHI].d[w] = 1.0;
+        else if (id < NIN) pd[id - NPHI - K].d[w] = 1.0;
+      }
+      const AK<DT> D = make_ak<DT>(c, pd);
+      DT d[N];
+      dphi_cell<DT, N, K, A>(D, Sd, md, d);
+      for (int w = 0; w < ADJ_W; w++) {
+        const int id = base + w;
+        if (id >= NIN) break;
+        double gsum = 0.0;
+#pragma unroll
+        for (int a = 0; a < N; a++) gsum += db[a] * d[a].d[w];
+        if (gsum == 0.0) continue;
+        if (id < NPHI) {
+          const int a = id / 9, r = id % 9;
+          const int xs = rmx(x + r / 3 - 1, g, c, 0), ys = rmy(y + r % 3 - 1, g, c, 0);
+          atomicAdd(xbar + a * g.plane + (long long)xs * g.pitch + ys, gsum);
+        } else if (id < NPHI + K) {
+          const int xs = rmx(x, g, c, 1), ys = rmy(y, g, c, 1);
+          atomicAdd(xbar + (N + id - NPHI) * g.plane + (long long)xs * g.pitch + ys, gsum);
+        } else {
+          pacc[id - NPHI - K] += gsum;
+        }
+      }
+    }
+  }
+  flush_params(pacc, pbar);
+}
+
+/* ---- launchers ---------------------------------------------------------- */
+
+template <int N, int K, bool A>
+struct AdjKernels {
+  static cudaError_t dphi(cudaStream_t s, const void *c, AdjParams p, Grid g, const double *st, double *dp) {
+    dim3 grid((g.my + 2 + AB - 1) / AB, g.mx + 2);
+    ka_dphi<N, K, A><<<grid, AB, 0, s>>>((const Consts<double> *)c, p, g, st, dp);
+    return cudaGetLastError();
+  }
+  static cudaError_t update(cudaStream_t s, const void *c, AdjParams p, Grid g, const double *st, const double *dp,
+                            double *next) {
+    dim3 grid((g.my + AB - 1) / AB, g.mx);
+    ka_update<N, K><<<grid, AB, 0, s>>>((const Consts<double> *)c, p, g, st, dp, next);
+    return cudaGetLastError();
+  }
+  static cudaError_t rev_update(cudaStream_t s, const void *c, AdjParams p, Grid g, const double *st,
+                                const double *dp, const double *ybar, double *xbar, double *dpbar, double *pbar) {
+    dim3 grid((g.my + AB - 1) / AB, g.mx);
+    ka_rev_update<N, K><<<grid, AB, 0, s>>>((const Consts<double> *)c, p, g, st, dp, ybar, xbar, dpbar, pbar);
+    return cudaGetLastError();
+  }
+  static cudaError_t rev_dphi(cudaStream_t s, const void *c, AdjParams p, Grid g, const double *st,
+                              const double *dpbar, double *xbar, double *pbar) {
+    dim3 grid((g.my + 2 + AB - 1) / AB, g.mx + 2);
+    ka_rev_dphi<N, K, A><<<grid, AB, 0, s>>>((const Consts<double> *)c, p, g, st, dpbar, xbar, pbar);
+    return cudaGetLastError();
+  }
+};
+
+}  // namespace gpd
+
+bool gp_adjoint_launch(int N, int K, bool aniso, gpd::AdjLaunch *out) {
+  if (N != 2 || K != 1) return false;
+  if (aniso) {
+    out->dphi = gpd::AdjKernels<2, 1, true>::dphi;
+    out->update = gpd::AdjKernels<2, 1, true>::update;
+    out->rev_update = gpd::AdjKernels<2, 1, true>::rev_update;
+    out->rev_dphi = gpd::AdjKernels<2, 1, true>::rev_dphi;
+  } else {
+    out->dphi = gpd::AdjKernels<2, 1, false>::dphi;
+    out->update = gpd::AdjKernels<2, 1, false>::update;
+    out->rev_update = gpd::AdjKernels<2, 1, false>::rev_update;
+    out->rev_dphi = gpd::AdjKernels<2, 1, false>::rev_dphi;
+  }
+  return true;
+}

@@ -1,0 +1,34 @@
+/*
+ * gp_adjoint_launch.h -- launcher table of the adjoint kernels (gp_adjoint.cu)
+ * for the host driver in gp_device.cu.
+ */
+#pragma once
+#include <cuda_runtime.h>
+
+#include "gp_tiles.cuh"
+
+namespace gpd {
+
+enum { ADJ_TAU = 0, ADJ_DAB = 1, ADJ_EPS = 2, ADJ_GAMMA = 3, ADJ_NPARAM = 4 };
+
+/* values of the differentiable parameters */
+struct AdjParams {
+  double v[ADJ_NPARAM];   /* Tau_01, dab_01, epsilon, GAMMA_01 */
+};
+
+struct AdjLaunch {
+  /* delta-phi of the interior plus ring of a state (dplane layout) */
+  cudaError_t (*dphi)(cudaStream_t s, const void *consts, AdjParams p, Grid g, const double *state, double *dphi);
+  /* the step from a state and its delta-phi, by the adjoint's cell functions */
+  cudaError_t (*update)(cudaStream_t s, const void *consts, AdjParams p, Grid g, const double *state,
+                        const double *dphi, double *next);
+  /* reverse of the concentration pass: ybar -> xbar, dphibar, pbar (accumulated) */
+  cudaError_t (*rev_update)(cudaStream_t s, const void *consts, AdjParams p, Grid g, const double *state,
+                            const double *dphi, const double *ybar, double *xbar, double *dphibar, double *pbar);
+  /* reverse of the phase-field pass: dphibar -> xbar, pbar (accumulated) */
+  cudaError_t (*rev_dphi)(cudaStream_t s, const void *consts, AdjParams p, Grid g, const double *state,
+                          const double *dphibar, double *xbar, double *pbar);
+};
+}  // namespace gpd
+
+bool gp_adjoint_launch(int N, int K, bool aniso, gpd::AdjLaunch *out);

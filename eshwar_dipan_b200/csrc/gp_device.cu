@@ -21,8 +21,10 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <algorithm>
 #include <vector>
 
+#include "gp_adjoint_launch.h"
 #include "gp_batch_impl.cuh"
 
 static __constant__ gpd::Consts<double> cD;
@@ -777,6 +779,235 @@ int gp_set_dev(gp_ctx *c, const double *phi, const double *mu) {
 
 }  /* extern "C" */
 
+
+/* ======================================================================= */
+/* adjoint                                                                 */
+/* ======================================================================= */
+
+namespace {
+
+/* host planes [nf][mx][my] <-> device planes with the state layout */
+int planes_copy(gp_batch *b, double *dst, size_t dpitch, const double *src, size_t spitch, int nf, size_t dplane,
+                size_t splane, size_t mx, size_t my, cudaMemcpyKind kind) {
+  for (int f = 0; f < nf; f++)
+    BK(cudaMemcpy2DAsync(dst + f * dplane, dpitch * 8, src + f * splane, spitch * 8, my * 8, mx, kind, b->stream));
+  return GP_OK;
+}
+
+struct AdjBufs {
+  double *snap = nullptr, *seg = nullptr, *ybar = nullptr, *xbar = nullptr, *dphi = nullptr, *dphibar = nullptr,
+         *pbar = nullptr, *final_state = nullptr;
+  ~AdjBufs() {
+    cudaFree(snap); cudaFree(seg); cudaFree(ybar); cudaFree(xbar); cudaFree(dphi); cudaFree(dphibar);
+    cudaFree(pbar); cudaFree(final_state);
+  }
+};
+
+int adj_check(gp_ctx *c, gpd::AdjLaunch *L) {
+  if (!c || !c->b) return fail(c, GP_EINVAL, "gp_adjoint: NULL context");
+  gp_batch *b = c->b;
+  const gp_derived &d = b->derived[0];
+  if (b->elem != 8) return fail(c, GP_EUNSUPPORTED, "gp_adjoint: FP64 contexts only");
+  if (d.N != 2 || d.K != 1 || d.inv_mode != GP_INV_BINARY)
+    return fail(c, GP_EUNSUPPORTED, "gp_adjoint: NUMPHASES=2 with one BINARY component only (have N=%d K=%d)", d.N,
+                d.K);
+  if (!gp_adjoint_launch(d.N, d.K, d.aniso != 0, L)) return fail(c, GP_EUNSUPPORTED, "gp_adjoint: no kernels");
+  return GP_OK;
+}
+
+gpd::AdjParams adj_params(const gp_params &p) {
+  gpd::AdjParams a;
+  a.v[gpd::ADJ_TAU] = p.tau_ab[0][1];
+  a.v[gpd::ADJ_DAB] = p.dab[0][1];
+  a.v[gpd::ADJ_EPS] = p.epsilon;
+  a.v[gpd::ADJ_GAMMA] = p.gamma[0][1];
+  return a;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gp_adjoint(gp_ctx *c, const gp_adj_req *req, gp_adj_out *out) {
+  gpd::AdjLaunch L;
+  int rc = adj_check(c, &L);
+  if (rc) return rc;
+  if (!req || !out || req->nsteps < 1 || (!req->phi_bar && !req->target_phi))
+    return fail(c, GP_EINVAL, "gp_adjoint: need nsteps >= 1 and phi_bar or target_phi");
+  c->err[0] = 0;
+  gp_batch *b = c->b;
+  const gp_derived &d = b->derived[0];
+  const gpd::SimDesc &sd = b->desc[0];
+  const gpd::Grid &g = sd.g;
+  const int N = d.N, K = d.K;
+  const size_t mx = g.mx, my = g.my, S = (size_t)(N + K) * g.plane, Sd = (size_t)N * g.dplane;
+  const long T = req->nsteps;
+  long C = req->checkpoint_every > 0 ? req->checkpoint_every : (long)ceil(sqrt((double)T));
+  if (C > T) C = T;
+  const long nseg = (T + C - 1) / C;
+  const gpd::AdjParams prm = adj_params(b->params[0]);
+  const void *consts = b->d_consts;
+  AdjBufs m;
+#define AALLOC(ptr, n)                                                                                  \
+  do {                                                                                                  \
+    if (cudaMalloc((void **)&(ptr), (n) * sizeof(double)) != cudaSuccess)                               \
+      return fail(c, GP_ENOMEM, "gp_adjoint: cudaMalloc of %zu bytes failed", (size_t)(n) * sizeof(double)); \
+  } while (0)
+  AALLOC(m.snap, S * nseg);
+  AALLOC(m.seg, S * C);
+  AALLOC(m.ybar, S);
+  AALLOC(m.xbar, S);
+  AALLOC(m.dphi, Sd);
+  AALLOC(m.dphibar, Sd);
+  AALLOC(m.pbar, gpd::ADJ_NPARAM);
+  AALLOC(m.final_state, S);
+#undef AALLOC
+  double *state = (double *)b->state[b->cur];   /* a batch of one starts at offset 0 */
+  const long long steps0 = b->steps;
+  cudaEvent_t e0, e1, e2;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  CK(cudaEventCreate(&e2));
+  CK(cudaEventRecord(e0, b->stream));
+
+  /* ---- forward, keeping the state at the start of every segment */
+  for (long s = 0; s < nseg; s++) {
+    state = (double *)b->state[b->cur];
+    CK(cudaMemcpyAsync(m.snap + S * s, state, S * 8, cudaMemcpyDeviceToDevice, b->stream));
+    const long n = std::min(C, T - s * C);
+    if ((rc = batch_step_impl(b, n, nullptr, nullptr, nullptr, nullptr)) != GP_OK) return rc;
+  }
+  state = (double *)b->state[b->cur];
+  CK(cudaMemcpyAsync(m.final_state, state, S * 8, cudaMemcpyDeviceToDevice, b->stream));
+  CK(cudaEventRecord(e1, b->stream));
+
+  /* ---- seed: dL/d(final state) */
+  out->loss = 0.0;
+  CK(cudaMemsetAsync(m.ybar, 0, S * 8, b->stream));
+  if (req->phi_bar) {
+    if ((rc = planes_copy(b, m.ybar, g.pitch, req->phi_bar, my, N, g.plane, mx * my, mx, my,
+                          cudaMemcpyHostToDevice)) != GP_OK)
+      return rc;
+    if (req->mu_bar &&
+        (rc = planes_copy(b, m.ybar + N * g.plane, g.pitch, req->mu_bar, my, K, g.plane, mx * my, mx, my,
+                          cudaMemcpyHostToDevice)) != GP_OK)
+      return rc;
+  } else {
+    std::vector<double> phT((size_t)N * mx * my);
+    if ((rc = planes_copy(b, phT.data(), my, state, g.pitch, N, mx * my, g.plane, mx, my,
+                          cudaMemcpyDeviceToHost)) != GP_OK)
+      return rc;
+    CK(cudaStreamSynchronize(b->stream));
+    double loss = 0.0;
+    for (size_t i = 0; i < phT.size(); i++) {
+      phT[i] -= req->target_phi[i];
+      loss += phT[i] * phT[i];
+    }
+    out->loss = 0.5 * loss;
+    if ((rc = planes_copy(b, m.ybar, g.pitch, phT.data(), my, N, g.plane, mx * my, mx, my,
+                          cudaMemcpyHostToDevice)) != GP_OK)
+      return rc;
+    CK(cudaStreamSynchronize(b->stream));
+  }
+  CK(cudaMemsetAsync(m.pbar, 0, gpd::ADJ_NPARAM * 8, b->stream));
+
+  /* ---- reverse sweep, segment by segment from the last */
+  for (long s = nseg - 1; s >= 0; s--) {
+    const long n = std::min(C, T - s * C);
+    state = (double *)b->state[b->cur];
+    CK(cudaMemcpyAsync(state, m.snap + S * s, S * 8, cudaMemcpyDeviceToDevice, b->stream));
+    if ((rc = batch_reflag(b, true)) != GP_OK) return rc;
+    for (long j = 0; j < n; j++) {
+      state = (double *)b->state[b->cur];
+      CK(cudaMemcpyAsync(m.seg + S * j, state, S * 8, cudaMemcpyDeviceToDevice, b->stream));
+      if (j + 1 < n && (rc = batch_step_impl(b, 1, nullptr, nullptr, nullptr, nullptr)) != GP_OK) return rc;
+    }
+    for (long j = n - 1; j >= 0; j--) {
+      const double *x = m.seg + S * j;
+      CK(L.dphi(b->stream, consts, prm, g, x, m.dphi));
+      CK(cudaMemsetAsync(m.xbar, 0, S * 8, b->stream));
+      CK(cudaMemsetAsync(m.dphibar, 0, Sd * 8, b->stream));
+      CK(L.rev_update(b->stream, consts, prm, g, x, m.dphi, m.ybar, m.xbar, m.dphibar, m.pbar));
+      CK(L.rev_dphi(b->stream, consts, prm, g, x, m.dphibar, m.xbar, m.pbar));
+      std::swap(m.ybar, m.xbar);
+    }
+  }
+  CK(cudaEventRecord(e2, b->stream));
+
+  /* ---- results; the context goes back to the final state */
+  double pb[gpd::ADJ_NPARAM];
+  CK(cudaMemcpyAsync(pb, m.pbar, sizeof pb, cudaMemcpyDeviceToHost, b->stream));
+  if (out->phi0_bar &&
+      (rc = planes_copy(b, out->phi0_bar, my, m.ybar, g.pitch, N, mx * my, g.plane, mx, my,
+                        cudaMemcpyDeviceToHost)) != GP_OK)
+    return rc;
+  if (out->mu0_bar &&
+      (rc = planes_copy(b, out->mu0_bar, my, m.ybar + N * g.plane, g.pitch, K, mx * my, g.plane, mx, my,
+                        cudaMemcpyDeviceToHost)) != GP_OK)
+    return rc;
+  state = (double *)b->state[b->cur];
+  CK(cudaMemcpyAsync(state, m.final_state, S * 8, cudaMemcpyDeviceToDevice, b->stream));
+  if ((rc = batch_reflag(b, true)) != GP_OK) return rc;
+  CK(cudaStreamSynchronize(b->stream));
+  b->steps = steps0 + T;
+  out->d_tau = pb[gpd::ADJ_TAU];
+  out->d_dab = pb[gpd::ADJ_DAB];
+  out->d_epsilon = pb[gpd::ADJ_EPS];
+  out->d_gamma = pb[gpd::ADJ_GAMMA];
+  float f1 = 0.f, f2 = 0.f;
+  CK(cudaEventElapsedTime(&f1, e0, e1));
+  CK(cudaEventElapsedTime(&f2, e1, e2));
+  out->ms_forward = f1;
+  out->ms_reverse = f2;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaEventDestroy(e2);
+  return GP_OK;
+}
+
+int gp_adjoint_replay(gp_ctx *c, long nsteps, double *max_abs_diff, long long *n_diff) {
+  gpd::AdjLaunch L;
+  int rc = adj_check(c, &L);
+  if (rc) return rc;
+  if (nsteps < 0 || !max_abs_diff || !n_diff) return fail(c, GP_EINVAL, "gp_adjoint_replay: bad argument");
+  c->err[0] = 0;
+  gp_batch *b = c->b;
+  const gpd::Grid &g = b->desc[0].g;
+  const int N = b->N, K = b->K;
+  const size_t S = (size_t)(N + K) * g.plane, Sd = (size_t)N * g.dplane;
+  const gpd::AdjParams prm = adj_params(b->params[0]);
+  AdjBufs m;
+  if (cudaMalloc((void **)&m.seg, 2 * S * 8) != cudaSuccess || cudaMalloc((void **)&m.dphi, Sd * 8) != cudaSuccess)
+    return fail(c, GP_ENOMEM, "gp_adjoint_replay: cudaMalloc failed");
+  double *a = m.seg, *a2 = m.seg + S;
+  CK(cudaMemcpyAsync(a, b->state[b->cur], S * 8, cudaMemcpyDeviceToDevice, b->stream));
+  for (long s = 0; s < nsteps; s++) {
+    CK(L.dphi(b->stream, b->d_consts, prm, g, a, m.dphi));
+    CK(L.update(b->stream, b->d_consts, prm, g, a, m.dphi, a2));
+    std::swap(a, a2);
+  }
+  if ((rc = batch_step_impl(b, nsteps, nullptr, nullptr, nullptr, nullptr)) != GP_OK) return rc;
+  std::vector<double> x(S), y(S);
+  CK(cudaMemcpyAsync(x.data(), a, S * 8, cudaMemcpyDeviceToHost, b->stream));
+  CK(cudaMemcpyAsync(y.data(), b->state[b->cur], S * 8, cudaMemcpyDeviceToHost, b->stream));
+  CK(cudaStreamSynchronize(b->stream));
+  double mxd = 0.0;
+  long long nd = 0;
+  for (int f = 0; f < N + K; f++)
+    for (int i = 0; i < g.mx; i++)
+      for (int j = 0; j < g.my; j++) {
+        const size_t o = (size_t)f * g.plane + (size_t)i * g.pitch + j;
+        if (memcmp(&x[o], &y[o], 8) != 0) {
+          nd++;
+          mxd = std::max(mxd, fabs(x[o] - y[o]));
+        }
+      }
+  *max_abs_diff = mxd;
+  *n_diff = nd;
+  return GP_OK;
+}
+
+}  /* extern "C" */
 
 /* ======================================================================= */
 /* One time step without any allocation (gp_step_noalloc in gp.h).          */

@@ -809,7 +809,7 @@ __global__ void __launch_bounds__(NT, 2) kf_bulk(const SimDesc *__restrict__ sim
 #pragma unroll
     for (int f = 0; f < (SUMS ? NS : 1); f++) acc[f] = 0.0;
     if (yvalid) {
-#pragma unroll 1
+#pragma unroll 2
       for (int i = 1; i <= rows; i++) {
         const int x = x0 + i - 1;
         R m[K], cn[K], nm[K];

@@ -217,11 +217,56 @@ void gp_batch_destroy(gp_batch *b);
  * device looks up that array's device address (cudaGetSymbolAddress); make
  * that first call before any stream capture.  All calls share the array, so
  * calls that overlap on the GPU (other streams, other host threads) race; the
- * same holds for the constant block shared with the contexts.  The call is
+ * same holds for the constant block its kernels read.  The call is
  * asynchronous on `stream`; no progress record is produced.  Results are those
  * of gp_step. */
 int gp_step_noalloc(const gp_params *p, const double *phi_in, const double *mu_in,
                     double *phi_out, double *mu_out, void *stream);
+
+/* ---- adjoint --------------------------------------------------------- */
+
+/* Gradients of a loss of the final state with respect to the start state and
+ * four parameters, through nsteps FP64 time steps of a context: the discrete
+ * adjoint of the step, i.e. exact derivatives of the computed trajectory.  The
+ * reference has no adjoint.  Contexts with NUMPHASES = 2, NUMCOMPONENTS = 2
+ * (one independent component, BINARY) and FP64 only; others get
+ * GP_EUNSUPPORTED.  The step is not differentiated where it branches (active
+ * phases, simplex projection, bulk test): derivatives are those of the branch
+ * the trajectory took.
+ * The forward pass runs from the context's current state and leaves the
+ * context at the final state (as gp_step would); states every
+ * checkpoint_every steps are kept on the device and each segment between them
+ * is recomputed once during the reverse sweep (about 2*sqrt(nsteps) stored
+ * states with the default). */
+typedef struct gp_adj_req {
+  long nsteps;                 /* time steps, >= 1 */
+  const double *phi_bar;       /* NULL, or [N][X][Y]: dL/dphi of the final state */
+  const double *mu_bar;        /* NULL (zero), or [K][X][Y]: dL/dmu of the final state */
+  const double *target_phi;    /* used when phi_bar is NULL: L = 1/2 sum over phases and
+                                  cells of (phi_final - target)^2 */
+  long checkpoint_every;       /* steps between stored states; 0 = ceil(sqrt(nsteps)) */
+} gp_adj_req;
+
+typedef struct gp_adj_out {
+  double loss;                 /* L with target_phi, else 0 */
+  double d_tau;                /* dL/dTau of phases (0,1); the mobility is 1/Tau */
+  double d_dab;                /* dL/d dab of phases (0,1): anisotropy strength */
+  double d_epsilon;            /* dL/d epsilon: interface width */
+  double d_gamma;              /* dL/d GAMMA of phases (0,1): interface energy */
+  double *phi0_bar;            /* NULL, or [N][X][Y]: receives dL/dphi of the start state */
+  double *mu0_bar;             /* NULL, or [K][X][Y]: receives dL/dmu of the start state */
+  double ms_forward;           /* device time of the forward pass */
+  double ms_reverse;           /* device time of the recomputation and reverse sweep */
+} gp_adj_out;
+
+int gp_adjoint(gp_ctx *ctx, const gp_adj_req *req, gp_adj_out *out);
+
+/* Verification of the adjoint's cell functions: nsteps steps evaluated with
+ * them (one thread per cell, no tiles) against gp_step's kernels from the same
+ * start state; *max_abs_diff receives the largest difference of any field
+ * value and *n_diff the number of values whose bits differ.  The context
+ * advances by nsteps. */
+int gp_adjoint_replay(gp_ctx *ctx, long nsteps, double *max_abs_diff, long long *n_diff);
 
 /* Stream the context's work is ordered on (a cudaStream_t as an opaque pointer). */
 void *gp_stream(gp_ctx *ctx);
