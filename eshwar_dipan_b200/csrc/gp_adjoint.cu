@@ -27,7 +27,10 @@
 
 namespace gpd {
 
-constexpr int ADJ_W = 8;
+#ifndef GP_ADJ_W
+#define GP_ADJ_W 1
+#endif
+constexpr int ADJ_W = GP_ADJ_W;
 constexpr int AB = 128;   /* threads per block along y */
 
 __device__ __forceinline__ int rmx(int x, const Grid &g, const Consts<double> *c, int f) {
@@ -54,6 +57,19 @@ __device__ __forceinline__ void gather(const Consts<double> *c, const Grid &g, c
       for (int k = 0; k < K; k++) M[k][di][dj] = st[(N + k) * g.plane + (long long)xm * g.pitch + ym];
     }
   }
+}
+
+/* phase whose exact one-hot phi (1.0 and +0.0) the values hold, or -1 */
+template <int N>
+__device__ __forceinline__ int one_hot_bits(const double *v) {
+  int p = -1, ones = 0, zeros = 0;
+#pragma unroll
+  for (int a = 0; a < N; a++) {
+    const long long b = __double_as_longlong(v[a]);
+    if (b == 0x3ff0000000000000LL) { p = a; ones++; }
+    else if (b == 0) zeros++;
+  }
+  return (ones == 1 && zeros == N - 1) ? p : -1;
 }
 
 __device__ __forceinline__ long long didx(const Grid &g, int a, int x, int y) {
@@ -121,6 +137,75 @@ __device__ __forceinline__ void flush_params(double (&pacc)[ADJ_NPARAM], double 
   }
 }
 
+/* Transposed update of a bulk cell (phase p one-hot over its 3x3 window, one
+ * independent component): nm = twoA*(cmu*(m - E) + dt*divflux - divjat) + E,
+ * divflux = (Fxf - Fxb)/dx + (Fyr - Fyl)/dy, F = (D(lower)+D(upper))/2 *
+ * (m(upper) - m(lower))/h with D(e) = sum_b DC_b phi_b(e), divjat constant;
+ * nphi = phi + dphi. */
+template <int N>
+__device__ __forceinline__ void bulk_rev(const Consts<double> *c, const Grid &g, int x, int y, int p,
+                                         const double (&S)[N][3][3], const double (&M)[1][3][3], const double *yb,
+                                         double *xbar, double *dphibar) {
+  const double idx = c->mul_dx ? c->inv_dx : 1.0 / c->dx, idy = c->mul_dy ? c->inv_dy : 1.0 / c->dy;
+  /* phi passes through, and so does the cell's own delta-phi */
+  const long long oc = (long long)x * g.pitch + y;
+#pragma unroll
+  for (int a = 0; a < N; a++) {
+    if (yb[a] == 0.0) continue;
+    atomicAdd(xbar + a * g.plane + oc, yb[a]);
+    atomicAdd(dphibar + didx(g, a, x, y), yb[a]);
+  }
+  const double ym = yb[N];
+  if (ym == 0.0) return;
+  const double cnb = ym * c->twoA[p][0];
+  /* the cell's own mu through c_mu */
+  double mbar_c = cnb * c->cmu[p][0][0];
+  const double dfb = cnb * c->dt;
+  /* faces: lower/upper cells in the window, the face's gradient scale, sign in divflux */
+  const int li[4] = {1, 0, 1, 1}, lj[4] = {1, 1, 1, 0}, ui[4] = {2, 1, 1, 1}, uj[4] = {1, 1, 2, 1};
+  const double sc[4] = {idx, idx, idy, idy}, sg[4] = {1.0, -1.0, 1.0, -1.0};
+  double Dw[3][3];
+#pragma unroll
+  for (int di = 0; di < 3; di++)
+#pragma unroll
+    for (int dj = 0; dj < 3; dj++) {
+      double d = 0.0;
+#pragma unroll
+      for (int b = 0; b < N; b++) d += c->DC[b][0][0][0] * S[b][di][dj];
+      Dw[di][dj] = d;
+    }
+  double Dbar[3][3] = {}, Mbar[3][3] = {};
+  Mbar[1][1] = mbar_c;
+#pragma unroll
+  for (int f = 0; f < 4; f++) {
+    const double Fb = dfb * sg[f] * sc[f];
+    const double dm = (Dw[ui[f]][uj[f]] + Dw[li[f]][lj[f]]) * 0.5;
+    const double gr = (M[0][ui[f]][uj[f]] - M[0][li[f]][lj[f]]) * sc[f];
+    const double gb = Fb * dm, dmb = Fb * gr;
+    Mbar[ui[f]][uj[f]] += gb * sc[f];
+    Mbar[li[f]][lj[f]] -= gb * sc[f];
+    Dbar[ui[f]][uj[f]] += 0.5 * dmb;
+    Dbar[li[f]][lj[f]] += 0.5 * dmb;
+  }
+  const int pi[5] = {1, 0, 2, 1, 1}, pj[5] = {1, 1, 1, 0, 2};
+#pragma unroll
+  for (int r = 0; r < 5; r++) {
+    const int di = pi[r], dj = pj[r];
+    if (Mbar[di][dj] != 0.0) {
+      const int xs = rmx(x + di - 1, g, c, 1), ys = rmy(y + dj - 1, g, c, 1);
+      atomicAdd(xbar + N * g.plane + (long long)xs * g.pitch + ys, Mbar[di][dj]);
+    }
+    if (Dbar[di][dj] != 0.0) {
+      const int xs = rmx(x + di - 1, g, c, 0), ys = rmy(y + dj - 1, g, c, 0);
+#pragma unroll
+      for (int b = 0; b < N; b++) {
+        const double v = Dbar[di][dj] * c->DC[b][0][0][0];
+        if (v != 0.0) atomicAdd(xbar + b * g.plane + (long long)xs * g.pitch + ys, v);
+      }
+    }
+  }
+}
+
 template <int N, int K>
 __global__ void __launch_bounds__(AB) ka_rev_update(const Consts<double> *__restrict__ c, AdjParams prm, Grid g,
                                                     const double *__restrict__ st, const double *__restrict__ dphi,
@@ -151,6 +236,31 @@ __global__ void __launch_bounds__(AB) ka_rev_update(const Consts<double> *__rest
 #pragma unroll
         for (int dj = 0; dj < 3; dj++) DP[a][di][dj] = dphi[didx(g, a, x + di - 1, y + dj - 1)];
     const int pi[5] = {1, 0, 2, 1, 1}, pj[5] = {1, 1, 1, 0, 2};
+    /* A cell whose 3x3 phi window holds one phase's exact one-hot phi has
+     * every face phi gradient 0.0 (no anti-trapping current is evaluated) and
+     * takes the bulk branch: its update is linear diffusion of mu with the
+     * face means of D(phi), transposed here directly (bulk_rev). */
+    int ph = -1;
+    bool uni;
+    {
+      double c0[N];
+#pragma unroll
+      for (int a = 0; a < N; a++) c0[a] = S[a][1][1];
+      ph = one_hot_bits<N>(c0);
+      uni = ph >= 0;
+#pragma unroll
+      for (int di = 0; di < 3; di++)
+#pragma unroll
+        for (int dj = 0; dj < 3; dj++) {
+          double v[N];
+#pragma unroll
+          for (int a = 0; a < N; a++) v[a] = S[a][di][dj];
+          uni = uni && one_hot_bits<N>(v) == ph;
+        }
+    }
+    if (uni && K == 1) {
+      bulk_rev<N>(c, g, x, y, ph, S, M, yb, xbar, dphibar);
+    } else
     for (int base = 0; base < NIN; base += ADJ_W) {
       DT Sd[N][3][3], Md[K][3][3], DPd[N][3][3], pd[ADJ_NPARAM];
 #pragma unroll
@@ -171,7 +281,7 @@ __global__ void __launch_bounds__(AB) ka_rev_update(const Consts<double> *__rest
 #pragma unroll
       for (int j = 0; j < ADJ_NPARAM; j++) pd[j] = DT(prm.v[j]);
       /* seed inputs base .. base+W-1 */
-      for (int w = 0; w < ADJ_W; w++) {
+      for (int w = 0; w < ADJ_W && base + w < NIN; w++) {
         const int id = base + w;
         if (id < NPHI) {
           const int a = id / 9, r = id % 9;
@@ -189,9 +299,8 @@ __global__ void __launch_bounds__(AB) ka_rev_update(const Consts<double> *__rest
       const AK<DT> D = make_ak<DT>(c, pd);
       DT nph[N], nm[K];
       update_cell<DT, N, K>(D, Sd, Md, DPd, y, g.my, nph, nm);
-      for (int w = 0; w < ADJ_W; w++) {
+      for (int w = 0; w < ADJ_W && base + w < NIN; w++) {
         const int id = base + w;
-        if (id >= NIN) break;
         double gsum = 0.0;
 #pragma unroll
         for (int a = 0; a < N; a++) gsum += yb[a] * nph[a].d[w];
@@ -236,9 +345,21 @@ __global__ void __launch_bounds__(AB) ka_rev_dphi(const Consts<double> *__restri
       any |= db[a] != 0.0;
     }
   }
+  double S[N][3][3], M[K][3][3];
   if (live && any) {
-    double S[N][3][3], M[K][3][3];
     gather<N, K>(c, g, st, x, y, S, M);
+    /* a cell with no active phase and no negative phi has delta-phi +0.0 whatever
+     * its inputs within the branch (dphi_cell's first return): no derivative */
+    bool active = false;
+#pragma unroll
+    for (int a = 0; a < N; a++) {
+      double gxf = (S[a][2][1] - S[a][1][1]), gxb = (S[a][1][1] - S[a][0][1]);
+      double gyr = (S[a][1][2] - S[a][1][1]), gyl = (S[a][1][1] - S[a][1][0]);
+      active |= (gxf - gxb) != 0.0 || (gyr - gyl) != 0.0 || S[a][1][1] < 0.0;
+    }
+    any = active;
+  }
+  if (live && any) {
     for (int base = 0; base < NIN; base += ADJ_W) {
       DT Sd[N][3][3], md[K], pd[ADJ_NPARAM];
 #pragma unroll
