@@ -71,6 +71,12 @@ def workload(name, scale=1):
         m = kw["mesh"][0]
         desc = ("ensemble member 0: %dx%d binary 2-phase, delta %.4f, c0 %.4f, %d seeds"
                 % (m, m, kw["dab"], kw["liquid_c"][0], len(seeds)))
+    elif name == "cfg5":
+        m = 512 // scale
+        kw = dict(N=2, K=1, mesh=(m, m), aniso=True, dab=0.04, d_solid=0.0, d_liquid=[1.0], dt=0.02, eps=4.0,
+                  T=1.0, liquid_c=[0.42])
+        seeds = [(0, m // 2, m // 2, 12.0 / scale)]
+        desc = "%dx%d binary 2-phase dendrite FP64, aniso 0.04, Neumann, one seed r=12" % (m, m)
     elif name == "cfg1":
         m = 256 // scale
         kw = dict(N=2, K=1, mesh=(m, m), aniso=False, dab=0.0, d_solid=0.0, d_liquid=[1.0], dt=0.02, eps=4.0,
@@ -301,7 +307,7 @@ def run_ensemble(args, rank, world, local, dist):
                 "h2d_bytes_per_step": host_bytes / e2e_steps, "d2h_bytes_per_step": host_bytes / e2e_steps,
                 "includes": "gp_batch_create upload of 256 simulations, %d smoothing sweeps, %d steps, "
                             "read-back of every simulation" % (params[0].nsmooth - 1, e2e_steps)},
-        "gpu_launches": 2 * args.steps + 2,
+        "gpu_launches": 3 * args.steps + 1,
         "clocks": clk.summary(),
         "nonfinite": nonfinite,
     }
@@ -311,13 +317,65 @@ def run_ensemble(args, rank, world, local, dist):
     return 0
 
 
+def run_adjoint(args, rank, world, local, dist):
+    """cfg5: gradients of the L2 mismatch of the final phi (target from a run with
+    Tau, dab, epsilon, GAMMA 5% larger) through the FP64 steps, by gp_adjoint."""
+    import ctypes
+    import eshwar_dipan_b200 as gp
+    work = tempfile.mkdtemp(prefix="gpadj")
+    ip, fp, desc, kw = write_workload(work, "cfg5")
+    p = gp.load_params(ip)
+    phi0, mu0 = gp.fill(p, fp)
+    with gp.Simulation(p, phi0, mu0) as s:
+        s.smooth(p.nsmooth - 1)
+        phi, mu = s.get()
+    nsteps = args.steps
+    q = gp.Params()
+    ctypes.memmove(ctypes.byref(q), ctypes.byref(p), ctypes.sizeof(p))
+    q.tau_ab[0][1] = q.tau_ab[1][0] = 1.05 * p.tau_ab[0][1]
+    q.dab[0][1] = q.dab[1][0] = 1.05 * p.dab[0][1]
+    q.epsilon = 1.05 * p.epsilon
+    q.gamma[0][1] = q.gamma[1][0] = 1.05 * p.gamma[0][1]
+    with gp.Simulation(q, phi, mu) as s:
+        s.step(nsteps, stats=False)
+        target = s.get()[0]
+    with gp.Simulation(p, phi, mu) as s:
+        s.step(args.warmup, stats=False)
+    with gp.Simulation(p, phi, mu) as s:
+        fwd_ms, _, _, _ = s.step_timed(nsteps)
+    with ClockSampler(local) as clk:
+        with gp.Simulation(p, phi, mu) as s:
+            g = s.adjoint(nsteps, target_phi=target)
+    cells = p.mesh_x * p.mesh_y
+    adj_ms = g["ms_forward"] + g["ms_reverse"]
+    if rank == 0:
+        out = {"metric": "cell-updates/s", "value": world * cells * nsteps / (adj_ms / 1e3), "unit": "cell-updates/s",
+               "n_gpus": world, "steps": nsteps, "warmup": args.warmup, "ms_per_step": adj_ms / nsteps,
+               "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+               "data": "synthetic (one seed at the centre)",
+               "config": {"workload": "cfg5: " + desc, "grid": [p.mesh_x, p.mesh_y], "phases": 2, "components": 1,
+                          "loss": "1/2 sum (phi_T - target)^2, target from Tau, dab, epsilon, GAMMA x 1.05",
+                          "checkpoints": "every ceil(sqrt(steps)) steps", "parallelism": "single"},
+               "adjoint": {"loss": g["loss"], "d_tau": g["d_tau"], "d_mobility": -g["d_tau"] * p.tau_ab[0][1] ** 2,
+                           "d_dab": g["d_dab"], "d_epsilon": g["d_epsilon"], "d_gamma": g["d_gamma"],
+                           "max_abs_dphi0": float(np.abs(g["phi0_bar"]).max()),
+                           "ms_forward_pass": g["ms_forward"], "ms_reverse_pass": g["ms_reverse"],
+                           "ms_plain_forward": fwd_ms, "cost_vs_forward": adj_ms / fwd_ms},
+               "gpu_launches": 3 * nsteps + 3 * (nsteps - int(np.ceil(nsteps / np.ceil(np.sqrt(nsteps))))) + 3 * nsteps,
+               "clocks": clk.summary(),
+               "note": "value = cell-updates of the differentiated steps per second of forward + reverse"}
+        print(json.dumps(out), flush=True)
+    shutil.rmtree(work, ignore_errors=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="cfg2", choices=["cfg1", "cfg2", "cfg3", "cfg4"])
+    ap.add_argument("--workload", default="cfg2", choices=["cfg1", "cfg2", "cfg3", "cfg4", "cfg5"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp32", action="store_true", help="skip the FP32 form beside the FP64 headline")
     args = ap.parse_args()
@@ -342,8 +400,8 @@ def main():
             dist.destroy_process_group()
         return rc
 
-    if args.workload == "cfg3":
-        rc = run_ensemble(args, rank, world, local, dist)
+    if args.workload in ("cfg3", "cfg5"):
+        rc = (run_ensemble if args.workload == "cfg3" else run_adjoint)(args, rank, world, local, dist)
         if dist:
             dist.destroy_process_group()
         return rc
@@ -457,7 +515,7 @@ def main():
                     "d2h_bytes_per_step": state_bytes * ngets / e2e_steps,
                     "includes": "gp_init upload, %d smoothing sweeps, %d steps, a state read-back every %d steps"
                                 % (p.nsmooth - 1, e2e_steps, savet)},
-            "gpu_launches": 2 * args.steps + 2,
+            "gpu_launches": 3 * args.steps + 1,
             "clocks": clk.summary(),
             "stats_last_step": st,
         }
@@ -474,7 +532,7 @@ def main():
                            "clocks": clk32,
                            "form": "fields stored and stepped in FP32, stochastic rounding of each commit; "
                                    "dc/dmu inversion, bulk dmu/dc and all sums in FP64"}
-            out["gpu_launches"] += 2 * args.steps + 2
+            out["gpu_launches"] += 3 * args.steps + 1
         if not args.no_cpu_baseline:
             out["cpu_baseline"] = cpu_baseline(args.workload)
         print(json.dumps(out), flush=True)

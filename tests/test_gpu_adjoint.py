@@ -158,3 +158,35 @@ def test_adjoint_rejects_unsupported(tmp_path):
     with gp.Simulation(p, phi, mu) as s:
         with pytest.raises(gp.GpError):
             s.adjoint(3, target_phi=phi)
+
+
+def test_torch_integrator_gradients(tmp_path):
+    """GPRollout (torch.autograd.Function over gp_step / gp_adjoint): torch's
+    backward returns the adjoint's gradients, and a torch gradient check of
+    the parameter gradient along one direction agrees with central differences."""
+    import torch
+    from eshwar_dipan_b200.integrator import GPRollout
+    p, phi0, mu0 = _params(tmp_path, "dendrite_aniso")
+    phi, mu = _start(p, phi0, mu0)
+    nsteps = 25
+    target = torch.from_numpy(_target(p, phi, mu, nsteps))
+    roll = GPRollout(p, nsteps)
+    th = roll.theta0().clone().requires_grad_(True)
+    a = torch.from_numpy(phi.copy()).requires_grad_(True)
+    m = torch.from_numpy(mu.copy()).requires_grad_(True)
+    phi_t, mu_t = roll(a, m, th)
+    loss = 0.5 * ((phi_t - target) ** 2).sum()
+    loss.backward()
+    with gp.Simulation(p, phi, mu) as s:
+        g = s.adjoint(nsteps, target_phi=target.numpy())
+    assert float(loss) == pytest.approx(g["loss"], rel=1e-12)
+    np.testing.assert_allclose(a.grad.numpy(), g["phi0_bar"], rtol=1e-9, atol=1e-14)
+    np.testing.assert_allclose(th.grad.numpy(), [g["d_tau"], g["d_dab"], g["d_epsilon"], g["d_gamma"]], rtol=1e-9)
+    v = torch.tensor([1.0, 0.5, -0.25, 0.75], dtype=torch.float64)
+    h = 1e-6
+    with torch.no_grad():
+        lp = 0.5 * ((roll(a, m, th + h * v)[0] - target) ** 2).sum()
+        lm = 0.5 * ((roll(a, m, th - h * v)[0] - target) ** 2).sum()
+    fd = float((lp - lm) / (2 * h))
+    ad = float((th.grad * v).sum())
+    assert abs(ad - fd) <= 1e-5 * abs(fd), (ad, fd)
