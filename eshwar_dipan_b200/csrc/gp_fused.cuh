@@ -708,7 +708,7 @@ __global__ void __launch_bounds__(NT, 2) kf_bulk(const SimDesc *__restrict__ sim
   const int per = (nbulk + nwarps - 1) / nwarps;
   const int i0 = gw * per, i1 = min(nbulk, i0 + per);
 
-  double emax[K], emin[K];
+  R emax[K], emin[K];   /* running mu extremes of the cells this warp stepped */
 #pragma unroll
   for (int k = 0; k < K; k++) { emax[k] = -INFINITY; emin[k] = INFINITY; }
   int cur_sim = -1;
@@ -791,15 +791,16 @@ __global__ void __launch_bounds__(NT, 2) kf_bulk(const SimDesc *__restrict__ sim
       }
     /* constants of c_mu / Mu of phase p (FP64 update) */
     R cmu[K][K], E[K], twoA[K], Aoff[K][K];
-    double muc[K][K];
+    R muc[K][K];
 #pragma unroll
     for (int k = 0; k < K; k++) {
       E[k] = D.E[p][k];
       twoA[k] = D.twoA[p][k];
 #pragma unroll
-      for (int l = 0; l < K; l++) { cmu[k][l] = D.cmu[p][k][l]; Aoff[k][l] = D.A[p][k][l]; muc[k][l] = D.muc64[p][k][l]; }
+      for (int l = 0; l < K; l++) { cmu[k][l] = D.cmu[p][k][l]; Aoff[k][l] = D.A[p][k][l]; muc[k][l] = (R)D.muc64[p][k][l]; }
     }
-    const unsigned rkey = sizeof(R) == 4 ? __ldg(st.round_step) : 0u;
+    /* FP32: the step's part of the rounding key, hashed once per tile */
+    const unsigned skey = sizeof(R) == 4 ? mix32(__ldg(st.round_step) * 0x9e3779b9u + 0x632be5abu) : 0u;
     R *phin = next + sd.off_state;
     R *mun = phin + (long long)N * g.plane;
     const int y = y0 + lane, j = lane + 1;
@@ -853,21 +854,23 @@ __global__ void __launch_bounds__(NT, 2) kf_bulk(const SimDesc *__restrict__ sim
             dmu[k] = (double)nm[k] - (double)m[k];
           }
         } else {
-          const unsigned key = round_key(rkey, x, y);
+          /* mu += (dmu/dc) dc of the pure phase in float (no c -> mu round
+           * trip), the sum rounded stochastically from its exact TwoSum
+           * split, 16 random bits per field from one hash of the cell */
+          const unsigned key = mix32(skey ^ ((unsigned)x * 0x85ebca6bu + (unsigned)y * 0xc2b2ae35u));
 #pragma unroll
           for (int k = 0; k < K; k++) {
-            double sdm = 0.0;
+            R sdm = R(0.0);
 #pragma unroll
-            for (int l = 0; l < K; l++) sdm += muc[k][l] * (double)cn[l];
-            dmu[k] = sdm;
-            nm[k] = (R)round_stochastic((double)m[k] + sdm, key, N + k);
+            for (int l = 0; l < K; l++) sdm += muc[k][l] * cn[l];
+            dmu[k] = (double)sdm;
+            nm[k] = (R)add_stochastic((float)m[k], (float)sdm, (key >> (16 * (k & 1))) & 0xffffu);
           }
         }
 #pragma unroll
         for (int k = 0; k < K; k++) {
           mun[k * g.plane + o] = nm[k];
-          const double w = (double)nm[k];
-          if (w == w) { emax[k] = fmax(emax[k], w); emin[k] = fmin(emin[k], w); }
+          if (nm[k] == nm[k]) { emax[k] = fmax(emax[k], nm[k]); emin[k] = fmin(emin[k], nm[k]); }
         }
         if (have != p) {
 #pragma unroll

@@ -463,6 +463,20 @@ __device__ __forceinline__ float round_stochastic(double v, unsigned key, int fi
   return fabs(rem) > u * fabs(span) ? hi : lo;
 }
 
+/* a + b rounded to float stochastically without leaving float: TwoSum gives
+ * the round-to-nearest sum s and the exact remainder e (s + e = a + b); the
+ * neighbour t of s on the side of e is taken with probability |e| / |t - s|,
+ * decided by the 16-bit uniform r16 (the probability is exact to 2^-16). */
+__device__ __forceinline__ float add_stochastic(float a, float b, unsigned r16) {
+  const float s = a + b;
+  const float bb = s - a;
+  const float e = (a - (s - bb)) + (b - bb);
+  if (e == 0.0f) return s;
+  const float t = nextafterf(s, e > 0.0f ? INFINITY : -INFINITY);
+  const float u = (float)r16 * (1.0f / 65536.0f);
+  return fabsf(e) > u * fabsf(t - s) ? t : s;
+}
+
 /* FP32 commit of a pure-phase cell: mu += muc_a * dc in FP64, phi += dphi,
  * both rounded stochastically. */
 template <typename R, int N, int K>
