@@ -472,13 +472,18 @@ __device__ __forceinline__ TileFlags general_tile(const CT &D, const Grid &g, co
   }
   const bool blockact = __syncthreads_or(any);
   if (ANISO && blockact) {
+    /* only the faces of active ring cells are read by ring_dphi */
     for (int e = threadIdx.x; e < RXF + RYF; e += NT) {
       if (e < RXF) {
         const int fi = e / (TY + 2), fj = e - fi * (TY + 2) + 1;
-        ring_face_terms<R, N>(D, sm.P, sm.w.T, true, fi, fj, e);
+        /* ring cells (fi-1, fj-1) and (fi, fj-1) */
+        const bool need = (fi >= 1 && sm.ACT[LI(fi - 1, fj - 1)]) || (fi < SH && sm.ACT[LI(fi, fj - 1)]);
+        if (need) ring_face_terms<R, N>(D, sm.P, sm.w.T, true, fi, fj, e);
       } else {
         const int f = e - RXF, fi = f / (TY + 3) + 1, fj = f - (fi - 1) * (TY + 3);
-        ring_face_terms<R, N>(D, sm.P, sm.w.T, false, fi, fj, e);
+        /* ring cells (fi-1, fj-1) and (fi-1, fj) */
+        const bool need = (fj >= 1 && sm.ACT[LI(fi - 1, fj - 1)]) || (fj < SW && sm.ACT[LI(fi - 1, fj)]);
+        if (need) ring_face_terms<R, N>(D, sm.P, sm.w.T, false, fi, fj, e);
       }
     }
   }
