@@ -19,11 +19,12 @@ struct BatchLaunch {
   cudaError_t (*classify)(int ntiles, cudaStream_t s, const SimDesc *sims, const void *consts, const int *tsim,
                           const TileFlags *flag_in, int *glist, int *blist, int *ctr);
   /* mul: every simulation's spacings are powers of two (x/dx == x*(1/dx)) */
+  /* ndone: the CTAs of this step's kf_bulk and kf_general together */
   cudaError_t (*bulk)(int grid, bool mul, cudaStream_t s, const SimDesc *sims, const void *consts, const int *tsim,
-                      const int *blist, const void *state, void *next, TileFlags *flag_out, const int *ctr,
+                      const int *blist, const void *state, void *next, TileFlags *flag_out, int *ctr, int ndone,
                       StatBufs st);
   cudaError_t (*general)(int grid, bool mul, cudaStream_t s, const SimDesc *sims, const void *consts, const int *tsim,
-                         const void *state, void *next, TileFlags *flag_out, const int *glist, int *ctr,
+                         const void *state, void *next, TileFlags *flag_out, const int *glist, int *ctr, int ndone,
                          StatBufs st);
   cudaError_t (*flags)(int ntiles, cudaStream_t s, const SimDesc *sims, const int *tsim, const void *state,
                        TileFlags *flags);
@@ -65,10 +66,10 @@ struct BatchKernels {
   }
   static cudaError_t bulk(int grid, bool mul, cudaStream_t s, const SimDesc *sims, const void *consts,
                           const int *tsim, const int *blist, const void *state, void *next, TileFlags *flag_out,
-                          const int *ctr, StatBufs st) {
+                          int *ctr, int ndone, StatBufs st) {
 #define GP_BULK(SUMS, MUL)                                                                                     \
   kf_bulk<R, N, K, SUMS, MUL><<<grid, NT, bulk_smem, s>>>(sims, (const Consts<R> *)consts, tsim, blist,         \
-                                                          (const R *)state, (R *)next, flag_out, ctr, st)
+                                                          (const R *)state, (R *)next, flag_out, ctr, ndone, st)
     if (st.want_sums) {
       if (mul) GP_BULK(true, true);
       else GP_BULK(true, false);
@@ -81,13 +82,13 @@ struct BatchKernels {
   }
   static cudaError_t general(int grid, bool mul, cudaStream_t s, const SimDesc *sims, const void *consts,
                              const int *tsim, const void *state, void *next, TileFlags *flag_out, const int *glist,
-                             int *ctr, StatBufs st) {
+                             int *ctr, int ndone, StatBufs st) {
     if (mul)
       kf_general<R, N, K, A, true><<<grid, NT, sizeof(GenSmem<R, N, K>), s>>>(
-          sims, (const Consts<R> *)consts, tsim, (const R *)state, (R *)next, flag_out, glist, ctr, st);
+          sims, (const Consts<R> *)consts, tsim, (const R *)state, (R *)next, flag_out, glist, ctr, ndone, st);
     else
       kf_general<R, N, K, A, false><<<grid, NT, sizeof(GenSmem<R, N, K>), s>>>(
-          sims, (const Consts<R> *)consts, tsim, (const R *)state, (R *)next, flag_out, glist, ctr, st);
+          sims, (const Consts<R> *)consts, tsim, (const R *)state, (R *)next, flag_out, glist, ctr, ndone, st);
     return cudaGetLastError();
   }
   static cudaError_t flags(int ntiles, cudaStream_t s, const SimDesc *sims, const int *tsim, const void *state,

@@ -309,11 +309,13 @@ static int batch_step_once(gp_batch *b, int want_sums, cudaEvent_t *ev) {
   if (ev) BK(cudaEventRecord(ev[0], b->stream));
   BK(b->L.classify(b->ntiles, b->stream, b->d_desc, b->d_consts, b->d_tsim, b->flags[in], b->glist, b->blist,
                    b->counters));
+  /* kf_bulk then kf_general; the last CTA of the two resets the lists */
+  const int nd = b->grid_b + b->grid_g;
   BK(b->L.bulk(b->grid_b, b->mul, b->stream, b->d_desc, b->d_consts, b->d_tsim, b->blist, b->state[in],
-               b->state[out], b->flags[out], b->counters, st));
+               b->state[out], b->flags[out], b->counters, nd, st));
   if (ev) BK(cudaEventRecord(ev[1], b->stream));
   BK(b->L.general(b->grid_g, b->mul, b->stream, b->d_desc, b->d_consts, b->d_tsim, b->state[in], b->state[out],
-                  b->flags[out], b->glist, b->counters, st));
+                  b->flags[out], b->glist, b->counters, nd, st));
   if (ev) BK(cudaEventRecord(ev[2], b->stream));
   b->cur = out;
   b->steps++;

@@ -625,11 +625,33 @@ __device__ __forceinline__ TileFlags general_tile(const CT &D, const Grid &g, co
 /* ------------------------------------------------------------------ */
 
 /* Work-list counters of a batch: [0] interface tiles listed by kf_classify,
- * [1] next interface entry to take, [2] kf_general CTAs finished, [3] step
- * number (keys the FP32 rounding stream), [4] bulk tiles listed.  kf_general's
- * last CTA resets [0..2] and [4] and advances [3], so a step is exactly the
- * three launches kf_classify, kf_bulk, kf_general. */
+ * [1] next interface entry to take, [2] CTAs of kf_bulk and kf_general
+ * finished, [3] step number (keys the FP32 rounding stream), [4] bulk tiles
+ * listed.  The last CTA of the two kernels resets [0..2] and [4] and advances
+ * [3], so a step is exactly the three launches kf_classify, then kf_bulk and
+ * kf_general (in either order or side by side). */
 enum { CTR_LIST = 0, CTR_HEAD = 1, CTR_DONE = 2, CTR_STEP = 3, CTR_BULK = 4, CTR_COUNT = 8 };
+
+/* End of one CTA of the step's bulk or interface kernel (they may run
+ * concurrently): the last of the step's ndone CTAs empties the lists and
+ * advances the step counter.  Call with all threads. */
+__device__ __forceinline__ void step_finish(int *ctr, int ndone) {
+  __shared__ int s_last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    s_last = atomicAdd(ctr + CTR_DONE, 1) == ndone - 1;
+  }
+  __syncthreads();
+  if (s_last && threadIdx.x == 0) {
+    ctr[CTR_LIST] = 0;
+    ctr[CTR_HEAD] = 0;
+    ctr[CTR_DONE] = 0;
+    ctr[CTR_BULK] = 0;
+    ctr[CTR_STEP] = (int)((unsigned)ctr[CTR_STEP] + 1u);
+    __threadfence();
+  }
+}
 
 /* One thread per tile: the bulk test, then the tile goes on the bulk list
  * (entry t | phase << 28) or the interface list; one atomic per warp and
@@ -702,8 +724,8 @@ template <typename R, int N, int K, bool SUMS, bool MUL>
 __global__ void __launch_bounds__(NT, 2) kf_bulk(const SimDesc *__restrict__ sims, const Consts<R> *__restrict__ consts,
                                                  const int *__restrict__ tsim, const int *__restrict__ blist,
                                                  const R *__restrict__ state, R *__restrict__ next,
-                                                 TileFlags *__restrict__ flag_out, const int *__restrict__ ctr,
-                                                 StatBufs st) {
+                                                 TileFlags *__restrict__ flag_out, int *__restrict__ ctr,
+                                                 int ndone, StatBufs st) {
   constexpr int NW = NT / 32, NS = 2 * N + 2 * K + 1;
   extern __shared__ __align__(16) unsigned char smraw[];
   BulkWarpStage<R, N, K> &stg = reinterpret_cast<BulkWarpStage<R, N, K> *>(smraw)[threadIdx.x >> 5];
@@ -916,6 +938,7 @@ __global__ void __launch_bounds__(NT, 2) kf_bulk(const SimDesc *__restrict__ sim
     b ^= 1;
   }
   if (cur_sim >= 0) flush(cur_sim);
+  step_finish(ctr, ndone);
 }
 
 /* Persistent CTAs over the interface list.  Each simulation's constants are
@@ -925,11 +948,11 @@ __global__ void __launch_bounds__(NT, (N <= 3 ? 2 : 1)) kf_general(const SimDesc
                                                  const Consts<R> *__restrict__ consts, const int *__restrict__ tsim,
                                                  const R *__restrict__ state, R *__restrict__ next,
                                                  TileFlags *__restrict__ flag_out, const int *__restrict__ glist,
-                                                 int *__restrict__ ctr, StatBufs st) {
+                                                 int *__restrict__ ctr, int ndone, StatBufs st) {
   extern __shared__ __align__(16) unsigned char smraw[];
   GenSmem<R, N, K> &sm = *reinterpret_cast<GenSmem<R, N, K> *>(smraw);
   __shared__ Consts<R> sc;
-  __shared__ int s_item, s_last;
+  __shared__ int s_item;
   const int nlist = *(volatile int *)(ctr + CTR_LIST);
   int cur_sim = -1;
   for (;;) {
@@ -955,20 +978,7 @@ __global__ void __launch_bounds__(NT, (N <= 3 ? 2 : 1)) kf_general(const SimDesc
     if (threadIdx.x == 0) flag_out[t] = f;
     __syncthreads();
   }
-  /* the last CTA to finish empties the list for the next step */
-  if (threadIdx.x == 0) {
-    __threadfence();
-    s_last = atomicAdd(ctr + CTR_DONE, 1) == (int)gridDim.x - 1;
-  }
-  __syncthreads();
-  if (s_last && threadIdx.x == 0) {
-    ctr[CTR_LIST] = 0;
-    ctr[CTR_HEAD] = 0;
-    ctr[CTR_DONE] = 0;
-    ctr[CTR_BULK] = 0;
-    ctr[CTR_STEP] = (int)((unsigned)ctr[CTR_STEP] + 1u);
-    __threadfence();
-  }
+  step_finish(ctr, ndone);
 }
 
 /* Flags of every tile of a state buffer from its phi (after an upload,
