@@ -221,10 +221,13 @@ def fp32_form(gp, p, phi0, mu0, args, phi64, st64, local):
     with ClockSampler(local) as clk:
         ms, _, _, st = s.step_timed(args.steps, stats=True)
     phi32, _ = s.get()
+    nsplit = min(args.steps, 50)
+    _, bulk_ms, iface_ms, _ = s.step_timed(nsplit, split=True)
     s.close()
     err = np.abs(phi32 - phi64)
     drift = [abs(a - b) / abs(b) for a, b in zip(st["comp_sum"], st64["comp_sum"])]
-    return ms, clk.summary(), float(err.max()), float(np.sqrt((err ** 2).mean())), drift
+    split = {"kf_bulk": bulk_ms / nsplit, "kf_general": iface_ms / nsplit, "split_run_steps": nsplit}
+    return ms, clk.summary(), float(err.max()), float(np.sqrt((err ** 2).mean())), drift, split
 
 
 def run_ensemble(args, rank, world, local, dist):
@@ -453,11 +456,13 @@ def main():
             fp32 = (float(t.item()),) + fp32[1:]
 
     # ---- end to end through the C ABI with host buffers ----------------------
-    # gp_init uploads the host state, gp_smooth + gp_step run, and every SAVET=50
-    # steps the state is read back to the host (what the CLI does before writing
-    # a VTK file); wall clock around the whole sequence.
+    # gp_init uploads the host state, gp_smooth + gp_step run, and every
+    # SAVET=1000 steps the step statistics are returned and the state is read
+    # back to the host (what the CLI does before printing its progress line and
+    # writing a VTK file); wall clock around the whole sequence.
     L = gp._abi.lib()
-    savet = 50
+    savet = 1000
+    prog = gp.Stats()
     barrier()
     t0 = time.perf_counter()
     h = ctypes.c_void_p()
@@ -470,7 +475,7 @@ def main():
     done, ngets = 0, 0
     while done < args.steps:
         n = min(savet, args.steps - done)
-        gp._abi.check(L.gp_step(h, n, None), h)
+        gp._abi.check(L.gp_step(h, n, ctypes.byref(prog)), h)
         gp._abi.check(L.gp_get(h, phi_h.ctypes.data_as(ctypes.c_void_p), mu_h.ctypes.data_as(ctypes.c_void_p)), h)
         done += n
         ngets += 1
@@ -520,7 +525,7 @@ def main():
             "stats_last_step": st,
         }
         if fp32:
-            ms32, clk32, emax, el2, drift = fp32
+            ms32, clk32, emax, el2, drift, split32 = fp32
             v32 = world * cells * args.steps / (ms32 / 1e3)
             a32 = (N + K) * 2 * 4 * cells * args.steps / (ms32 / 1e3) / 1e9
             out["fp32"] = {"value": v32, "unit": "cell-updates/s", "ms_per_step": ms32 / args.steps,
@@ -529,9 +534,11 @@ def main():
                                         "bytes_per_cell": (N + K) * 2 * 4},
                            "error_vs_fp64": {"after_steps": args.warmup + args.steps, "max_abs_dphi": emax,
                                              "l2_dphi": el2, "mass_rel_diff": drift},
+                           "kernels_ms_per_step": split32,
                            "clocks": clk32,
                            "form": "fields stored and stepped in FP32, stochastic rounding of each commit; "
-                                   "dc/dmu inversion, bulk dmu/dc and all sums in FP64"}
+                                   "interface dc/dmu inversion, anisotropy and all sums in FP64; bulk "
+                                   "mu += (dmu/dc) dc in FP32 rounded stochastically from its exact TwoSum split"}
             out["gpu_launches"] += 3 * args.steps + 1
         if not args.no_cpu_baseline:
             out["cpu_baseline"] = cpu_baseline(args.workload)
