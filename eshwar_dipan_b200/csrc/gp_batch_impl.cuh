@@ -20,9 +20,11 @@ struct BatchLaunch {
                           const TileFlags *flag_in, int *glist, int *blist, int *ctr);
   /* mul: every simulation's spacings are powers of two (x/dx == x*(1/dx)) */
   /* ndone: the CTAs of this step's kf_bulk and kf_general together */
+  /* tmaps: per simulation two tensor maps of its mu planes (state buffer 0
+   * and 1); buf: the buffer `state` is */
   cudaError_t (*bulk)(int grid, bool mul, cudaStream_t s, const SimDesc *sims, const void *consts, const int *tsim,
-                      const int *blist, const void *state, void *next, TileFlags *flag_out, int *ctr, int ndone,
-                      StatBufs st);
+                      const int *blist, const TensorMapSlot *tmaps, int buf, const void *state, void *next,
+                      TileFlags *flag_out, int *ctr, int ndone, StatBufs st);
   cudaError_t (*general)(int grid, bool mul, cudaStream_t s, const SimDesc *sims, const void *consts, const int *tsim,
                          const void *state, void *next, TileFlags *flag_out, const int *glist, int *ctr, int ndone,
                          StatBufs st);
@@ -36,7 +38,7 @@ struct BatchLaunch {
 
 template <typename R, int N, int K, bool A>
 struct BatchKernels {
-  static constexpr size_t bulk_smem = (NT / 32) * sizeof(BulkWarpStage<R, N, K>);
+  static constexpr size_t bulk_smem = bulk_smem_bytes<R, K>();
   template <bool SUMS, bool MUL>
   static cudaError_t bulk_attr() {
     return cudaFuncSetAttribute(kf_bulk<R, N, K, SUMS, MUL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -65,11 +67,11 @@ struct BatchKernels {
     return cudaGetLastError();
   }
   static cudaError_t bulk(int grid, bool mul, cudaStream_t s, const SimDesc *sims, const void *consts,
-                          const int *tsim, const int *blist, const void *state, void *next, TileFlags *flag_out,
-                          int *ctr, int ndone, StatBufs st) {
+                          const int *tsim, const int *blist, const TensorMapSlot *tmaps, int buf,
+                          const void *state, void *next, TileFlags *flag_out, int *ctr, int ndone, StatBufs st) {
 #define GP_BULK(SUMS, MUL)                                                                                     \
-  kf_bulk<R, N, K, SUMS, MUL><<<grid, NT, bulk_smem, s>>>(sims, (const Consts<R> *)consts, tsim, blist,         \
-                                                          (const R *)state, (R *)next, flag_out, ctr, ndone, st)
+  kf_bulk<R, N, K, SUMS, MUL><<<grid, NT, bulk_smem, s>>>(sims, (const Consts<R> *)consts, tsim, blist, tmaps,  \
+                                                          buf, (const R *)state, (R *)next, flag_out, ctr, ndone, st)
     if (st.want_sums) {
       if (mul) GP_BULK(true, true);
       else GP_BULK(true, false);

@@ -13,6 +13,8 @@
  *  - gp_step_noalloc: one FP64 step on caller-owned buffers, two-pass kernels
  *    with constants in __constant__ memory and a fixed scratch array.
  */
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -270,6 +272,7 @@ struct gp_batch {
   int *glist;                   /* interface tiles of the current step */
   int *blist;                   /* bulk tiles of the current step (tile | phase << 28) */
   int *counters;                /* gpd::CTR_* */
+  gpd::TensorMapSlot *tmaps;    /* [nsims][2]: TMA maps of each simulation's mu planes in state[0], state[1] */
   int cur;
   long long *ext;               /* running extremes per simulation [nsims][2(N+K)] */
   double *partials, *sums_sim;
@@ -311,8 +314,8 @@ static int batch_step_once(gp_batch *b, int want_sums, cudaEvent_t *ev) {
                    b->counters));
   /* kf_bulk then kf_general; the last CTA of the two resets the lists */
   const int nd = b->grid_b + b->grid_g;
-  BK(b->L.bulk(b->grid_b, b->mul, b->stream, b->d_desc, b->d_consts, b->d_tsim, b->blist, b->state[in],
-               b->state[out], b->flags[out], b->counters, nd, st));
+  BK(b->L.bulk(b->grid_b, b->mul, b->stream, b->d_desc, b->d_consts, b->d_tsim, b->blist, b->tmaps, in,
+               b->state[in], b->state[out], b->flags[out], b->counters, nd, st));
   if (ev) BK(cudaEventRecord(ev[1], b->stream));
   BK(b->L.general(b->grid_g, b->mul, b->stream, b->d_desc, b->d_consts, b->d_tsim, b->state[in], b->state[out],
                   b->flags[out], b->glist, b->counters, nd, st));
@@ -343,6 +346,19 @@ static int batch_fold_stats(gp_batch *b, gp_stats *out) {
   for (int s = 0; s < b->nsims; s++) {
     stats_from(&b->last[s], &mm[(size_t)s * ne], &sums[(size_t)s * ns], N, K, b->steps);
     if (out) out[s] = b->last[s];
+  }
+  return GP_OK;
+}
+
+/* The error flag of the step kernels (a TMA box of kf_bulk that did not
+ * arrive within its poll limit): read, clear, report. */
+static int batch_check_error(gp_batch *b) {
+  int e = 0;
+  BK(cudaMemcpyAsync(&e, b->counters + gpd::CTR_ERR, sizeof e, cudaMemcpyDeviceToHost, b->stream));
+  BK(cudaStreamSynchronize(b->stream));
+  if (e) {
+    BK(cudaMemsetAsync(b->counters + gpd::CTR_ERR, 0, sizeof e, b->stream));
+    return bfail(b, GP_ECUDA, "kf_bulk: a tile's mu did not arrive within the wait limit; the state is not valid");
   }
   return GP_OK;
 }
@@ -398,6 +414,8 @@ static int batch_step_impl(gp_batch *b, long nsteps, gp_stats *stats, double *to
   }
   if (ms_bulk) *ms_bulk = tb;
   if (ms_iface) *ms_iface = ti;
+  int rc = batch_check_error(b);
+  if (rc != GP_OK) return rc;
   if (stats && nsteps > 0) return batch_fold_stats(b, stats);
   BK(cudaStreamSynchronize(b->stream));
   if (stats)
@@ -445,6 +463,49 @@ static int batch_copy(gp_batch *b, int s, const double *phi, const double *mu, d
   return GP_OK;
 }
 
+static_assert(sizeof(CUtensorMap) == sizeof(gpd::TensorMapSlot), "tensor map size");
+
+/* cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+ * against libcuda) */
+static PFN_cuTensorMapEncodeTiled_v12000 encode_tiled_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+  }
+  return fn;
+}
+
+/* The TMA maps of kf_bulk: per simulation and state buffer, the K mu planes
+ * as a 3-D tensor {pitch, mx, K} (strides one row, one plane) read in boxes
+ * of {BW, SH, K}; coordinates outside the tensor read zeros. */
+static int encode_mu_maps(gp_batch *b, gpd::TensorMapSlot *out) {
+  PFN_cuTensorMapEncodeTiled_v12000 fn = encode_tiled_fn();
+  if (!fn) return bfail(b, GP_ECUDA, "gp_batch_create: cuTensorMapEncodeTiled is not available");
+  const bool f64 = b->elem == 8;
+  const cuuint32_t bw = f64 ? gpd::BulkGeom<double, 1>::BW : gpd::BulkGeom<float, 1>::BW;
+  for (int s = 0; s < b->nsims; s++) {
+    const gpd::SimDesc &sd = b->desc[s];
+    for (int p = 0; p < 2; p++) {
+      void *base = (char *)b->state[p] + (size_t)(sd.off_state + (long long)b->N * sd.g.plane) * b->elem;
+      const cuuint64_t dims[3] = {(cuuint64_t)sd.g.pitch, (cuuint64_t)sd.g.mx, (cuuint64_t)b->K};
+      const cuuint64_t strides[2] = {(cuuint64_t)sd.g.pitch * b->elem, (cuuint64_t)sd.g.plane * b->elem};
+      const cuuint32_t box[3] = {bw, (cuuint32_t)gpd::SH, (cuuint32_t)b->K};
+      const cuuint32_t estr[3] = {1, 1, 1};
+      CUresult r = fn((CUtensorMap *)&out[2 * s + p],
+                      f64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims,
+                      strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                      CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+      if (r != CUDA_SUCCESS)
+        return bfail(b, GP_ECUDA, "gp_batch_create: cuTensorMapEncodeTiled failed (%d) for simulation %d", (int)r, s);
+    }
+  }
+  return GP_OK;
+}
+
 extern "C" {
 
 void gp_batch_destroy(gp_batch *b) {
@@ -469,6 +530,7 @@ void gp_batch_destroy(gp_batch *b) {
   cudaFree(b->partials);
   cudaFree(b->sums_sim);
   cudaFree(b->counters);
+  cudaFree(b->tmaps);
   if (b->stream) cudaStreamDestroy(b->stream);
   delete b;
 }
@@ -595,7 +657,14 @@ int gp_batch_create(gp_batch **out, int nsims, const gp_params *params, const do
   BALLOC(b->partials, sizeof(double) * (size_t)ns * nt);
   BALLOC(b->sums_sim, sizeof(double) * (size_t)ns * nsims);
   BALLOC(b->counters, gpd::CTR_COUNT * sizeof(int));
+  BALLOC(b->tmaps, sizeof(gpd::TensorMapSlot) * 2 * (size_t)nsims);
 #undef BALLOC
+  std::vector<gpd::TensorMapSlot> tm(2 * (size_t)nsims);
+  if (encode_mu_maps(b, tm.data()) != GP_OK) {
+    rc = GP_ECUDA;
+    gp_batch_destroy(b);
+    return rc;
+  }
   std::vector<long long> ext((size_t)ne * nsims);
   for (int t = 0; t < nsims; t++) init_ext(&ext[(size_t)t * ne], N, K);
 #define BUP(dst, src, bytes)                                                                       \
@@ -612,6 +681,7 @@ int gp_batch_create(gp_batch **out, int nsims, const gp_params *params, const do
   BUP(b->d_seg0, seg0.data(), sizeof(int) * nsims);
   BUP(b->d_segn, segn.data(), sizeof(int) * nsims);
   BUP(b->ext, ext.data(), sizeof(long long) * ext.size());
+  BUP(b->tmaps, tm.data(), sizeof(gpd::TensorMapSlot) * tm.size());
 #undef BUP
   if (cudaMemsetAsync(b->dphi, 0, (size_t)offd * b->elem, b->stream) != cudaSuccess ||
       cudaMemsetAsync(b->counters, 0, gpd::CTR_COUNT * sizeof(int), b->stream) != cudaSuccess) {

@@ -14,7 +14,7 @@
  *
  *  kf_classify one thread per tile: the bulk test; bulk and interface lists.
  *  kf_bulk     persistent warps over contiguous ranges of the bulk list, the
- *              next tile's mu in flight (cp.async) while one is stepped.  Bulk
+ *              next tile's mu in flight (one TMA box) while one is stepped.  Bulk
  *              tiles read and write mu only (phi is rewritten only when the
  *              output buffer does not already hold the same one-hot tile).
  *  kf_general  persistent CTAs over the interface list.  Stages phi with a
@@ -627,10 +627,11 @@ __device__ __forceinline__ TileFlags general_tile(const CT &D, const Grid &g, co
 /* Work-list counters of a batch: [0] interface tiles listed by kf_classify,
  * [1] next interface entry to take, [2] CTAs of kf_bulk and kf_general
  * finished, [3] step number (keys the FP32 rounding stream), [4] bulk tiles
- * listed.  The last CTA of the two kernels resets [0..2] and [4] and advances
- * [3], so a step is exactly the three launches kf_classify, then kf_bulk and
- * kf_general (in either order or side by side). */
-enum { CTR_LIST = 0, CTR_HEAD = 1, CTR_DONE = 2, CTR_STEP = 3, CTR_BULK = 4, CTR_COUNT = 8 };
+ * listed, [5] error flag (a TMA box of kf_bulk did not arrive; the host reads
+ * and clears it).  The last CTA of the two kernels resets [0..2] and [4] and
+ * advances [3], so a step is exactly the three launches kf_classify, then
+ * kf_bulk and kf_general (in either order or side by side). */
+enum { CTR_LIST = 0, CTR_HEAD = 1, CTR_DONE = 2, CTR_STEP = 3, CTR_BULK = 4, CTR_ERR = 5, CTR_COUNT = 8 };
 
 /* End of one CTA of the step's bulk or interface kernel (they may run
  * concurrently): the last of the step's ndone CTAs empties the lists and
@@ -686,17 +687,46 @@ __global__ void __launch_bounds__(NT) kf_classify(const SimDesc *__restrict__ si
   }
 }
 
-/* cp.async of one 4- or 8-byte element, global -> shared (completion tracked
- * by the issuing thread's commit/wait groups) */
-template <typename R>
-__device__ __forceinline__ void cp_async_elem(R *dst, const R *src) {
-  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-  if (sizeof(R) == 8) asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
-  else asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
+/* ---- TMA and mbarrier primitives (one CTA, no cluster, no multicast) ---- */
+__device__ __forceinline__ unsigned smem_addr(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(unsigned bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count) : "memory");
 }
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int NPEND>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(NPEND) : "memory"); }
+/* make barrier initialisation and earlier generic shared-memory writes
+ * visible to the async (TMA) proxy */
+__device__ __forceinline__ void fence_barrier_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(unsigned bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
+}
+/* tiled 3-D tensor copy global -> this CTA's shared memory, completion
+ * counted in bytes on bar; c0 is the innermost coordinate */
+__device__ __forceinline__ void tma_load_3d(unsigned dst, const void *tmap, int c0, int c1, int c2, unsigned bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];\n" ::"r"(dst),
+      "l"(tmap), "r"(c0), "r"(c1), "r"(c2), "r"(bar)
+      : "memory");
+}
+__device__ __forceinline__ bool mbar_test(unsigned bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+/* wait for phase `parity` of bar to complete, at most MBAR_TRIES polls (each
+ * poll may suspend the thread for a short while); false when it did not */
+constexpr int MBAR_TRIES = 1 << 20;
+__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity) {
+  for (int it = 0; it < MBAR_TRIES; it++)
+    if (mbar_test(bar, parity)) return true;
+  return false;
+}
 
 /* x/dx and y/dy of the bulk kernel: a multiplication by the reciprocal when
  * the spacing is a power of two (MUL, chosen at launch), else the division */
@@ -706,34 +736,76 @@ __device__ __forceinline__ R bdiv(R v, R inv, R d) {
   else return v / d;
 }
 
-/* Bulk tiles, one warp per tile.  Warps take contiguous ranges of the bulk
- * list.  The mu of a bulk tile with its one-cell halo is copied into the
- * warp's shared-memory stage by cp.async while the warp steps the previous
- * bulk tile from the other stage; lane j then steps column y0+j row
- * by row.  No block-wide barrier anywhere.  The running mu extremes of the
- * cells a warp steps stay in registers and are merged into the simulation's
- * slots (atomic max/min) when the warp moves to another simulation or
- * finishes; bulk tiles cannot move the phi extremes (their phi is 0 or 1,
- * inside the initial [0, 1]). */
-template <typename R, int N, int K>
-struct BulkWarpStage {
-  R M[2][K][SH][SW];   /* two stages of mu with a one-cell halo */
+/* A tensor map (CUtensorMap, 128 bytes) of the K mu planes of one simulation
+ * in one state buffer: dimensions {pitch, mx, K}, box {BW, SH, K}. */
+struct alignas(64) TensorMapSlot {
+  unsigned long long w[16];
 };
 
+/* Shared memory of one warp of kf_bulk: NST stages of mu with a one-cell halo,
+ * each filled by one TMA box.  A box starts CO columns left of the halo
+ * column so that its first column is 16-byte aligned (y0 - 1 - CO is a
+ * multiple of 16 bytes / sizeof(R)); stage column c holds y = y0 - 1 - CO + c. */
+template <typename R, int K>
+struct BulkGeom {
+  static constexpr int CO = sizeof(R) == 8 ? 1 : 3;
+  static constexpr int BW = SW + 2 * CO;   /* 36 doubles or 40 floats: a multiple of 16 bytes */
+  static constexpr int NST = 2;
+  static constexpr unsigned BOX_BYTES = (unsigned)(K * SH * BW * sizeof(R));
+};
+template <typename R, int K>
+struct alignas(128) BulkStage {
+  R M[K][SH][BulkGeom<R, K>::BW];
+};
+template <typename R, int K>
+struct alignas(128) BulkWarpSmem {
+  BulkStage<R, K> st[BulkGeom<R, K>::NST];
+  unsigned long long bar[BulkGeom<R, K>::NST];
+};
+/* dynamic shared memory of kf_bulk (the base is rounded up to 128 bytes in
+ * the kernel) */
+template <typename R, int K>
+constexpr size_t bulk_smem_bytes() {
+  return (NT / 32) * sizeof(BulkWarpSmem<R, K>) + 128;
+}
+
+/* Bulk tiles, one warp per tile.  Warps take contiguous ranges of the bulk
+ * list.  Lane 0 issues one TMA box per tile (the K mu planes of the tile with
+ * a one-cell halo, rows x0-1..x0+TX) into the warp's next stage while the warp
+ * steps the current one; an mbarrier per stage counts the bytes in.  Halo
+ * cells outside the domain (tiles on the boundary) are then overwritten with
+ * the cells the boundary copy tables name.  Lane j steps column y0+j row by
+ * row.  No block-wide barrier anywhere.  The running mu extremes of the cells
+ * a warp steps stay in registers and are merged into the simulation's slots
+ * (atomic max/min) when the warp moves to another simulation or finishes;
+ * bulk tiles cannot move the phi extremes (their phi is 0 or 1, inside the
+ * initial [0, 1]).  A stage whose bytes do not arrive within the poll limit
+ * sets ctr[CTR_ERR]; the warp then stops taking tiles. */
 template <typename R, int N, int K, bool SUMS, bool MUL>
 __global__ void __launch_bounds__(NT, 2) kf_bulk(const SimDesc *__restrict__ sims, const Consts<R> *__restrict__ consts,
                                                  const int *__restrict__ tsim, const int *__restrict__ blist,
+                                                 const TensorMapSlot *__restrict__ tmaps, int buf,
                                                  const R *__restrict__ state, R *__restrict__ next,
                                                  TileFlags *__restrict__ flag_out, int *__restrict__ ctr,
                                                  int ndone, StatBufs st) {
-  constexpr int NW = NT / 32, NS = 2 * N + 2 * K + 1;
-  extern __shared__ __align__(16) unsigned char smraw[];
-  BulkWarpStage<R, N, K> &stg = reinterpret_cast<BulkWarpStage<R, N, K> *>(smraw)[threadIdx.x >> 5];
+  using G = BulkGeom<R, K>;
+  constexpr int NW = NT / 32, NS = 2 * N + 2 * K + 1, NST = G::NST, CO = G::CO;
+  extern __shared__ __align__(128) unsigned char smraw[];
+  unsigned char *sbase = (unsigned char *)(((size_t)smraw + 127) & ~(size_t)127);
+  BulkWarpSmem<R, K> &ws = reinterpret_cast<BulkWarpSmem<R, K> *>(sbase)[threadIdx.x >> 5];
   const int lane = threadIdx.x & 31;
   const int gw = blockIdx.x * NW + (threadIdx.x >> 5), nwarps = gridDim.x * NW;
   const int nbulk = *(const volatile int *)(ctr + CTR_BULK);
   const int per = (nbulk + nwarps - 1) / nwarps;
   const int i0 = gw * per, i1 = min(nbulk, i0 + per);
+
+  if (lane == 0) {
+#pragma unroll
+    for (int q = 0; q < NST; q++) mbar_init(smem_addr(&ws.bar[q]), 1);
+    fence_barrier_init();
+    fence_proxy_async_smem();
+  }
+  __syncwarp();
 
   R emax[K], emin[K];   /* running mu extremes of the cells this warp stepped */
 #pragma unroll
@@ -753,46 +825,30 @@ __global__ void __launch_bounds__(NT, 2) kf_bulk(const SimDesc *__restrict__ sim
     }
   };
 
-  /* start copying tile t's mu with its halo into stage b */
+  /* lane 0: start the TMA box of tile t (list entry i) into stage b */
   auto issue = [&](int t, int b) {
-    const int s = __ldg(tsim + t);
-    const SimDesc &sd = sims[s];
-    const Consts<R> &D = consts[s];
-    const Grid g = sd.g;
-    const int lt = t - sd.tile0, by = lt / sd.tiles_x, bx = lt - by * sd.tiles_x;
-    const int x0 = by * TX, y0 = bx * TY;
-    const R *mu = state + sd.off_state + (long long)N * g.plane;
-    const int bx0 = D.bc_x[1][0], bx1 = D.bc_x[1][1], by0 = D.bc_y[1][0], by1 = D.bc_y[1][1];
-    for (int e = lane; e < SH * SW; e += 32) {
-      const int i = e / SW, j = e - i * SW;
-      int x = x0 - 1 + i, y = y0 - 1 + j;
-      if (x <= g.mx && y <= g.my) {
-        if (x < 0 || x >= g.mx) x = remap(x, g.mx, bx0, bx1);
-        if (y < 0 || y >= g.my) y = remap(y, g.my, by0, by1);
-        const R *src = mu + (long long)x * g.pitch + y;
-#pragma unroll
-        for (int k = 0; k < K; k++) cp_async_elem(&stg.M[b][k][i][j], src + (long long)k * g.plane);
-      } else {
-#pragma unroll
-        for (int k = 0; k < K; k++) stg.M[b][k][i][j] = R(0.0);
-      }
+    if (lane == 0) {
+      const int s = __ldg(tsim + t);
+      const SimDesc &sd = sims[s];
+      const int lt = t - sd.tile0, by = lt / sd.tiles_x, bx = lt - by * sd.tiles_x;
+      const unsigned bar = smem_addr(&ws.bar[b]);
+      mbar_expect_tx(bar, G::BOX_BYTES);
+      tma_load_3d(smem_addr(&ws.st[b]), tmaps + 2 * s + buf, bx * TY - 1 - CO, by * TX - 1, 0, bar);
     }
-    cp_async_commit();
   };
 
-  int item = i0 < i1 ? __ldg(blist + i0) : 0;
-  if (i0 < i1) issue(item & 0x0fffffff, 0);
-  int b = 0;
+  if (i0 < i1) issue(__ldg(blist + i0) & 0x0fffffff, 0);
   for (int i = i0; i < i1; i++) {
-    const int nitem = i + 1 < i1 ? __ldg(blist + i + 1) : 0;
-    if (i + 1 < i1) {
-      issue(nitem & 0x0fffffff, b ^ 1);
-      cp_async_wait<1>();
-    } else {
-      cp_async_wait<0>();
+    const int b = (i - i0) & 1;
+    if (i + 1 < i1) issue(__ldg(blist + i + 1) & 0x0fffffff, b ^ 1);
+    if (!mbar_wait(smem_addr(&ws.bar[b]), ((i - i0) >> 1) & 1)) {
+      /* bytes missing: record it, wait (bounded) for the other box in
+       * flight, step nothing more */
+      if (lane == 0) atomicExch(ctr + CTR_ERR, 1);
+      if (i + 1 < i1) mbar_wait(smem_addr(&ws.bar[b ^ 1]), ((i + 1 - i0) >> 1) & 1);
+      break;
     }
-    __syncwarp();
-
+    const int item = __ldg(blist + i);
     /* ---- step bulk tile t (phase p) from stage b */
     const int t = item & 0x0fffffff, p = item >> 28;
     const int s = __ldg(tsim + t);
@@ -806,6 +862,39 @@ __global__ void __launch_bounds__(NT, 2) kf_bulk(const SimDesc *__restrict__ sim
     const int lt = t - sd.tile0, by = lt / sd.tiles_x, bx = lt - by * sd.tiles_x;
     const int x0 = by * TX, y0 = bx * TY;
     const int have = flag_out[t].whole;
+    BulkStage<R, K> &sg = ws.st[b];
+    const int rows = min(TX, g.mx - x0), ncols = min(TY, g.my - y0);
+    if (x0 == 0 || x0 + TX >= g.mx || y0 == 0 || y0 + TY >= g.my) {
+      /* boundary tile: halo cells outside the domain are copies of interior
+       * cells (the box read zeros there) */
+      const R *mu = state + sd.off_state + (long long)N * g.plane;
+      const int bx0 = D.bc_x[1][0], bx1 = D.bc_x[1][1], by0 = D.bc_y[1][0], by1 = D.bc_y[1][1];
+      for (int e = lane; e < 2 * SW + 2 * SH; e += 32) {
+        int i, j;
+        bool need;
+        if (e < 2 * SW) {   /* halo rows x0-1 (top) and x0+rows (bottom) */
+          const int side = e >= SW;
+          j = e - side * SW;
+          i = side ? rows + 1 : 0;
+          need = side ? x0 + TX >= g.mx : x0 == 0;
+        } else {            /* halo columns y0-1 (left) and y0+ncols (right) */
+          const int side = e >= 2 * SW + SH;
+          i = e - 2 * SW - side * SH;
+          j = side ? ncols + 1 : 0;
+          need = side ? y0 + TY >= g.my : y0 == 0;
+        }
+        int x = x0 - 1 + i, y = y0 - 1 + j;
+        if (need && x <= g.mx && y <= g.my) {
+          if (x < 0 || x >= g.mx) x = remap(x, g.mx, bx0, bx1);
+          if (y < 0 || y >= g.my) y = remap(y, g.my, by0, by1);
+          const R *src = mu + (long long)x * g.pitch + y;
+#pragma unroll
+          for (int k = 0; k < K; k++) sg.M[k][i][j + CO] = __ldg(src + (long long)k * g.plane);
+        }
+      }
+      fence_proxy_async_smem();   /* before a later box overwrites this stage */
+      __syncwarp();
+    }
     const R idx = D.inv_dx, idy = D.inv_dy, ddx = D.dx, ddy = D.dy, dt = D.dt;
     const R cst = D.obstacle ? D.jat_obst : D.jat_well;
     R dmf[K][K];
@@ -830,9 +919,8 @@ __global__ void __launch_bounds__(NT, 2) kf_bulk(const SimDesc *__restrict__ sim
     const unsigned skey = sizeof(R) == 4 ? mix32(__ldg(st.round_step) * 0x9e3779b9u + 0x632be5abu) : 0u;
     R *phin = next + sd.off_state;
     R *mun = phin + (long long)N * g.plane;
-    const int y = y0 + lane, j = lane + 1;
+    const int y = y0 + lane, j = lane + 1 + CO;
     const bool yvalid = y < g.my;
-    const int rows = min(TX, g.mx - x0);
     double acc[SUMS ? NS : 1];
 #pragma unroll
     for (int f = 0; f < (SUMS ? NS : 1); f++) acc[f] = 0.0;
@@ -843,18 +931,18 @@ __global__ void __launch_bounds__(NT, 2) kf_bulk(const SimDesc *__restrict__ sim
         R m[K], cn[K], nm[K];
         double dmu[K];
 #pragma unroll
-        for (int k = 0; k < K; k++) m[k] = stg.M[b][k][i][j];
+        for (int k = 0; k < K; k++) m[k] = sg.M[k][i][j];
         /* the bulk expressions of the general path (update_tile's uniform path) */
 #pragma unroll
         for (int k = 0; k < K; k++) {
           R divflux = R(0.0);
 #pragma unroll
           for (int l = 0; l < K; l++) {
-            const R dm = dmf[k][l], c = stg.M[b][l][i][j];
-            R fx = dm * bdiv<MUL>(stg.M[b][l][i + 1][j] - c, idx, ddx);
-            R bx_ = dm * bdiv<MUL>(c - stg.M[b][l][i - 1][j], idx, ddx);
-            R fy = dm * bdiv<MUL>(stg.M[b][l][i][j + 1] - c, idy, ddy);
-            R by_ = dm * bdiv<MUL>(c - stg.M[b][l][i][j - 1], idy, ddy);
+            const R dm = dmf[k][l], c = sg.M[l][i][j];
+            R fx = dm * bdiv<MUL>(sg.M[l][i + 1][j] - c, idx, ddx);
+            R bx_ = dm * bdiv<MUL>(c - sg.M[l][i - 1][j], idx, ddx);
+            R fy = dm * bdiv<MUL>(sg.M[l][i][j + 1] - c, idy, ddy);
+            R by_ = dm * bdiv<MUL>(c - sg.M[l][i][j - 1], idy, ddy);
             divflux += bdiv<MUL>(fx - bx_, idx, ddx);
             divflux += bdiv<MUL>(fy - by_, idy, ddy);
           }
@@ -934,8 +1022,6 @@ __global__ void __launch_bounds__(NT, 2) kf_bulk(const SimDesc *__restrict__ sim
     }
     if (lane == 0) flag_out[t] = uniform_flags(p);
     __syncwarp();   /* stage b is refilled by the next issue */
-    item = nitem;
-    b ^= 1;
   }
   if (cur_sim >= 0) flush(cur_sim);
   step_finish(ctr, ndone);
