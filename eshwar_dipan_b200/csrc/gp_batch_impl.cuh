@@ -21,8 +21,10 @@ struct BatchLaunch {
   /* mul: every simulation's spacings are powers of two (x/dx == x*(1/dx)) */
   /* ndone: the CTAs of this step's kf_bulk and kf_general together */
   /* tmaps: per simulation two tensor maps of its mu planes (state buffer 0
-   * and 1); buf: the buffer `state` is */
-  cudaError_t (*bulk)(int grid, bool mul, cudaStream_t s, const SimDesc *sims, const void *consts, const int *tsim,
+   * and 1); buf: the buffer `state` is; diag: every phase's off-diagonal D,
+   * c_mu and A are zero and no E is -0 (the bulk kernel leaves those terms
+   * out) */
+  cudaError_t (*bulk)(int grid, bool mul, bool diag, cudaStream_t s, const SimDesc *sims, const void *consts, const int *tsim,
                       const int *blist, const TensorMapSlot *tmaps, int buf, const void *state, void *next,
                       TileFlags *flag_out, int *ctr, int ndone, StatBufs st);
   cudaError_t (*general)(int grid, bool mul, cudaStream_t s, const SimDesc *sims, const void *consts, const int *tsim,
@@ -39,9 +41,9 @@ struct BatchLaunch {
 template <typename R, int N, int K, bool A>
 struct BatchKernels {
   static constexpr size_t bulk_smem = bulk_smem_bytes<R, K>();
-  template <bool SUMS, bool MUL>
+  template <bool SUMS, bool MUL, bool DIAG>
   static cudaError_t bulk_attr() {
-    return cudaFuncSetAttribute(kf_bulk<R, N, K, SUMS, MUL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    return cudaFuncSetAttribute(kf_bulk<R, N, K, SUMS, MUL, DIAG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)bulk_smem);
   }
   static cudaError_t prepare(int *bb, int *bg) {
@@ -50,12 +52,14 @@ struct BatchKernels {
     if (e == cudaSuccess)
       e = cudaFuncSetAttribute(kf_general<R, N, K, A, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)sizeof(GenSmem<R, N, K>));
-    if (e == cudaSuccess) e = bulk_attr<false, false>();
-    if (e == cudaSuccess) e = bulk_attr<false, true>();
-    if (e == cudaSuccess) e = bulk_attr<true, false>();
-    if (e == cudaSuccess) e = bulk_attr<true, true>();
+    if (e == cudaSuccess) e = bulk_attr<false, false, false>();
+    if (e == cudaSuccess) e = bulk_attr<false, true, false>();
+    if (e == cudaSuccess) e = bulk_attr<false, false, true>();
+    if (e == cudaSuccess) e = bulk_attr<false, true, true>();
+    if (e == cudaSuccess) e = bulk_attr<true, false, false>();
+    if (e == cudaSuccess) e = bulk_attr<true, true, false>();
     if (e != cudaSuccess) return e;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(bb, kf_bulk<R, N, K, false, true>, NT, bulk_smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(bb, kf_bulk<R, N, K, false, true, false>, NT, bulk_smem);
     if (e != cudaSuccess) return e;
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bg, kf_general<R, N, K, A, true>, NT,
                                                          sizeof(GenSmem<R, N, K>));
@@ -66,18 +70,22 @@ struct BatchKernels {
                                                          blist, ctr);
     return cudaGetLastError();
   }
-  static cudaError_t bulk(int grid, bool mul, cudaStream_t s, const SimDesc *sims, const void *consts,
+  static cudaError_t bulk(int grid, bool mul, bool diag, cudaStream_t s, const SimDesc *sims, const void *consts,
                           const int *tsim, const int *blist, const TensorMapSlot *tmaps, int buf,
                           const void *state, void *next, TileFlags *flag_out, int *ctr, int ndone, StatBufs st) {
-#define GP_BULK(SUMS, MUL)                                                                                     \
-  kf_bulk<R, N, K, SUMS, MUL><<<grid, NT, bulk_smem, s>>>(sims, (const Consts<R> *)consts, tsim, blist, tmaps,  \
+#define GP_BULK(SUMS, MUL, DIAG)                                                                               \
+  kf_bulk<R, N, K, SUMS, MUL, DIAG><<<grid, NT, bulk_smem, s>>>(sims, (const Consts<R> *)consts, tsim, blist, tmaps,  \
                                                           buf, (const R *)state, (R *)next, flag_out, ctr, ndone, st)
+    /* the sums step (last of a call) takes every term: same results */
     if (st.want_sums) {
-      if (mul) GP_BULK(true, true);
-      else GP_BULK(true, false);
+      if (mul) GP_BULK(true, true, false);
+      else GP_BULK(true, false, false);
+    } else if (diag) {
+      if (mul) GP_BULK(false, true, true);
+      else GP_BULK(false, false, true);
     } else {
-      if (mul) GP_BULK(false, true);
-      else GP_BULK(false, false);
+      if (mul) GP_BULK(false, true, false);
+      else GP_BULK(false, false, false);
     }
 #undef GP_BULK
     return cudaGetLastError();

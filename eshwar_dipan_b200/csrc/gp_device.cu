@@ -260,6 +260,7 @@ struct gp_batch {
   std::vector<gpd::SimDesc> desc;
   int dev, nsm, grid_b, grid_g;
   bool mul;                     /* every simulation's dx and dy are powers of two (or FP32) */
+  bool diag;                    /* off-diagonal D, c_mu, A all zero and no E is -0, in every simulation */
   int ntiles;                   /* TX x TY tiles over all simulations */
   cudaStream_t stream;
   gpd::SimDesc *d_desc;
@@ -314,7 +315,7 @@ static int batch_step_once(gp_batch *b, int want_sums, cudaEvent_t *ev) {
                    b->counters));
   /* kf_bulk then kf_general; the last CTA of the two resets the lists */
   const int nd = b->grid_b + b->grid_g;
-  BK(b->L.bulk(b->grid_b, b->mul, b->stream, b->d_desc, b->d_consts, b->d_tsim, b->blist, b->tmaps, in,
+  BK(b->L.bulk(b->grid_b, b->mul, b->diag, b->stream, b->d_desc, b->d_consts, b->d_tsim, b->blist, b->tmaps, in,
                b->state[in], b->state[out], b->flags[out], b->counters, nd, st));
   if (ev) BK(cudaEventRecord(ev[1], b->stream));
   BK(b->L.general(b->grid_g, b->mul, b->stream, b->d_desc, b->d_consts, b->d_tsim, b->state[in], b->state[out],
@@ -624,6 +625,16 @@ int gp_batch_create(gp_batch **out, int nsims, const gp_params *params, const do
   b->mul = true;
   for (int s = 0; s < nsims; s++)
     if (b->elem == 8 && !(pow2(b->derived[s].dx) && pow2(b->derived[s].dy))) b->mul = false;
+  b->diag = true;
+  for (int s = 0; s < nsims; s++) {
+    const gp_derived &d = b->derived[s];
+    for (int a = 0; a < N; a++)
+      for (int k = 0; k < K; k++) {
+        if (std::signbit(d.E[a][k])) b->diag = false;
+        for (int l = 0; l < K; l++)
+          if (k != l && (d.Dbulk[a][k][l] != 0.0 || d.cmu[a][k][l] != 0.0 || d.A[a][k][l] != 0.0)) b->diag = false;
+      }
+  }
   int bpb = 1, bpg = 1;
   e = b->L.prepare(&bpb, &bpg);
   if (e != cudaSuccess) {

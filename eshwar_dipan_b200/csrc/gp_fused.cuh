@@ -781,7 +781,7 @@ constexpr size_t bulk_smem_bytes() {
  * bulk tiles cannot move the phi extremes (their phi is 0 or 1, inside the
  * initial [0, 1]).  A stage whose bytes do not arrive within the poll limit
  * sets ctr[CTR_ERR]; the warp then stops taking tiles. */
-template <typename R, int N, int K, bool SUMS, bool MUL>
+template <typename R, int N, int K, bool SUMS, bool MUL, bool DIAG>
 __global__ void __launch_bounds__(NT, 2) kf_bulk(const SimDesc *__restrict__ sims, const Consts<R> *__restrict__ consts,
                                                  const int *__restrict__ tsim, const int *__restrict__ blist,
                                                  const TensorMapSlot *__restrict__ tmaps, int buf,
@@ -924,64 +924,121 @@ __global__ void __launch_bounds__(NT, 2) kf_bulk(const SimDesc *__restrict__ sim
     double acc[SUMS ? NS : 1];
 #pragma unroll
     for (int f = 0; f < (SUMS ? NS : 1); f++) acc[f] = 0.0;
+    /* the anti-trapping divergence of a bulk cell: no phi gradient, so the
+     * same value for every cell of the tile */
+    R divjat = bdiv<MUL>((R(0.0) - R(0.0)) * cst, idx, ddx);
+    divjat += bdiv<MUL>((R(0.0) - R(0.0)) * cst, idy, ddy);
+    /* divergence of the diffusive flux of component k at row i (all K
+     * gradients, the reference's expressions in its order) */
+    auto divflux_full = [&](int k, int i) {
+      R divflux = R(0.0);
+#pragma unroll
+      for (int l = 0; l < K; l++) {
+        const R dm = dmf[k][l], c = sg.M[l][i][j];
+        R fx = dm * bdiv<MUL>(sg.M[l][i + 1][j] - c, idx, ddx);
+        R bx_ = dm * bdiv<MUL>(c - sg.M[l][i - 1][j], idx, ddx);
+        R fy = dm * bdiv<MUL>(sg.M[l][i][j + 1] - c, idy, ddy);
+        R by_ = dm * bdiv<MUL>(c - sg.M[l][i][j - 1], idy, ddy);
+        divflux += bdiv<MUL>(fx - bx_, idx, ddx);
+        divflux += bdiv<MUL>(fy - by_, idy, ddy);
+      }
+      return divflux;
+    };
+    /* new mu of a cell from its old mu and the flux divergences; `all`
+     * (std::true_type) keeps the off-diagonal terms in a DIAG kernel */
+    auto commit_mu = [&](auto all, const R (&m)[K], const R (&df)[K], int x, R (&nm)[K], double (&dmu)[K]) {
+      constexpr bool SKIP = DIAG && !decltype(all)::value;
+      R cn[K];
+#pragma unroll
+      for (int k = 0; k < K; k++) {
+        if constexpr (sizeof(R) == 8) {
+          R cm = R(0.0);   /* c_mu (functionF_01.h:30-37) */
+#pragma unroll
+          for (int l = 0; l < K; l++)
+            if (!SKIP || l == k) cm += cmu[k][l] * (m[l] - E[l]);
+          cn[k] = cm + dt * (df[k]) - divjat;
+        } else {
+          cn[k] = dt * df[k] - divjat;
+        }
+      }
+      if constexpr (sizeof(R) == 8) {
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+          R sm = twoA[k] * cn[k] + E[k];   /* Mu (functionF_01.h:19-29) */
+#pragma unroll
+          for (int l = 0; l < K; l++)
+            if (!SKIP && k != l) sm += Aoff[k][l] * cn[l];
+          nm[k] = sm;
+          dmu[k] = (double)nm[k] - (double)m[k];
+        }
+      } else {
+        /* mu += (dmu/dc) dc of the pure phase in float (no c -> mu round
+         * trip), the sum rounded stochastically from its exact TwoSum
+         * split, 16 random bits per field from one hash of the cell */
+        const unsigned key = mix32(skey ^ ((unsigned)x * 0x85ebca6bu + (unsigned)y * 0xc2b2ae35u));
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+          R sdm = R(0.0);
+#pragma unroll
+          for (int l = 0; l < K; l++)
+            if (!SKIP || l == k) sdm += muc[k][l] * cn[l];
+          dmu[k] = (double)sdm;
+          nm[k] = (R)add_stochastic((float)m[k], (float)sdm, (key >> (16 * (k & 1))) & 0xffffu);
+        }
+      }
+    };
     if (yvalid) {
+      /* x-face fluxes dm*(mu(i) - mu(i-1))/dx between rows i-1 and i: the
+       * forward flux of row i-1 is the backward flux of row i (the same
+       * expression on the same operands), so it is carried from row to row */
+      R fxp[K][K];
+#pragma unroll
+      for (int k = 0; k < K; k++)
+#pragma unroll
+        for (int l = 0; l < K; l++)
+          if (!DIAG || l == k) fxp[k][l] = dmf[k][l] * bdiv<MUL>(sg.M[l][1][j] - sg.M[l][0][j], idx, ddx);
 #pragma unroll 2
       for (int i = 1; i <= rows; i++) {
         const int x = x0 + i - 1;
-        R m[K], cn[K], nm[K];
+        R m[K], df[K], nm[K];
         double dmu[K];
 #pragma unroll
         for (int k = 0; k < K; k++) m[k] = sg.M[k][i][j];
-        /* the bulk expressions of the general path (update_tile's uniform path) */
+        /* the bulk expressions of the general path (update_tile's uniform
+         * path); DIAG: the off-diagonal D, c_mu and A of every phase are
+         * zero, their terms (+-0 added to sums that are never -0) are left
+         * out */
 #pragma unroll
         for (int k = 0; k < K; k++) {
           R divflux = R(0.0);
 #pragma unroll
           for (int l = 0; l < K; l++) {
-            const R dm = dmf[k][l], c = sg.M[l][i][j];
-            R fx = dm * bdiv<MUL>(sg.M[l][i + 1][j] - c, idx, ddx);
-            R bx_ = dm * bdiv<MUL>(c - sg.M[l][i - 1][j], idx, ddx);
-            R fy = dm * bdiv<MUL>(sg.M[l][i][j + 1] - c, idy, ddy);
-            R by_ = dm * bdiv<MUL>(c - sg.M[l][i][j - 1], idy, ddy);
-            divflux += bdiv<MUL>(fx - bx_, idx, ddx);
+            if (DIAG && l != k) continue;
+            const R dm = dmf[k][l], c = m[l];
+            const R fx = dm * bdiv<MUL>(sg.M[l][i + 1][j] - c, idx, ddx);
+            const R fy = dm * bdiv<MUL>(sg.M[l][i][j + 1] - c, idy, ddy);
+            const R by_ = dm * bdiv<MUL>(c - sg.M[l][i][j - 1], idy, ddy);
+            divflux += bdiv<MUL>(fx - fxp[k][l], idx, ddx);
             divflux += bdiv<MUL>(fy - by_, idy, ddy);
+            fxp[k][l] = fx;
           }
-          R divjat = bdiv<MUL>((R(0.0) - R(0.0)) * cst, idx, ddx);
-          divjat += bdiv<MUL>((R(0.0) - R(0.0)) * cst, idy, ddy);
-          if constexpr (sizeof(R) == 8) {
-            R cm = R(0.0);   /* c_mu (functionF_01.h:30-37) */
+          df[k] = divflux;
+        }
+        commit_mu(std::false_type(), m, df, x, nm, dmu);
+        if constexpr (DIAG) {
+          /* a left-out term is +-0 only when the values it multiplies are
+           * finite, and they are when every new mu is; otherwise the cell
+           * is redone with every term */
+          bool fin = true;
 #pragma unroll
-            for (int l = 0; l < K; l++) cm += cmu[k][l] * (m[l] - E[l]);
-            cn[k] = cm + dt * (divflux) - divjat;
-          } else {
-            cn[k] = dt * divflux - divjat;
+          for (int k = 0; k < K; k++) fin &= fabs(nm[k]) < R(INFINITY);
+          if (!fin) {
+#pragma unroll
+            for (int k = 0; k < K; k++) df[k] = divflux_full(k, i);
+            commit_mu(std::true_type(), m, df, x, nm, dmu);
           }
         }
         const long long o = (long long)x * g.pitch + y;
-        if constexpr (sizeof(R) == 8) {
-#pragma unroll
-          for (int k = 0; k < K; k++) {
-            R sm = twoA[k] * cn[k] + E[k];   /* Mu (functionF_01.h:19-29) */
-#pragma unroll
-            for (int l = 0; l < K; l++)
-              if (k != l) sm += Aoff[k][l] * cn[l];
-            nm[k] = sm;
-            dmu[k] = (double)nm[k] - (double)m[k];
-          }
-        } else {
-          /* mu += (dmu/dc) dc of the pure phase in float (no c -> mu round
-           * trip), the sum rounded stochastically from its exact TwoSum
-           * split, 16 random bits per field from one hash of the cell */
-          const unsigned key = mix32(skey ^ ((unsigned)x * 0x85ebca6bu + (unsigned)y * 0xc2b2ae35u));
-#pragma unroll
-          for (int k = 0; k < K; k++) {
-            R sdm = R(0.0);
-#pragma unroll
-            for (int l = 0; l < K; l++) sdm += muc[k][l] * cn[l];
-            dmu[k] = (double)sdm;
-            nm[k] = (R)add_stochastic((float)m[k], (float)sdm, (key >> (16 * (k & 1))) & 0xffffu);
-          }
-        }
 #pragma unroll
         for (int k = 0; k < K; k++) {
           mun[k * g.plane + o] = nm[k];

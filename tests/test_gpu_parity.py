@@ -73,6 +73,39 @@ def test_step_from_uploaded_state(tmp_path, name):
     assert bits_equal(a_mu, b_mu), mismatch_report(a_mu, b_mu)
 
 
+def _same_with_nans(a, b):
+    """bit for bit (zeros of either sign equal), every NaN equal to every NaN"""
+    na, nb = np.isnan(a), np.isnan(b)
+    return np.array_equal(na, nb) and bits_equal(np.where(na, 0.0, a), np.where(nb, 0.0, b))
+
+
+def test_nonfinite_mu_in_bulk_tiles(tmp_path):
+    """A ternary case whose off-diagonal D, c_mu and A are zero (the bulk
+    kernel leaves those terms out) with +inf and NaN planted in the mu of
+    liquid bulk tiles: the cells they reach take every term, as the oracle
+    does (NaN payloads aside)."""
+    from gp_cases import write_case
+    c = PARITY_CASES["four_phase_ternary_iso"]
+    kw = dict(c["kw"], mesh=(96, 96))
+    ip, fp = write_case(str(tmp_path), "nonfinite", kw, seeds=c["seeds"])
+    p = gp.load_params(ip)
+    phi, mu = gp.fill(p, fp)
+    mu[0, 70, 70] = np.inf
+    mu[1, 75, 40] = np.nan
+    mu[0, 88, 10] = -np.inf
+    o = Oracle(p, recip_div=1)
+    o.set(phi, mu)
+    sim = gp.Simulation(p, phi, mu)
+    for chunk in (1, 2):
+        o.step(chunk)
+        sim.step(chunk, stats=False)
+        a_phi, a_mu = sim.get()
+        b_phi, b_mu = o.get()
+        assert np.isnan(b_mu).sum() > 3
+        assert _same_with_nans(a_phi, b_phi), mismatch_report(a_phi, b_phi)
+        assert _same_with_nans(a_mu, b_mu), mismatch_report(a_mu, b_mu)
+
+
 def test_smoothing_vs_reference_reciprocal(tmp_path):
     """Against the oracle with the reference's pow(x,-1) reciprocal the
     smoothing differs only by rounding of the dc/dmu inverse (mu, few ulp)."""
