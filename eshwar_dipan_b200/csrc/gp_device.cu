@@ -630,7 +630,7 @@ int gp_batch_create(gp_batch **out, int nsims, const gp_params *params, const do
     const gp_derived &d = b->derived[s];
     for (int a = 0; a < N; a++)
       for (int k = 0; k < K; k++) {
-        if (std::signbit(d.E[a][k])) b->diag = false;
+        if (d.E[a][k] == 0.0 && std::signbit(d.E[a][k])) b->diag = false;   /* E = -0 */
         for (int l = 0; l < K; l++)
           if (k != l && (d.Dbulk[a][k][l] != 0.0 || d.cmu[a][k][l] != 0.0 || d.A[a][k][l] != 0.0)) b->diag = false;
       }

@@ -825,22 +825,87 @@ __global__ void __launch_bounds__(NT, 2) kf_bulk(const SimDesc *__restrict__ sim
     }
   };
 
-  /* lane 0: start the TMA box of tile t (list entry i) into stage b */
-  auto issue = [&](int t, int b) {
+  /* The warp's list entries, 32 at a time: lane r holds entry i0+base+r
+   * (tile | phase << 28), its simulation, its first cell and the flag its
+   * output buffer holds; a tile's values reach every lane by shuffles.  The
+   * dependent loads of a batch go out once per 32 tiles, not per tile. */
+  int q_item = 0, q_s = 0, q_x0 = 0, q_y0 = 0, q_have = 0;
+  auto load_batch = [&](int base) {
+    const int e = i0 + base + lane;
+    if (e < i1) {
+      q_item = __ldg(blist + e);
+      const int t = q_item & 0x0fffffff;
+      q_s = __ldg(tsim + t);
+      const int lt = t - sims[q_s].tile0, tx = sims[q_s].tiles_x, by = lt / tx;
+      q_x0 = by * TX;
+      q_y0 = (lt - by * tx) * TY;
+      q_have = flag_out[t].whole;
+    }
+  };
+  struct Entry {
+    int item, s, x0, y0, have;
+  };
+  auto entry = [&](int i) {
+    const int r = (i - i0) & 31;
+    Entry en;
+    en.item = __shfl_sync(0xffffffffu, q_item, r);
+    en.s = __shfl_sync(0xffffffffu, q_s, r);
+    en.x0 = __shfl_sync(0xffffffffu, q_x0, r);
+    en.y0 = __shfl_sync(0xffffffffu, q_y0, r);
+    en.have = __shfl_sync(0xffffffffu, q_have, r);
+    return en;
+  };
+  /* lane 0: start the TMA box of a tile into stage b */
+  auto issue = [&](const Entry &en, int b) {
     if (lane == 0) {
-      const int s = __ldg(tsim + t);
-      const SimDesc &sd = sims[s];
-      const int lt = t - sd.tile0, by = lt / sd.tiles_x, bx = lt - by * sd.tiles_x;
       const unsigned bar = smem_addr(&ws.bar[b]);
       mbar_expect_tx(bar, G::BOX_BYTES);
-      tma_load_3d(smem_addr(&ws.st[b]), tmaps + 2 * s + buf, bx * TY - 1 - CO, by * TX - 1, 0, bar);
+      tma_load_3d(smem_addr(&ws.st[b]), tmaps + 2 * en.s + buf, en.y0 - 1 - CO, en.x0 - 1, 0, bar);
     }
   };
 
-  if (i0 < i1) issue(__ldg(blist + i0) & 0x0fffffff, 0);
+  /* the current simulation's layout and the current (simulation, phase)'s
+   * constants stay in registers while consecutive tiles share them */
+  Grid g = {};
+  long long off_state = 0;
+  int cur_key = -1;
+  R idx = R(0), idy = R(0), ddx = R(1), ddy = R(1), dt = R(0), divjat = R(0);
+  /* the K x K constants of a phase: diffusive flux factor, c_mu, A and
+   * dmu/dc */
+  struct MatC {
+    R dm[K][K], cmu[K][K], A[K][K], muc[K][K];
+  };
+  auto load_mat = [&](MatC &c, const Consts<R> &D, int p) {
+#pragma unroll
+    for (int k = 0; k < K; k++)
+#pragma unroll
+      for (int l = 0; l < K; l++) {
+        const R Dv = D.Dbulk[p][k][l];
+        c.dm[k][l] = (Dv + Dv) * R(0.5);
+        c.cmu[k][l] = D.cmu[p][k][l];
+        c.A[k][l] = D.A[p][k][l];
+        c.muc[k][l] = (R)D.muc64[p][k][l];
+      }
+  };
+  R E[K], twoA[K];
+  MatC mc;
+  /* FP32: the step's part of the rounding key */
+  const unsigned skey = sizeof(R) == 4 ? mix32(__ldg(st.round_step) * 0x9e3779b9u + 0x632be5abu) : 0u;
+
+  Entry cur = {};
+  if (i0 < i1) {
+    load_batch(0);
+    cur = entry(i0);
+    issue(cur, 0);
+  }
   for (int i = i0; i < i1; i++) {
     const int b = (i - i0) & 1;
-    if (i + 1 < i1) issue(__ldg(blist + i + 1) & 0x0fffffff, b ^ 1);
+    Entry nxt = {};
+    if (i + 1 < i1) {
+      if (((i + 1 - i0) & 31) == 0) load_batch(i + 1 - i0);
+      nxt = entry(i + 1);
+      issue(nxt, b ^ 1);
+    }
     if (!mbar_wait(smem_addr(&ws.bar[b]), ((i - i0) >> 1) & 1)) {
       /* bytes missing: record it, wait (bounded) for the other box in
        * flight, step nothing more */
@@ -848,26 +913,38 @@ __global__ void __launch_bounds__(NT, 2) kf_bulk(const SimDesc *__restrict__ sim
       if (i + 1 < i1) mbar_wait(smem_addr(&ws.bar[b ^ 1]), ((i + 1 - i0) >> 1) & 1);
       break;
     }
-    const int item = __ldg(blist + i);
     /* ---- step bulk tile t (phase p) from stage b */
-    const int t = item & 0x0fffffff, p = item >> 28;
-    const int s = __ldg(tsim + t);
+    const int t = cur.item & 0x0fffffff, p = cur.item >> 28, s = cur.s;
+    const int x0 = cur.x0, y0 = cur.y0, have = cur.have;
+    const Consts<R> &D = consts[s];
     if (s != cur_sim) {
       if (cur_sim >= 0) flush(cur_sim);
       cur_sim = s;
+      g = sims[s].g;
+      off_state = sims[s].off_state;
     }
-    const SimDesc &sd = sims[s];
-    const Consts<R> &D = consts[s];
-    const Grid g = sd.g;
-    const int lt = t - sd.tile0, by = lt / sd.tiles_x, bx = lt - by * sd.tiles_x;
-    const int x0 = by * TX, y0 = bx * TY;
-    const int have = flag_out[t].whole;
+    if (cur_key != s * 16 + p) {
+      cur_key = s * 16 + p;
+      idx = D.inv_dx; idy = D.inv_dy; ddx = D.dx; ddy = D.dy; dt = D.dt;
+      const R cst = D.obstacle ? D.jat_obst : D.jat_well;
+      /* the anti-trapping divergence of a bulk cell: no phi gradient, the
+       * same value for every cell */
+      divjat = bdiv<MUL>((R(0.0) - R(0.0)) * cst, idx, ddx);
+      divjat += bdiv<MUL>((R(0.0) - R(0.0)) * cst, idy, ddy);
+#pragma unroll
+      for (int k = 0; k < K; k++) {
+        E[k] = D.E[p][k];
+        twoA[k] = D.twoA[p][k];
+      }
+      /* a DIAG kernel keeps only the diagonals live */
+      load_mat(mc, D, p);
+    }
     BulkStage<R, K> &sg = ws.st[b];
     const int rows = min(TX, g.mx - x0), ncols = min(TY, g.my - y0);
     if (x0 == 0 || x0 + TX >= g.mx || y0 == 0 || y0 + TY >= g.my) {
       /* boundary tile: halo cells outside the domain are copies of interior
        * cells (the box read zeros there) */
-      const R *mu = state + sd.off_state + (long long)N * g.plane;
+      const R *mu = state + off_state + (long long)N * g.plane;
       const int bx0 = D.bc_x[1][0], bx1 = D.bc_x[1][1], by0 = D.bc_y[1][0], by1 = D.bc_y[1][1];
       for (int e = lane; e < 2 * SW + 2 * SH; e += 32) {
         int i, j;
@@ -895,46 +972,20 @@ __global__ void __launch_bounds__(NT, 2) kf_bulk(const SimDesc *__restrict__ sim
       fence_proxy_async_smem();   /* before a later box overwrites this stage */
       __syncwarp();
     }
-    const R idx = D.inv_dx, idy = D.inv_dy, ddx = D.dx, ddy = D.dy, dt = D.dt;
-    const R cst = D.obstacle ? D.jat_obst : D.jat_well;
-    R dmf[K][K];
-#pragma unroll
-    for (int k = 0; k < K; k++)
-#pragma unroll
-      for (int l = 0; l < K; l++) {
-        const R Dv = D.Dbulk[p][k][l];
-        dmf[k][l] = (Dv + Dv) * R(0.5);
-      }
-    /* constants of c_mu / Mu of phase p (FP64 update) */
-    R cmu[K][K], E[K], twoA[K], Aoff[K][K];
-    R muc[K][K];
-#pragma unroll
-    for (int k = 0; k < K; k++) {
-      E[k] = D.E[p][k];
-      twoA[k] = D.twoA[p][k];
-#pragma unroll
-      for (int l = 0; l < K; l++) { cmu[k][l] = D.cmu[p][k][l]; Aoff[k][l] = D.A[p][k][l]; muc[k][l] = (R)D.muc64[p][k][l]; }
-    }
-    /* FP32: the step's part of the rounding key, hashed once per tile */
-    const unsigned skey = sizeof(R) == 4 ? mix32(__ldg(st.round_step) * 0x9e3779b9u + 0x632be5abu) : 0u;
-    R *phin = next + sd.off_state;
+    R *phin = next + off_state;
     R *mun = phin + (long long)N * g.plane;
     const int y = y0 + lane, j = lane + 1 + CO;
     const bool yvalid = y < g.my;
     double acc[SUMS ? NS : 1];
 #pragma unroll
     for (int f = 0; f < (SUMS ? NS : 1); f++) acc[f] = 0.0;
-    /* the anti-trapping divergence of a bulk cell: no phi gradient, so the
-     * same value for every cell of the tile */
-    R divjat = bdiv<MUL>((R(0.0) - R(0.0)) * cst, idx, ddx);
-    divjat += bdiv<MUL>((R(0.0) - R(0.0)) * cst, idy, ddy);
     /* divergence of the diffusive flux of component k at row i (all K
      * gradients, the reference's expressions in its order) */
-    auto divflux_full = [&](int k, int i) {
+    auto divflux_full = [&](int k, int i, const MatC &mt) {
       R divflux = R(0.0);
 #pragma unroll
       for (int l = 0; l < K; l++) {
-        const R dm = dmf[k][l], c = sg.M[l][i][j];
+        const R dm = mt.dm[k][l], c = sg.M[l][i][j];
         R fx = dm * bdiv<MUL>(sg.M[l][i + 1][j] - c, idx, ddx);
         R bx_ = dm * bdiv<MUL>(c - sg.M[l][i - 1][j], idx, ddx);
         R fy = dm * bdiv<MUL>(sg.M[l][i][j + 1] - c, idy, ddy);
@@ -946,7 +997,8 @@ __global__ void __launch_bounds__(NT, 2) kf_bulk(const SimDesc *__restrict__ sim
     };
     /* new mu of a cell from its old mu and the flux divergences; `all`
      * (std::true_type) keeps the off-diagonal terms in a DIAG kernel */
-    auto commit_mu = [&](auto all, const R (&m)[K], const R (&df)[K], int x, R (&nm)[K], double (&dmu)[K]) {
+    auto commit_mu = [&](auto all, const MatC &mt, const R (&m)[K], const R (&df)[K], int x, R (&nm)[K],
+                         double (&dmu)[K]) {
       constexpr bool SKIP = DIAG && !decltype(all)::value;
       R cn[K];
 #pragma unroll
@@ -955,7 +1007,7 @@ __global__ void __launch_bounds__(NT, 2) kf_bulk(const SimDesc *__restrict__ sim
           R cm = R(0.0);   /* c_mu (functionF_01.h:30-37) */
 #pragma unroll
           for (int l = 0; l < K; l++)
-            if (!SKIP || l == k) cm += cmu[k][l] * (m[l] - E[l]);
+            if (!SKIP || l == k) cm += mt.cmu[k][l] * (m[l] - E[l]);
           cn[k] = cm + dt * (df[k]) - divjat;
         } else {
           cn[k] = dt * df[k] - divjat;
@@ -967,7 +1019,7 @@ __global__ void __launch_bounds__(NT, 2) kf_bulk(const SimDesc *__restrict__ sim
           R sm = twoA[k] * cn[k] + E[k];   /* Mu (functionF_01.h:19-29) */
 #pragma unroll
           for (int l = 0; l < K; l++)
-            if (!SKIP && k != l) sm += Aoff[k][l] * cn[l];
+            if (!SKIP && k != l) sm += mt.A[k][l] * cn[l];
           nm[k] = sm;
           dmu[k] = (double)nm[k] - (double)m[k];
         }
@@ -981,7 +1033,7 @@ __global__ void __launch_bounds__(NT, 2) kf_bulk(const SimDesc *__restrict__ sim
           R sdm = R(0.0);
 #pragma unroll
           for (int l = 0; l < K; l++)
-            if (!SKIP || l == k) sdm += muc[k][l] * cn[l];
+            if (!SKIP || l == k) sdm += mt.muc[k][l] * cn[l];
           dmu[k] = (double)sdm;
           nm[k] = (R)add_stochastic((float)m[k], (float)sdm, (key >> (16 * (k & 1))) & 0xffffu);
         }
@@ -996,7 +1048,7 @@ __global__ void __launch_bounds__(NT, 2) kf_bulk(const SimDesc *__restrict__ sim
       for (int k = 0; k < K; k++)
 #pragma unroll
         for (int l = 0; l < K; l++)
-          if (!DIAG || l == k) fxp[k][l] = dmf[k][l] * bdiv<MUL>(sg.M[l][1][j] - sg.M[l][0][j], idx, ddx);
+          if (!DIAG || l == k) fxp[k][l] = mc.dm[k][l] * bdiv<MUL>(sg.M[l][1][j] - sg.M[l][0][j], idx, ddx);
 #pragma unroll 2
       for (int i = 1; i <= rows; i++) {
         const int x = x0 + i - 1;
@@ -1014,7 +1066,7 @@ __global__ void __launch_bounds__(NT, 2) kf_bulk(const SimDesc *__restrict__ sim
 #pragma unroll
           for (int l = 0; l < K; l++) {
             if (DIAG && l != k) continue;
-            const R dm = dmf[k][l], c = m[l];
+            const R dm = mc.dm[k][l], c = m[l];
             const R fx = dm * bdiv<MUL>(sg.M[l][i + 1][j] - c, idx, ddx);
             const R fy = dm * bdiv<MUL>(sg.M[l][i][j + 1] - c, idy, ddy);
             const R by_ = dm * bdiv<MUL>(c - sg.M[l][i][j - 1], idy, ddy);
@@ -1024,7 +1076,7 @@ __global__ void __launch_bounds__(NT, 2) kf_bulk(const SimDesc *__restrict__ sim
           }
           df[k] = divflux;
         }
-        commit_mu(std::false_type(), m, df, x, nm, dmu);
+        commit_mu(std::false_type(), mc, m, df, x, nm, dmu);
         if constexpr (DIAG) {
           /* a left-out term is +-0 only when the values it multiplies are
            * finite, and they are when every new mu is; otherwise the cell
@@ -1033,9 +1085,11 @@ __global__ void __launch_bounds__(NT, 2) kf_bulk(const SimDesc *__restrict__ sim
 #pragma unroll
           for (int k = 0; k < K; k++) fin &= fabs(nm[k]) < R(INFINITY);
           if (!fin) {
+            MatC fc;   /* every term, the constants read again */
+            load_mat(fc, D, p);
 #pragma unroll
-            for (int k = 0; k < K; k++) df[k] = divflux_full(k, i);
-            commit_mu(std::true_type(), m, df, x, nm, dmu);
+            for (int k = 0; k < K; k++) df[k] = divflux_full(k, i, fc);
+            commit_mu(std::true_type(), fc, m, df, x, nm, dmu);
           }
         }
         const long long o = (long long)x * g.pitch + y;
@@ -1079,6 +1133,7 @@ __global__ void __launch_bounds__(NT, 2) kf_bulk(const SimDesc *__restrict__ sim
     }
     if (lane == 0) flag_out[t] = uniform_flags(p);
     __syncwarp();   /* stage b is refilled by the next issue */
+    cur = nxt;
   }
   if (cur_sim >= 0) flush(cur_sim);
   step_finish(ctr, ndone);
