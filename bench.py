@@ -435,6 +435,9 @@ def main():
     with ClockSampler(local) as clk:
         tot_ms, _, _, st = sim.step_timed(args.steps, stats=True)
     barrier()
+    fp32 = None
+    if not args.no_fp32:
+        phi64, _ = sim.get()   # the state the FP32 run is compared with (same step count)
     # per-kernel split on a short extra run (steps one by one, events around each kernel)
     nsplit = min(args.steps, 50)
     split_ms, bulk_ms, iface_ms, _ = sim.step_timed(nsplit, split=True)
@@ -443,9 +446,6 @@ def main():
         t = torch.tensor([tot_ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         tot_ms = float(t.item())
-    fp32 = None
-    if not args.no_fp32:
-        phi64, _ = sim.get()
     sim.close()
     if not args.no_fp32:
         fp32 = fp32_form(gp, p, phi0, mu0, args, phi64, st, local)
