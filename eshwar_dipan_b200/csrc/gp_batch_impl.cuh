@@ -16,8 +16,9 @@ struct BatchLaunch {
   /* occupancy of the bulk and interface kernels (blocks per SM) */
   cudaError_t (*prepare)(int *blocks_per_sm_bulk, int *blocks_per_sm_general);
   /* one step: bulk tiles + interface list, then the interface tiles */
+  /* flag_out: the flags of the buffer the step writes (copied into the bulk entries) */
   cudaError_t (*classify)(int ntiles, cudaStream_t s, const SimDesc *sims, const void *consts, const int *tsim,
-                          const TileFlags *flag_in, int *glist, int *blist, int *ctr);
+                          const TileFlags *flag_in, const TileFlags *flag_out, int *glist, int4 *blist, int *ctr);
   /* mul: every simulation's spacings are powers of two (x/dx == x*(1/dx)) */
   /* ndone: the CTAs of this step's kf_bulk and kf_general together */
   /* tmaps: per simulation two tensor maps of its mu planes (state buffer 0
@@ -25,8 +26,14 @@ struct BatchLaunch {
    * c_mu and A are zero and no E is -0 (the bulk kernel leaves those terms
    * out) */
   cudaError_t (*bulk)(int grid, bool mul, bool diag, cudaStream_t s, const SimDesc *sims, const void *consts, const int *tsim,
-                      const int *blist, const TensorMapSlot *tmaps, int buf, const void *state, void *next,
+                      const int4 *blist, const TensorMapSlot *tmaps, int buf, const void *state, void *next,
                       TileFlags *flag_out, int *ctr, int ndone, StatBufs st);
+  /* bulk and interface tiles in one launch (kf_step; not for a sums step) */
+  cudaError_t (*step)(int grid, bool mul, bool diag, cudaStream_t s, const SimDesc *sims, const void *consts,
+                      const int *tsim, const int4 *blist, const int *glist, const TensorMapSlot *tmaps, int buf,
+                      const void *state, void *next, TileFlags *flag_out, int *ctr, int ndone, StatBufs st);
+  /* blocks per SM of kf_step */
+  int (*step_occupancy)();
   cudaError_t (*general)(int grid, bool mul, cudaStream_t s, const SimDesc *sims, const void *consts, const int *tsim,
                          const void *state, void *next, TileFlags *flag_out, const int *glist, int *ctr, int ndone,
                          StatBufs st);
@@ -41,6 +48,38 @@ struct BatchLaunch {
 template <typename R, int N, int K, bool A>
 struct BatchKernels {
   static constexpr size_t bulk_smem = bulk_smem_bytes<R, K>();
+  static constexpr size_t step_smem =
+      sizeof(GenSmem<R, N, K>) > bulk_smem ? sizeof(GenSmem<R, N, K>) : bulk_smem;
+  template <bool MUL, bool DIAG>
+  static cudaError_t step_attr() {
+    return cudaFuncSetAttribute(kf_step<R, N, K, A, MUL, DIAG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)step_smem);
+  }
+  static int step_occupancy() {
+    int n = 0;
+    if (step_attr<true, false>() != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kf_step<R, N, K, A, true, false>, NT, step_smem) !=
+            cudaSuccess)
+      return 0;
+    return n;
+  }
+  static cudaError_t step(int grid, bool mul, bool diag, cudaStream_t s, const SimDesc *sims, const void *consts,
+                          const int *tsim, const int4 *blist, const int *glist, const TensorMapSlot *tmaps, int buf,
+                          const void *state, void *next, TileFlags *flag_out, int *ctr, int ndone, StatBufs st) {
+#define GP_STEP(MUL, DIAG)                                                                                      \
+  kf_step<R, N, K, A, MUL, DIAG><<<grid, NT, step_smem, s>>>(sims, (const Consts<R> *)consts, tsim, blist, glist,  \
+                                                             tmaps, buf, (const R *)state, (R *)next, flag_out, ctr, \
+                                                             ndone, st)
+    if (diag) {
+      if (mul) GP_STEP(true, true);
+      else GP_STEP(false, true);
+    } else {
+      if (mul) GP_STEP(true, false);
+      else GP_STEP(false, false);
+    }
+#undef GP_STEP
+    return cudaGetLastError();
+  }
   template <bool SUMS, bool MUL, bool DIAG>
   static cudaError_t bulk_attr() {
     return cudaFuncSetAttribute(kf_bulk<R, N, K, SUMS, MUL, DIAG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -58,6 +97,10 @@ struct BatchKernels {
     if (e == cudaSuccess) e = bulk_attr<false, true, true>();
     if (e == cudaSuccess) e = bulk_attr<true, false, false>();
     if (e == cudaSuccess) e = bulk_attr<true, true, false>();
+    if (e == cudaSuccess) e = step_attr<false, false>();
+    if (e == cudaSuccess) e = step_attr<true, false>();
+    if (e == cudaSuccess) e = step_attr<false, true>();
+    if (e == cudaSuccess) e = step_attr<true, true>();
     if (e != cudaSuccess) return e;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(bb, kf_bulk<R, N, K, false, true, false>, NT, bulk_smem);
     if (e != cudaSuccess) return e;
@@ -65,13 +108,14 @@ struct BatchKernels {
                                                          sizeof(GenSmem<R, N, K>));
   }
   static cudaError_t classify(int ntiles, cudaStream_t s, const SimDesc *sims, const void *consts,
-                              const int *tsim, const TileFlags *flag_in, int *glist, int *blist, int *ctr) {
-    kf_classify<R><<<(ntiles + NT - 1) / NT, NT, 0, s>>>(sims, (const Consts<R> *)consts, tsim, ntiles, flag_in, glist,
+                              const int *tsim, const TileFlags *flag_in, const TileFlags *flag_out, int *glist,
+                              int4 *blist, int *ctr) {
+    kf_classify<R><<<(ntiles + NTC - 1) / NTC, NTC, 0, s>>>(sims, (const Consts<R> *)consts, tsim, ntiles, flag_in, flag_out, glist,
                                                          blist, ctr);
     return cudaGetLastError();
   }
   static cudaError_t bulk(int grid, bool mul, bool diag, cudaStream_t s, const SimDesc *sims, const void *consts,
-                          const int *tsim, const int *blist, const TensorMapSlot *tmaps, int buf,
+                          const int *tsim, const int4 *blist, const TensorMapSlot *tmaps, int buf,
                           const void *state, void *next, TileFlags *flag_out, int *ctr, int ndone, StatBufs st) {
 #define GP_BULK(SUMS, MUL, DIAG)                                                                               \
   kf_bulk<R, N, K, SUMS, MUL, DIAG><<<grid, NT, bulk_smem, s>>>(sims, (const Consts<R> *)consts, tsim, blist, tmaps,  \
@@ -123,6 +167,8 @@ struct BatchKernels {
     t.prepare = prepare;
     t.classify = classify;
     t.bulk = bulk;
+    t.step = step;
+    t.step_occupancy = step_occupancy;
     t.general = general;
     t.flags = flags;
     t.sdphi = sdphi;

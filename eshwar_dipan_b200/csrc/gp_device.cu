@@ -258,7 +258,7 @@ struct gp_batch {
   std::vector<gp_params> params;
   std::vector<gp_derived> derived;
   std::vector<gpd::SimDesc> desc;
-  int dev, nsm, grid_b, grid_g;
+  int dev, nsm, grid_b, grid_g, grid_s;   /* grid_s: kf_step (0: bulk and interface kernels apart) */
   bool mul;                     /* every simulation's dx and dy are powers of two (or FP32) */
   bool diag;                    /* off-diagonal D, c_mu, A all zero and no E is -0, in every simulation */
   int ntiles;                   /* TX x TY tiles over all simulations */
@@ -271,7 +271,7 @@ struct gp_batch {
   void *dphi;                   /* delta-phi planes of the smoothing sweeps */
   gpd::TileFlags *flags[2];     /* per tile and state buffer: one-hot phase of the tile and its edge bands */
   int *glist;                   /* interface tiles of the current step */
-  int *blist;                   /* bulk tiles of the current step (tile | phase << 28) */
+  int4 *blist;                  /* bulk tiles of the current step (entries written by kf_classify) */
   int *counters;                /* gpd::CTR_* */
   gpd::TensorMapSlot *tmaps;    /* [nsims][2]: TMA maps of each simulation's mu planes in state[0], state[1] */
   int cur;
@@ -311,8 +311,16 @@ static int batch_step_once(gp_batch *b, int want_sums, cudaEvent_t *ev) {
   st.round_step = (const unsigned *)(b->counters + gpd::CTR_STEP);
   const int in = b->cur, out = b->cur ^ 1;
   if (ev) BK(cudaEventRecord(ev[0], b->stream));
-  BK(b->L.classify(b->ntiles, b->stream, b->d_desc, b->d_consts, b->d_tsim, b->flags[in], b->glist, b->blist,
-                   b->counters));
+  BK(b->L.classify(b->ntiles, b->stream, b->d_desc, b->d_consts, b->d_tsim, b->flags[in], b->flags[out], b->glist,
+                   b->blist, b->counters));
+  if (!ev && !want_sums && b->grid_s > 0) {
+    /* one launch for both kinds of tile */
+    BK(b->L.step(b->grid_s, b->mul, b->diag, b->stream, b->d_desc, b->d_consts, b->d_tsim, b->blist, b->glist,
+                 b->tmaps, in, b->state[in], b->state[out], b->flags[out], b->counters, b->grid_s, st));
+    b->cur = out;
+    b->steps++;
+    return GP_OK;
+  }
   /* kf_bulk then kf_general; the last CTA of the two resets the lists */
   const int nd = b->grid_b + b->grid_g;
   BK(b->L.bulk(b->grid_b, b->mul, b->diag, b->stream, b->d_desc, b->d_consts, b->d_tsim, b->blist, b->tmaps, in,
@@ -617,6 +625,16 @@ int gp_batch_create(gp_batch **out, int nsims, const gp_params *params, const do
     }
   }
   b->ntiles = nt;
+  for (int s = 0; s < nsims; s++) {
+    /* kf_bulk packs a tile's row and column into 15 and 16 bits */
+    const gpd::SimDesc &sd = b->desc[s];
+    if ((sd.g.mx + gpd::TX - 1) / gpd::TX >= (1 << 15) || sd.tiles_x >= (1 << 16)) {
+      rc = bfail(b, GP_EINVAL, "gp_batch_create: simulation %d: grid %dx%d has more than 2^15 tile rows or 2^16 tile "
+                               "columns", s, sd.g.mx, sd.g.my);
+      gp_batch_destroy(b);
+      return rc;
+    }
+  }
   if (nt >= (1 << 28)) {
     rc = bfail(b, GP_EINVAL, "gp_batch_create: %d tiles of %dx%d cells, at most 2^28", nt, gpd::TX, gpd::TY);
     gp_batch_destroy(b);
@@ -644,6 +662,11 @@ int gp_batch_create(gp_batch **out, int nsims, const gp_params *params, const do
   }
   b->grid_b = std::min(nt, b->nsm * std::max(1, bpb));
   b->grid_g = b->nsm * std::max(1, bpg);
+  /* the single-launch step when it keeps the bulk kernel's occupancy */
+  {
+    const int bps = b->L.step_occupancy();
+    b->grid_s = (bps >= bpb && getenv("GP_SPLIT_KERNELS") == nullptr) ? b->nsm * bps : 0;
+  }
 #define BALLOC(ptr, bytes)                                                                        \
   do {                                                                                            \
     if (cudaMalloc((void **)&(ptr), (bytes)) != cudaSuccess) {                                     \
@@ -658,7 +681,7 @@ int gp_batch_create(gp_batch **out, int nsims, const gp_params *params, const do
   BALLOC(b->flags[0], 2 * sizeof(gpd::TileFlags) * (size_t)nt);
   b->flags[1] = b->flags[0] + nt;
   BALLOC(b->glist, sizeof(int) * (size_t)nt);
-  BALLOC(b->blist, sizeof(int) * (size_t)nt);
+  BALLOC(b->blist, sizeof(int4) * (size_t)nt);
   BALLOC(b->d_desc, sizeof(gpd::SimDesc) * nsims);
   BALLOC(b->d_consts, csz * nsims);
   BALLOC(b->d_tsim, sizeof(int) * (size_t)nt);

@@ -631,7 +631,8 @@ __device__ __forceinline__ TileFlags general_tile(const CT &D, const Grid &g, co
  * and clears it).  The last CTA of the two kernels resets [0..2] and [4] and
  * advances [3], so a step is exactly the three launches kf_classify, then
  * kf_bulk and kf_general (in either order or side by side). */
-enum { CTR_LIST = 0, CTR_HEAD = 1, CTR_DONE = 2, CTR_STEP = 3, CTR_BULK = 4, CTR_ERR = 5, CTR_COUNT = 8 };
+enum { CTR_LIST = 0, CTR_HEAD = 1, CTR_DONE = 2, CTR_STEP = 3, CTR_BULK = 4, CTR_ERR = 5, CTR_BHEAD = 6,
+       CTR_COUNT = 8 };
 
 /* End of one CTA of the step's bulk or interface kernel (they may run
  * concurrently): the last of the step's ndone CTAs empties the lists and
@@ -649,26 +650,32 @@ __device__ __forceinline__ void step_finish(int *ctr, int ndone) {
     ctr[CTR_HEAD] = 0;
     ctr[CTR_DONE] = 0;
     ctr[CTR_BULK] = 0;
+    ctr[CTR_BHEAD] = 0;
     ctr[CTR_STEP] = (int)((unsigned)ctr[CTR_STEP] + 1u);
     __threadfence();
   }
 }
 
 /* One thread per tile: the bulk test, then the tile goes on the bulk list
- * (entry t | phase << 28) or the interface list; one atomic per warp and
- * list. */
+ * or the interface list; one atomic per warp and list.  A bulk entry holds
+ * everything kf_bulk needs to start the tile: {t | phase << 28, simulation |
+ * flag of the output buffer << 24, tile row << 16 | tile column, 0}.  Small CTAs (NTC threads) spread the flag reads over every SM. */
+constexpr int NTC = 64;
 template <typename R>
-__global__ void __launch_bounds__(NT) kf_classify(const SimDesc *__restrict__ sims,
+__global__ void __launch_bounds__(NTC) kf_classify(const SimDesc *__restrict__ sims,
                                                   const Consts<R> *__restrict__ consts, const int *__restrict__ tsim,
                                                   int ntiles, const TileFlags *__restrict__ flag_in,
-                                                  int *__restrict__ glist, int *__restrict__ blist,
+                                                  const TileFlags *__restrict__ flag_outbuf,
+                                                  int *__restrict__ glist, int4 *__restrict__ blist,
                                                   int *__restrict__ ctr) {
-  const int t = blockIdx.x * NT + threadIdx.x, lane = threadIdx.x & 31;
-  int p = -1;
+  const int t = blockIdx.x * NTC + threadIdx.x, lane = threadIdx.x & 31;
+  int p = -1, s = 0, by = 0, bx = 0;
   if (t < ntiles) {
-    const int s = __ldg(tsim + t);
+    s = __ldg(tsim + t);
     const SimDesc &sd = sims[s];
-    const int lt = t - sd.tile0, by = lt / sd.tiles_x, bx = lt - by * sd.tiles_x;
+    const int lt = t - sd.tile0;
+    by = lt / sd.tiles_x;
+    bx = lt - by * sd.tiles_x;
     p = bulk_phase<R>(consts[s], sd.g, flag_in, sd.tile0, sd.tiles_x, by, bx);
   }
   const unsigned mb = __ballot_sync(0xffffffffu, t < ntiles && p >= 0);
@@ -682,7 +689,9 @@ __global__ void __launch_bounds__(NT) kf_classify(const SimDesc *__restrict__ si
   bg = __shfl_sync(0xffffffffu, bg, 0);
   const unsigned below = (1u << lane) - 1u;
   if (t < ntiles) {
-    if (p >= 0) blist[bb + __popc(mb & below)] = t | (p << 28);
+    if (p >= 0)
+      blist[bb + __popc(mb & below)] =
+          make_int4(t | (p << 28), s | (((int)flag_outbuf[t].whole & 0xff) << 24), (by << 16) | bx, 0);
     else glist[bg + __popc(mg & below)] = t;
   }
 }
@@ -750,17 +759,24 @@ template <typename R, int K>
 struct BulkGeom {
   static constexpr int CO = sizeof(R) == 8 ? 1 : 3;
   static constexpr int BW = SW + 2 * CO;   /* 36 doubles or 40 floats: a multiple of 16 bytes */
-  static constexpr int NST = 2;
+  /* boxes in flight per warp: 4 of FP32 or 2 of FP64 (the same bytes) */
+  static constexpr int NST = sizeof(R) == 4 ? 4 : 2;
   static constexpr unsigned BOX_BYTES = (unsigned)(K * SH * BW * sizeof(R));
 };
 template <typename R, int K>
 struct alignas(128) BulkStage {
   R M[K][SH][BulkGeom<R, K>::BW];
 };
+/* list entry of a tile in flight: tile | phase << 28, simulation, first
+ * cell, the flag of its output buffer */
+struct BulkEntry {
+  int item, s, x0, y0, have;
+};
 template <typename R, int K>
 struct alignas(128) BulkWarpSmem {
   BulkStage<R, K> st[BulkGeom<R, K>::NST];
   unsigned long long bar[BulkGeom<R, K>::NST];
+  BulkEntry meta[BulkGeom<R, K>::NST];
 };
 /* dynamic shared memory of kf_bulk (the base is rounded up to 128 bytes in
  * the kernel) */
@@ -782,22 +798,18 @@ constexpr size_t bulk_smem_bytes() {
  * initial [0, 1]).  A stage whose bytes do not arrive within the poll limit
  * sets ctr[CTR_ERR]; the warp then stops taking tiles. */
 template <typename R, int N, int K, bool SUMS, bool MUL, bool DIAG>
-__global__ void __launch_bounds__(NT, 2) kf_bulk(const SimDesc *__restrict__ sims, const Consts<R> *__restrict__ consts,
-                                                 const int *__restrict__ tsim, const int *__restrict__ blist,
-                                                 const TensorMapSlot *__restrict__ tmaps, int buf,
-                                                 const R *__restrict__ state, R *__restrict__ next,
-                                                 TileFlags *__restrict__ flag_out, int *__restrict__ ctr,
-                                                 int ndone, StatBufs st) {
+__device__ __forceinline__ void bulk_tiles(const SimDesc *__restrict__ sims, const Consts<R> *__restrict__ consts,
+                                           const int *__restrict__ tsim, const int4 *__restrict__ blist,
+                                           const TensorMapSlot *__restrict__ tmaps, int buf,
+                                           const R *__restrict__ state, R *__restrict__ next,
+                                           TileFlags *__restrict__ flag_out, int *__restrict__ ctr, StatBufs st,
+                                           unsigned char *smraw) {
   using G = BulkGeom<R, K>;
-  constexpr int NW = NT / 32, NS = 2 * N + 2 * K + 1, NST = G::NST, CO = G::CO;
-  extern __shared__ __align__(128) unsigned char smraw[];
+  constexpr int NS = 2 * N + 2 * K + 1, NST = G::NST, CO = G::CO;
   unsigned char *sbase = (unsigned char *)(((size_t)smraw + 127) & ~(size_t)127);
   BulkWarpSmem<R, K> &ws = reinterpret_cast<BulkWarpSmem<R, K> *>(sbase)[threadIdx.x >> 5];
   const int lane = threadIdx.x & 31;
-  const int gw = blockIdx.x * NW + (threadIdx.x >> 5), nwarps = gridDim.x * NW;
   const int nbulk = *(const volatile int *)(ctr + CTR_BULK);
-  const int per = (nbulk + nwarps - 1) / nwarps;
-  const int i0 = gw * per, i1 = min(nbulk, i0 + per);
 
   if (lane == 0) {
 #pragma unroll
@@ -825,39 +837,63 @@ __global__ void __launch_bounds__(NT, 2) kf_bulk(const SimDesc *__restrict__ sim
     }
   };
 
-  /* The warp's list entries, 32 at a time: lane r holds entry i0+base+r
-   * (tile | phase << 28), its simulation, its first cell and the flag its
-   * output buffer holds; a tile's values reach every lane by shuffles.  The
-   * dependent loads of a batch go out once per 32 tiles, not per tile. */
-  int q_item = 0, q_s = 0, q_x0 = 0, q_y0 = 0, q_have = 0;
-  auto load_batch = [&](int base) {
-    const int e = i0 + base + lane;
-    if (e < i1) {
-      q_item = __ldg(blist + e);
-      const int t = q_item & 0x0fffffff;
-      q_s = __ldg(tsim + t);
-      const int lt = t - sims[q_s].tile0, tx = sims[q_s].tiles_x, by = lt / tx;
-      q_x0 = by * TX;
-      q_y0 = (lt - by * tx) * TY;
-      q_have = flag_out[t].whole;
+  /* Work comes in chunks of list entries taken from the bulk head counter
+   * (one atomic per warp and chunk), so warps that run faster take more; the
+   * chunk size shrinks as the list drains (a few chunks per warp in all).
+   * Two chunks are held: A (being issued) and B (next).  Lane h*16+r holds
+   * entry r of the chunk in half h; B's entries are loaded when it is taken,
+   * one 16-byte load per lane, and used one tile later. */
+  constexpr int BCH = 16;
+  const int nwarps = gridDim.x * (NT / 32);
+  int q_item = 0, q_s = 0, q_xy = 0;   /* q_s: simulation | output flag << 24; q_xy: tile row << 16 | column */
+  auto grab = [&](int half, int &start, int &n) {
+    int v = 0, c = 0;
+    if (lane == 0) {
+      const int left = nbulk - *(volatile int *)(ctr + CTR_BHEAD);
+      c = max(2, min(BCH, left / (2 * nwarps)));
+      v = atomicAdd(ctr + CTR_BHEAD, c);
+    }
+    start = __shfl_sync(0xffffffffu, v, 0);
+    c = __shfl_sync(0xffffffffu, c, 0);
+    n = max(0, min(c, nbulk - start));
+    const int r = lane - 16 * half;
+    if (r >= 0 && r < n) {
+      const int4 e = __ldg(blist + start + r);
+      q_item = e.x;
+      q_s = e.y;
+      q_xy = e.z;
     }
   };
-  struct Entry {
-    int item, s, x0, y0, have;
-  };
-  auto entry = [&](int i) {
-    const int r = (i - i0) & 31;
-    Entry en;
+  int ha = 0, na = 0, pa = 0;   /* chunk A: half, entries, next to issue */
+  int cb = 0, nb = 0;           /* chunk B (half ha ^ 1) */
+  {
+    int ca = 0;
+    grab(0, ca, na);
+  }
+  if (na > 0) grab(1, cb, nb);
+  /* the next entry in issue order; false when the list is used up */
+  auto next_entry = [&](BulkEntry &en) {
+    if (pa == na) {
+      if (nb == 0) return false;
+      ha ^= 1;
+      na = nb;
+      pa = 0;
+      grab(ha ^ 1, cb, nb);
+    }
+    const int r = 16 * ha + pa;
     en.item = __shfl_sync(0xffffffffu, q_item, r);
-    en.s = __shfl_sync(0xffffffffu, q_s, r);
-    en.x0 = __shfl_sync(0xffffffffu, q_x0, r);
-    en.y0 = __shfl_sync(0xffffffffu, q_y0, r);
-    en.have = __shfl_sync(0xffffffffu, q_have, r);
-    return en;
+    const int sh = __shfl_sync(0xffffffffu, q_s, r), xy = __shfl_sync(0xffffffffu, q_xy, r);
+    en.s = sh & 0xffffff;
+    en.have = (signed char)(sh >> 24);
+    en.x0 = (xy >> 16) * TX;
+    en.y0 = (xy & 0xffff) * TY;
+    pa++;
+    return true;
   };
-  /* lane 0: start the TMA box of a tile into stage b */
-  auto issue = [&](const Entry &en, int b) {
+  /* lane 0: start the TMA box of a tile into stage b and note its entry */
+  auto issue = [&](const BulkEntry &en, int b) {
     if (lane == 0) {
+      ws.meta[b] = en;
       const unsigned bar = smem_addr(&ws.bar[b]);
       mbar_expect_tx(bar, G::BOX_BYTES);
       tma_load_3d(smem_addr(&ws.st[b]), tmaps + 2 * en.s + buf, en.y0 - 1 - CO, en.x0 - 1, 0, bar);
@@ -892,28 +928,36 @@ __global__ void __launch_bounds__(NT, 2) kf_bulk(const SimDesc *__restrict__ sim
   /* FP32: the step's part of the rounding key */
   const unsigned skey = sizeof(R) == 4 ? mix32(__ldg(st.round_step) * 0x9e3779b9u + 0x632be5abu) : 0u;
 
-  Entry cur = {};
-  if (i0 < i1) {
-    load_batch(0);
-    cur = entry(i0);
-    issue(cur, 0);
+  /* the qi-th box a warp issues goes to stage qi % NST and completes phase
+   * (qi / NST) & 1 of that stage's barrier; NST-1 boxes are in flight while a
+   * tile is stepped */
+  int qi = 0, ci = 0;
+  for (int q = 0; q < NST - 1; q++) {
+    BulkEntry en;
+    if (!next_entry(en)) break;
+    issue(en, qi % NST);
+    qi++;
   }
-  for (int i = i0; i < i1; i++) {
-    const int b = (i - i0) & 1;
-    Entry nxt = {};
-    if (i + 1 < i1) {
-      if (((i + 1 - i0) & 31) == 0) load_batch(i + 1 - i0);
-      nxt = entry(i + 1);
-      issue(nxt, b ^ 1);
+  __syncwarp();
+  while (ci < qi) {
+    {
+      BulkEntry en;
+      if (next_entry(en)) {   /* into the stage of tile ci-1, stepped already */
+        issue(en, qi % NST);
+        qi++;
+      }
     }
-    if (!mbar_wait(smem_addr(&ws.bar[b]), ((i - i0) >> 1) & 1)) {
-      /* bytes missing: record it, wait (bounded) for the other box in
+    const int b = ci % NST;
+    if (!mbar_wait(smem_addr(&ws.bar[b]), (ci / NST) & 1)) {
+      /* bytes missing: record it, wait (bounded) for the other boxes in
        * flight, step nothing more */
       if (lane == 0) atomicExch(ctr + CTR_ERR, 1);
-      if (i + 1 < i1) mbar_wait(smem_addr(&ws.bar[b ^ 1]), ((i + 1 - i0) >> 1) & 1);
+      for (int q = ci + 1; q < qi; q++) mbar_wait(smem_addr(&ws.bar[q % NST]), (q / NST) & 1);
       break;
     }
+    ci++;
     /* ---- step bulk tile t (phase p) from stage b */
+    const BulkEntry cur = ws.meta[b];
     const int t = cur.item & 0x0fffffff, p = cur.item >> 28, s = cur.s;
     const int x0 = cur.x0, y0 = cur.y0, have = cur.have;
     const Consts<R> &D = consts[s];
@@ -1132,22 +1176,33 @@ __global__ void __launch_bounds__(NT, 2) kf_bulk(const SimDesc *__restrict__ sim
       }
     }
     if (lane == 0) flag_out[t] = uniform_flags(p);
-    __syncwarp();   /* stage b is refilled by the next issue */
-    cur = nxt;
+    __syncwarp();   /* stage b is refilled by a later issue */
   }
   if (cur_sim >= 0) flush(cur_sim);
+}
+
+template <typename R, int N, int K, bool SUMS, bool MUL, bool DIAG>
+__global__ void __launch_bounds__(NT, 2) kf_bulk(const SimDesc *__restrict__ sims, const Consts<R> *__restrict__ consts,
+                                                 const int *__restrict__ tsim, const int4 *__restrict__ blist,
+                                                 const TensorMapSlot *__restrict__ tmaps, int buf,
+                                                 const R *__restrict__ state, R *__restrict__ next,
+                                                 TileFlags *__restrict__ flag_out, int *__restrict__ ctr,
+                                                 int ndone, StatBufs st) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  bulk_tiles<R, N, K, SUMS, MUL, DIAG>(sims, consts, tsim, blist, tmaps, buf, state, next, flag_out, ctr, st, smraw);
   step_finish(ctr, ndone);
 }
 
-/* Persistent CTAs over the interface list.  Each simulation's constants are
- * copied into shared memory when a CTA moves to it. */
+/* Interface tiles of one step: the CTA takes tiles from the interface list
+ * until it is empty.  Each simulation's constants are copied into shared
+ * memory when the CTA moves to it.  Not inlined: the step kernel and the
+ * interface-only kernel share one copy of this code. */
 template <typename R, int N, int K, bool ANISO, bool MUL>
-__global__ void __launch_bounds__(NT, (N <= 3 ? 2 : 1)) kf_general(const SimDesc *__restrict__ sims,
-                                                 const Consts<R> *__restrict__ consts, const int *__restrict__ tsim,
-                                                 const R *__restrict__ state, R *__restrict__ next,
-                                                 TileFlags *__restrict__ flag_out, const int *__restrict__ glist,
-                                                 int *__restrict__ ctr, int ndone, StatBufs st) {
-  extern __shared__ __align__(16) unsigned char smraw[];
+__device__ __noinline__ void general_tiles(const SimDesc *__restrict__ sims, const Consts<R> *__restrict__ consts,
+                                           const int *__restrict__ tsim, const R *__restrict__ state,
+                                           R *__restrict__ next, TileFlags *__restrict__ flag_out,
+                                           const int *__restrict__ glist, int *__restrict__ ctr, StatBufs st,
+                                           unsigned char *smraw) {
   GenSmem<R, N, K> &sm = *reinterpret_cast<GenSmem<R, N, K> *>(smraw);
   __shared__ Consts<R> sc;
   __shared__ int s_item;
@@ -1176,6 +1231,34 @@ __global__ void __launch_bounds__(NT, (N <= 3 ? 2 : 1)) kf_general(const SimDesc
     if (threadIdx.x == 0) flag_out[t] = f;
     __syncthreads();
   }
+}
+
+template <typename R, int N, int K, bool ANISO, bool MUL>
+__global__ void __launch_bounds__(NT, (N <= 3 ? 2 : 1)) kf_general(const SimDesc *__restrict__ sims,
+                                                 const Consts<R> *__restrict__ consts, const int *__restrict__ tsim,
+                                                 const R *__restrict__ state, R *__restrict__ next,
+                                                 TileFlags *__restrict__ flag_out, const int *__restrict__ glist,
+                                                 int *__restrict__ ctr, int ndone, StatBufs st) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  general_tiles<R, N, K, ANISO, MUL>(sims, consts, tsim, state, next, flag_out, glist, ctr, st, smraw);
+  step_finish(ctr, ndone);
+}
+
+/* One step in one persistent launch: each CTA takes interface tiles while
+ * the interface list lasts, then its warps take bulk tiles, so the two kinds
+ * of work share the SMs and the step ends with one tail instead of two. */
+template <typename R, int N, int K, bool ANISO, bool MUL, bool DIAG>
+__global__ void __launch_bounds__(NT, (N <= 3 ? 2 : 1)) kf_step(const SimDesc *__restrict__ sims,
+                                                 const Consts<R> *__restrict__ consts, const int *__restrict__ tsim,
+                                                 const int4 *__restrict__ blist, const int *__restrict__ glist,
+                                                 const TensorMapSlot *__restrict__ tmaps, int buf,
+                                                 const R *__restrict__ state, R *__restrict__ next,
+                                                 TileFlags *__restrict__ flag_out, int *__restrict__ ctr,
+                                                 int ndone, StatBufs st) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  general_tiles<R, N, K, ANISO, MUL>(sims, consts, tsim, state, next, flag_out, glist, ctr, st, smraw);
+  __syncthreads();   /* the interface tiles' shared memory becomes the bulk stages */
+  bulk_tiles<R, N, K, false, MUL, DIAG>(sims, consts, tsim, blist, tmaps, buf, state, next, flag_out, ctr, st, smraw);
   step_finish(ctr, ndone);
 }
 

@@ -191,3 +191,25 @@ def test_fp32_precision_workload(tmp_path):
     for k in range(p.numcomponents - 1):
         drift = abs(st32["comp_sum"][k] - st64["comp_sum"][k]) / abs(st64["comp_sum"][k])
         assert drift <= FP32_MASS_TOL, "comp %d: mass drift %.3e" % (k, drift)
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_single_launch_step_matches_two_kernels(tmp_path, monkeypatch, prec):
+    """Steps as one launch (kf_step: interface tiles, then bulk tiles) and as
+    two launches (kf_bulk, kf_general; GP_SPLIT_KERNELS=1 at batch creation)
+    give the same bits."""
+    sims = _ternary_group(tmp_path)
+    args = ([s[0] for s in sims], [(s[1], s[2]) for s in sims])
+    pr = gp.GP_FP64 if prec == "fp64" else gp.GP_FP32
+    b1 = gp.Batch(*args, precision=pr)
+    monkeypatch.setenv("GP_SPLIT_KERNELS", "1")
+    b2 = gp.Batch(*args, precision=pr)
+    monkeypatch.delenv("GP_SPLIT_KERNELS")
+    for b in (b1, b2):
+        b.smooth(5)
+        b.step(230, stats=False)
+    for i in range(len(sims)):
+        x, y = b1.get(i), b2.get(i)
+        assert bits_equal(x[0], y[0]) and bits_equal(x[1], y[1]), "sim %d" % i
+    b1.close()
+    b2.close()
