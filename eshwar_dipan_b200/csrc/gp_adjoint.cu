@@ -28,7 +28,7 @@
 namespace gpd {
 
 #ifndef GP_ADJ_W
-#define GP_ADJ_W 1
+#define GP_ADJ_W 2   /* two seeded inputs per pass: fewer passes, few spills (1 and 3, 4 were slower) */
 #endif
 constexpr int ADJ_W = GP_ADJ_W;
 constexpr int AB = 128;   /* threads per block along y */
