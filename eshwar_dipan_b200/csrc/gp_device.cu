@@ -24,6 +24,8 @@
 #include <cstdlib>
 #include <cstring>
 #include <algorithm>
+#include <mutex>
+#include <thread>
 #include <vector>
 
 #include "gp_adjoint_launch.h"
@@ -34,6 +36,8 @@ static __constant__ gpd::Consts<double> cD;
 extern "C" const char *gp_host_thread_error(void);
 
 #define GP_GRAPH_STEPS 100
+#define GP_STAGE_BYTES ((size_t)8 << 20)   /* each of a device's two pinned host staging buffers */
+#define GP_STAGE_MAX_DEVICES 64
 
 /* ======================================================================= */
 /* helpers                                                                 */
@@ -432,39 +436,132 @@ static int batch_step_impl(gp_batch *b, long nsteps, gp_stats *stats, double *to
   return GP_OK;
 }
 
-/* host <-> state of one simulation (kind: H2D, D2H, D2D).  FP32 converts
- * through a host staging buffer and exchanges host buffers only. */
+/* Pinned host staging buffers of gp_set/gp_get, one pair per device. */
+struct StagePair {
+  void *buf[2];
+  cudaEvent_t ev[2];
+};
+static StagePair g_stage[GP_STAGE_MAX_DEVICES];
+static std::mutex g_stage_mutex;
+
+/* Host-side copy of n bytes (or conversion of n elements) split over a few
+ * threads when it is large: a single thread moves about 10 GB/s, below what
+ * the DMA engines take from pinned memory. */
+template <typename F>
+static void host_parallel(size_t n, size_t grain, F &&part) {
+  const int nt = (int)std::min<size_t>(8, std::max<size_t>(1, n / grain));
+  if (nt == 1) {
+    part((size_t)0, n);
+    return;
+  }
+  std::vector<std::thread> th;
+  const size_t per = (n + nt - 1) / nt;
+  for (int i = 1; i < nt; i++) {
+    const size_t lo = std::min(n, i * per), hi = std::min(n, lo + per);
+    th.emplace_back([&part, lo, hi] { part(lo, hi); });
+  }
+  part((size_t)0, std::min(n, per));
+  for (auto &t : th) t.join();
+}
+
+/* host <-> state of one simulation (kind: H2D, D2H, D2D).  Host buffers move
+ * through the batch's two pinned staging buffers in chunks of rows: the DMA
+ * of one chunk overlaps the host copy (FP64) or conversion (FP32) of the
+ * other.  FP32 exchanges host buffers only. */
 static int batch_copy(gp_batch *b, int s, const double *phi, const double *mu, double *ophi, double *omu,
                       cudaMemcpyKind kind) {
   const gpd::SimDesc &sd = b->desc[s];
   const int N = b->N, K = b->K;
-  const size_t mx = sd.g.mx, my = sd.g.my;
-  char *base = (char *)b->state[b->cur] + (size_t)sd.off_state * b->elem;
+  const size_t mx = sd.g.mx, my = sd.g.my, es = b->elem, dpitch = (size_t)sd.g.pitch * es;
+  char *base = (char *)b->state[b->cur] + (size_t)sd.off_state * es;
   const bool up = phi != nullptr;
-  for (int f = 0; f < N + K; f++) {
-    char *plane = base + (size_t)f * sd.g.plane * b->elem;
-    if (b->elem == 8) {
+  if (kind == cudaMemcpyDeviceToDevice) {
+    for (int f = 0; f < N + K; f++) {
+      char *plane = base + (size_t)f * sd.g.plane * es;
       if (up) {
         const double *src = f < N ? phi + (size_t)f * mx * my : mu + (size_t)(f - N) * mx * my;
-        BK(cudaMemcpy2DAsync(plane, (size_t)sd.g.pitch * 8, src, my * 8, my * 8, mx, kind, b->stream));
+        BK(cudaMemcpy2DAsync(plane, dpitch, src, my * 8, my * 8, mx, kind, b->stream));
       } else {
         double *dst = f < N ? ophi + (size_t)f * mx * my : omu + (size_t)(f - N) * mx * my;
-        BK(cudaMemcpy2DAsync(dst, my * 8, plane, (size_t)sd.g.pitch * 8, my * 8, mx, kind, b->stream));
+        BK(cudaMemcpy2DAsync(dst, my * 8, plane, dpitch, my * 8, mx, kind, b->stream));
       }
-    } else {
-      std::vector<float> tmp(mx * my);
-      if (up) {
-        const double *src = f < N ? phi + (size_t)f * mx * my : mu + (size_t)(f - N) * mx * my;
-        for (size_t i = 0; i < mx * my; i++) tmp[i] = (float)src[i];
-        BK(cudaMemcpy2DAsync(plane, (size_t)sd.g.pitch * 4, tmp.data(), my * 4, my * 4, mx, cudaMemcpyHostToDevice,
-                             b->stream));
-        BK(cudaStreamSynchronize(b->stream));
+    }
+    BK(cudaStreamSynchronize(b->stream));
+    return GP_OK;
+  }
+  /* the device's staging pair, held for the life of the process (freeing
+   * pinned memory waits on the whole device); one copy at a time uses it */
+  std::lock_guard<std::mutex> lock(g_stage_mutex);
+  if (b->dev < 0 || b->dev >= GP_STAGE_MAX_DEVICES) return bfail(b, GP_EINVAL, "batch copy: device %d", b->dev);
+  StagePair &sp = g_stage[b->dev];
+  if (!sp.buf[0]) {
+    for (int i = 0; i < 2; i++) {
+      BK(cudaHostAlloc(&sp.buf[i], GP_STAGE_BYTES, cudaHostAllocDefault));
+      BK(cudaEventCreateWithFlags(&sp.ev[i], cudaEventDisableTiming));
+    }
+  }
+  void *const *stage = sp.buf;
+  cudaEvent_t const *sev = sp.ev;
+  /* chunks: (field, first row, rows) */
+  const size_t rows_per = std::max<size_t>(1, GP_STAGE_BYTES / (my * es));
+  struct Chunk {
+    int f;
+    size_t r0, nr;
+  };
+  std::vector<Chunk> ch;
+  for (int f = 0; f < N + K; f++)
+    for (size_t r = 0; r < mx; r += rows_per) ch.push_back({f, r, std::min(rows_per, mx - r)});
+  auto host_rows = [&](const Chunk &c, bool in) -> const double * {
+    const double *h = in ? (c.f < N ? phi + (size_t)c.f * mx * my : mu + (size_t)(c.f - N) * mx * my)
+                         : (c.f < N ? ophi + (size_t)c.f * mx * my : omu + (size_t)(c.f - N) * mx * my);
+    return h + c.r0 * my;
+  };
+  auto dev_rows = [&](const Chunk &c) { return base + (size_t)c.f * sd.g.plane * es + c.r0 * dpitch; };
+  const size_t grain = (size_t)1 << 20;
+  if (up) {
+    for (size_t i = 0; i < ch.size(); i++) {
+      const int k = (int)(i & 1);
+      if (i >= 2) BK(cudaEventSynchronize(sev[k]));   /* the DMA that last read this buffer */
+      const double *src = host_rows(ch[i], true);
+      const size_t n = ch[i].nr * my;
+      if (es == 8) {
+        char *dst = (char *)stage[k];
+        host_parallel(n * 8, grain, [&](size_t lo, size_t hi) { memcpy(dst + lo, (const char *)src + lo, hi - lo); });
       } else {
-        BK(cudaMemcpy2DAsync(tmp.data(), my * 4, plane, (size_t)sd.g.pitch * 4, my * 4, mx, cudaMemcpyDeviceToHost,
-                             b->stream));
-        BK(cudaStreamSynchronize(b->stream));
-        double *dst = f < N ? ophi + (size_t)f * mx * my : omu + (size_t)(f - N) * mx * my;
-        for (size_t i = 0; i < mx * my; i++) dst[i] = (double)tmp[i];
+        float *dst = (float *)stage[k];
+        host_parallel(n, grain / 4, [&](size_t lo, size_t hi) {
+          for (size_t j = lo; j < hi; j++) dst[j] = (float)src[j];
+        });
+      }
+      BK(cudaMemcpy2DAsync(dev_rows(ch[i]), dpitch, stage[k], my * es, my * es, ch[i].nr, cudaMemcpyHostToDevice,
+                           b->stream));
+      BK(cudaEventRecord(sev[k], b->stream));
+    }
+  } else {
+    auto fetch = [&](size_t i) -> int {
+      const int k = (int)(i & 1);
+      BK(cudaMemcpy2DAsync(stage[k], my * es, dev_rows(ch[i]), dpitch, my * es, ch[i].nr, cudaMemcpyDeviceToHost,
+                           b->stream));
+      BK(cudaEventRecord(sev[k], b->stream));
+      return GP_OK;
+    };
+    int rc = fetch(0);
+    if (rc != GP_OK) return rc;
+    for (size_t i = 0; i < ch.size(); i++) {
+      const int k = (int)(i & 1);
+      /* the other buffer was emptied by the previous iteration */
+      if (i + 1 < ch.size() && (rc = fetch(i + 1)) != GP_OK) return rc;
+      BK(cudaEventSynchronize(sev[k]));
+      double *dst = (double *)host_rows(ch[i], false);
+      const size_t n = ch[i].nr * my;
+      if (es == 8) {
+        const char *src = (const char *)stage[k];
+        host_parallel(n * 8, grain, [&](size_t lo, size_t hi) { memcpy((char *)dst + lo, src + lo, hi - lo); });
+      } else {
+        const float *src = (const float *)stage[k];
+        host_parallel(n, grain / 4, [&](size_t lo, size_t hi) {
+          for (size_t j = lo; j < hi; j++) dst[j] = (double)src[j];
+        });
       }
     }
   }
