@@ -164,6 +164,15 @@ class Simulation:
         mu = np.ascontiguousarray(mu, dtype=np.float64)
         check(lib().gp_set(self._h, _ptr(phi), _ptr(mu)), self._h)
 
+    def vtk_write_async(self, path, ascii=None):
+        """gp_vtk_write_async: write the current state to `path` in the
+        background while stepping goes on; complete after vtk_wait()."""
+        a = self.params.ascii if ascii is None else int(ascii)
+        check(lib().gp_vtk_write_async(self._h, str(path).encode(), a), self._h)
+
+    def vtk_wait(self):
+        check(lib().gp_vtk_wait(self._h), self._h)
+
     def close(self):
         if getattr(self, "_h", None):
             lib().gp_destroy(self._h)

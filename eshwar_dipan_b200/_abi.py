@@ -117,6 +117,8 @@ SIGNATURES = {
     "gp_fill": (c_int, [POINTER(Params), ctypes.c_char_p, c_void_p, c_void_p]),
     "gp_vtk_write": (c_int, [POINTER(Params), ctypes.c_char_p, c_void_p, c_void_p, c_int]),
     "gp_vtk_read": (c_int, [POINTER(Params), ctypes.c_char_p, c_void_p, c_void_p, c_int]),
+    "gp_vtk_write_async": (c_int, [c_void_p, ctypes.c_char_p, c_int]),
+    "gp_vtk_wait": (c_int, [c_void_p]),
     "gp_init": (c_int, [POINTER(c_void_p), POINTER(Params), c_void_p, c_void_p, c_int]),
     "gp_smooth": (c_int, [c_void_p, c_long]),
     "gp_step": (c_int, [c_void_p, c_long, POINTER(Stats)]),

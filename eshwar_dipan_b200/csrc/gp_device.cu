@@ -25,6 +25,7 @@
 #include <cstring>
 #include <algorithm>
 #include <mutex>
+#include <string>
 #include <thread>
 #include <vector>
 
@@ -229,6 +230,14 @@ struct gp_batch;
 struct gp_ctx {
   gp_batch *b;
   char err[256];
+  /* background VTK write (gp_vtk_write_async) */
+  std::thread *writer;          /* the write in flight, or NULL */
+  int wstatus;                  /* its result */
+  char werr[256];
+  void *snap;                   /* device copy of the state being written */
+  cudaStream_t wstream;         /* the writer's copies */
+  cudaEvent_t wready;           /* the snapshot is complete */
+  double *hphi, *hmu;           /* host copies of the snapshot */
 };
 
 static int fail(gp_ctx *c, int code, const char *fmt, ...) {
@@ -464,6 +473,102 @@ static void host_parallel(size_t n, size_t grain, F &&part) {
   for (auto &t : th) t.join();
 }
 
+/* nf device planes (rows of my elements of es bytes, dpitch bytes apart;
+ * planes plane_bytes apart from base) and nf host arrays of mx*my doubles */
+struct StagedPlanes {
+  int dev;
+  char *base;
+  size_t plane_bytes, dpitch, mx, my, es;
+  int nf;
+};
+
+/* Host arrays -> device planes through the device's pinned staging pair, in
+ * chunks of rows: the host copy (FP64) or conversion (FP32) of one chunk
+ * overlaps the DMA of the other.  Work is ordered on `stream`; returns when
+ * the last DMA is queued. */
+static cudaError_t stage_up(const StagedPlanes &sp, double *const *host, cudaStream_t stream) {
+  std::lock_guard<std::mutex> lock(g_stage_mutex);
+  if (sp.dev < 0 || sp.dev >= GP_STAGE_MAX_DEVICES) return cudaErrorInvalidDevice;
+  StagePair &pr = g_stage[sp.dev];
+  cudaError_t e = cudaSuccess;
+  for (int i = 0; i < 2 && !pr.buf[0 + i]; i++) {
+    if ((e = cudaHostAlloc(&pr.buf[i], GP_STAGE_BYTES, cudaHostAllocDefault)) != cudaSuccess) return e;
+    if ((e = cudaEventCreateWithFlags(&pr.ev[i], cudaEventDisableTiming)) != cudaSuccess) return e;
+  }
+  const size_t rows_per = std::max<size_t>(1, GP_STAGE_BYTES / (sp.my * sp.es)), grain = (size_t)1 << 20;
+  size_t i = 0;
+  for (int f = 0; f < sp.nf; f++)
+    for (size_t r0 = 0; r0 < sp.mx; r0 += rows_per, i++) {
+      const size_t nr = std::min(rows_per, sp.mx - r0), n = nr * sp.my;
+      const int k = (int)(i & 1);
+      if (i >= 2 && (e = cudaEventSynchronize(pr.ev[k])) != cudaSuccess) return e;   /* last DMA from it */
+      const double *src = host[f] + r0 * sp.my;
+      if (sp.es == 8) {
+        char *dst = (char *)pr.buf[k];
+        host_parallel(n * 8, grain, [&](size_t lo, size_t hi) { memcpy(dst + lo, (const char *)src + lo, hi - lo); });
+      } else {
+        float *dst = (float *)pr.buf[k];
+        host_parallel(n, grain / 4, [&](size_t lo, size_t hi) {
+          for (size_t j = lo; j < hi; j++) dst[j] = (float)src[j];
+        });
+      }
+      if ((e = cudaMemcpy2DAsync(sp.base + f * sp.plane_bytes + r0 * sp.dpitch, sp.dpitch, pr.buf[k], sp.my * sp.es,
+                                 sp.my * sp.es, nr, cudaMemcpyHostToDevice, stream)) != cudaSuccess)
+        return e;
+      if ((e = cudaEventRecord(pr.ev[k], stream)) != cudaSuccess) return e;
+    }
+  /* the staging pair is reused by the next caller: wait for the last DMAs */
+  for (int k = 0; k < 2; k++)
+    if ((e = cudaEventSynchronize(pr.ev[k])) != cudaSuccess) return e;
+  return cudaSuccess;
+}
+
+/* Device planes -> host arrays, the DMA of one chunk overlapping the host
+ * copy of the previous one. */
+static cudaError_t stage_down(const StagedPlanes &sp, double *const *host, cudaStream_t stream) {
+  std::lock_guard<std::mutex> lock(g_stage_mutex);
+  if (sp.dev < 0 || sp.dev >= GP_STAGE_MAX_DEVICES) return cudaErrorInvalidDevice;
+  StagePair &pr = g_stage[sp.dev];
+  cudaError_t e = cudaSuccess;
+  for (int i = 0; i < 2 && !pr.buf[0 + i]; i++) {
+    if ((e = cudaHostAlloc(&pr.buf[i], GP_STAGE_BYTES, cudaHostAllocDefault)) != cudaSuccess) return e;
+    if ((e = cudaEventCreateWithFlags(&pr.ev[i], cudaEventDisableTiming)) != cudaSuccess) return e;
+  }
+  const size_t rows_per = std::max<size_t>(1, GP_STAGE_BYTES / (sp.my * sp.es)), grain = (size_t)1 << 20;
+  struct Chunk {
+    int f;
+    size_t r0, nr;
+  };
+  std::vector<Chunk> ch;
+  for (int f = 0; f < sp.nf; f++)
+    for (size_t r = 0; r < sp.mx; r += rows_per) ch.push_back({f, r, std::min(rows_per, sp.mx - r)});
+  auto fetch = [&](size_t i) {
+    const int k = (int)(i & 1);
+    cudaError_t x = cudaMemcpy2DAsync(pr.buf[k], sp.my * sp.es, sp.base + ch[i].f * sp.plane_bytes + ch[i].r0 * sp.dpitch,
+                                      sp.dpitch, sp.my * sp.es, ch[i].nr, cudaMemcpyDeviceToHost, stream);
+    return x != cudaSuccess ? x : cudaEventRecord(pr.ev[k], stream);
+  };
+  if (!ch.empty() && (e = fetch(0)) != cudaSuccess) return e;
+  for (size_t i = 0; i < ch.size(); i++) {
+    const int k = (int)(i & 1);
+    /* the other buffer was emptied by the previous iteration */
+    if (i + 1 < ch.size() && (e = fetch(i + 1)) != cudaSuccess) return e;
+    if ((e = cudaEventSynchronize(pr.ev[k])) != cudaSuccess) return e;
+    double *dst = host[ch[i].f] + ch[i].r0 * sp.my;
+    const size_t n = ch[i].nr * sp.my;
+    if (sp.es == 8) {
+      const char *src = (const char *)pr.buf[k];
+      host_parallel(n * 8, grain, [&](size_t lo, size_t hi) { memcpy((char *)dst + lo, src + lo, hi - lo); });
+    } else {
+      const float *src = (const float *)pr.buf[k];
+      host_parallel(n, grain / 4, [&](size_t lo, size_t hi) {
+        for (size_t j = lo; j < hi; j++) dst[j] = (double)src[j];
+      });
+    }
+  }
+  return cudaSuccess;
+}
+
 /* host <-> state of one simulation (kind: H2D, D2H, D2D).  Host buffers move
  * through the batch's two pinned staging buffers in chunks of rows: the DMA
  * of one chunk overlaps the host copy (FP64) or conversion (FP32) of the
@@ -489,82 +594,13 @@ static int batch_copy(gp_batch *b, int s, const double *phi, const double *mu, d
     BK(cudaStreamSynchronize(b->stream));
     return GP_OK;
   }
-  /* the device's staging pair, held for the life of the process (freeing
-   * pinned memory waits on the whole device); one copy at a time uses it */
-  std::lock_guard<std::mutex> lock(g_stage_mutex);
-  if (b->dev < 0 || b->dev >= GP_STAGE_MAX_DEVICES) return bfail(b, GP_EINVAL, "batch copy: device %d", b->dev);
-  StagePair &sp = g_stage[b->dev];
-  if (!sp.buf[0]) {
-    for (int i = 0; i < 2; i++) {
-      BK(cudaHostAlloc(&sp.buf[i], GP_STAGE_BYTES, cudaHostAllocDefault));
-      BK(cudaEventCreateWithFlags(&sp.ev[i], cudaEventDisableTiming));
-    }
-  }
-  void *const *stage = sp.buf;
-  cudaEvent_t const *sev = sp.ev;
-  /* chunks: (field, first row, rows) */
-  const size_t rows_per = std::max<size_t>(1, GP_STAGE_BYTES / (my * es));
-  struct Chunk {
-    int f;
-    size_t r0, nr;
-  };
-  std::vector<Chunk> ch;
+  double *hp[GP_MAX_PHASES + GP_MAX_COMP];
   for (int f = 0; f < N + K; f++)
-    for (size_t r = 0; r < mx; r += rows_per) ch.push_back({f, r, std::min(rows_per, mx - r)});
-  auto host_rows = [&](const Chunk &c, bool in) -> const double * {
-    const double *h = in ? (c.f < N ? phi + (size_t)c.f * mx * my : mu + (size_t)(c.f - N) * mx * my)
-                         : (c.f < N ? ophi + (size_t)c.f * mx * my : omu + (size_t)(c.f - N) * mx * my);
-    return h + c.r0 * my;
-  };
-  auto dev_rows = [&](const Chunk &c) { return base + (size_t)c.f * sd.g.plane * es + c.r0 * dpitch; };
-  const size_t grain = (size_t)1 << 20;
-  if (up) {
-    for (size_t i = 0; i < ch.size(); i++) {
-      const int k = (int)(i & 1);
-      if (i >= 2) BK(cudaEventSynchronize(sev[k]));   /* the DMA that last read this buffer */
-      const double *src = host_rows(ch[i], true);
-      const size_t n = ch[i].nr * my;
-      if (es == 8) {
-        char *dst = (char *)stage[k];
-        host_parallel(n * 8, grain, [&](size_t lo, size_t hi) { memcpy(dst + lo, (const char *)src + lo, hi - lo); });
-      } else {
-        float *dst = (float *)stage[k];
-        host_parallel(n, grain / 4, [&](size_t lo, size_t hi) {
-          for (size_t j = lo; j < hi; j++) dst[j] = (float)src[j];
-        });
-      }
-      BK(cudaMemcpy2DAsync(dev_rows(ch[i]), dpitch, stage[k], my * es, my * es, ch[i].nr, cudaMemcpyHostToDevice,
-                           b->stream));
-      BK(cudaEventRecord(sev[k], b->stream));
-    }
-  } else {
-    auto fetch = [&](size_t i) -> int {
-      const int k = (int)(i & 1);
-      BK(cudaMemcpy2DAsync(stage[k], my * es, dev_rows(ch[i]), dpitch, my * es, ch[i].nr, cudaMemcpyDeviceToHost,
-                           b->stream));
-      BK(cudaEventRecord(sev[k], b->stream));
-      return GP_OK;
-    };
-    int rc = fetch(0);
-    if (rc != GP_OK) return rc;
-    for (size_t i = 0; i < ch.size(); i++) {
-      const int k = (int)(i & 1);
-      /* the other buffer was emptied by the previous iteration */
-      if (i + 1 < ch.size() && (rc = fetch(i + 1)) != GP_OK) return rc;
-      BK(cudaEventSynchronize(sev[k]));
-      double *dst = (double *)host_rows(ch[i], false);
-      const size_t n = ch[i].nr * my;
-      if (es == 8) {
-        const char *src = (const char *)stage[k];
-        host_parallel(n * 8, grain, [&](size_t lo, size_t hi) { memcpy((char *)dst + lo, src + lo, hi - lo); });
-      } else {
-        const float *src = (const float *)stage[k];
-        host_parallel(n, grain / 4, [&](size_t lo, size_t hi) {
-          for (size_t j = lo; j < hi; j++) dst[j] = (double)src[j];
-        });
-      }
-    }
-  }
+    hp[f] = up ? (double *)(f < N ? phi + (size_t)f * mx * my : mu + (size_t)(f - N) * mx * my)
+               : (f < N ? ophi + (size_t)f * mx * my : omu + (size_t)(f - N) * mx * my);
+  const StagedPlanes sp = {b->dev, base, (size_t)sd.g.plane * es, dpitch, mx, my, es, N + K};
+  const cudaError_t e = up ? stage_up(sp, hp, b->stream) : stage_down(sp, hp, b->stream);
+  if (e != cudaSuccess) return bfail(b, GP_ECUDA, "state copy: %s", cudaGetErrorString(e));
   BK(cudaStreamSynchronize(b->stream));
   return GP_OK;
 }
@@ -904,8 +940,84 @@ void *gp_stream(gp_ctx *ctx) { return ctx && ctx->b ? (void *)ctx->b->stream : n
 
 void gp_destroy(gp_ctx *c) {
   if (!c) return;
+  gp_vtk_wait(c);
+  cudaFree(c->snap);
+  if (c->wstream) cudaStreamDestroy(c->wstream);
+  if (c->wready) cudaEventDestroy(c->wready);
+  free(c->hphi);
+  free(c->hmu);
   gp_batch_destroy(c->b);
   free(c);
+}
+
+/* The writer thread of gp_vtk_write_async: wait for the snapshot, bring it
+ * down through the staging buffers on the writer's own stream (the context's
+ * stream keeps stepping), write the file. */
+static void vtk_writer(gp_ctx *c, std::string path, int ascii) {
+  gp_batch *b = c->b;
+  const gpd::SimDesc &sd = b->desc[0];
+  const int N = b->N, K = b->K;
+  const size_t mx = sd.g.mx, my = sd.g.my, es = b->elem;
+  int rc = GP_OK;
+  cudaError_t e = cudaSetDevice(b->dev);
+  if (e == cudaSuccess) e = cudaEventSynchronize(c->wready);
+  if (e == cudaSuccess) {
+    double *hp[GP_MAX_PHASES + GP_MAX_COMP];
+    for (int f = 0; f < N + K; f++) hp[f] = f < N ? c->hphi + (size_t)f * mx * my : c->hmu + (size_t)(f - N) * mx * my;
+    const StagedPlanes sp = {b->dev, (char *)c->snap, (size_t)sd.g.plane * es, (size_t)sd.g.pitch * es, mx, my, es,
+                             N + K};
+    e = stage_down(sp, hp, c->wstream);
+  }
+  if (e != cudaSuccess) {
+    snprintf(c->werr, sizeof c->werr, "gp_vtk_write_async: %s", cudaGetErrorString(e));
+    rc = GP_ECUDA;
+  } else if ((rc = gp_vtk_write(&b->params[0], path.c_str(), c->hphi, c->hmu, ascii)) != GP_OK) {
+    snprintf(c->werr, sizeof c->werr, "%s", gp_host_thread_error());
+  }
+  c->wstatus = rc;
+}
+
+int gp_vtk_wait(gp_ctx *c) {
+  if (!c) return fail(nullptr, GP_EINVAL, "gp_vtk_wait: NULL context");
+  if (c->writer) {
+    c->writer->join();
+    delete c->writer;
+    c->writer = nullptr;
+  }
+  const int rc = c->wstatus;
+  c->wstatus = GP_OK;
+  if (rc != GP_OK) return fail(c, rc, "%s", c->werr);
+  return GP_OK;
+}
+
+int gp_vtk_write_async(gp_ctx *c, const char *path, int ascii) {
+  if (!c || !path) return fail(c, GP_EINVAL, "gp_vtk_write_async: NULL argument");
+  int rc = gp_vtk_wait(c);   /* one write in flight per context */
+  if (rc != GP_OK) return rc;
+  c->err[0] = 0;
+  gp_batch *b = c->b;
+  const gpd::SimDesc &sd = b->desc[0];
+  const size_t bytes = (size_t)(b->N + b->K) * sd.g.plane * b->elem;
+  if (!c->snap) {
+    const size_t cells = (size_t)sd.g.mx * sd.g.my;
+    CK(cudaMalloc(&c->snap, bytes));
+    CK(cudaStreamCreateWithFlags(&c->wstream, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&c->wready, cudaEventDisableTiming));
+    c->hphi = (double *)malloc(sizeof(double) * cells * b->N);
+    c->hmu = (double *)malloc(sizeof(double) * cells * b->K);
+    if (!c->hphi || !c->hmu) return fail(c, GP_ENOMEM, "gp_vtk_write_async: out of host memory");
+  }
+  /* the snapshot is ordered after the steps already queued; later steps
+   * write the other state buffer or this one after the copy has read it */
+  CK(cudaMemcpyAsync(c->snap, (char *)b->state[b->cur] + (size_t)sd.off_state * b->elem, bytes,
+                     cudaMemcpyDeviceToDevice, b->stream));
+  CK(cudaEventRecord(c->wready, b->stream));
+  try {
+    c->writer = new std::thread(vtk_writer, c, std::string(path), ascii);
+  } catch (...) {
+    return fail(c, GP_ENOMEM, "gp_vtk_write_async: cannot start the writer thread");
+  }
+  return GP_OK;
 }
 
 int gp_init(gp_ctx **out, const gp_params *p, const double *phi, const double *mu, gp_precision prec) {

@@ -230,14 +230,6 @@ int gp_fill(const gp_params *p, const char *filling_path, double *phi, double *m
 
 /* ------------------------------------------------------------------ VTK */
 
-static double be_double(double v) {
-  uint64_t u;
-  memcpy(&u, &v, 8);
-  u = __builtin_bswap64(u);
-  memcpy(&v, &u, 8);
-  return v;
-}
-
 /* hphi (functionH.h:24-36) */
 static double host_hphi(const double *ph, int N, int a) {
   int b, c;
@@ -250,14 +242,47 @@ static double host_hphi(const double *ph, int N, int a) {
   return sum + sum1;
 }
 
-/* write_cells_vtk_2D / write_cells_vtk_2D_binary (file_writer.h:71-255) */
+static double be_double(double v) {
+  uint64_t u;
+  memcpy(&u, &v, 8);
+  u = __builtin_bswap64(u);
+  memcpy(&v, &u, 8);
+  return v;
+}
+
+/* One row of MY values: lines of `fmt` (ASCII) or big-endian doubles
+ * (binary), in one fwrite. */
+static int put_row(FILE *f, const double *v, long MY, int ascii, const char *fmt, char *buf, size_t bufn) {
+  long y;
+  size_t n = 0;
+  if (!ascii) {
+    uint64_t *u = (uint64_t *)buf;
+    for (y = 0; y < MY; y++) {
+      memcpy(&u[y], &v[y], 8);
+      u[y] = __builtin_bswap64(u[y]);
+    }
+    return fwrite(buf, 8, (size_t)MY, f) == (size_t)MY ? 0 : -1;
+  }
+  for (y = 0; y < MY; y++) {
+    int w = snprintf(buf + n, bufn - n, fmt, v[y]);
+    if (w < 0 || (size_t)w >= bufn - n) return -1;
+    n += (size_t)w;
+  }
+  return fwrite(buf, 1, n, f) == n ? 0 : -1;
+}
+
+/* write_cells_vtk_2D / write_cells_vtk_2D_binary (file_writer.h:71-255):
+ * the same bytes, written a row at a time. */
 int gp_vtk_write(const gp_params *p, const char *path, const double *phi, const double *mu, int ascii) {
   FILE *f;
   long x, y, MX, MY;
-  int a, k, N, K;
+  int a, k, N, K, bad = 0;
   gp_derived d;
   char err[256];
   int have_d = 0;
+  char *buf;
+  double *row;
+  size_t bufn;
   if (!p || !path || !phi || !mu) { gp_set_thread_error("gp_vtk_write: NULL argument"); return GP_EINVAL; }
   N = p->numphases; K = p->numcomponents - 1; MX = p->mesh_x; MY = p->mesh_y;
   if (p->writecomposition) {
@@ -267,8 +292,23 @@ int gp_vtk_write(const gp_params *p, const char *path, const double *phi, const 
     }
     have_d = 1;
   }
+  bufn = (size_t)MY * 32 + 64;   /* "%le" is at most 13 characters plus sign and separators */
+  buf = malloc(bufn);
+  row = malloc(sizeof(double) * (size_t)MY);
+  if (!buf || !row) {
+    free(buf);
+    free(row);
+    gp_set_thread_error("gp_vtk_write: out of host memory");
+    return GP_ENOMEM;
+  }
   f = fopen(path, ascii ? "w" : "wb");
-  if (!f) { gp_set_thread_error("cannot write %s", path); return GP_EIO; }
+  if (!f) {
+    free(buf);
+    free(row);
+    gp_set_thread_error("cannot write %s", path);
+    return GP_EIO;
+  }
+  setvbuf(f, NULL, _IOFBF, (size_t)1 << 22);
   fprintf(f, "# vtk DataFile Version 3.0\n");
   fprintf(f, "Microsim_fields\n");
   fprintf(f, ascii ? "ASCII\n" : "BINARY\n");
@@ -280,30 +320,20 @@ int gp_vtk_write(const gp_params *p, const char *path, const double *phi, const 
   for (a = 0; a < N; a++) {
     fprintf(f, "SCALARS %s double 1\n", p->phases[a]);
     fprintf(f, "LOOKUP_TABLE default\n");
-    for (x = 0; x < MX; x++)
-      for (y = 0; y < MY; y++) {
-        double v = phi[((long)a * MX + x) * MY + y];
-        if (ascii) fprintf(f, "%le\n", v);
-        else { v = be_double(v); fwrite(&v, 8, 1, f); }
-      }
+    for (x = 0; x < MX && !bad; x++) bad = put_row(f, phi + ((long)a * MX + x) * MY, MY, ascii, "%le\n", buf, bufn);
     if (ascii) fprintf(f, "\n");
   }
   for (k = 0; k < K; k++) {
     fprintf(f, "SCALARS Mu_%s double 1\n", p->components[k]);
     fprintf(f, "LOOKUP_TABLE default\n");
-    for (x = 0; x < MX; x++)
-      for (y = 0; y < MY; y++) {
-        double v = mu[((long)k * MX + x) * MY + y];
-        if (ascii) fprintf(f, "%le\n", v);
-        else { v = be_double(v); fwrite(&v, 8, 1, f); }
-      }
+    for (x = 0; x < MX && !bad; x++) bad = put_row(f, mu + ((long)k * MX + x) * MY, MY, ascii, "%le\n", buf, bufn);
     if (ascii) fprintf(f, "\n");
   }
   if (p->writecomposition && have_d) {
     for (k = 0; k < K; k++) {
       fprintf(f, "SCALARS Composition_%s double 1\n", p->components[k]);
       fprintf(f, "LOOKUP_TABLE default\n");
-      for (x = 0; x < MX; x++)
+      for (x = 0; x < MX && !bad; x++) {
         for (y = 0; y < MY; y++) {
           double ph[GP_MAX_PHASES], m[GP_MAX_COMP], comp = 0.0;
           int b, l;
@@ -314,13 +344,16 @@ int gp_vtk_write(const gp_params *p, const char *path, const double *phi, const 
             for (l = 0; l < K; l++) cmu_v += d.cmu[b][k][l] * (m[l] - d.E[b][l]);
             comp += cmu_v * host_hphi(ph, N, b);
           }
-          if (ascii) fprintf(f, "%le \n", comp);
-          else { comp = be_double(comp); fwrite(&comp, 8, 1, f); }
+          row[y] = comp;
         }
+        bad = put_row(f, row, MY, ascii, "%le \n", buf, bufn);
+      }
       if (ascii) fprintf(f, "\n");
     }
   }
-  if (fclose(f) != 0) { gp_set_thread_error("error writing %s", path); return GP_EIO; }
+  free(buf);
+  free(row);
+  if (fclose(f) != 0 || bad) { gp_set_thread_error("error writing %s", path); return GP_EIO; }
   return GP_OK;
 }
 

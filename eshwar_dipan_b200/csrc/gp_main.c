@@ -6,8 +6,9 @@
  * Same flow and files as main() of the serial solver (microsim_gp.c:41-151):
  * parse the input, fill (or restart from DATA/NAME_<STARTTIME>.vtk), write the
  * t=0 VTK, run NSMOOTH-1 smoothing sweeps, then NTIMESTEPS steps on the GPU,
- * writing DATA/NAME_<t>.vtk every SAVET steps (plus DATA/shift.dat) and the
- * progress record every TRACK_PROGRESS steps.  The progress sums cover the
+ * writing DATA/NAME_<t>.vtk every SAVET steps (in the background, while the
+ * next steps run; plus DATA/shift.dat) and the progress record every
+ * TRACK_PROGRESS steps.  The progress sums cover the
  * interior cells only (see gp_stats in gp.h).
  */
 #include <math.h>
@@ -85,9 +86,9 @@ int main(int argc, char **argv) {
     t += n;
     if (p.savet > 0 && t % p.savet == 0) {
       FILE *f;
-      if ((rc = gp_get(c, phi, mu)) != GP_OK) return die("gp_get", rc, c);
+      /* written in the background while the next steps run */
       snprintf(path, sizeof path, "DATA/%s_%ld.vtk", argv[3], t + p.starttime);
-      if ((rc = gp_vtk_write(&p, path, phi, mu, p.ascii)) != GP_OK) return die("writing VTK", rc, c);
+      if ((rc = gp_vtk_write_async(c, path, p.ascii)) != GP_OK) return die("writing VTK", rc, c);
       f = fopen("DATA/shift.dat", "a");
       if (f) {
         fprintf(f, "%ld %ld\n", t + p.starttime, 0L);
@@ -106,6 +107,7 @@ int main(int argc, char **argv) {
       if (st.nonfinite) fprintf(stderr, "gp_microsim: %lld cells are not finite\n", st.nonfinite);
     }
   }
+  if ((rc = gp_vtk_wait(c)) != GP_OK) return die("writing VTK", rc, c);
   gp_destroy(c);
   free(phi);
   free(mu);

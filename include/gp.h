@@ -133,6 +133,18 @@ int gp_fill(const gp_params *p, const char *filling_path, double *phi, double *m
 int gp_vtk_write(const gp_params *p, const char *path, const double *phi, const double *mu, int ascii);
 int gp_vtk_read(const gp_params *p, const char *path, double *phi, double *mu, int ascii);
 
+/* Write the context's current state to `path` as gp_vtk_write does, in the
+ * background: the state is copied on the device (ordered after the steps
+ * already queued), and a host thread brings the copy down through pinned
+ * memory and writes the file while the caller keeps stepping.  Replaces the
+ * periodic writetofile_serial2D[_binary] of the time loop
+ * (microsim_gp.c:129-134) without stopping the GPU.  One write is in flight
+ * per context: a call first waits for the previous one and returns its error,
+ * if any.  The file is complete after gp_vtk_wait or gp_destroy. */
+int gp_vtk_write_async(gp_ctx *ctx, const char *path, int ascii);
+/* Wait for the context's background write; its result. */
+int gp_vtk_wait(gp_ctx *ctx);
+
 /* ---- device path ------------------------------------------------------- */
 
 /* Create a context on the current CUDA device, upload the interior state and

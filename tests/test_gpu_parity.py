@@ -137,3 +137,32 @@ def test_golden_vtk_replay(tmp_path, key):
         ref = recipes.golden_text(z, key, name)
         bad = sum(a != b for a, b in zip(ours, ref))
         assert bad == 0, "%s/%s: %d values differ" % (key, name, bad)
+
+
+@pytest.mark.parametrize("ascii", [0, 1])
+def test_vtk_write_async_matches_sync(tmp_path, ascii):
+    """gp_vtk_write_async writes the bytes gp_get + gp_vtk_write write, while
+    the steps queued after it go on (and are not disturbed by it)."""
+    ip, fp = build_case(tmp_path, "ternary3_aniso_periodic")
+    p = gp.load_params(ip)
+    phi, mu = gp.fill(p, fp)
+    with gp.Simulation(p, phi, mu) as s:
+        s.smooth(p.nsmooth - 1)
+        s.step(17, stats=False)
+        ph, m = s.get()
+        gp.vtk_write(p, str(tmp_path / "sync.vtk"), ph, m, ascii=ascii)
+        s.vtk_write_async(str(tmp_path / "async.vtk"), ascii=ascii)
+        s.step(9, stats=False)
+        s.vtk_write_async(str(tmp_path / "async2.vtk"), ascii=ascii)   # waits for the first
+        s.step(3, stats=False)
+        s.vtk_wait()
+        end = s.get()
+    assert (tmp_path / "sync.vtk").read_bytes() == (tmp_path / "async.vtk").read_bytes()
+    with gp.Simulation(p, ph, m) as s:
+        s.step(9, stats=False)
+        ph9, m9 = s.get()
+        gp.vtk_write(p, str(tmp_path / "sync2.vtk"), ph9, m9, ascii=ascii)
+        s.step(3, stats=False)
+        ref = s.get()
+    assert (tmp_path / "sync2.vtk").read_bytes() == (tmp_path / "async2.vtk").read_bytes()
+    assert bits_equal(end[0], ref[0]) and bits_equal(end[1], ref[1])
