@@ -245,6 +245,34 @@ def fp32_form(gp, p, phi0, mu0, args, phi64, st64, local):
     return ms, clk.summary(), float(err.max()), float(np.sqrt((err ** 2).mean())), drift, split
 
 
+def vtk_overlap(gp, p, phi0, mu0, work, steps=3000, every=1000):
+    """`steps` steps with a binary VTK of the state every `every` steps,
+    written (a) after gp_get, stopping the steps, as the reference's time loop
+    does, and (b) by gp_vtk_write_async while the next steps run; wall clock
+    of each, and of the steps alone."""
+    out = {"steps": steps, "every": every, "format": "binary"}
+    with gp.Simulation(p, phi0, mu0) as s:
+        s.step(102, stats=False)
+        t0 = time.perf_counter()
+        s.step(steps, stats=False)
+        s.get()
+        out["steps_only_s"] = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        for i in range(steps // every):
+            s.step(every, stats=False)
+            ph, m = s.get()
+            gp.vtk_write(p, os.path.join(work, "sync_%d.vtk" % i), ph, m, ascii=0)
+        out["sync_s"] = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        for i in range(steps // every):
+            s.step(every, stats=False)
+            s.vtk_write_async(os.path.join(work, "async_%d.vtk" % i), ascii=0)
+        s.vtk_wait()
+        out["async_s"] = time.perf_counter() - t0
+    out["bytes_per_file"] = os.path.getsize(os.path.join(work, "async_0.vtk"))
+    return out
+
+
 def run_ensemble(args, rank, world, local, dist):
     """cfg3: the batched ensemble through gp_batch_* (FP32 storage)."""
     import ctypes
@@ -566,6 +594,8 @@ def main():
             out["gpu_launches"] += step_launches(N, args.steps)
         if not args.no_cpu_baseline:
             out["cpu_baseline"] = cpu_baseline(args.workload)
+        if world == 1 and args.steps >= 1000:
+            out["vtk_output"] = vtk_overlap(gp, p, phi0, mu0, work)
         print(json.dumps(out), flush=True)
     shutil.rmtree(work, ignore_errors=True)
     if dist:
