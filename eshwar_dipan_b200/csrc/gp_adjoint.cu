@@ -17,6 +17,11 @@
  *                  same way.
  * The local Jacobians are exact: the cell functions are evaluated on
  * Dual<ADJ_W> numbers seeded on ADJ_W of the stencil inputs at a time.
+ * Each reverse pass runs in two launches: a sort over the grid that handles
+ * the cheap cells (pure-phase windows: bulk_rev; no active phase: nothing)
+ * and lists the others, then one thread per (listed cell, dual pass), so the
+ * expensive work fills every SM with whole warps of it instead of a few
+ * lanes per warp along the interface.
  * Scatter-adds are atomic (FP64), so the last bits of a gradient may differ
  * between runs; values are exact derivatives up to summation order.
  */
@@ -206,16 +211,20 @@ __device__ __forceinline__ void bulk_rev(const Consts<double> *c, const Grid &g,
   }
 }
 
-template <int N, int K>
-__global__ void __launch_bounds__(AB) ka_rev_update(const Consts<double> *__restrict__ c, AdjParams prm, Grid g,
-                                                    const double *__restrict__ st, const double *__restrict__ dphi,
-                                                    const double *__restrict__ ybar, double *__restrict__ xbar,
-                                                    double *__restrict__ dphibar, double *__restrict__ pbar) {
+/* Reverse of the concentration pass at cell (x, y).  SORT: cells whose 3x3
+ * window is one pure phase take bulk_rev here; the others are returned
+ * (true) for the dual passes, which run with SORT false over the list of
+ * such cells, so that a warp's lanes all take the expensive path together. */
+template <int N, int K, bool SORT>
+__device__ __forceinline__ bool rev_update_cell(const Consts<double> *__restrict__ c, const AdjParams &prm,
+                                                const Grid &g, const double *__restrict__ st,
+                                                const double *__restrict__ dphi, const double *__restrict__ ybar,
+                                                double *__restrict__ xbar, double *__restrict__ dphibar, int x, int y,
+                                                bool live, double (&pacc)[ADJ_NPARAM], int pass = -1) {
   using DT = Dual<ADJ_W>;
   constexpr int NPHI = 9 * N, NMU = 5 * K, NDP = 5 * N, NIN = NPHI + NMU + NDP + ADJ_NPARAM;
-  const int y = blockIdx.x * AB + threadIdx.x, x = blockIdx.y;
-  double pacc[ADJ_NPARAM] = {};
-  const bool live = y < g.my;
+  /* pass >= 0: only the dual pass seeding inputs pass*ADJ_W .. */
+  const int b0 = pass >= 0 ? pass * ADJ_W : 0, b1 = pass >= 0 ? min(NIN, b0 + ADJ_W) : NIN;
   double yb[N + K];
   bool any = false;
   if (live) {
@@ -258,10 +267,11 @@ __global__ void __launch_bounds__(AB) ka_rev_update(const Consts<double> *__rest
           uni = uni && one_hot_bits<N>(v) == ph;
         }
     }
-    if (uni && K == 1) {
-      bulk_rev<N>(c, g, x, y, ph, S, M, yb, xbar, dphibar);
+    if (SORT) {
+      if (uni && K == 1) bulk_rev<N>(c, g, x, y, ph, S, M, yb, xbar, dphibar);
+      else return true;
     } else
-    for (int base = 0; base < NIN; base += ADJ_W) {
+    for (int base = b0; base < b1; base += ADJ_W) {
       DT Sd[N][3][3], Md[K][3][3], DPd[N][3][3], pd[ADJ_NPARAM];
 #pragma unroll
       for (int a = 0; a < N; a++)
@@ -324,18 +334,62 @@ __global__ void __launch_bounds__(AB) ka_rev_update(const Consts<double> *__rest
       }
     }
   }
+  return false;
+}
+
+/* warp-aggregated append of (x, y) to a cell list; call with the whole warp */
+__device__ __forceinline__ void push_cell(bool want, int x, int y, int2 *__restrict__ cells, int *__restrict__ count) {
+  const unsigned m = __ballot_sync(0xffffffffu, want);
+  if (!m) return;
+  const int lane = threadIdx.x & 31, lead = __ffs(m) - 1;
+  int base = 0;
+  if (lane == lead) base = atomicAdd(count, __popc(m));
+  base = __shfl_sync(0xffffffffu, base, lead);
+  if (want) cells[base + __popc(m & ((1u << lane) - 1u))] = make_int2(x, y);
+}
+
+template <int N, int K>
+__global__ void __launch_bounds__(AB) ka_rev_update(const Consts<double> *__restrict__ c, AdjParams prm, Grid g,
+                                                    const double *__restrict__ st, const double *__restrict__ dphi,
+                                                    const double *__restrict__ ybar, double *__restrict__ xbar,
+                                                    double *__restrict__ dphibar, int2 *__restrict__ cells,
+                                                    int *__restrict__ count) {
+  const int y = blockIdx.x * AB + threadIdx.x, x = blockIdx.y;
+  double pacc[ADJ_NPARAM] = {};
+  const bool want = rev_update_cell<N, K, true>(c, prm, g, st, dphi, ybar, xbar, dphibar, x, y, y < g.my, pacc);
+  push_cell(want, x, y, cells, count);
+}
+
+template <int N, int K>
+__global__ void __launch_bounds__(AB) ka_rev_update_list(const Consts<double> *__restrict__ c, AdjParams prm, Grid g,
+                                                         const double *__restrict__ st,
+                                                         const double *__restrict__ dphi,
+                                                         const double *__restrict__ ybar, double *__restrict__ xbar,
+                                                         double *__restrict__ dphibar, double *__restrict__ pbar,
+                                                         const int2 *__restrict__ cells,
+                                                         const int *__restrict__ count) {
+  /* one thread per (cell, dual pass): every SM gets work */
+  constexpr int NIN = 9 * N + 5 * K + 5 * N + ADJ_NPARAM, NPASS = (NIN + ADJ_W - 1) / ADJ_W;
+  double pacc[ADJ_NPARAM] = {};
+  const long long n = (long long)*count * NPASS;
+  for (long long i = (long long)blockIdx.x * AB + threadIdx.x; i < n; i += (long long)gridDim.x * AB) {
+    const int2 e = cells[i / NPASS];
+    rev_update_cell<N, K, false>(c, prm, g, st, dphi, ybar, xbar, dphibar, e.x, e.y, true, pacc, (int)(i % NPASS));
+  }
   flush_params(pacc, pbar);
 }
 
-template <int N, int K, bool A>
-__global__ void __launch_bounds__(AB) ka_rev_dphi(const Consts<double> *__restrict__ c, AdjParams prm, Grid g,
-                                                  const double *__restrict__ st, const double *__restrict__ dphibar,
-                                                  double *__restrict__ xbar, double *__restrict__ pbar) {
+/* Reverse of the phase-field pass at ring or interior cell (x, y).  SORT:
+ * returns whether the cell has an active phase (the only cells with a
+ * derivative); the dual passes run with SORT false over the list of those. */
+template <int N, int K, bool A, bool SORT>
+__device__ __forceinline__ bool rev_dphi_cell(const Consts<double> *__restrict__ c, const AdjParams &prm,
+                                              const Grid &g, const double *__restrict__ st,
+                                              const double *__restrict__ dphibar, double *__restrict__ xbar, int x,
+                                              int y, bool live, double (&pacc)[ADJ_NPARAM], int pass = -1) {
   using DT = Dual<ADJ_W>;
   constexpr int NPHI = 9 * N, NIN = NPHI + K + ADJ_NPARAM;
-  const int y = blockIdx.x * AB + threadIdx.x - 1, x = (int)blockIdx.y - 1;
-  double pacc[ADJ_NPARAM] = {};
-  const bool live = y <= g.my;
+  const int b0 = pass >= 0 ? pass * ADJ_W : 0, b1 = pass >= 0 ? min(NIN, b0 + ADJ_W) : NIN;
   double db[N];
   bool any = false;
   if (live) {
@@ -359,8 +413,9 @@ __global__ void __launch_bounds__(AB) ka_rev_dphi(const Consts<double> *__restri
     }
     any = active;
   }
+  if (SORT) return live && any;
   if (live && any) {
-    for (int base = 0; base < NIN; base += ADJ_W) {
+    for (int base = b0; base < b1; base += ADJ_W) {
       DT Sd[N][3][3], md[K], pd[ADJ_NPARAM];
 #pragma unroll
       for (int a = 0; a < N; a++)
@@ -401,6 +456,34 @@ __global__ void __launch_bounds__(AB) ka_rev_dphi(const Consts<double> *__restri
       }
     }
   }
+  return false;
+}
+
+template <int N, int K, bool A>
+__global__ void __launch_bounds__(AB) ka_rev_dphi(const Consts<double> *__restrict__ c, AdjParams prm, Grid g,
+                                                  const double *__restrict__ st, const double *__restrict__ dphibar,
+                                                  double *__restrict__ xbar, int2 *__restrict__ cells,
+                                                  int *__restrict__ count) {
+  const int y = blockIdx.x * AB + threadIdx.x - 1, x = (int)blockIdx.y - 1;
+  double pacc[ADJ_NPARAM] = {};
+  const bool want = rev_dphi_cell<N, K, A, true>(c, prm, g, st, dphibar, xbar, x, y, y <= g.my, pacc);
+  push_cell(want, x, y, cells, count);
+}
+
+template <int N, int K, bool A>
+__global__ void __launch_bounds__(AB) ka_rev_dphi_list(const Consts<double> *__restrict__ c, AdjParams prm, Grid g,
+                                                       const double *__restrict__ st,
+                                                       const double *__restrict__ dphibar, double *__restrict__ xbar,
+                                                       double *__restrict__ pbar, const int2 *__restrict__ cells,
+                                                       const int *__restrict__ count) {
+  /* one thread per (cell, dual pass) */
+  constexpr int NIN = 9 * N + K + ADJ_NPARAM, NPASS = (NIN + ADJ_W - 1) / ADJ_W;
+  double pacc[ADJ_NPARAM] = {};
+  const long long n = (long long)*count * NPASS;
+  for (long long i = (long long)blockIdx.x * AB + threadIdx.x; i < n; i += (long long)gridDim.x * AB) {
+    const int2 e = cells[i / NPASS];
+    rev_dphi_cell<N, K, A, false>(c, prm, g, st, dphibar, xbar, e.x, e.y, true, pacc, (int)(i % NPASS));
+  }
   flush_params(pacc, pbar);
 }
 
@@ -419,16 +502,31 @@ struct AdjKernels {
     ka_update<N, K><<<grid, AB, 0, s>>>((const Consts<double> *)c, p, g, st, dp, next);
     return cudaGetLastError();
   }
+  /* the list passes: a persistent grid over the listed cells */
+  static int list_grid() {
+    int dev = 0, nsm = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    return 16 * nsm;
+  }
   static cudaError_t rev_update(cudaStream_t s, const void *c, AdjParams p, Grid g, const double *st,
-                                const double *dp, const double *ybar, double *xbar, double *dpbar, double *pbar) {
+                                const double *dp, const double *ybar, double *xbar, double *dpbar, double *pbar,
+                                int2 *cells, int *count) {
+    cudaError_t e = cudaMemsetAsync(count, 0, sizeof(int), s);
+    if (e != cudaSuccess) return e;
     dim3 grid((g.my + AB - 1) / AB, g.mx);
-    ka_rev_update<N, K><<<grid, AB, 0, s>>>((const Consts<double> *)c, p, g, st, dp, ybar, xbar, dpbar, pbar);
+    ka_rev_update<N, K><<<grid, AB, 0, s>>>((const Consts<double> *)c, p, g, st, dp, ybar, xbar, dpbar, cells, count);
+    ka_rev_update_list<N, K><<<list_grid(), AB, 0, s>>>((const Consts<double> *)c, p, g, st, dp, ybar, xbar, dpbar,
+                                                        pbar, cells, count);
     return cudaGetLastError();
   }
   static cudaError_t rev_dphi(cudaStream_t s, const void *c, AdjParams p, Grid g, const double *st,
-                              const double *dpbar, double *xbar, double *pbar) {
+                              const double *dpbar, double *xbar, double *pbar, int2 *cells, int *count) {
+    cudaError_t e = cudaMemsetAsync(count, 0, sizeof(int), s);
+    if (e != cudaSuccess) return e;
     dim3 grid((g.my + 2 + AB - 1) / AB, g.mx + 2);
-    ka_rev_dphi<N, K, A><<<grid, AB, 0, s>>>((const Consts<double> *)c, p, g, st, dpbar, xbar, pbar);
+    ka_rev_dphi<N, K, A><<<grid, AB, 0, s>>>((const Consts<double> *)c, p, g, st, dpbar, xbar, cells, count);
+    ka_rev_dphi_list<N, K, A><<<list_grid(), AB, 0, s>>>((const Consts<double> *)c, p, g, st, dpbar, xbar, pbar,
+                                                         cells, count);
     return cudaGetLastError();
   }
 };

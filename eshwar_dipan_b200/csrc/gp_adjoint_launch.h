@@ -22,12 +22,14 @@ struct AdjLaunch {
   /* the step from a state and its delta-phi, by the adjoint's cell functions */
   cudaError_t (*update)(cudaStream_t s, const void *consts, AdjParams p, Grid g, const double *state,
                         const double *dphi, double *next);
-  /* reverse of the concentration pass: ybar -> xbar, dphibar, pbar (accumulated) */
+  /* reverse of the concentration pass: ybar -> xbar, dphibar, pbar
+   * (accumulated); cells/count: scratch list of (mx+2)*(my+2) cells */
   cudaError_t (*rev_update)(cudaStream_t s, const void *consts, AdjParams p, Grid g, const double *state,
-                            const double *dphi, const double *ybar, double *xbar, double *dphibar, double *pbar);
+                            const double *dphi, const double *ybar, double *xbar, double *dphibar, double *pbar,
+                            int2 *cells, int *count);
   /* reverse of the phase-field pass: dphibar -> xbar, pbar (accumulated) */
   cudaError_t (*rev_dphi)(cudaStream_t s, const void *consts, AdjParams p, Grid g, const double *state,
-                          const double *dphibar, double *xbar, double *pbar);
+                          const double *dphibar, double *xbar, double *pbar, int2 *cells, int *count);
 };
 }  // namespace gpd
 

@@ -1112,9 +1112,11 @@ int planes_copy(gp_batch *b, double *dst, size_t dpitch, const double *src, size
 struct AdjBufs {
   double *snap = nullptr, *seg = nullptr, *ybar = nullptr, *xbar = nullptr, *dphi = nullptr, *dphibar = nullptr,
          *pbar = nullptr, *final_state = nullptr;
+  int2 *cells = nullptr;   /* cells of a reverse pass that take the dual passes */
+  int *ncells = nullptr;
   ~AdjBufs() {
     cudaFree(snap); cudaFree(seg); cudaFree(ybar); cudaFree(xbar); cudaFree(dphi); cudaFree(dphibar);
-    cudaFree(pbar); cudaFree(final_state);
+    cudaFree(pbar); cudaFree(final_state); cudaFree(cells); cudaFree(ncells);
   }
 };
 
@@ -1177,6 +1179,12 @@ int gp_adjoint(gp_ctx *c, const gp_adj_req *req, gp_adj_out *out) {
   AALLOC(m.pbar, gpd::ADJ_NPARAM);
   AALLOC(m.final_state, S);
 #undef AALLOC
+  {
+    const size_t ncell = (size_t)(g.mx + 2) * (g.my + 2);
+    if (cudaMalloc((void **)&m.cells, ncell * sizeof(int2)) != cudaSuccess ||
+        cudaMalloc((void **)&m.ncells, sizeof(int)) != cudaSuccess)
+      return fail(c, GP_ENOMEM, "gp_adjoint: cudaMalloc of the cell list failed");
+  }
   double *state = (double *)b->state[b->cur];   /* a batch of one starts at offset 0 */
   const long long steps0 = b->steps;
   cudaEvent_t e0, e1, e2;
@@ -1242,8 +1250,8 @@ int gp_adjoint(gp_ctx *c, const gp_adj_req *req, gp_adj_out *out) {
       CK(L.dphi(b->stream, consts, prm, g, x, m.dphi));
       CK(cudaMemsetAsync(m.xbar, 0, S * 8, b->stream));
       CK(cudaMemsetAsync(m.dphibar, 0, Sd * 8, b->stream));
-      CK(L.rev_update(b->stream, consts, prm, g, x, m.dphi, m.ybar, m.xbar, m.dphibar, m.pbar));
-      CK(L.rev_dphi(b->stream, consts, prm, g, x, m.dphibar, m.xbar, m.pbar));
+      CK(L.rev_update(b->stream, consts, prm, g, x, m.dphi, m.ybar, m.xbar, m.dphibar, m.pbar, m.cells, m.ncells));
+      CK(L.rev_dphi(b->stream, consts, prm, g, x, m.dphibar, m.xbar, m.pbar, m.cells, m.ncells));
       std::swap(m.ybar, m.xbar);
     }
   }
