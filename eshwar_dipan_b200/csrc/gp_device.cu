@@ -1240,11 +1240,13 @@ int gp_adjoint(gp_ctx *c, const gp_adj_req *req, gp_adj_out *out) {
     state = (double *)b->state[b->cur];
     CK(cudaMemcpyAsync(state, m.snap + S * s, S * 8, cudaMemcpyDeviceToDevice, b->stream));
     if ((rc = batch_reflag(b, true)) != GP_OK) return rc;
+    /* the segment's states, queued without a host round trip per step */
     for (long j = 0; j < n; j++) {
       state = (double *)b->state[b->cur];
       CK(cudaMemcpyAsync(m.seg + S * j, state, S * 8, cudaMemcpyDeviceToDevice, b->stream));
-      if (j + 1 < n && (rc = batch_step_impl(b, 1, nullptr, nullptr, nullptr, nullptr)) != GP_OK) return rc;
+      if (j + 1 < n && (rc = batch_step_once(b, 0, nullptr)) != GP_OK) return rc;
     }
+    if ((rc = batch_check_error(b)) != GP_OK) return rc;
     for (long j = n - 1; j >= 0; j--) {
       const double *x = m.seg + S * j;
       CK(L.dphi(b->stream, consts, prm, g, x, m.dphi));
