@@ -33,7 +33,7 @@
 namespace gpd {
 
 #ifndef GP_ADJ_W
-#define GP_ADJ_W 2   /* two seeded inputs per pass: fewer passes, few spills (1 and 3, 4 were slower) */
+#define GP_ADJ_W 1   /* one seeded input per pass: with a thread per (cell, pass), the leanest pass is fastest (2 and 4 were slower) */
 #endif
 constexpr int ADJ_W = GP_ADJ_W;
 constexpr int AB = 128;   /* threads per block along y */
