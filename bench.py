@@ -408,7 +408,7 @@ def run_adjoint(args, rank, world, local, dist):
                            "ms_forward_pass": g["ms_forward"], "ms_reverse_pass": g["ms_reverse"],
                            "ms_plain_forward": fwd_ms, "cost_vs_forward": adj_ms / fwd_ms},
                "gpu_launches": (2 * nsteps + 2 * (nsteps - int(np.ceil(nsteps / np.ceil(np.sqrt(nsteps)))))
-                                + 3 * nsteps),
+                                + 5 * nsteps),
                "clocks": clk.summary(),
                "note": "value = cell-updates of the differentiated steps per second of forward + reverse"}
         print(json.dumps(out), flush=True)
