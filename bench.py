@@ -153,6 +153,25 @@ class ClockSampler:
 NCU_TRAFFIC = {"cfg2": 116.6e6}
 
 
+def reduce_over_ranks(dist, value, op="max"):
+    """max (or sum) of a float over the ranks of the process group; the
+    value itself without one.  NCCL reduces a CUDA tensor, gloo a CPU one."""
+    if not dist:
+        return value
+    import torch
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(value)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def ensemble_shard(rank):
+    """The simulations of one rank: rank r steps the 256-member ensemble
+    drawn with seed r, its own shard of a 256*N-member ensemble (rank 0's is
+    the cfg3 ensemble)."""
+    return ensemble(seed=rank)
+
+
 def step_launches(N, steps):
     """Kernel launches of `steps` steps through gp_step / gp_batch_step with
     statistics: kf_classify + kf_step per step (kf_classify + kf_bulk +
@@ -277,7 +296,7 @@ def run_ensemble(args, rank, world, local, dist):
     """cfg3: the batched ensemble through gp_batch_* (FP32 storage)."""
     import ctypes
     import eshwar_dipan_b200 as gp
-    specs = ensemble()
+    specs = ensemble_shard(rank)
     work = tempfile.mkdtemp(prefix="gpens")
     params, fields = [], []
     for i, (kw, seeds) in enumerate(specs):
@@ -302,11 +321,7 @@ def run_ensemble(args, rank, world, local, dist):
         tot_ms, st = b.step_timed(args.steps, stats=True)
     barrier()
     b.close()
-    if dist:
-        import torch
-        t = torch.tensor([tot_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        tot_ms = float(t.item())
+    tot_ms = reduce_over_ranks(dist, tot_ms)
 
     # end to end: upload of every simulation, smoothing, steps, read-back of all
     barrier()
@@ -319,18 +334,15 @@ def run_ensemble(args, rank, world, local, dist):
     t_e2e = time.perf_counter() - t0
     b.close()
     barrier()
-    if dist:
-        import torch
-        t = torch.tensor([t_e2e], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_e2e = float(t.item())
+    t_e2e = reduce_over_ranks(dist, t_e2e)
+    all_cells = reduce_over_ranks(dist, cells, op="sum")   # every rank's shard
     shutil.rmtree(work, ignore_errors=True)
     if rank != 0:
         return 0
     peaks = measured_peaks()
     hbm = peaks.get("hbm_gbs") or 6650.0
     bpc = 2 * (N + K) * 4
-    value = world * cells * args.steps / (tot_ms / 1e3)
+    value = all_cells * args.steps / (tot_ms / 1e3)
     achieved = bpc * cells * args.steps / (tot_ms / 1e3) / 1e9
     e2e_steps = args.warmup + args.steps
     host_bytes = cells * (N + K) * 8
@@ -345,11 +357,12 @@ def run_ensemble(args, rank, world, local, dist):
                    "simulations": len(params), "cells": cells,
                    "sides": [int(p.mesh_x) for p in params],
                    "l2": "inputs larger than L2: %.0f MB state per step" % (2 * cells * (N + K) * 4 / 1e6),
-                   "graph_steps": 100, "parallelism": "replicas" if world > 1 else "single"},
+                   "graph_steps": 100,
+                   "parallelism": "ensemble shards (rank r: the 256 simulations of seed r)" if world > 1 else "single"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                      "traffic": None, "bytes_per_cell": bpc,
                      "peak_source": "measured" if peaks.get("hbm_gbs") else "fallback"},
-        "e2e": {"value": world * cells * e2e_steps / t_e2e, "unit": "cell-updates/s",
+        "e2e": {"value": all_cells * e2e_steps / t_e2e, "unit": "cell-updates/s",
                 "h2d_bytes_per_step": host_bytes / e2e_steps, "d2h_bytes_per_step": host_bytes / e2e_steps,
                 "includes": "gp_batch_create upload of 256 simulations, %d smoothing sweeps, %d steps, "
                             "read-back of every simulation" % (params[0].nsmooth - 1, e2e_steps)},
@@ -487,19 +500,11 @@ def main():
     # per-kernel split on a short extra run (steps one by one, events around each kernel)
     nsplit = min(args.steps, 50)
     split_ms, bulk_ms, iface_ms, _ = sim.step_timed(nsplit, split=True)
-    if dist:
-        import torch
-        t = torch.tensor([tot_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        tot_ms = float(t.item())
+    tot_ms = reduce_over_ranks(dist, tot_ms)
     sim.close()
     if not args.no_fp32:
         fp32 = fp32_form(gp, p, phi0, mu0, args, phi64, st, local)
-        if dist:
-            import torch
-            t = torch.tensor([fp32[0]], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            fp32 = (float(t.item()),) + fp32[1:]
+        fp32 = (reduce_over_ranks(dist, fp32[0]),) + fp32[1:]
 
     # ---- end to end through the C ABI with host buffers ----------------------
     # gp_init uploads the host state, gp_smooth + gp_step run, and every
@@ -528,11 +533,7 @@ def main():
     t_e2e = time.perf_counter() - t0
     L.gp_destroy(h)
     barrier()
-    if dist:
-        import torch
-        t = torch.tensor([t_e2e], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_e2e = float(t.item())
+    t_e2e = reduce_over_ranks(dist, t_e2e)
 
     if rank == 0:
         peaks = measured_peaks()
