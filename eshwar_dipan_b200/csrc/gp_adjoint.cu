@@ -211,6 +211,22 @@ __device__ __forceinline__ void bulk_rev(const Consts<double> *c, const Grid &g,
   }
 }
 
+/* The inputs of update_cell, in seeding order (phi 3x3 per phase, mu and
+ * delta-phi 5-point per field, the four parameters), less those it does not
+ * read: the liquid's delta-phi enters only at the centre (the commit and the
+ * dh/dphi coupling; the anti-trapping current reads the solids'), and of the
+ * parameters only epsilon (the anti-trapping factor).  upd_inputs: how many
+ * remain; upd_input(u): the seeding index of the u-th. */
+template <int N, int K>
+__host__ __device__ constexpr int upd_inputs() {
+  return 9 * N + 5 * K + 5 * (N - 1) + 1 + 1;
+}
+template <int N, int K>
+__device__ __forceinline__ int upd_input(int u) {
+  constexpr int NPHI = 9 * N, NMU = 5 * K, NDP = 5 * N, LIQ = NPHI + NMU + 5 * (N - 1);
+  return u <= LIQ ? u : NPHI + NMU + NDP + ADJ_EPS;
+}
+
 /* Reverse of the concentration pass at cell (x, y).  SORT: cells whose 3x3
  * window is one pure phase take bulk_rev here; the others are returned
  * (true) for the dual passes, which run with SORT false over the list of
@@ -223,8 +239,10 @@ __device__ __forceinline__ bool rev_update_cell(const Consts<double> *__restrict
                                                 bool live, double (&pacc)[ADJ_NPARAM], int pass = -1) {
   using DT = Dual<ADJ_W>;
   constexpr int NPHI = 9 * N, NMU = 5 * K, NDP = 5 * N, NIN = NPHI + NMU + NDP + ADJ_NPARAM;
-  /* pass >= 0: only the dual pass seeding inputs pass*ADJ_W .. */
-  const int b0 = pass >= 0 ? pass * ADJ_W : 0, b1 = pass >= 0 ? min(NIN, b0 + ADJ_W) : NIN;
+  /* pass >= 0: only the dual pass seeding inputs pass*ADJ_W .. (one input
+   * per pass: the pass-th input update_cell depends on, upd_input) */
+  const int b0 = pass < 0 ? 0 : (ADJ_W == 1 ? upd_input<N, K>(pass) : pass * ADJ_W);
+  const int b1 = pass < 0 ? NIN : min(NIN, b0 + ADJ_W);
   double yb[N + K];
   bool any = false;
   if (live) {
@@ -369,7 +387,8 @@ __global__ void __launch_bounds__(AB) ka_rev_update_list(const Consts<double> *_
                                                          const int2 *__restrict__ cells,
                                                          const int *__restrict__ count) {
   /* one thread per (cell, dual pass): every SM gets work */
-  constexpr int NIN = 9 * N + 5 * K + 5 * N + ADJ_NPARAM, NPASS = (NIN + ADJ_W - 1) / ADJ_W;
+  constexpr int NIN = 9 * N + 5 * K + 5 * N + ADJ_NPARAM;
+  constexpr int NPASS = ADJ_W == 1 ? upd_inputs<N, K>() : (NIN + ADJ_W - 1) / ADJ_W;
   double pacc[ADJ_NPARAM] = {};
   const long long n = (long long)*count * NPASS;
   for (long long i = (long long)blockIdx.x * AB + threadIdx.x; i < n; i += (long long)gridDim.x * AB) {
