@@ -274,6 +274,8 @@ struct gp_batch {
   int dev, nsm, grid_b, grid_g, grid_s;   /* grid_s: kf_step (0: bulk and interface kernels apart) */
   bool mul;                     /* every simulation's dx and dy are powers of two (or FP32) */
   bool diag;                    /* off-diagonal D, c_mu, A all zero and no E is -0, in every simulation */
+  int mbar_tries;               /* kf_bulk's polls of a box barrier before it reports an error */
+  unsigned tma_extra;           /* 0; a test sets more (GP_TEST_TMA_SHORTFALL) to make the boxes never complete */
   int ntiles;                   /* TX x TY tiles over all simulations */
   cudaStream_t stream;
   gpd::SimDesc *d_desc;
@@ -322,6 +324,8 @@ static int batch_step_once(gp_batch *b, int want_sums, cudaEvent_t *ev) {
   st.partials = b->partials;
   st.want_sums = want_sums;
   st.round_step = (const unsigned *)(b->counters + gpd::CTR_STEP);
+  st.mbar_tries = b->mbar_tries;
+  st.tma_extra = b->tma_extra;
   const int in = b->cur, out = b->cur ^ 1;
   if (ev) BK(cudaEventRecord(ev[0], b->stream));
   BK(b->L.classify(b->ntiles, b->stream, b->d_desc, b->d_consts, b->d_tsim, b->flags[in], b->flags[out], b->glist,
@@ -785,6 +789,14 @@ int gp_batch_create(gp_batch **out, int nsims, const gp_params *params, const do
         for (int l = 0; l < K; l++)
           if (k != l && (d.Dbulk[a][k][l] != 0.0 || d.cmu[a][k][l] != 0.0 || d.A[a][k][l] != 0.0)) b->diag = false;
       }
+  }
+  /* the give-up path of kf_bulk's barrier waits, exercised by a test: the
+   * barriers expect more bytes than a box brings, and the polls are few */
+  b->mbar_tries = gpd::MBAR_TRIES;
+  b->tma_extra = 0;
+  if (const char *v = getenv("GP_TEST_TMA_SHORTFALL")) {
+    b->tma_extra = (unsigned)std::max(0, std::min(4096, atoi(v)));
+    if (b->tma_extra) b->mbar_tries = 256;
   }
   int bpb = 1, bpg = 1;
   e = b->L.prepare(&bpb, &bpg);

@@ -728,11 +728,11 @@ __device__ __forceinline__ bool mbar_test(unsigned bar, unsigned parity) {
       : "memory");
   return ok != 0;
 }
-/* wait for phase `parity` of bar to complete, at most MBAR_TRIES polls (each
+/* wait for phase `parity` of bar to complete, at most `tries` polls (each
  * poll may suspend the thread for a short while); false when it did not */
 constexpr int MBAR_TRIES = 1 << 20;
-__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity) {
-  for (int it = 0; it < MBAR_TRIES; it++)
+__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity, int tries) {
+  for (int it = 0; it < tries; it++)
     if (mbar_test(bar, parity)) return true;
   return false;
 }
@@ -895,7 +895,7 @@ __device__ __forceinline__ void bulk_tiles(const SimDesc *__restrict__ sims, con
     if (lane == 0) {
       ws.meta[b] = en;
       const unsigned bar = smem_addr(&ws.bar[b]);
-      mbar_expect_tx(bar, G::BOX_BYTES);
+      mbar_expect_tx(bar, G::BOX_BYTES + st.tma_extra);
       tma_load_3d(smem_addr(&ws.st[b]), tmaps + 2 * en.s + buf, en.y0 - 1 - CO, en.x0 - 1, 0, bar);
     }
   };
@@ -948,11 +948,11 @@ __device__ __forceinline__ void bulk_tiles(const SimDesc *__restrict__ sims, con
       }
     }
     const int b = ci % NST;
-    if (!mbar_wait(smem_addr(&ws.bar[b]), (ci / NST) & 1)) {
+    if (!mbar_wait(smem_addr(&ws.bar[b]), (ci / NST) & 1, st.mbar_tries)) {
       /* bytes missing: record it, wait (bounded) for the other boxes in
        * flight, step nothing more */
       if (lane == 0) atomicExch(ctr + CTR_ERR, 1);
-      for (int q = ci + 1; q < qi; q++) mbar_wait(smem_addr(&ws.bar[q % NST]), (q / NST) & 1);
+      for (int q = ci + 1; q < qi; q++) mbar_wait(smem_addr(&ws.bar[q % NST]), (q / NST) & 1, st.mbar_tries);
       break;
     }
     ci++;

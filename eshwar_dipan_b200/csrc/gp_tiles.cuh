@@ -427,6 +427,8 @@ struct StatBufs {
   double *partials;    /* [tiles][2N+2K+1] sums when want_sums */
   int want_sums;
   const unsigned *round_step;  /* FP32 form: device step counter keying the rounding stream */
+  int mbar_tries;      /* polls of a TMA box's barrier before kf_bulk gives up (MBAR_TRIES) */
+  unsigned tma_extra;  /* bytes a box's barrier expects beyond the box: 0, or more to test the give-up path */
 };
 
 /* ---- FP32 storage rounding ------------------------------------------------

@@ -166,3 +166,31 @@ def test_vtk_write_async_matches_sync(tmp_path, ascii):
         ref = s.get()
     assert (tmp_path / "sync2.vtk").read_bytes() == (tmp_path / "async2.vtk").read_bytes()
     assert bits_equal(end[0], ref[0]) and bits_equal(end[1], ref[1])
+
+
+@pytest.mark.parametrize("name", ["four_phase_ternary_iso", "ternary3_aniso_periodic"])
+def test_bulk_box_wait_gives_up_and_reports(tmp_path, monkeypatch, name):
+    """The bounded wait of the bulk tiles on their TMA boxes: with every box
+    barrier set to expect 16 bytes more than a box brings
+    (GP_TEST_TMA_SHORTFALL), each wait runs out after its few polls, the
+    kernel raises its error flag and returns, and gp_step reports it.  The
+    GPU stays usable: a new context then steps bit-identically to the oracle.
+    (N=4 steps through kf_bulk, N=3 through kf_step.)"""
+    from gp_cases import write_case
+    c = PARITY_CASES[name]
+    ip, fp = write_case(str(tmp_path), name + "_wait", dict(c["kw"], mesh=(96, 96)), seeds=c["seeds"])
+    p = gp.load_params(ip)
+    phi, mu = gp.fill(p, fp)
+    monkeypatch.setenv("GP_TEST_TMA_SHORTFALL", "16")
+    with gp.Simulation(p, phi, mu) as s:
+        with pytest.raises(gp.GpError, match="did not arrive"):
+            s.step(1, stats=False)
+    monkeypatch.delenv("GP_TEST_TMA_SHORTFALL")
+    o = Oracle(p, recip_div=1)
+    o.set(phi, mu)
+    o.step(3)
+    with gp.Simulation(p, phi, mu) as s:
+        s.step(3, stats=False)
+        a_phi, a_mu = s.get()
+    b_phi, b_mu = o.get()
+    assert bits_equal(a_phi, b_phi) and bits_equal(a_mu, b_mu)
