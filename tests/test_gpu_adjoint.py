@@ -179,7 +179,7 @@ def test_torch_integrator_gradients(tmp_path):
     loss.backward()
     with gp.Simulation(p, phi, mu) as s:
         g = s.adjoint(nsteps, target_phi=target.numpy())
-    assert float(loss) == pytest.approx(g["loss"], rel=1e-12)
+    assert float(loss.detach()) == pytest.approx(g["loss"], rel=1e-12)
     np.testing.assert_allclose(a.grad.numpy(), g["phi0_bar"], rtol=1e-9, atol=1e-14)
     np.testing.assert_allclose(th.grad.numpy(), [g["d_tau"], g["d_dab"], g["d_epsilon"], g["d_gamma"]], rtol=1e-9)
     v = torch.tensor([1.0, 0.5, -0.25, 0.75], dtype=torch.float64)
