@@ -322,6 +322,15 @@ def run_ensemble(args, rank, world, local, dist):
     barrier()
     b.close()
     tot_ms = reduce_over_ranks(dist, tot_ms)
+    # the same ensemble stepped in FP64 (the plain form), same steps
+    b = gp.Batch(params, fields, precision=gp.GP_FP64)
+    b.smooth(params[0].nsmooth - 1)
+    b.step(args.warmup, stats=False)
+    barrier()
+    ms64, _ = b.step_timed(args.steps, stats=False)
+    barrier()
+    b.close()
+    ms64 = reduce_over_ranks(dist, ms64)
 
     # end to end: upload of every simulation, smoothing, steps, read-back of all
     barrier()
@@ -366,9 +375,12 @@ def run_ensemble(args, rank, world, local, dist):
                 "h2d_bytes_per_step": host_bytes / e2e_steps, "d2h_bytes_per_step": host_bytes / e2e_steps,
                 "includes": "gp_batch_create upload of 256 simulations, %d smoothing sweeps, %d steps, "
                             "read-back of every simulation" % (params[0].nsmooth - 1, e2e_steps)},
-        "gpu_launches": step_launches(N, args.steps),
+        "gpu_launches": step_launches(N, args.steps) + step_launches(N, args.steps) - 2,
         "clocks": clk.summary(),
         "nonfinite": nonfinite,
+        "fp64_same_ensemble": {"value": all_cells * args.steps / (ms64 / 1e3), "unit": "cell-updates/s",
+                               "ms_per_step": ms64 / args.steps,
+                               "fp32_speedup": ms64 / tot_ms},
     }
     if not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline("cfg3")
