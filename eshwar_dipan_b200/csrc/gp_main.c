@@ -48,7 +48,7 @@ int main(int argc, char **argv) {
   mkdir("DATA", 0777);
   if ((rc = gp_params_load(&p, argv[1])) != GP_OK) return die("reading the input file", rc, NULL);
   if (p.shift) {
-    fprintf(stderr, "gp_microsim: Shift=1 (moving frame) is not implemented in this build\n");
+    fprintf(stderr, "gp_microsim: Shift=1 (moving frame) is not implemented\n");
     return 1;
   }
   N = p.numphases;
