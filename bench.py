@@ -451,9 +451,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp32", action="store_true", help="skip the FP32 form beside the FP64 headline")
     args = ap.parse_args()
-    # at least one full 100-step chunk untimed, so that the CUDA graphs are
-    # captured and instantiated before the timed region
-    args.warmup = max(102, args.warmup)
+    # untimed: the launch-shape autotuning (one 100-step chunk per candidate
+    # shape, at most four) and the capture of the chosen shape's CUDA graph
+    args.warmup = max(502, args.warmup)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

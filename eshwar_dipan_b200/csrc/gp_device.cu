@@ -24,7 +24,9 @@
 #include <cstdlib>
 #include <cstring>
 #include <algorithm>
+#include <map>
 #include <mutex>
+#include <tuple>
 #include <string>
 #include <thread>
 #include <vector>
@@ -263,6 +265,24 @@ static int fail(gp_ctx *c, int code, const char *fmt, ...) {
 /* batches                                                                 */
 /* ======================================================================= */
 
+/* How a step is launched; every shape gives the same bits (tiles are
+ * independent of the warp or CTA that steps them), so shapes can be timed on
+ * the live simulation. */
+struct LaunchShape {
+  bool fused;        /* kf_step (one launch) rather than kf_bulk + kf_general */
+  int bch_max, bch_div;
+};
+/* batches that share these tune alike: the first one's choice is kept for
+ * the process */
+struct ShapeKey {
+  int N, K, aniso, elem, tiles_log2;
+  bool operator<(const ShapeKey &o) const {
+    return std::tie(N, K, aniso, elem, tiles_log2) < std::tie(o.N, o.K, o.aniso, o.elem, o.tiles_log2);
+  }
+};
+static std::map<ShapeKey, LaunchShape> g_shapes;
+static std::mutex g_shapes_mutex;
+
 struct gp_batch {
   int nsims, N, K, aniso;
   gp_precision prec;
@@ -275,6 +295,11 @@ struct gp_batch {
   bool mul;                     /* every simulation's dx and dy are powers of two (or FP32) */
   bool diag;                    /* off-diagonal D, c_mu, A all zero and no E is -0, in every simulation */
   int mbar_tries;               /* kf_bulk's polls of a box barrier before it reports an error */
+  LaunchShape shape;            /* how a step is launched (tuned on the first graph chunks) */
+  LaunchShape cand[4];          /* the candidates */
+  float cand_ms[4];
+  int ncand, tune_next;         /* tuning is over when tune_next == ncand */
+  ShapeKey key;
   unsigned tma_extra;           /* 0; a test sets more (GP_TEST_TMA_SHORTFALL) to make the boxes never complete */
   int ntiles;                   /* TX x TY tiles over all simulations */
   cudaStream_t stream;
@@ -326,11 +351,13 @@ static int batch_step_once(gp_batch *b, int want_sums, cudaEvent_t *ev) {
   st.round_step = (const unsigned *)(b->counters + gpd::CTR_STEP);
   st.mbar_tries = b->mbar_tries;
   st.tma_extra = b->tma_extra;
+  st.bch_max = b->shape.bch_max;
+  st.bch_div = b->shape.bch_div;
   const int in = b->cur, out = b->cur ^ 1;
   if (ev) BK(cudaEventRecord(ev[0], b->stream));
   BK(b->L.classify(b->ntiles, b->stream, b->d_desc, b->d_consts, b->d_tsim, b->flags[in], b->flags[out], b->glist,
                    b->blist, b->counters));
-  if (!ev && !want_sums && b->grid_s > 0) {
+  if (!ev && !want_sums && b->grid_s > 0 && b->shape.fused) {
     /* one launch for both kinds of tile */
     BK(b->L.step(b->grid_s, b->mul, b->diag, b->stream, b->d_desc, b->d_consts, b->d_tsim, b->blist, b->glist,
                  b->tmaps, in, b->state[in], b->state[out], b->flags[out], b->counters, b->grid_s, st));
@@ -402,6 +429,40 @@ static int batch_step_impl(gp_batch *b, long nsteps, gp_stats *stats, double *to
   long s = 0;
   while (!split && nsteps - s > GP_GRAPH_STEPS) {
     const int p = b->cur;
+    if (b->tune_next < b->ncand) {
+      /* autotuning: one 100-step chunk per candidate shape, each captured
+       * afresh and timed with events; then the fastest is kept */
+      b->shape = b->cand[b->tune_next];
+      cudaGraph_t gr;
+      cudaGraphExec_t ge;
+      BK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+      int rc = GP_OK;
+      for (int i = 0; i < GP_GRAPH_STEPS && rc == GP_OK; i++) rc = batch_step_once(b, 0, nullptr);
+      b->steps -= GP_GRAPH_STEPS;
+      cudaError_t ec = cudaStreamEndCapture(b->stream, &gr);
+      if (rc != GP_OK) return rc;
+      if (ec != cudaSuccess) return bfail(b, GP_ECUDA, "graph capture: %s", cudaGetErrorString(ec));
+      ec = cudaGraphInstantiate(&ge, gr, 0);
+      cudaGraphDestroy(gr);
+      if (ec != cudaSuccess) return bfail(b, GP_ECUDA, "graph instantiate: %s", cudaGetErrorString(ec));
+      BK(cudaEventRecord(b->ev[0], b->stream));
+      BK(cudaGraphLaunch(ge, b->stream));
+      BK(cudaEventRecord(b->ev[1], b->stream));
+      BK(cudaEventSynchronize(b->ev[1]));
+      cudaGraphExecDestroy(ge);
+      BK(cudaEventElapsedTime(&b->cand_ms[b->tune_next], b->ev[0], b->ev[1]));
+      if (++b->tune_next == b->ncand) {
+        int best = 0;
+        for (int i = 1; i < b->ncand; i++)
+          if (b->cand_ms[i] < b->cand_ms[best]) best = i;
+        b->shape = b->cand[best];
+        std::lock_guard<std::mutex> lock(g_shapes_mutex);
+        g_shapes[b->key] = b->shape;
+      }
+      b->steps += GP_GRAPH_STEPS;
+      s += GP_GRAPH_STEPS;
+      continue;
+    }
     if (!b->graph[p]) {
       cudaGraph_t gr;
       BK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
@@ -811,6 +872,30 @@ int gp_batch_create(gp_batch **out, int nsims, const gp_params *params, const do
   {
     const int bps = b->L.step_occupancy();
     b->grid_s = (bps >= bpb && getenv("GP_SPLIT_KERNELS") == nullptr) ? b->nsm * bps : 0;
+  }
+  /* launch shapes: the first graph chunks of the first batch of its kind time
+   * each candidate; later batches of that kind take its choice (GP_NO_TUNING:
+   * the first candidate, untimed) */
+  {
+    int lg = 0;
+    while ((1 << lg) < nt) lg++;
+    b->key = ShapeKey{N, K, b->aniso, (int)b->elem, lg};
+    const LaunchShape fused16 = {true, 16, 2}, fused8 = {true, 8, 2}, fused16q = {true, 16, 4}, two = {false, 16, 2};
+    b->ncand = 0;
+    if (b->grid_s > 0) {
+      b->cand[b->ncand++] = fused16;
+      b->cand[b->ncand++] = fused8;
+      b->cand[b->ncand++] = fused16q;
+    }
+    b->cand[b->ncand++] = two;
+    b->shape = b->cand[0];
+    b->tune_next = b->ncand;   /* nothing to tune */
+    if (getenv("GP_NO_TUNING") == nullptr) {
+      std::lock_guard<std::mutex> lock(g_shapes_mutex);
+      auto it = g_shapes.find(b->key);
+      if (it != g_shapes.end()) b->shape = it->second;
+      else if (b->ncand > 1) b->tune_next = 0;
+    }
   }
 #define BALLOC(ptr, bytes)                                                                        \
   do {                                                                                            \

@@ -839,7 +839,8 @@ __device__ __forceinline__ void bulk_tiles(const SimDesc *__restrict__ sims, con
 
   /* Work comes in chunks of list entries taken from the bulk head counter
    * (one atomic per warp and chunk), so warps that run faster take more; the
-   * chunk size shrinks as the list drains (a few chunks per warp in all).
+   * chunk size shrinks as the list drains (a few chunks per warp in all; the
+   * batch's launch shape sets the largest chunk and the divisor).
    * Two chunks are held: A (being issued) and B (next).  Lane h*16+r holds
    * entry r of the chunk in half h; B's entries are loaded when it is taken,
    * one 16-byte load per lane, and used one tile later. */
@@ -850,7 +851,7 @@ __device__ __forceinline__ void bulk_tiles(const SimDesc *__restrict__ sims, con
     int v = 0, c = 0;
     if (lane == 0) {
       const int left = nbulk - *(volatile int *)(ctr + CTR_BHEAD);
-      c = max(2, min(BCH, left / (2 * nwarps)));
+      c = max(2, min(min(BCH, st.bch_max), left / (st.bch_div * nwarps)));
       v = atomicAdd(ctr + CTR_BHEAD, c);
     }
     start = __shfl_sync(0xffffffffu, v, 0);

@@ -201,10 +201,12 @@ def test_single_launch_step_matches_two_kernels(tmp_path, monkeypatch, prec):
     sims = _ternary_group(tmp_path)
     args = ([s[0] for s in sims], [(s[1], s[2]) for s in sims])
     pr = gp.GP_FP64 if prec == "fp64" else gp.GP_FP32
+    monkeypatch.setenv("GP_NO_TUNING", "1")   # the single-launch shape, not a tuned one
     b1 = gp.Batch(*args, precision=pr)
     monkeypatch.setenv("GP_SPLIT_KERNELS", "1")
     b2 = gp.Batch(*args, precision=pr)
     monkeypatch.delenv("GP_SPLIT_KERNELS")
+    monkeypatch.delenv("GP_NO_TUNING")
     for b in (b1, b2):
         b.smooth(5)
         b.step(230, stats=False)
@@ -213,3 +215,22 @@ def test_single_launch_step_matches_two_kernels(tmp_path, monkeypatch, prec):
         assert bits_equal(x[0], y[0]) and bits_equal(x[1], y[1]), "sim %d" % i
     b1.close()
     b2.close()
+
+
+def test_autotuned_shapes_give_the_same_bits(tmp_path, monkeypatch):
+    """The launch-shape autotuner times its candidates on the first 100-step
+    chunks of the live simulation: the result equals an untuned run bit for
+    bit (every shape steps the same tiles the same way)."""
+    sims = _ternary_group(tmp_path)
+    args = ([s[0] for s in sims], [(s[1], s[2]) for s in sims])
+    monkeypatch.setenv("GP_NO_TUNING", "1")
+    ref = gp.Batch(*args, precision=gp.GP_FP64)
+    monkeypatch.delenv("GP_NO_TUNING")
+    tuned = gp.Batch(*args, precision=gp.GP_FP64)
+    for b in (ref, tuned):
+        b.step(650, stats=False)
+    for i in range(len(sims)):
+        x, y = ref.get(i), tuned.get(i)
+        assert bits_equal(x[0], y[0]) and bits_equal(x[1], y[1]), "sim %d" % i
+    ref.close()
+    tuned.close()
