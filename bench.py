@@ -42,58 +42,10 @@ sys.path.insert(0, os.path.join(ROOT, "tests"))
 
 import numpy as np  # noqa: E402
 
-from eshwar_dipan_b200.workloads import ensemble, filling_text, input_text, random_seeds  # noqa: E402
+from eshwar_dipan_b200.workloads import ensemble, filling_text, input_text, workload, write_workload  # noqa: E402
 
 HARNESS = os.path.join(ROOT, "oracle", "_ref", "gp_ref_harness")
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
-
-
-def workload(name, scale=1):
-    """(input text, filling text, description) of a benchmark configuration;
-    scale>1 shrinks the grid by that factor per axis with the same seed density."""
-    if name == "cfg2":
-        m = 2048 // scale
-        nseeds = max(1, 64 // (scale * scale))
-        kw = dict(N=3, K=2, mesh=(m, m), dab=0.02, bc_phi=(3, 3, 3, 3), d_liquid=[1.0, 0.5], d_solid=0.0,
-                  A_off=0.0, dt=0.02, eps=4.0, T=0.97)
-        seeds = random_seeds(nseeds, (m, m), 4.0, 12.0, 2, seed=0)
-        desc = "%dx%d ternary 3-phase FP64, aniso 0.02, periodic, %d seeds r~U[4,12]" % (m, m, nseeds)
-    elif name == "cfg4":
-        m = 4096 // scale
-        nseeds = max(1, 256 // (scale * scale))
-        kw = dict(N=3, K=2, mesh=(m, m), dab=0.0, aniso=False, bc_phi=(1, 1, 1, 1), d_liquid=[1.0, 0.5],
-                  d_solid=0.0, dt=0.02, eps=4.0, T=0.97)
-        seeds = random_seeds(nseeds, (m, m), 4.0, 12.0, 2, seed=0)
-        desc = "%dx%d ternary 3-phase FP64, isotropic, Neumann, %d seeds" % (m, m, nseeds)
-    elif name == "cfg3":
-        kw, seeds = ensemble(shrink=scale)[0]
-        kw = dict(kw)
-        m = kw["mesh"][0]
-        desc = ("ensemble member 0: %dx%d binary 2-phase, delta %.4f, c0 %.4f, %d seeds"
-                % (m, m, kw["dab"], kw["liquid_c"][0], len(seeds)))
-    elif name == "cfg5":
-        m = 512 // scale
-        kw = dict(N=2, K=1, mesh=(m, m), aniso=True, dab=0.04, d_solid=0.0, d_liquid=[1.0], dt=0.02, eps=4.0,
-                  T=1.0, liquid_c=[0.42])
-        seeds = [(0, m // 2, m // 2, 12.0 / scale)]
-        desc = "%dx%d binary 2-phase dendrite FP64, aniso 0.04, Neumann, one seed r=12" % (m, m)
-    elif name == "cfg1":
-        m = 256 // scale
-        kw = dict(N=2, K=1, mesh=(m, m), aniso=False, dab=0.0, d_solid=0.0, d_liquid=[1.0], dt=0.02, eps=4.0,
-                  T=1.0, liquid_c=[0.45])
-        seeds = [(0, m // 2, m // 2, 40.0 / scale)]
-        desc = "%dx%d binary 2-phase FP64, isotropic, Neumann, one supercritical seed r=40" % (m, m)
-    else:
-        raise SystemExit("unknown workload " + name)
-    return input_text(**kw), filling_text(seeds), desc, kw
-
-
-def write_workload(d, name, scale=1):
-    it, ft, desc, kw = workload(name, scale)
-    ip, fp = os.path.join(d, name + ".in"), os.path.join(d, name + "_fill.in")
-    open(ip, "w").write(it)
-    open(fp, "w").write(ft)
-    return ip, fp, desc, kw
 
 
 class ClockSampler:

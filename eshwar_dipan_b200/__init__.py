@@ -17,9 +17,10 @@ import ctypes
 
 import numpy as np
 
-from ._abi import (GP_FP32, GP_FP64, AdjOut, AdjReq, GpError, Params, Stats, check, lib)
+from ._abi import (GP_ENONFINITE, GP_ETIMEOUT, GP_FP32, GP_FP64, AdjOut, AdjReq, GpError, NonFiniteError, Params,
+                   Stats, check, lib)
 
-__all__ = ["Params", "Stats", "GpError", "Simulation", "Batch", "load_params", "fill", "vtk_write", "vtk_read",
+__all__ = ["Params", "Stats", "GpError", "NonFiniteError", "Simulation", "Batch", "load_params", "fill", "vtk_write", "vtk_read",
            "GP_FP64", "GP_FP32", "version"]
 
 
@@ -90,9 +91,15 @@ class Simulation:
         check(lib().gp_smooth(self._h, int(n)), self._h)
 
     def step(self, n, stats=True):
+        """n time steps; with stats, the progress record of the last one.
+        Raises NonFiniteError (carrying that record) when the state then
+        holds non-finite cells."""
         if stats:
             s = Stats()
-            check(lib().gp_step(self._h, int(n), ctypes.byref(s)), self._h)
+            rc = lib().gp_step(self._h, int(n), ctypes.byref(s))
+            if rc == GP_ENONFINITE:
+                raise NonFiniteError(rc, lib().gp_last_error(self._h).decode(), s.as_dict(self.N, self.K))
+            check(rc, self._h)
             return s.as_dict(self.N, self.K)
         check(lib().gp_step(self._h, int(n), None), self._h)
         return None
@@ -234,7 +241,11 @@ class Batch:
     def step(self, n, stats=True):
         if stats:
             s = (Stats * self.n)()
-            _bcheck(lib().gp_batch_step(self._h, int(n), s), self._h)
+            rc = lib().gp_batch_step(self._h, int(n), s)
+            if rc == GP_ENONFINITE:
+                raise NonFiniteError(rc, lib().gp_batch_last_error(self._h).decode(),
+                                     [x.as_dict(self.N, self.K) for x in s])
+            _bcheck(rc, self._h)
             return [x.as_dict(self.N, self.K) for x in s]
         _bcheck(lib().gp_batch_step(self._h, int(n), None), self._h)
         return None

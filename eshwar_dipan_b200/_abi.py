@@ -177,6 +177,16 @@ class GpError(RuntimeError):
         self.code = code
 
 
+class NonFiniteError(GpError):
+    """GP_ENONFINITE: the steps are done, but the state holds non-finite
+    cells; `stats` is the progress record of the last step (per simulation
+    for a batch)."""
+
+    def __init__(self, code, msg, stats):
+        super().__init__(code, msg)
+        self.stats = stats
+
+
 def check(code, ctx=None):
     if code != GP_OK:
         m = lib().gp_last_error(ctx)

@@ -411,8 +411,18 @@ static int batch_check_error(gp_batch *b) {
   BK(cudaStreamSynchronize(b->stream));
   if (e) {
     BK(cudaMemsetAsync(b->counters + gpd::CTR_ERR, 0, sizeof e, b->stream));
-    return bfail(b, GP_ECUDA, "kf_bulk: a tile's mu did not arrive within the wait limit; the state is not valid");
+    return bfail(b, GP_ETIMEOUT, "kf_bulk: a tile's mu did not arrive within the wait limit; the state is not valid");
   }
+  return GP_OK;
+}
+
+/* GP_ENONFINITE when the statistics just folded count non-finite interior
+ * cells in any simulation (the steps are done and the statistics filled). */
+static int batch_check_finite(gp_batch *b) {
+  for (int s = 0; s < b->nsims; s++)
+    if (b->last[s].nonfinite > 0)
+      return bfail(b, GP_ENONFINITE, "simulation %d: %lld interior cells hold a non-finite phi or mu after step %lld", s,
+                   b->last[s].nonfinite, b->steps);
   return GP_OK;
 }
 
@@ -503,7 +513,10 @@ static int batch_step_impl(gp_batch *b, long nsteps, gp_stats *stats, double *to
   if (ms_iface) *ms_iface = ti;
   int rc = batch_check_error(b);
   if (rc != GP_OK) return rc;
-  if (stats && nsteps > 0) return batch_fold_stats(b, stats);
+  if (stats && nsteps > 0) {
+    if ((rc = batch_fold_stats(b, stats)) != GP_OK) return rc;
+    return batch_check_finite(b);
+  }
   BK(cudaStreamSynchronize(b->stream));
   if (stats)
     for (int i = 0; i < b->nsims; i++) stats[i] = b->last[i];
@@ -1439,9 +1452,9 @@ int gp_adjoint_replay(gp_ctx *c, long nsteps, double *max_abs_diff, long long *n
 /* other allocation (memory budgets fixed up front, allocator locks it     */
 /* must not contend on, or code paths where a failing allocation cannot be */
 /* handled).  For them the step's only scratch buffer, delta-phi over the  */
-/* interior plus a one-cell ring, and the running-extreme counters live in */
-/* this fixed array instead of per-context cudaMalloc'd memory.  Every GPU */
-/* that loads the library holds these 32 MiB until the process exits.      */
+/* interior plus a one-cell ring, lives in this fixed array instead of      */
+/* per-context cudaMalloc'd memory.  Every GPU that loads the library holds */
+/* these 32 MiB until the process exits.                                    */
 
 
 #define GP_NOALLOC_SCRATCH_DOUBLES (4u * 1024u * 1024u)   /* 32 MiB */
@@ -1458,8 +1471,6 @@ extern "C" int gp_step_noalloc(const gp_params *p, const double *phi_in, const d
   gp_ctx *c = nullptr; /* CK() reports through the thread's error slot */
   if (!p || !phi_in || !mu_in || !phi_out || !mu_out)
     return fail(nullptr, GP_EINVAL, "gp_step_noalloc: NULL argument");
-  if (phi_in == phi_out || mu_in == mu_out)
-    return fail(nullptr, GP_EINVAL, "gp_step_noalloc: input and output buffers must differ");
   gp_derived d;
   char err[256] = "";
   if (gp_host_derive(p, &d, err, sizeof err) != GP_OK) return fail(nullptr, GP_EINVAL, "gp_step_noalloc: %s", err);
@@ -1467,14 +1478,35 @@ extern "C" int gp_step_noalloc(const gp_params *p, const double *phi_in, const d
   if (!pick(d.N, d.K, d.aniso != 0, &k)) return fail(nullptr, GP_EINVAL, "gp_step_noalloc: no kernel for N=%d K=%d", d.N, d.K);
   gpd::Grid g = make_grid(d, 1); /* caller's planes are contiguous [field][MESH_X][MESH_Y] */
   gpd::Consts<double> cs = make_consts<double>(d);
-  /* scratch layout: [running extremes, 2(N+K) long longs][pad to 256 B][delta-phi, N planes] */
-  const size_t head = 32;  /* doubles; holds 2*(4+2) long longs and keeps delta-phi 256-B aligned */
-  const size_t need = head + (size_t)d.N * (size_t)g.dplane;
+  /* the scratch holds the delta-phi planes (N of them, interior plus a
+   * one-cell ring); k_dphi rewrites all of it before k_update reads it, so
+   * what an earlier call left there needs no clearing */
+  const size_t need = (size_t)d.N * (size_t)g.dplane;
   if (need > GP_NOALLOC_SCRATCH_DOUBLES)
     return fail(nullptr, GP_EINVAL,
                 "gp_step_noalloc: grid %ldx%ld with %d phases needs %zu doubles of scratch, the fixed maximum is %u "
                 "(about 1.3 million cells for 3 phases); use gp_init/gp_step for larger grids",
                 d.mx, d.my, d.N, need, GP_NOALLOC_SCRATCH_DOUBLES);
+  /* the step reads every input cell's neighbours after other cells' outputs
+   * are written: an output range may share no byte with an input range or
+   * with the other output range */
+  {
+    const size_t cells = (size_t)d.mx * (size_t)d.my;
+    struct Range {
+      const char *lo, *hi;
+    };
+    const Range in[2] = {{(const char *)phi_in, (const char *)(phi_in + (size_t)d.N * cells)},
+                         {(const char *)mu_in, (const char *)(mu_in + (size_t)d.K * cells)}};
+    const Range out[2] = {{(const char *)phi_out, (const char *)(phi_out + (size_t)d.N * cells)},
+                          {(const char *)mu_out, (const char *)(mu_out + (size_t)d.K * cells)}};
+    auto overlap = [](const Range &a, const Range &b) { return a.lo < b.hi && b.lo < a.hi; };
+    for (int o = 0; o < 2; o++)
+      for (int i = 0; i < 2; i++)
+        if (overlap(out[o], in[i]))
+          return fail(nullptr, GP_EINVAL, "gp_step_noalloc: output %s overlaps input %s", o ? "mu" : "phi",
+                      i ? "mu" : "phi");
+    if (overlap(out[0], out[1])) return fail(nullptr, GP_EINVAL, "gp_step_noalloc: outputs phi and mu overlap");
+  }
   int dev = 0;
   CK(cudaGetDevice(&dev));
   if (dev < 0 || dev >= GP_NOALLOC_MAX_DEVICES) return fail(nullptr, GP_EINVAL, "gp_step_noalloc: device %d", dev);
@@ -1490,13 +1522,11 @@ extern "C" int gp_step_noalloc(const gp_params *p, const double *phi_in, const d
   CK(cudaFuncSetAttribute(k.dphi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem_dphi));
   CK(cudaFuncSetAttribute(k.upd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem_upd));
   CK(cudaMemcpyToSymbolAsync(cD, &cs, sizeof(cs), 0, cudaMemcpyHostToDevice, s));
-  /* the previous call's extremes are still in the array: start them from zero */
-  CK(cudaMemsetAsync(scratch, 0, head * sizeof(double), s));
   gpd::StatBufs st = {};
-  st.ext = nullptr; /* no progress record on this path */
-  st.partials = scratch; /* not written: no sums requested */
+  st.ext = nullptr;      /* no progress record on this path: no extremes */
+  st.partials = nullptr; /* and no sums */
   st.want_sums = 0;
-  double *dphi = scratch + head;
+  double *dphi = scratch;
   dim3 gd((g.my + 2 + gpd::TY - 1) / gpd::TY, (g.mx + 2 + gpd::TX - 1) / gpd::TX);
   dim3 gu((g.my + gpd::TY - 1) / gpd::TY, (g.mx + gpd::TX - 1) / gpd::TX);
   k.dphi<<<gd, gpd::NT, k.smem_dphi, s>>>(phi_in, mu_in, dphi, g);

@@ -82,7 +82,9 @@ int main(int argc, char **argv) {
   for (t = 0; t < p.ntimesteps;) {
     long n = chunk - (t % chunk);
     if (t + n > p.ntimesteps) n = p.ntimesteps - t;
-    if ((rc = gp_step(c, n, &st)) != GP_OK) return die("gp_step", rc, c);
+    /* non-finite cells do not stop the run (the reference keeps stepping);
+     * they are reported with the progress record */
+    if ((rc = gp_step(c, n, &st)) != GP_OK && rc != GP_ENONFINITE) return die("gp_step", rc, c);
     t += n;
     if (p.savet > 0 && t % p.savet == 0) {
       FILE *f;

@@ -202,3 +202,59 @@ def ensemble(n=256, seed=0, side_min=128, side_max=1024, shrink=1):
                   eps=4.0, T=1.0, liquid_c=[c0])
         out.append((kw, random_seeds(nseeds, (side, side), 4.0, 12.0, 1, seed=seed * 1000003 + s + 1)))
     return out
+
+
+def workload(name, scale=1):
+    """(Input.in text, Filling.in text, description, input kwargs) of a
+    benchmark configuration:
+      cfg1  256^2 binary 2-phase, isotropic, Neumann, one supercritical seed r=40
+      cfg2  2048^2 ternary 3-phase, 4-fold anisotropy 0.02, periodic, 64 seeds
+      cfg3  member 0 of the batched ensemble (see ensemble())
+      cfg4  4096^2 ternary 3-phase, isotropic, Neumann, 256 seeds
+      cfg5  512^2 binary 2-phase dendrite, anisotropy 0.04, one seed r=12
+    scale > 1 shrinks the grid by that factor per axis with the same seed
+    density (at least one seed)."""
+    if name == "cfg2":
+        m = 2048 // scale
+        nseeds = max(1, 64 // (scale * scale))
+        kw = dict(N=3, K=2, mesh=(m, m), dab=0.02, bc_phi=(3, 3, 3, 3), d_liquid=[1.0, 0.5], d_solid=0.0,
+                  A_off=0.0, dt=0.02, eps=4.0, T=0.97)
+        seeds = random_seeds(nseeds, (m, m), 4.0, 12.0, 2, seed=0)
+        desc = "%dx%d ternary 3-phase FP64, aniso 0.02, periodic, %d seeds r~U[4,12]" % (m, m, nseeds)
+    elif name == "cfg4":
+        m = 4096 // scale
+        nseeds = max(1, 256 // (scale * scale))
+        kw = dict(N=3, K=2, mesh=(m, m), dab=0.0, aniso=False, bc_phi=(1, 1, 1, 1), d_liquid=[1.0, 0.5],
+                  d_solid=0.0, dt=0.02, eps=4.0, T=0.97)
+        seeds = random_seeds(nseeds, (m, m), 4.0, 12.0, 2, seed=0)
+        desc = "%dx%d ternary 3-phase FP64, isotropic, Neumann, %d seeds" % (m, m, nseeds)
+    elif name == "cfg3":
+        kw, seeds = ensemble(shrink=scale)[0]
+        kw = dict(kw)
+        m = kw["mesh"][0]
+        desc = ("ensemble member 0: %dx%d binary 2-phase, delta %.4f, c0 %.4f, %d seeds"
+                % (m, m, kw["dab"], kw["liquid_c"][0], len(seeds)))
+    elif name == "cfg5":
+        m = 512 // scale
+        kw = dict(N=2, K=1, mesh=(m, m), aniso=True, dab=0.04, d_solid=0.0, d_liquid=[1.0], dt=0.02, eps=4.0,
+                  T=1.0, liquid_c=[0.42])
+        seeds = [(0, m // 2, m // 2, 12.0 / scale)]
+        desc = "%dx%d binary 2-phase dendrite FP64, aniso 0.04, Neumann, one seed r=12" % (m, m)
+    elif name == "cfg1":
+        m = 256 // scale
+        kw = dict(N=2, K=1, mesh=(m, m), aniso=False, dab=0.0, d_solid=0.0, d_liquid=[1.0], dt=0.02, eps=4.0,
+                  T=1.0, liquid_c=[0.45])
+        seeds = [(0, m // 2, m // 2, 40.0 / scale)]
+        desc = "%dx%d binary 2-phase FP64, isotropic, Neumann, one supercritical seed r=40" % (m, m)
+    else:
+        raise ValueError("unknown workload " + name)
+    return input_text(**kw), filling_text(seeds), desc, kw
+
+
+def write_workload(d, name, scale=1):
+    """workload() written to d/<name>.in and d/<name>_fill.in: (paths, description, kwargs)."""
+    it, ft, desc, kw = workload(name, scale)
+    ip, fp = os.path.join(d, name + ".in"), os.path.join(d, name + "_fill.in")
+    open(ip, "w").write(it)
+    open(fp, "w").write(ft)
+    return ip, fp, desc, kw

@@ -165,7 +165,15 @@ int gp_smooth(gp_ctx *ctx, long nsteps);
 /* nsteps explicit time steps; each replaces solverloop_phasefield +
  * apply_boundary_conditions + solverloop_concentration + apply_boundary_conditions
  * (microsim_gp.c:103-106, solverloop.h:21-71, boundary_serial.h:176-203).
- * stats may be NULL. */
+ * stats may be NULL.  Besides GP_EINVAL/GP_ECUDA it returns
+ *   GP_ETIMEOUT    when a bounded device-side wait of the step kernels gave up
+ *                  (a tile's staged fields did not arrive); the state is then
+ *                  not valid and the error flag is cleared for the next call;
+ *   GP_ENONFINITE  when stats were asked for and the state after the steps
+ *                  holds interior cells with a non-finite phi or mu: the steps
+ *                  are done and *stats is filled (stats->nonfinite counts the
+ *                  cells), as the reference, which keeps stepping, would have
+ *                  them.  Without stats the count is not made. */
 int gp_step(gp_ctx *ctx, long nsteps, gp_stats *stats);
 
 /* Copy the interior state out / in (host buffers, layouts as above). */
@@ -205,7 +213,8 @@ typedef struct gp_batch gp_batch;
 int gp_batch_create(gp_batch **b, int nsims, const gp_params *params, const double *const *phi,
                     const double *const *mu, gp_precision prec);
 int gp_batch_smooth(gp_batch *b, long nsteps);
-/* stats: NULL or nsims records, in simulation order */
+/* stats: NULL or nsims records, in simulation order; return codes as gp_step
+ * (GP_ENONFINITE names the first simulation with non-finite cells) */
 int gp_batch_step(gp_batch *b, long nsteps, gp_stats *stats);
 int gp_batch_step_timed(gp_batch *b, long nsteps, gp_stats *stats, double *total_ms);
 int gp_batch_get(gp_batch *b, int sim, double *phi, double *mu);
@@ -220,8 +229,9 @@ void gp_batch_destroy(gp_batch *b);
  * or arena, run under a fixed memory budget, or sit on a path where a failed
  * allocation cannot be handled.  They pass their own device buffers:
  * phi_in/mu_in (read) and phi_out/mu_out (written), contiguous planes
- * [N][MESH_X][MESH_Y] and [K][MESH_X][MESH_Y] on the current device, outputs not
- * aliasing inputs; stream is a cudaStream_t (NULL = default stream).
+ * [N][MESH_X][MESH_Y] and [K][MESH_X][MESH_Y] on the current device; neither
+ * output may share a byte with an input or with the other output (GP_EINVAL
+ * otherwise); stream is a cudaStream_t (NULL = default stream).
  * The step's scratch (delta-phi over the interior plus a one-cell ring) lives
  * in a fixed 32 MiB array inside the library that every GPU which loads the
  * library keeps until exit; grids needing more (about 1.3 million cells with

@@ -104,6 +104,19 @@ def test_nonfinite_mu_in_bulk_tiles(tmp_path):
         assert np.isnan(b_mu).sum() > 3
         assert _same_with_nans(a_phi, b_phi), mismatch_report(a_phi, b_phi)
         assert _same_with_nans(a_mu, b_mu), mismatch_report(a_mu, b_mu)
+    # with a progress record the step reports the non-finite cells
+    # (GP_ENONFINITE), after stepping as the reference does
+    o.step(1)
+    with pytest.raises(gp.NonFiniteError) as ei:
+        sim.step(1, stats=True)
+    assert ei.value.code == gp.GP_ENONFINITE
+    b_phi, b_mu = o.get()
+    n_bad = int((~(np.isfinite(b_phi).all(axis=0) & np.isfinite(b_mu).all(axis=0))).sum())
+    assert n_bad > 0
+    assert ei.value.stats["nonfinite"] == n_bad and ei.value.stats["steps_done"] == 4
+    a_phi, a_mu = sim.get()
+    assert _same_with_nans(a_phi, b_phi), mismatch_report(a_phi, b_phi)
+    assert _same_with_nans(a_mu, b_mu), mismatch_report(a_mu, b_mu)
 
 
 def test_smoothing_vs_reference_reciprocal(tmp_path):
@@ -183,8 +196,9 @@ def test_bulk_box_wait_gives_up_and_reports(tmp_path, monkeypatch, name):
     phi, mu = gp.fill(p, fp)
     monkeypatch.setenv("GP_TEST_TMA_SHORTFALL", "16")
     with gp.Simulation(p, phi, mu) as s:
-        with pytest.raises(gp.GpError, match="did not arrive"):
+        with pytest.raises(gp.GpError, match="did not arrive") as ei:
             s.step(1, stats=False)
+        assert ei.value.code == gp.GP_ETIMEOUT
     monkeypatch.delenv("GP_TEST_TMA_SHORTFALL")
     o = Oracle(p, recip_div=1)
     o.set(phi, mu)

@@ -84,3 +84,26 @@ def test_oracle_smoothing_division_variant_close(tmp_path):
     assert bits_equal(a_phi, b_phi)
     rel = np.abs(a_mu - b_mu) / np.maximum(np.abs(a_mu), 1e-300)
     assert rel.max() <= 8 * np.finfo(np.float64).eps
+
+
+@needs_ref
+def test_oracle_matches_reference_on_shrunk_cfg2(tmp_path):
+    """The benchmarked ternary 3-phase anisotropic periodic configuration,
+    shrunk to 512^2 with the same seed density (4 seeds), over 200 steps: the
+    oracle equals the reference built from its own sources bit for bit (full
+    ghosted phi and mu)."""
+    from eshwar_dipan_b200.workloads import workload
+    it, ft, _, _ = workload("cfg2", 4)
+    ip, fp = str(tmp_path / "c2.in"), str(tmp_path / "c2_fill.in")
+    open(ip, "w").write(it)
+    open(fp, "w").write(ft)
+    import concurrent.futures
+    with concurrent.futures.ThreadPoolExecutor(1) as pool:   # the two CPU runs side by side
+        fut = pool.submit(harness_run, ip, fp, 9, 200, tmp_path)
+        p, o = _run_oracle(ip, fp, 9, 200, recip_div=0)
+        ref = fut.result()
+    phi, mu, _ = o.get_full()
+    assert bits_equal(phi, ref["phi"]), mismatch_report(phi, ref["phi"])
+    assert bits_equal(mu, ref["mu"]), mismatch_report(mu, ref["mu"])
+    inner = phi[:, 3:p.mesh_x + 3, 3:p.mesh_y + 3]
+    assert not np.all((inner == 0) | (inner == 1))
