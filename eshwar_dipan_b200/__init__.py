@@ -17,8 +17,8 @@ import ctypes
 
 import numpy as np
 
-from ._abi import (GP_ENONFINITE, GP_ETIMEOUT, GP_FP32, GP_FP64, AdjOut, AdjReq, GpError, NonFiniteError, Params,
-                   Stats, check, lib)
+from ._abi import (GP_ENONFINITE, GP_ETIMEOUT, GP_FP32, GP_FP64, AdjOut, AdjReq, GpError, KernelTimes,
+                   NonFiniteError, Params, Stats, check, lib)
 
 __all__ = ["Params", "Stats", "GpError", "NonFiniteError", "Simulation", "Batch", "load_params", "fill", "vtk_write", "vtk_read",
            "GP_FP64", "GP_FP32", "version"]
@@ -115,6 +115,16 @@ class Simulation:
               self._h)
         return (tot.value, a.value if split else None, b.value if split else None,
                 s.as_dict(self.N, self.K) if stats else None)
+
+    def kernel_times(self, n):
+        """gp_step_kernel_times: n steps launched one by one with events around
+        each kernel of the launch shape in use; a dict of summed milliseconds
+        (classify_ms and step_ms for the fused shape, bulk_ms and iface_ms for
+        the two-launch shape) and launches_per_step."""
+        t = KernelTimes()
+        check(lib().gp_step_kernel_times(self._h, int(n), ctypes.byref(t)), self._h)
+        return {"classify_ms": t.classify_ms, "step_ms": t.step_ms, "bulk_ms": t.bulk_ms, "iface_ms": t.iface_ms,
+                "launches_per_step": t.launches_per_step, "fused": bool(t.fused)}
 
     def get(self):
         sp, sm = _shapes(self.params)

@@ -111,6 +111,12 @@ class AdjOut(ctypes.Structure):
                 ("ms_forward", c_double), ("ms_reverse", c_double)]
 
 
+class KernelTimes(ctypes.Structure):
+    """gp_kernel_times (include/gp.h)."""
+    _fields_ = [("classify_ms", c_double), ("step_ms", c_double), ("bulk_ms", c_double), ("iface_ms", c_double),
+                ("launches_per_step", c_int), ("fused", c_int)]
+
+
 # Every entry point declared in include/gp.h, with its ctypes signature.
 SIGNATURES = {
     "gp_params_load": (c_int, [POINTER(Params), ctypes.c_char_p]),
@@ -129,6 +135,7 @@ SIGNATURES = {
     "gp_get_stats": (c_int, [c_void_p, POINTER(Stats)]),
     "gp_step_timed": (c_int, [c_void_p, c_long, POINTER(Stats), POINTER(c_double), POINTER(c_double),
                               POINTER(c_double)]),
+    "gp_step_kernel_times": (c_int, [c_void_p, c_long, POINTER(KernelTimes)]),
     "gp_step_noalloc": (c_int, [POINTER(Params), c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     "gp_batch_create": (c_int, [POINTER(c_void_p), c_int, POINTER(Params), POINTER(c_void_p), POINTER(c_void_p),
                                 c_int]),

@@ -39,6 +39,7 @@ static __constant__ gpd::Consts<double> cD;
 extern "C" const char *gp_host_thread_error(void);
 
 #define GP_GRAPH_STEPS 100
+#define GP_GRAPH_CACHE 16     /* captured step sequences kept per batch */
 #define GP_STAGE_BYTES ((size_t)8 << 20)   /* each of a device's two pinned host staging buffers */
 #define GP_STAGE_MAX_DEVICES 64
 
@@ -317,7 +318,8 @@ struct gp_batch {
   int cur;
   long long *ext;               /* running extremes per simulation [nsims][2(N+K)] */
   double *partials, *sums_sim;
-  cudaGraphExec_t graph[2];
+  /* captured step sequences: graphs[(starting parity, steps)], steps <= GP_GRAPH_STEPS */
+  std::map<std::pair<int, long>, cudaGraphExec_t> graphs;
   cudaEvent_t ev[4];
   long long steps;
   std::vector<gp_stats> last;
@@ -357,10 +359,13 @@ static int batch_step_once(gp_batch *b, int want_sums, cudaEvent_t *ev) {
   if (ev) BK(cudaEventRecord(ev[0], b->stream));
   BK(b->L.classify(b->ntiles, b->stream, b->d_desc, b->d_consts, b->d_tsim, b->flags[in], b->flags[out], b->glist,
                    b->blist, b->counters));
-  if (!ev && !want_sums && b->grid_s > 0 && b->shape.fused) {
-    /* one launch for both kinds of tile */
+  if (!want_sums && b->grid_s > 0 && b->shape.fused && (!ev || ev[3] == nullptr)) {
+    /* one launch for both kinds of tile; ev (with ev[3] null): events after
+     * the classification and after the step */
+    if (ev) BK(cudaEventRecord(ev[1], b->stream));
     BK(b->L.step(b->grid_s, b->mul, b->diag, b->stream, b->d_desc, b->d_consts, b->d_tsim, b->blist, b->glist,
                  b->tmaps, in, b->state[in], b->state[out], b->flags[out], b->counters, b->grid_s, st));
+    if (ev) BK(cudaEventRecord(ev[2], b->stream));
     b->cur = out;
     b->steps++;
     return GP_OK;
@@ -426,20 +431,59 @@ static int batch_check_finite(gp_batch *b) {
   return GP_OK;
 }
 
-/* nsteps steps.  Whole chunks of GP_GRAPH_STEPS steps are replayed as CUDA
- * graphs (an even number of steps returns the ping-pong parity to where it
- * started, so one graph per starting parity suffices); the last step runs
- * outside so that it can produce the sums.  With ms_bulk/ms_iface every step
- * runs outside graphs with events around the two kernels. */
+/* Drop every captured graph (the launch shape they were captured with is no
+ * longer the batch's). */
+static void batch_drop_graphs(gp_batch *b) {
+  for (auto &kv : b->graphs) cudaGraphExecDestroy(kv.second);
+  b->graphs.clear();
+}
+
+/* The graph of n steps from the current parity, captured on first use; null
+ * when the cache is full (the caller then launches the steps one by one). */
+static int batch_graph(gp_batch *b, long n, cudaGraphExec_t *out) {
+  *out = nullptr;
+  const auto key = std::make_pair(b->cur, n);
+  auto it = b->graphs.find(key);
+  if (it != b->graphs.end()) {
+    *out = it->second;
+    return GP_OK;
+  }
+  if (b->graphs.size() >= GP_GRAPH_CACHE) return GP_OK;
+  cudaGraph_t gr;
+  BK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+  int rc = GP_OK;
+  const int cur0 = b->cur;
+  for (long i = 0; i < n && rc == GP_OK; i++) rc = batch_step_once(b, 0, nullptr);
+  b->steps -= n; /* captured, not run */
+  b->cur = cur0;
+  cudaError_t ec = cudaStreamEndCapture(b->stream, &gr);
+  if (rc != GP_OK) return rc;
+  if (ec != cudaSuccess) return bfail(b, GP_ECUDA, "graph capture: %s", cudaGetErrorString(ec));
+  cudaGraphExec_t ge;
+  ec = cudaGraphInstantiate(&ge, gr, 0);
+  cudaGraphDestroy(gr);
+  if (ec != cudaSuccess) return bfail(b, GP_ECUDA, "graph instantiate: %s", cudaGetErrorString(ec));
+  b->graphs[key] = ge;
+  *out = ge;
+  return GP_OK;
+}
+
+/* nsteps steps, replayed as CUDA graphs of up to GP_GRAPH_STEPS steps (one
+ * graph per starting ping-pong parity and length, captured on first use);
+ * when statistics are asked for, the last step runs outside a graph so that
+ * it can produce the sums.  While the launch-shape autotuner has candidates
+ * left, whole GP_GRAPH_STEPS chunks time them.  With ms_bulk/ms_iface every
+ * step runs outside graphs with events around the two kernels. */
 static int batch_step_impl(gp_batch *b, long nsteps, gp_stats *stats, double *total_ms, double *ms_bulk,
                            double *ms_iface) {
   const bool split = ms_bulk || ms_iface;
   double tb = 0.0, ti = 0.0;
   if (total_ms) BK(cudaEventRecord(b->ev[3], b->stream));
   long s = 0;
-  while (!split && nsteps - s > GP_GRAPH_STEPS) {
-    const int p = b->cur;
-    if (b->tune_next < b->ncand) {
+  const long graphed = stats ? nsteps - 1 : nsteps;   /* steps that may run inside graphs */
+  while (!split && graphed - s >= 2) {
+    const long n = std::min<long>(GP_GRAPH_STEPS, graphed - s);
+    if (b->tune_next < b->ncand && n == GP_GRAPH_STEPS) {
       /* autotuning: one 100-step chunk per candidate shape, each captured
        * afresh and timed with events; then the fastest is kept */
       b->shape = b->cand[b->tune_next];
@@ -466,6 +510,7 @@ static int batch_step_impl(gp_batch *b, long nsteps, gp_stats *stats, double *to
         for (int i = 1; i < b->ncand; i++)
           if (b->cand_ms[i] < b->cand_ms[best]) best = i;
         b->shape = b->cand[best];
+        batch_drop_graphs(b);   /* captured with a candidate's shape */
         std::lock_guard<std::mutex> lock(g_shapes_mutex);
         g_shapes[b->key] = b->shape;
       }
@@ -473,22 +518,14 @@ static int batch_step_impl(gp_batch *b, long nsteps, gp_stats *stats, double *to
       s += GP_GRAPH_STEPS;
       continue;
     }
-    if (!b->graph[p]) {
-      cudaGraph_t gr;
-      BK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-      int rc = GP_OK;
-      for (int i = 0; i < GP_GRAPH_STEPS && rc == GP_OK; i++) rc = batch_step_once(b, 0, nullptr);
-      b->steps -= GP_GRAPH_STEPS; /* captured, not run */
-      cudaError_t ec = cudaStreamEndCapture(b->stream, &gr);
-      if (rc != GP_OK) return rc;
-      if (ec != cudaSuccess) return bfail(b, GP_ECUDA, "graph capture: %s", cudaGetErrorString(ec));
-      ec = cudaGraphInstantiate(&b->graph[p], gr, 0);
-      cudaGraphDestroy(gr);
-      if (ec != cudaSuccess) return bfail(b, GP_ECUDA, "graph instantiate: %s", cudaGetErrorString(ec));
-    }
-    BK(cudaGraphLaunch(b->graph[p], b->stream));
-    b->steps += GP_GRAPH_STEPS;
-    s += GP_GRAPH_STEPS;
+    cudaGraphExec_t ge = nullptr;
+    int rc = batch_graph(b, n, &ge);
+    if (rc != GP_OK) return rc;
+    if (!ge) break;   /* cache full: the rest one by one */
+    BK(cudaGraphLaunch(ge, b->stream));
+    if (n & 1) b->cur ^= 1;
+    b->steps += n;
+    s += n;
   }
   for (; s < nsteps; s++) {
     int rc = batch_step_once(b, stats != nullptr && s == nsteps - 1, split ? b->ev : nullptr);
@@ -731,10 +768,8 @@ extern "C" {
 void gp_batch_destroy(gp_batch *b) {
   if (!b) return;
   if (b->stream) cudaStreamSynchronize(b->stream);
-  for (int p = 0; p < 2; p++) {
-    if (b->graph[p]) cudaGraphExecDestroy(b->graph[p]);
-    cudaFree(b->state[p]);
-  }
+  batch_drop_graphs(b);
+  for (int p = 0; p < 2; p++) cudaFree(b->state[p]);
   for (int i = 0; i < 4; i++)
     if (b->ev[i]) cudaEventDestroy(b->ev[i]);
   cudaFree(b->dphi);
@@ -1162,6 +1197,36 @@ int gp_step_timed(gp_ctx *c, long nsteps, gp_stats *stats, double *total_ms, dou
   if (!c || nsteps < 0) return fail(c, GP_EINVAL, "gp_step_timed: bad argument");
   c->err[0] = 0;
   return batch_step_impl(c->b, nsteps, stats, total_ms, ms_bulk, ms_iface);
+}
+
+int gp_step_kernel_times(gp_ctx *c, long nsteps, gp_kernel_times *t) {
+  if (!c || nsteps < 1 || !t) return fail(c, GP_EINVAL, "gp_step_kernel_times: bad argument");
+  c->err[0] = 0;
+  gp_batch *b = c->b;
+  memset(t, 0, sizeof *t);
+  const bool fused = b->grid_s > 0 && b->shape.fused;
+  cudaEvent_t ev[4] = {b->ev[0], b->ev[1], b->ev[2], fused ? nullptr : b->ev[3]};
+  for (long i = 0; i < nsteps; i++) {
+    int rc = batch_step_once(b, 0, ev);
+    if (rc != GP_OK) return rc;
+    float x = 0.f, y = 0.f, z = 0.f;
+    BK(cudaEventSynchronize(ev[2]));
+    if (fused) {
+      BK(cudaEventElapsedTime(&x, ev[0], ev[1]));
+      BK(cudaEventElapsedTime(&y, ev[1], ev[2]));
+      t->classify_ms += x;
+      t->step_ms += y;
+    } else {
+      /* two-launch form: ev[0] classify+bulk ev[1] general ev[2] */
+      BK(cudaEventElapsedTime(&z, ev[0], ev[1]));
+      BK(cudaEventElapsedTime(&y, ev[1], ev[2]));
+      t->bulk_ms += z;
+      t->iface_ms += y;
+    }
+  }
+  t->launches_per_step = fused ? 2 : 3;
+  t->fused = fused ? 1 : 0;
+  return batch_check_error(b);
 }
 
 int gp_get_stats(gp_ctx *c, gp_stats *s) {

@@ -197,6 +197,22 @@ int gp_get_stats(gp_ctx *ctx, gp_stats *stats);
 int gp_step_timed(gp_ctx *ctx, long nsteps, gp_stats *stats, double *total_ms,
                   double *ms_bulk, double *ms_iface);
 
+/* Per-kernel device times of nsteps steps launched one by one (no graphs) in
+ * the launch shape the context uses, CUDA events around each launch.  Fused
+ * shape: kf_classify then kf_step (interface tiles, then bulk tiles, in one
+ * launch); two-launch shape: kf_classify + kf_bulk, then kf_general.
+ * Measurement entry point with no counterpart in the reference; the state
+ * advances by nsteps as with gp_step. */
+typedef struct gp_kernel_times {
+  double classify_ms;          /* fused shape: kf_classify, summed over the steps */
+  double step_ms;              /* fused shape: kf_step, summed */
+  double bulk_ms;              /* two-launch shape: kf_classify + kf_bulk, summed */
+  double iface_ms;             /* two-launch shape: kf_general, summed */
+  int launches_per_step;       /* kernels of one step in this shape (2 or 3) */
+  int fused;                   /* 1: fused shape */
+} gp_kernel_times;
+int gp_step_kernel_times(gp_ctx *ctx, long nsteps, gp_kernel_times *t);
+
 /* ---- batches of simulations ------------------------------------------- */
 
 /* Many independent simulations stepped together: grids of different sizes,
