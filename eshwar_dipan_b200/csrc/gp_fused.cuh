@@ -42,6 +42,63 @@ constexpr int RYF = (TX + 2) * (TY + 3);                 /* y-faces around the r
 
 constexpr signed char FLAG_MIXED = -1, FLAG_UNKNOWN = -2;
 
+/* A pair of floats in one 64-bit register pair, for sm_100's packed FP32
+ * arithmetic (add/sub/mul/fma .rn.f32x2: two IEEE single-precision results,
+ * round to nearest, per instruction). */
+typedef unsigned long long f2;
+__device__ __forceinline__ f2 f2pack(float lo, float hi) {
+  f2 r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+  return r;
+}
+__device__ __forceinline__ float f2lo(f2 v) {
+  float lo, hi;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+  return lo;
+}
+__device__ __forceinline__ float f2hi(f2 v) {
+  float lo, hi;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+  return hi;
+}
+__device__ __forceinline__ f2 f2add(f2 a, f2 b) {
+  f2 d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ f2 f2sub(f2 a, f2 b) {
+  f2 d;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ f2 f2mul(f2 a, f2 b) {
+  f2 d;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ f2 f2fma(f2 a, f2 b, f2 c) {
+  f2 d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+/* three-operand max/min (a NaN operand is ignored, as by fmaxf) */
+__device__ __forceinline__ float fmax3f(float a, float b, float c) {
+  float d;
+  asm("max.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+  return d;
+}
+__device__ __forceinline__ float fmin3f(float a, float b, float c) {
+  float d;
+  asm("min.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+  return d;
+}
+/* spacing of the floats at |v| (2^(e-23) for a normal v of exponent e; the
+ * subnormal spacing below) */
+__device__ __forceinline__ float ulpf(float v) {
+  const unsigned e = max(__float_as_uint(v) & 0x7f800000u, 24u << 23);
+  return __uint_as_float(e - (23u << 23));
+}
+
 /* Phase flags of one tile in one state buffer: for the whole tile and for its
  * four two-cell-deep edge bands (top = first two rows, bot = last two rows,
  * left/right = first/last two columns, over the tile's cells inside the
@@ -785,6 +842,54 @@ constexpr size_t bulk_smem_bytes() {
   return (NT / 32) * sizeof(BulkWarpSmem<R, K>) + 128;
 }
 
+/* The FP64 bulk update of one cell (stage row i, column j) of phase p with
+ * every term of the K x K matrices: the expressions of a non-DIAG kernel in
+ * their order (calculate_divergence_concentration.h:43-57 through
+ * functionF_01.h:19-37).  A DIAG kernel calls it, after a tile's rows, for
+ * the rare cells whose result was not finite. */
+template <int K, bool MUL>
+__device__ __forceinline__ void bulk_cell_full_f64(const double *__restrict__ st, int i, int j,
+                                                const Consts<double> *__restrict__ Dp, int p, const double *m,
+                                                double *nm, double *dmu) {
+  constexpr int BW = BulkGeom<double, K>::BW;
+  const Consts<double> &D = *Dp;
+  const double idx = D.inv_dx, idy = D.inv_dy, ddx = D.dx, ddy = D.dy, dt = D.dt;
+  const double cst = D.obstacle ? D.jat_obst : D.jat_well;
+  double divjat = bdiv<MUL>((0.0 - 0.0) * cst, idx, ddx);
+  divjat += bdiv<MUL>((0.0 - 0.0) * cst, idy, ddy);
+#define BM(l, r, c) st[((l) * SH + (r)) * BW + (c)]
+  double cn[K];
+#pragma unroll
+  for (int k = 0; k < K; k++) {
+    double divflux = 0.0;
+#pragma unroll
+    for (int l = 0; l < K; l++) {
+      const double Dv = D.Dbulk[p][k][l];
+      const double dm = (Dv + Dv) * 0.5, c = BM(l, i, j);
+      const double fx = dm * bdiv<MUL>(BM(l, i + 1, j) - c, idx, ddx);
+      const double bx_ = dm * bdiv<MUL>(c - BM(l, i - 1, j), idx, ddx);
+      const double fy = dm * bdiv<MUL>(BM(l, i, j + 1) - c, idy, ddy);
+      const double by_ = dm * bdiv<MUL>(c - BM(l, i, j - 1), idy, ddy);
+      divflux += bdiv<MUL>(fx - bx_, idx, ddx);
+      divflux += bdiv<MUL>(fy - by_, idy, ddy);
+    }
+    double cm = 0.0;   /* c_mu (functionF_01.h:30-37) */
+#pragma unroll
+    for (int l = 0; l < K; l++) cm += D.cmu[p][k][l] * (m[l] - D.E[p][l]);
+    cn[k] = cm + dt * (divflux) - divjat;
+  }
+#undef BM
+#pragma unroll
+  for (int k = 0; k < K; k++) {
+    double sm = D.twoA[p][k] * cn[k] + D.E[p][k];   /* Mu (functionF_01.h:19-29) */
+#pragma unroll
+    for (int l = 0; l < K; l++)
+      if (k != l) sm += D.A[p][k][l] * cn[l];
+    nm[k] = sm;
+    dmu[k] = sm - m[k];
+  }
+}
+
 /* Bulk tiles, one warp per tile.  Warps take contiguous ranges of the bulk
  * list.  Lane 0 issues one TMA box per tile (the K mu planes of the tile with
  * a one-cell halo, rows x0-1..x0+TX) into the warp's next stage while the warp
@@ -926,6 +1031,8 @@ __device__ __forceinline__ void bulk_tiles(const SimDesc *__restrict__ sims, con
   };
   R E[K], twoA[K];
   MatC mc;
+  /* FP32: flux-divergence coefficients of the bulk update (x and y) */
+  f2 CX2[K][K], CY2[K][K];
   /* FP32: the step's part of the rounding key */
   const unsigned skey = sizeof(R) == 4 ? mix32(__ldg(st.round_step) * 0x9e3779b9u + 0x632be5abu) : 0u;
 
@@ -983,6 +1090,22 @@ __device__ __forceinline__ void bulk_tiles(const SimDesc *__restrict__ sims, con
       }
       /* a DIAG kernel keeps only the diagonals live */
       load_mat(mc, D, p);
+      if constexpr (sizeof(R) == 4) {
+        /* dt * sum_l (dmu/dc)_kl D_lm / dx^2 (and / dy^2), from the FP64
+         * constants, rounded once */
+        const double dtd = (double)D.dt, ix = 1.0 / (double)D.dx, iy = 1.0 / (double)D.dy;
+#pragma unroll
+        for (int k = 0; k < K; k++)
+#pragma unroll
+          for (int m = 0; m < K; m++) {
+            double sv = 0.0;
+#pragma unroll
+            for (int l = 0; l < K; l++) sv += D.muc64[p][k][l] * (double)D.Dbulk[p][l][m];
+            const float cx = (float)(sv * dtd * ix * ix), cy = (float)(sv * dtd * iy * iy);
+            CX2[k][m] = f2pack(cx, cx);
+            CY2[k][m] = f2pack(cy, cy);
+          }
+      }
     }
     BulkStage<R, K> &sg = ws.st[b];
     const int rows = min(TX, g.mx - x0), ncols = min(TY, g.my - y0);
@@ -1019,153 +1142,277 @@ __device__ __forceinline__ void bulk_tiles(const SimDesc *__restrict__ sims, con
     }
     R *phin = next + off_state;
     R *mun = phin + (long long)N * g.plane;
-    const int y = y0 + lane, j = lane + 1 + CO;
-    const bool yvalid = y < g.my;
+    /* lane 16h + q steps tile rows 4h..4h+3 at columns 2q and 2q+1: stage
+     * columns c and c+1 (c = 2q + 1 + CO, so the pair is 16-byte aligned in
+     * FP64 and 8-byte aligned in FP32); the y-face between the two cells is
+     * computed once, and the x-face below a row is carried to the next */
+    const int hh = lane >> 4, qq = lane & 15;
+    const int jc = 2 * qq, c = jc + 1 + CO, y = y0 + jc;
+    const bool v0 = y < g.my, v1 = y + 1 < g.my;
+    const int r0 = 4 * hh, nr = max(0, min(4, rows - r0));
     double acc[SUMS ? NS : 1];
 #pragma unroll
     for (int f = 0; f < (SUMS ? NS : 1); f++) acc[f] = 0.0;
-    /* divergence of the diffusive flux of component k at row i (all K
-     * gradients, the reference's expressions in its order) */
-    auto divflux_full = [&](int k, int i, const MatC &mt) {
-      R divflux = R(0.0);
+    /* the progress sums of one new cell of phase p */
+    auto sum_cell = [&](const R (&nm)[K], const double (&dmu)[K]) {
+      if constexpr (SUMS) {
+        R nph[N];
 #pragma unroll
-      for (int l = 0; l < K; l++) {
-        const R dm = mt.dm[k][l], c = sg.M[l][i][j];
-        R fx = dm * bdiv<MUL>(sg.M[l][i + 1][j] - c, idx, ddx);
-        R bx_ = dm * bdiv<MUL>(c - sg.M[l][i - 1][j], idx, ddx);
-        R fy = dm * bdiv<MUL>(sg.M[l][i][j + 1] - c, idy, ddy);
-        R by_ = dm * bdiv<MUL>(c - sg.M[l][i][j - 1], idy, ddy);
-        divflux += bdiv<MUL>(fx - bx_, idx, ddx);
-        divflux += bdiv<MUL>(fy - by_, idy, ddy);
+        for (int a = 0; a < N; a++) nph[a] = a == p ? R(1.0) : R(0.0);
+#pragma unroll
+        for (int k = 0; k < K; k++) acc[N + k] += dmu[k] * dmu[k];
+#pragma unroll
+        for (int a = 0; a < N; a++) acc[N + K + a] += (double)nph[a];
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+          R comp = R(0.0);
+#pragma unroll
+          for (int b2 = 0; b2 < N; b2++) comp += c_mu<R, K>(D, nm, b2, k) * h<R, N>(nph, b2);
+          acc[2 * N + K + k] += (double)comp;
+        }
+        bool bad = false;
+#pragma unroll
+        for (int k = 0; k < K; k++) bad |= !isfinite(nm[k]);
+        acc[NS - 1] += bad ? 1.0 : 0.0;
       }
-      return divflux;
     };
-    /* new mu of a cell from its old mu and the flux divergences; `all`
-     * (std::true_type) keeps the off-diagonal terms in a DIAG kernel */
-    auto commit_mu = [&](auto all, const MatC &mt, const R (&m)[K], const R (&df)[K], int x, R (&nm)[K],
-                         double (&dmu)[K]) {
-      constexpr bool SKIP = DIAG && !decltype(all)::value;
+    /* FP64: the new mu of a cell from its old mu and the flux divergences,
+     * every term of the K x K matrices (non-DIAG kernels) */
+    auto commit_mu = [&](const MatC &mt, const R (&m)[K], const R (&df)[K], R (&nm)[K], double (&dmu)[K]) {
       R cn[K];
 #pragma unroll
       for (int k = 0; k < K; k++) {
-        if constexpr (sizeof(R) == 8) {
-          R cm = R(0.0);   /* c_mu (functionF_01.h:30-37) */
+        R cm = R(0.0);   /* c_mu (functionF_01.h:30-37) */
 #pragma unroll
-          for (int l = 0; l < K; l++)
-            if (!SKIP || l == k) cm += mt.cmu[k][l] * (m[l] - E[l]);
-          cn[k] = cm + dt * (df[k]) - divjat;
-        } else {
-          cn[k] = dt * df[k] - divjat;
-        }
+        for (int l = 0; l < K; l++) cm += mt.cmu[k][l] * (m[l] - E[l]);
+        cn[k] = cm + dt * (df[k]) - divjat;
       }
-      if constexpr (sizeof(R) == 8) {
 #pragma unroll
-        for (int k = 0; k < K; k++) {
-          R sm = twoA[k] * cn[k] + E[k];   /* Mu (functionF_01.h:19-29) */
-#pragma unroll
-          for (int l = 0; l < K; l++)
-            if (!SKIP && k != l) sm += mt.A[k][l] * cn[l];
-          nm[k] = sm;
-          dmu[k] = (double)nm[k] - (double)m[k];
-        }
-      } else {
-        /* mu += (dmu/dc) dc of the pure phase in float (no c -> mu round
-         * trip), the sum rounded stochastically from its exact TwoSum
-         * split, 16 random bits per field from one hash of the cell */
-        const unsigned key = mix32(skey ^ ((unsigned)x * 0x85ebca6bu + (unsigned)y * 0xc2b2ae35u));
-#pragma unroll
-        for (int k = 0; k < K; k++) {
-          R sdm = R(0.0);
-#pragma unroll
-          for (int l = 0; l < K; l++)
-            if (!SKIP || l == k) sdm += mt.muc[k][l] * cn[l];
-          dmu[k] = (double)sdm;
-          nm[k] = (R)add_stochastic((float)m[k], (float)sdm, (key >> (16 * (k & 1))) & 0xffffu);
-        }
-      }
-    };
-    if (yvalid) {
-      /* x-face fluxes dm*(mu(i) - mu(i-1))/dx between rows i-1 and i: the
-       * forward flux of row i-1 is the backward flux of row i (the same
-       * expression on the same operands), so it is carried from row to row */
-      R fxp[K][K];
-#pragma unroll
-      for (int k = 0; k < K; k++)
+      for (int k = 0; k < K; k++) {
+        R sm = twoA[k] * cn[k] + E[k];   /* Mu (functionF_01.h:19-29) */
 #pragma unroll
         for (int l = 0; l < K; l++)
-          if (!DIAG || l == k) fxp[k][l] = mc.dm[k][l] * bdiv<MUL>(sg.M[l][1][j] - sg.M[l][0][j], idx, ddx);
-#pragma unroll 2
-      for (int i = 1; i <= rows; i++) {
-        const int x = x0 + i - 1;
-        R m[K], df[K], nm[K];
-        double dmu[K];
+          if (k != l) sm += mt.A[k][l] * cn[l];
+        nm[k] = sm;
+        dmu[k] = (double)nm[k] - (double)m[k];
+      }
+    };
+    if (v0 && nr > 0) {
+      if constexpr (sizeof(R) == 8) {
+        /* ---- FP64: the reference's bulk expressions (update_tile's uniform
+         * path) in their order, two cells at a time */
+        double2 P[K], FXP[K][K];
+        unsigned redo = 0;   /* DIAG: bit 2 rr + e, cell e of row rr to redo with every term */
 #pragma unroll
-        for (int k = 0; k < K; k++) m[k] = sg.M[k][i][j];
-        /* the bulk expressions of the general path (update_tile's uniform
-         * path); DIAG: the off-diagonal D, c_mu and A of every phase are
-         * zero, their terms (+-0 added to sums that are never -0) are left
-         * out */
+        for (int l = 0; l < K; l++) {
+          const double2 pp = *reinterpret_cast<const double2 *>(&sg.M[l][r0][c]);
+          P[l] = *reinterpret_cast<const double2 *>(&sg.M[l][r0 + 1][c]);
+          const R g0 = bdiv<MUL>(P[l].x - pp.x, idx, ddx), g1 = bdiv<MUL>(P[l].y - pp.y, idx, ddx);
 #pragma unroll
-        for (int k = 0; k < K; k++) {
-          R divflux = R(0.0);
-#pragma unroll
-          for (int l = 0; l < K; l++) {
-            if (DIAG && l != k) continue;
-            const R dm = mc.dm[k][l], c = m[l];
-            const R fx = dm * bdiv<MUL>(sg.M[l][i + 1][j] - c, idx, ddx);
-            const R fy = dm * bdiv<MUL>(sg.M[l][i][j + 1] - c, idy, ddy);
-            const R by_ = dm * bdiv<MUL>(c - sg.M[l][i][j - 1], idy, ddy);
-            divflux += bdiv<MUL>(fx - fxp[k][l], idx, ddx);
-            divflux += bdiv<MUL>(fy - by_, idy, ddy);
-            fxp[k][l] = fx;
-          }
-          df[k] = divflux;
+          for (int k = 0; k < K; k++)
+            if (!DIAG || l == k) FXP[k][l] = make_double2(mc.dm[k][l] * g0, mc.dm[k][l] * g1);
         }
-        commit_mu(std::false_type(), mc, m, df, x, nm, dmu);
-        if constexpr (DIAG) {
+        for (int rr = 0; rr < nr; rr++) {
+          const int i = r0 + 1 + rr, x = x0 + i - 1;
+          double2 Pn[K];
+          R m0[K], m1[K], n0[K], n1[K];
+          double d0[K], d1[K];
+#pragma unroll
+          for (int k = 0; k < K; k++) { m0[k] = P[k].x; m1[k] = P[k].y; }
+          if constexpr (DIAG) {
+            /* only the diagonal terms: one component at a time */
+#pragma unroll
+            for (int k = 0; k < K; k++) {
+              Pn[k] = *reinterpret_cast<const double2 *>(&sg.M[k][i + 1][c]);
+              const R L = sg.M[k][i][c - 1], Rn = sg.M[k][i][c + 2];
+              const R dm = mc.dm[k][k];
+              const R fx0 = dm * bdiv<MUL>(Pn[k].x - P[k].x, idx, ddx);
+              const R fx1 = dm * bdiv<MUL>(Pn[k].y - P[k].y, idx, ddx);
+              const R fl = dm * bdiv<MUL>(P[k].x - L, idy, ddy);
+              const R fm = dm * bdiv<MUL>(P[k].y - P[k].x, idy, ddy);
+              const R fr = dm * bdiv<MUL>(Rn - P[k].y, idy, ddy);
+              R a0 = R(0.0), a1 = R(0.0);
+              a0 += bdiv<MUL>(fx0 - FXP[k][k].x, idx, ddx);
+              a0 += bdiv<MUL>(fm - fl, idy, ddy);
+              a1 += bdiv<MUL>(fx1 - FXP[k][k].y, idx, ddx);
+              a1 += bdiv<MUL>(fr - fm, idy, ddy);
+              FXP[k][k] = make_double2(fx0, fx1);
+              /* c_mu, the bulk update and Mu (functionF_01.h:19-37) of the
+               * pure phase, diagonal terms only */
+              R cm0 = R(0.0), cm1 = R(0.0);
+              cm0 += mc.cmu[k][k] * (m0[k] - E[k]);
+              cm1 += mc.cmu[k][k] * (m1[k] - E[k]);
+              const R cn0 = cm0 + dt * (a0) - divjat, cn1 = cm1 + dt * (a1) - divjat;
+              n0[k] = twoA[k] * cn0 + E[k];
+              n1[k] = twoA[k] * cn1 + E[k];
+              d0[k] = (double)n0[k] - (double)m0[k];
+              d1[k] = (double)n1[k] - (double)m1[k];
+            }
+          } else {
+            R gx0[K], gx1[K], gl[K], gm[K], gr[K];
+#pragma unroll
+            for (int l = 0; l < K; l++) {
+              Pn[l] = *reinterpret_cast<const double2 *>(&sg.M[l][i + 1][c]);
+              const R L = sg.M[l][i][c - 1], Rn = sg.M[l][i][c + 2];
+              gx0[l] = bdiv<MUL>(Pn[l].x - P[l].x, idx, ddx);
+              gx1[l] = bdiv<MUL>(Pn[l].y - P[l].y, idx, ddx);
+              gl[l] = bdiv<MUL>(P[l].x - L, idy, ddy);
+              gm[l] = bdiv<MUL>(P[l].y - P[l].x, idy, ddy);
+              gr[l] = bdiv<MUL>(Rn - P[l].y, idy, ddy);
+            }
+            R df0[K], df1[K];
+#pragma unroll
+            for (int k = 0; k < K; k++) {
+              R a0 = R(0.0), a1 = R(0.0);
+#pragma unroll
+              for (int l = 0; l < K; l++) {
+                const R dm = mc.dm[k][l];
+                const R fx0 = dm * gx0[l], fx1 = dm * gx1[l];
+                const R fl = dm * gl[l], fm = dm * gm[l], fr = dm * gr[l];
+                a0 += bdiv<MUL>(fx0 - FXP[k][l].x, idx, ddx);
+                a0 += bdiv<MUL>(fm - fl, idy, ddy);
+                a1 += bdiv<MUL>(fx1 - FXP[k][l].y, idx, ddx);
+                a1 += bdiv<MUL>(fr - fm, idy, ddy);
+                FXP[k][l] = make_double2(fx0, fx1);
+              }
+              df0[k] = a0;
+              df1[k] = a1;
+            }
+            commit_mu(mc, m0, df0, n0, d0);
+            commit_mu(mc, m1, df1, n1, d1);
+          }
           /* a left-out term is +-0 only when the values it multiplies are
-           * finite, and they are when every new mu is; otherwise the cell
-           * is redone with every term */
-          bool fin = true;
+           * finite, and they are when every new mu is; otherwise (DIAG) the
+           * cell is redone with every term after the rows (its extremes and
+           * sums are taken then) */
+          bool f0 = true, f1 = v1;
+          if constexpr (DIAG) {
 #pragma unroll
-          for (int k = 0; k < K; k++) fin &= fabs(nm[k]) < R(INFINITY);
-          if (!fin) {
-            MatC fc;   /* every term, the constants read again */
-            load_mat(fc, D, p);
-#pragma unroll
-            for (int k = 0; k < K; k++) df[k] = divflux_full(k, i, fc);
-            commit_mu(std::true_type(), fc, m, df, x, nm, dmu);
+            for (int k = 0; k < K; k++) { f0 &= fabs(n0[k]) < R(INFINITY); f1 &= fabs(n1[k]) < R(INFINITY); }
+            redo |= (f0 ? 0u : 1u) << (2 * rr);
+            redo |= (v1 && !f1 ? 2u : 0u) << (2 * rr);
           }
-        }
-        const long long o = (long long)x * g.pitch + y;
-#pragma unroll
-        for (int k = 0; k < K; k++) {
-          mun[k * g.plane + o] = nm[k];
-          if (nm[k] == nm[k]) { emax[k] = fmax(emax[k], nm[k]); emin[k] = fmin(emin[k], nm[k]); }
-        }
-        if (have != p) {
-#pragma unroll
-          for (int a = 0; a < N; a++) phin[a * g.plane + o] = a == p ? R(1.0) : R(0.0);
-        }
-        if constexpr (SUMS) {
-          R nph[N];
-#pragma unroll
-          for (int a = 0; a < N; a++) nph[a] = a == p ? R(1.0) : R(0.0);
-#pragma unroll
-          for (int k = 0; k < K; k++) acc[N + k] += dmu[k] * dmu[k];
-#pragma unroll
-          for (int a = 0; a < N; a++) acc[N + K + a] += (double)nph[a];
+          const long long o = (long long)x * g.pitch + y;
 #pragma unroll
           for (int k = 0; k < K; k++) {
-            R comp = R(0.0);
-#pragma unroll
-            for (int b2 = 0; b2 < N; b2++) comp += c_mu<R, K>(D, nm, b2, k) * h<R, N>(nph, b2);
-            acc[2 * N + K + k] += (double)comp;
+            if (v1) *reinterpret_cast<double2 *>(mun + k * g.plane + o) = make_double2(n0[k], n1[k]);
+            else mun[k * g.plane + o] = n0[k];
+            /* NaN is ignored by fmax/fmin; a cell to be redone is left out */
+            const R x0 = f0 ? n0[k] : R(NAN), x1 = f1 ? n1[k] : R(NAN);
+            emax[k] = fmax(emax[k], fmax(x0, x1));
+            emin[k] = fmin(emin[k], fmin(x0, x1));
           }
-          bool bad = false;
+          if (have != p) {
 #pragma unroll
-          for (int k = 0; k < K; k++) bad |= !isfinite(nm[k]);
-          acc[NS - 1] += bad ? 1.0 : 0.0;
+            for (int a = 0; a < N; a++) {
+              const R v = a == p ? R(1.0) : R(0.0);
+              if (v1) *reinterpret_cast<double2 *>(phin + a * g.plane + o) = make_double2(v, v);
+              else phin[a * g.plane + o] = v;
+            }
+          }
+          if (f0) sum_cell(n0, d0);
+          if (f1) sum_cell(n1, d1);
+#pragma unroll
+          for (int l = 0; l < K; l++) P[l] = Pn[l];
+        }
+        if constexpr (DIAG) {
+          while (redo) {
+            const int bit = __ffs(redo) - 1;
+            redo &= redo - 1;
+            const int i = r0 + 1 + (bit >> 1), cc = c + (bit & 1), x = x0 + i - 1;
+            R m[K], nm[K];
+            double dmu[K];
+#pragma unroll
+            for (int k = 0; k < K; k++) m[k] = sg.M[k][i][cc];
+            bulk_cell_full_f64<K, MUL>(&sg.M[0][0][0], i, cc, &D, p, m, nm, dmu);
+            const long long o = (long long)x * g.pitch + y + (bit & 1);
+#pragma unroll
+            for (int k = 0; k < K; k++) {
+              mun[k * g.plane + o] = nm[k];
+              emax[k] = fmax(emax[k], nm[k]);
+              emin[k] = fmin(emin[k], nm[k]);
+            }
+            sum_cell(nm, dmu);
+          }
+        }
+      } else {
+        /* ---- FP32: the new mu of a bulk cell is mu + sum_m (CX[k][m] lapx(mu_m)
+         * + CY[k][m] lapy(mu_m)) -- the flux divergence of the pure phase's
+         * constant D times dt and dmu/dc folded into one coefficient per
+         * direction -- in packed f32x2 arithmetic on the cell pair, rounded
+         * stochastically by dithering: RN(mu + (s + w ulp(mu))) with w
+         * uniform in [-1/2, 1/2) takes the upper neighbour with probability
+         * equal to the fraction of the ulp. */
+        f2 P[K], DXP[K];
+#pragma unroll
+        for (int m = 0; m < K; m++) {
+          const f2 pp = *reinterpret_cast<const f2 *>(&sg.M[m][r0][c]);
+          P[m] = *reinterpret_cast<const f2 *>(&sg.M[m][r0 + 1][c]);
+          DXP[m] = f2sub(P[m], pp);
+        }
+        unsigned rng = mix32(skey ^ ((unsigned)(x0 + r0) * 0x85ebca6bu + (unsigned)y * 0xc2b2ae35u));
+        for (int rr = 0; rr < nr; rr++) {
+          const int i = r0 + 1 + rr, x = x0 + i - 1;
+          f2 Pn[K], LX[K], LY[K];
+#pragma unroll
+          for (int m = 0; m < K; m++) {
+            Pn[m] = *reinterpret_cast<const f2 *>(&sg.M[m][i + 1][c]);
+            const float L = (float)sg.M[m][i][c - 1], Rn = (float)sg.M[m][i][c + 2];
+            const f2 dxn = f2sub(Pn[m], P[m]);
+            LX[m] = f2sub(dxn, DXP[m]);
+            DXP[m] = dxn;
+            const float px = f2lo(P[m]), py = f2hi(P[m]);
+            const f2 o = f2sub(f2pack(px, Rn), f2pack(L, py));   /* (yl, yr) */
+            const float ym = __fsub_rn(py, px);
+            LY[m] = f2sub(f2pack(ym, f2hi(o)), f2pack(f2lo(o), ym));
+          }
+          const long long o = (long long)x * g.pitch + y;
+          R n0[K], n1[K];
+          double d0[K], d1[K];
+#pragma unroll
+          for (int k = 0; k < K; k++) {
+            f2 sdm = f2mul(CY2[k][k], LY[k]);
+            sdm = f2fma(CX2[k][k], LX[k], sdm);
+            if constexpr (!DIAG) {
+#pragma unroll
+              for (int m = 0; m < K; m++) {
+                if (m == k) continue;
+                sdm = f2fma(CY2[k][m], LY[m], sdm);
+                sdm = f2fma(CX2[k][m], LX[m], sdm);
+              }
+            }
+            const float m0 = f2lo(P[k]), m1 = f2hi(P[k]);
+            rng = rng * 1664525u + 1013904223u;
+            const float w0 = __uint_as_float(0x3f800000u | (rng >> 9)) - 1.5f;
+            rng = rng * 1664525u + 1013904223u;
+            const float w1 = __uint_as_float(0x3f800000u | (rng >> 9)) - 1.5f;
+            const f2 nm = f2add(P[k], f2fma(f2pack(w0, w1), f2pack(ulpf(m0), ulpf(m1)), sdm));
+            n0[k] = f2lo(nm);
+            n1[k] = f2hi(nm);
+            d0[k] = (double)f2lo(sdm);
+            d1[k] = (double)f2hi(sdm);
+            if (v1) {
+              *reinterpret_cast<f2 *>(mun + k * g.plane + o) = nm;
+              emax[k] = fmax3f(emax[k], n0[k], n1[k]);
+              emin[k] = fmin3f(emin[k], n0[k], n1[k]);
+            } else {
+              mun[k * g.plane + o] = n0[k];
+              emax[k] = fmaxf(emax[k], n0[k]);
+              emin[k] = fminf(emin[k], n0[k]);
+            }
+          }
+          if (have != p) {
+#pragma unroll
+            for (int a = 0; a < N; a++) {
+              const R v = a == p ? R(1.0) : R(0.0);
+              if (v1) *reinterpret_cast<f2 *>(phin + a * g.plane + o) = f2pack(v, v);
+              else phin[a * g.plane + o] = v;
+            }
+          }
+          sum_cell(n0, d0);
+          if (v1) sum_cell(n1, d1);
+#pragma unroll
+          for (int m = 0; m < K; m++) P[m] = Pn[m];
         }
       }
     }

@@ -16,6 +16,12 @@
  *     (utility_functions.h:880-891) and crash the reference at random;
  *   - no VTK files are written unless asked for (mode "vtk");
  *   - the state can be loaded from a raw binary file instead of filled.
+ * Mode "main" runs the sequence of the reference's main() (microsim_gp.c:48-150)
+ * with the reference's own routines: fill or read the restart file
+ * DATA/NAME_<STARTTIME>.vtk, boundary copies, the t=0 file, NSMOOTH-1
+ * smoothing sweeps, then NTIMESTEPS steps writing DATA/NAME_<t>.vtk and a
+ * DATA/shift.dat line every SAVET steps and the progress record every
+ * TRACK_PROGRESS steps on stdout (isothermal, no moving frame).
  *
  * Usage:
  *   gp_ref_harness IN FILL run   NSMOOTH NSTEPS OUT.bin   (NSMOOTH<0: from IN)
@@ -23,6 +29,7 @@
  *   gp_ref_harness IN FILL time  NSTEPS                   (prints seconds)
  *   gp_ref_harness IN FILL consts OUT.txt
  *   gp_ref_harness IN FILL vtk   NSTEPS NAME              (reference writer)
+ *   gp_ref_harness IN FILL main  NAME                     (main()'s flow: see below)
  *
  * OUT.bin layout (little endian): "GPRF", int32 rows_x, rows_y, N, K, then
  * float64 phi[N][rows_x][rows_y], mu[K][..], dphi[N][..], then the reference's
@@ -260,6 +267,49 @@ int main(int argc, char *argv[]) {
     time_steps(atol(argv[4]));
     if (ASCII) writetofile_serial2D(gridinfo, av, atol(argv[4]));
     else writetofile_serial2D_binary(gridinfo, av, atol(argv[4]));
+  } else if (strcmp(mode, "main") == 0 && argc == 5) {
+    char *av[4];
+    FILE *fs;
+    av[0] = argv[0]; av[1] = argv[1]; av[2] = argv[2]; av[3] = argv[4];
+    mkdir("DATA", 0777);
+    if ((STARTTIME == 0) && (RESTART == 0)) {
+      fill(argv);
+    } else {
+      if (ASCII) readfromfile_serial2D(gridinfo, av, STARTTIME);
+      else readfromfile_serial2D_binary(gridinfo, av, STARTTIME);
+      init_propertymatrices(T);
+    }
+    apply_boundary_conditions(0);
+    if ((RESTART == 0) || (STARTTIME == 0)) {
+      if (ASCII == 0) writetofile_serial2D_binary(gridinfo, av, 0);
+      else writetofile_serial2D(gridinfo, av, 0);
+    }
+    smooth_steps(nsmooth);
+    for (t = 1; t <= ntimesteps; t++) {
+      solverloop_phasefield(start, end);
+      apply_boundary_conditions(0);
+      solverloop_concentration(start, end);
+      apply_boundary_conditions(0);
+      if (t % saveT == 0) {
+        if (ASCII == 0) writetofile_serial2D_binary(gridinfo, av, t + STARTTIME);
+        else writetofile_serial2D(gridinfo, av, t + STARTTIME);
+        fs = fopen("DATA/shift.dat", "a");
+        if (fs) {
+          fprintf(fs, "%ld %ld\n", t + STARTTIME, shift_OFFSET + shift_position);
+          fclose(fs);
+        }
+      }
+      if (t % time_output == 0) {
+        fprintf(stdout, "Time=%le\n", t * deltat);
+        for (b = 0; b < NUMPHASES; b++)
+          fprintf(stdout, "%*s, Max = %le, Min = %le, Relative_Change=%le\n", max_length, Phases[b],
+                  global_max_min.phi_max[b], global_max_min.phi_min[b], sqrt(global_max_min.rel_change_phi[b]));
+        for (k = 0; k < NUMCOMPONENTS - 1; k++)
+          fprintf(stdout, "%*s, Max = %le, Min = %le, Relative_Change=%le\n", max_length, Components[k],
+                  global_max_min.mu_max[k], global_max_min.mu_min[k], sqrt(global_max_min.rel_change_mu[k]));
+        fprintf(stdout, "\n");
+      }
+    }
   } else {
     fprintf(stderr, "bad arguments for mode %s\n", mode);
     return 2;

@@ -62,8 +62,9 @@ def test_long_run_bitwise(tmp_path, name, scale, chunks):
         ost = o.stats()
         for k in ("phi_max", "phi_min", "mu_max", "mu_min"):
             assert st[k] == ost[k], k
+        # the sums run in another order on the GPU: about n*eps relative
         for k in ("rel_change_phi", "rel_change_mu", "phi_sum", "comp_sum"):
-            np.testing.assert_allclose(st[k], ost[k], rtol=1e-12, atol=1e-300, err_msg=k)
+            np.testing.assert_allclose(st[k], ost[k], rtol=1e-10, atol=1e-300, err_msg=k)
     # the interface moved: the run exercises the interface tiles throughout
     solid = ph[:-1].sum()
     assert solid > 0 and not np.all((ph == 0) | (ph == 1))
