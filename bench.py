@@ -64,9 +64,9 @@ PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 NCU_TRAFFIC = {"cfg2": 116.6e6}
 
 # steps run untimed before the warm-up: the launch-shape autotuner times one
-# 100-step chunk per candidate shape (at most four), then the chosen shape's
+# 100-step chunk per candidate shape (at most five), then the chosen shape's
 # 100-step graph is captured
-PREP_STEPS = 500
+PREP_STEPS = 600
 
 
 def cpu_info():

@@ -272,6 +272,7 @@ static int fail(gp_ctx *c, int code, const char *fmt, ...) {
 struct LaunchShape {
   bool fused;        /* kf_step (one launch) rather than kf_bulk + kf_general */
   int bch_max, bch_div;
+  bool mixed;        /* kf_step: odd CTAs start with bulk tiles, even ones with interface tiles */
 };
 /* batches that share these tune alike: the first one's choice is kept for
  * the process */
@@ -297,8 +298,8 @@ struct gp_batch {
   bool diag;                    /* off-diagonal D, c_mu, A all zero and no E is -0, in every simulation */
   int mbar_tries;               /* kf_bulk's polls of a box barrier before it reports an error */
   LaunchShape shape;            /* how a step is launched (tuned on the first graph chunks) */
-  LaunchShape cand[4];          /* the candidates */
-  float cand_ms[4];
+  LaunchShape cand[6];          /* the candidates */
+  float cand_ms[6];
   int ncand, tune_next;         /* tuning is over when tune_next == ncand */
   ShapeKey key;
   unsigned tma_extra;           /* 0; a test sets more (GP_TEST_TMA_SHORTFALL) to make the boxes never complete */
@@ -354,6 +355,7 @@ static int batch_step_once(gp_batch *b, int want_sums, cudaEvent_t *ev) {
   st.mbar_tries = b->mbar_tries;
   st.tma_extra = b->tma_extra;
   st.bch_max = b->shape.bch_max;
+  st.mixed = b->shape.mixed ? 1 : 0;
   st.bch_div = b->shape.bch_div;
   const int in = b->cur, out = b->cur ^ 1;
   if (ev) BK(cudaEventRecord(ev[0], b->stream));
@@ -928,12 +930,14 @@ int gp_batch_create(gp_batch **out, int nsims, const gp_params *params, const do
     int lg = 0;
     while ((1 << lg) < nt) lg++;
     b->key = ShapeKey{N, K, b->aniso, (int)b->elem, lg};
-    const LaunchShape fused16 = {true, 16, 2}, fused8 = {true, 8, 2}, fused16q = {true, 16, 4}, two = {false, 16, 2};
+    const LaunchShape fused16 = {true, 16, 2, false}, fused8 = {true, 8, 2, false}, mixed16 = {true, 16, 2, true},
+                      mixed8 = {true, 8, 2, true}, two = {false, 16, 2, false};
     b->ncand = 0;
     if (b->grid_s > 0) {
       b->cand[b->ncand++] = fused16;
       b->cand[b->ncand++] = fused8;
-      b->cand[b->ncand++] = fused16q;
+      b->cand[b->ncand++] = mixed16;
+      b->cand[b->ncand++] = mixed8;
     }
     b->cand[b->ncand++] = two;
     b->shape = b->cand[0];

@@ -247,6 +247,9 @@ struct GenSmem {
   R M[K][SS];              /* mu, one-cell halo, origin (x0-1, y0-1)  */
   R DP[N][SS];             /* delta-phi of the ring region (same origin as M) */
   unsigned char ACT[SS];   /* active phases of each ring cell (bit a) */
+  short LIST[SS];          /* ring cells with an active phase, in no particular order */
+  short FLIST[RXF + RYF];  /* anisotropy faces those cells read */
+  int nlist, nflist;
   union {
     R T[NP<N>::v][4][RXF + RYF];   /* anisotropy face terms of the ring region */
     struct {
@@ -508,8 +511,12 @@ __device__ __forceinline__ TileFlags general_tile(const CT &D, const Grid &g, co
   }
   __syncthreads();
 
-  /* ---- active phases of the ring cells (interior plus ring: x <= mx, y <= my) */
-  bool any = false;
+  /* ---- active phases of the ring cells (interior plus ring: x <= mx, y <= my).
+   * A cell with no active phase gets its delta-phi here (no phase active:
+   * 0, then the projection's clamp of a negative phi; outside the needed
+   * region: 0); the others go on a list, so that the expensive delta-phi
+   * work is spread over every thread of the CTA wherever the active cells
+   * lie in the tile. */
   for (int e = threadIdx.x; e < SS; e += NT) {
     const int ri = e / SW, rj = e - ri * SW, i = ri + 1, j = rj + 1;
     const bool vd = (x0 - 1 + ri <= g.mx) && (y0 - 1 + rj <= g.my);
@@ -525,40 +532,65 @@ __device__ __forceinline__ TileFlags general_tile(const CT &D, const Grid &g, co
     }
     if (!vd) mask = 0;
     sm.ACT[e] = (unsigned char)mask;
-    any |= mask != 0;
-  }
-  const bool blockact = __syncthreads_or(any);
-  if (ANISO && blockact) {
-    /* only the faces of active ring cells are read by ring_dphi */
-    for (int e = threadIdx.x; e < RXF + RYF; e += NT) {
-      if (e < RXF) {
-        const int fi = e / (TY + 2), fj = e - fi * (TY + 2) + 1;
-        /* ring cells (fi-1, fj-1) and (fi, fj-1) */
-        const bool need = (fi >= 1 && sm.ACT[LI(fi - 1, fj - 1)]) || (fi < SH && sm.ACT[LI(fi, fj - 1)]);
-        if (need) ring_face_terms<R, N>(D, sm.P, sm.w.T, true, fi, fj, e);
-      } else {
-        const int f = e - RXF, fi = f / (TY + 3) + 1, fj = f - (fi - 1) * (TY + 3);
-        /* ring cells (fi-1, fj-1) and (fi-1, fj) */
-        const bool need = (fj >= 1 && sm.ACT[LI(fi - 1, fj - 1)]) || (fj < SW && sm.ACT[LI(fi - 1, fj)]);
-        if (need) ring_face_terms<R, N>(D, sm.P, sm.w.T, false, fi, fj, e);
+    if (mask) {
+      sm.LIST[atomicAdd(&sm.nlist, 1)] = (short)e;
+    } else {
+#pragma unroll
+      for (int a = 0; a < N; a++) {
+        R d = R(0.0);
+        if (vd) {
+          const R ph = sm.P[a][L2I(i, j)];
+          if ((ph + d) < R(0.0)) d += fabs(d + ph);
+        }
+        sm.DP[a][e] = d;
       }
     }
   }
   __syncthreads();
-  for (int e = threadIdx.x; e < SS; e += NT) {
-    const int ri = e / SW, rj = e - ri * SW;
-    const bool vd = (x0 - 1 + ri <= g.mx) && (y0 - 1 + rj <= g.my);
-    R d[N];
-    if (vd) {
-      ring_dphi<R, N, K, ANISO>(D, sm, ri, rj, sm.ACT[e], d);
-    } else {
-#pragma unroll
-      for (int a = 0; a < N; a++) d[a] = R(0.0);
+  const int nact = sm.nlist;
+  if (ANISO && nact > 0) {
+    /* only the faces of active ring cells are read by ring_dphi: list them,
+     * then compute them spread over the CTA */
+    for (int e = threadIdx.x; e < RXF + RYF; e += NT) {
+      bool need;
+      if (e < RXF) {
+        const int fi = e / (TY + 2), fj = e - fi * (TY + 2) + 1;
+        /* ring cells (fi-1, fj-1) and (fi, fj-1) */
+        need = (fi >= 1 && sm.ACT[LI(fi - 1, fj - 1)]) || (fi < SH && sm.ACT[LI(fi, fj - 1)]);
+      } else {
+        const int f = e - RXF, fi = f / (TY + 3) + 1, fj = f - (fi - 1) * (TY + 3);
+        /* ring cells (fi-1, fj-1) and (fi-1, fj) */
+        need = (fj >= 1 && sm.ACT[LI(fi - 1, fj - 1)]) || (fj < SW && sm.ACT[LI(fi - 1, fj)]);
+      }
+      if (need) sm.FLIST[atomicAdd(&sm.nflist, 1)] = (short)e;
     }
+    __syncthreads();
+    const int nf = sm.nflist;
+    for (int q = threadIdx.x; q < nf; q += NT) {
+      const int e = sm.FLIST[q];
+      if (e < RXF) {
+        const int fi = e / (TY + 2), fj = e - fi * (TY + 2) + 1;
+        ring_face_terms<R, N>(D, sm.P, sm.w.T, true, fi, fj, e);
+      } else {
+        const int f = e - RXF, fi = f / (TY + 3) + 1, fj = f - (fi - 1) * (TY + 3);
+        ring_face_terms<R, N>(D, sm.P, sm.w.T, false, fi, fj, e);
+      }
+    }
+    __syncthreads();
+  }
+  for (int q = threadIdx.x; q < nact; q += NT) {
+    const int e = sm.LIST[q];
+    const int ri = e / SW, rj = e - ri * SW;
+    R d[N];
+    ring_dphi<R, N, K, ANISO>(D, sm, ri, rj, sm.ACT[e], d);
 #pragma unroll
     for (int a = 0; a < N; a++) sm.DP[a][e] = d[a];
   }
   __syncthreads();   /* the face-term cache is dead from here: its space holds the update's arrays */
+  if (threadIdx.x == 0) {
+    sm.nlist = 0;    /* for the CTA's next tile */
+    sm.nflist = 0;
+  }
 
 #define PR(a, e) sm.P[a][L2I((e) / SW + 1, (e) % SW + 1)]
   /* ---- per-cell quantities of the ring region */
@@ -1429,6 +1461,21 @@ __device__ __forceinline__ void bulk_tiles(const SimDesc *__restrict__ sims, con
   if (cur_sim >= 0) flush(cur_sim);
 }
 
+/* End of a warp's bulk tiles when the same shared memory is used otherwise
+ * afterwards: its stage barriers are invalidated (every box it issued has
+ * completed or been waited for). */
+template <typename R, int K>
+__device__ __forceinline__ void bulk_release_warp(unsigned char *smraw) {
+  unsigned char *sbase = (unsigned char *)(((size_t)smraw + 127) & ~(size_t)127);
+  BulkWarpSmem<R, K> &ws = reinterpret_cast<BulkWarpSmem<R, K> *>(sbase)[threadIdx.x >> 5];
+  if ((threadIdx.x & 31) == 0) {
+#pragma unroll
+    for (int q = 0; q < BulkGeom<R, K>::NST; q++)
+      asm volatile("mbarrier.inval.shared::cta.b64 [%0];\n" ::"r"(smem_addr(&ws.bar[q])) : "memory");
+  }
+  __syncwarp();
+}
+
 template <typename R, int N, int K, bool SUMS, bool MUL, bool DIAG>
 __global__ void __launch_bounds__(NT, 2) kf_bulk(const SimDesc *__restrict__ sims, const Consts<R> *__restrict__ consts,
                                                  const int *__restrict__ tsim, const int4 *__restrict__ blist,
@@ -1456,6 +1503,10 @@ __device__ __noinline__ void general_tiles(const SimDesc *__restrict__ sims, con
   __shared__ int s_item;
   const int nlist = *(volatile int *)(ctr + CTR_LIST);
   int cur_sim = -1;
+  if (threadIdx.x == 0) {   /* the tile's list counters (reset again after each tile) */
+    sm.nlist = 0;
+    sm.nflist = 0;
+  }
   for (;;) {
     if (threadIdx.x == 0) s_item = atomicAdd(ctr + CTR_HEAD, 1);
     __syncthreads();
@@ -1504,9 +1555,20 @@ __global__ void __launch_bounds__(NT, (N <= 3 ? 2 : 1)) kf_step(const SimDesc *_
                                                  TileFlags *__restrict__ flag_out, int *__restrict__ ctr,
                                                  int ndone, StatBufs st) {
   extern __shared__ __align__(16) unsigned char smraw[];
-  general_tiles<R, N, K, ANISO, MUL>(sims, consts, tsim, state, next, flag_out, glist, ctr, st, smraw);
-  __syncthreads();   /* the interface tiles' shared memory becomes the bulk stages */
-  bulk_tiles<R, N, K, false, MUL, DIAG>(sims, consts, tsim, blist, tmaps, buf, state, next, flag_out, ctr, st, smraw);
+  if (st.mixed && (blockIdx.x & 1)) {
+    /* bulk tiles first, then whatever is left of the interface list: the two
+     * kinds of work share every SM from the start of the step */
+    bulk_tiles<R, N, K, false, MUL, DIAG>(sims, consts, tsim, blist, tmaps, buf, state, next, flag_out, ctr, st,
+                                          smraw);
+    bulk_release_warp<R, K>(smraw);
+    __syncthreads();   /* the bulk stages' shared memory becomes the interface tile's */
+    general_tiles<R, N, K, ANISO, MUL>(sims, consts, tsim, state, next, flag_out, glist, ctr, st, smraw);
+  } else {
+    general_tiles<R, N, K, ANISO, MUL>(sims, consts, tsim, state, next, flag_out, glist, ctr, st, smraw);
+    __syncthreads();   /* the interface tiles' shared memory becomes the bulk stages */
+    bulk_tiles<R, N, K, false, MUL, DIAG>(sims, consts, tsim, blist, tmaps, buf, state, next, flag_out, ctr, st,
+                                          smraw);
+  }
   step_finish(ctr, ndone);
 }
 

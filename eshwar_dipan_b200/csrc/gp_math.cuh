@@ -262,10 +262,11 @@ __device__ __forceinline__ void rot2(const Consts<R> &D, const R (&M)[2][2], R q
   }
 }
 
-/* Anisotropy functions.  They are evaluated in FP64 for both field types: in
- * float, |q|^6 of a gradient just above the reference's |q|^2 > 1e-15 guard is
- * about 1e-45 and underflows, which turns dA/dq into inf or NaN.  For FP64
- * fields the expressions are exactly the reference's. */
+/* Anisotropy functions.  For FP64 fields the expressions are exactly the
+ * reference's.  The FP32 form evaluates them in float on the normalised
+ * gradient (below): written as the reference writes them, |q|^6 of a gradient
+ * just above the reference's |q|^2 > 1e-15 guard is about 1e-45 and
+ * underflows in float, which turns dA/dq into inf or NaN. */
 
 /* anisotropy_01_function_ac (anisotropy_01.h:30-48), q_z = 0 */
 template <typename R>
@@ -300,6 +301,36 @@ __device__ __forceinline__ R dadq_c(R qi_, const QPow<R> &p, R dab16) {
   const double qi = qi_;
   if (fabs(p.q2) > 1.0e-15) return (R)((double)dab16 * (qi * qi * qi / p.q22 - qi * p.q4 / p.q23));
   return R(0.0);
+}
+
+/* The FP32 form: with r2 = 1/|q|^2 and s4 = sum q^4 r2^2 (the sum of the
+ * fourth powers of the unit vector q/|q|, between 1/2 and 1),
+ *   a_c   = 1 - dab (3 - 4 s4),
+ *   dA/dq_i = 16 dab (q_i r2) (q_i^2 r2 - s4),
+ * the same functions as above, with no intermediate below about 1e-30. */
+template <>
+struct QPow<float> {
+  float q2, r2, s4;
+};
+template <>
+__device__ __forceinline__ QPow<float> qpow<float>(float qx, float qy) {
+  QPow<float> r;
+  r.q2 = qx * qx + qy * qy;
+  r.r2 = r.q2 > 0.0f ? 1.0f / r.q2 : 0.0f;
+  const float nx = qx * qx * r.r2, ny = qy * qy * r.r2;
+  r.s4 = nx * nx + ny * ny;
+  return r;
+}
+template <>
+__device__ __forceinline__ float dadq_c<float>(float qi, const QPow<float> &p, float dab16) {
+  if (fabsf(p.q2) > 1.0e-15f) return dab16 * (qi * p.r2) * (qi * qi * p.r2 - p.s4);
+  return 0.0f;
+}
+template <>
+__device__ __forceinline__ float ac<float>(float qx, float qy, float dab) {
+  const QPow<float> p = qpow<float>(qx, qy);
+  if (fabsf(p.q2) > 1.0e-15f) return 1.0f - dab * (3.0f - 4.0f * p.s4);
+  return 1.0f;
 }
 
 /* matinvnew (matrix.h:50-218) for n = K <= 2 with 1.0/x as the reciprocal

@@ -429,6 +429,7 @@ struct StatBufs {
   const unsigned *round_step;  /* FP32 form: device step counter keying the rounding stream */
   int mbar_tries;      /* polls of a TMA box's barrier before kf_bulk gives up (MBAR_TRIES) */
   int bch_max, bch_div;  /* bulk chunks: at most bch_max (<= 16) entries, left / (bch_div * warps) */
+  int mixed;           /* kf_step: odd CTAs take bulk tiles first, then interface tiles */
   unsigned tma_extra;  /* bytes a box's barrier expects beyond the box: 0, or more to test the give-up path */
 };
 
