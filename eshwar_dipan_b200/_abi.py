@@ -85,6 +85,7 @@ class Stats(ctypes.Structure):
         ("comp_sum", _arr(c_double, _MK)),
         ("nonfinite", c_longlong),
         ("steps_done", c_longlong),
+        ("shift_offset", c_longlong),
     ]
 
     def as_dict(self, N, K):
@@ -95,6 +96,7 @@ class Stats(ctypes.Structure):
             d[name] = list(getattr(self, name))[:K]
         d["nonfinite"] = int(self.nonfinite)
         d["steps_done"] = int(self.steps_done)
+        d["shift_offset"] = int(self.shift_offset)
         return d
 
 

@@ -41,7 +41,16 @@ struct BatchLaunch {
                        TileFlags *flags);
   cudaError_t (*sdphi)(cudaStream_t s, const void *consts, const void *phi, void *dphi, Grid g);
   cudaError_t (*supd)(cudaStream_t s, const void *consts, const void *phi, const void *mu, const void *dphi,
-                      void *phin, void *mun, Grid g);
+                      void *phin, void *mun, Grid g, const double *tcc);
+  /* moving frame: interface position into pos[s] (zeroed by the caller),
+   * then the shifted (or copied) state into next */
+  cudaError_t (*shift_pos)(int ntiles, cudaStream_t s, const SimDesc *sims, const void *consts, const int *tsim,
+                           const void *state, int *pos);
+  cudaError_t (*shift_apply)(int ntiles, cudaStream_t s, const SimDesc *sims, const void *consts, const int *tsim,
+                             const void *state, void *next, const int *pos, SimDyn *dyn);
+  /* the temperature rows of the coming step (non-isothermal simulations) */
+  cudaError_t (*trows)(int nsims, cudaStream_t s, const SimDesc *sims, const void *consts, const int *ctr,
+                       SimDyn *dyn, double *rows);
   size_t elem;
 };
 
@@ -156,10 +165,26 @@ struct BatchKernels {
     return cudaGetLastError();
   }
   static cudaError_t supd(cudaStream_t s, const void *consts, const void *phi, const void *mu, const void *dphi,
-                          void *phin, void *mun, Grid g) {
+                          void *phin, void *mun, Grid g, const double *tcc) {
     dim3 grid((g.my + 127) / 128, g.mx);
     k_supdate<R, N, K><<<grid, 128, 0, s>>>((const Consts<R> *)consts, (const R *)phi, (const R *)mu,
-                                            (const R *)dphi, (R *)phin, (R *)mun, g);
+                                            (const R *)dphi, (R *)phin, (R *)mun, g, tcc);
+    return cudaGetLastError();
+  }
+  static cudaError_t shift_pos(int ntiles, cudaStream_t s, const SimDesc *sims, const void *consts, const int *tsim,
+                               const void *state, int *pos) {
+    ks_pos<R, N><<<ntiles, NT, 0, s>>>(sims, (const Consts<R> *)consts, tsim, (const R *)state, pos);
+    return cudaGetLastError();
+  }
+  static cudaError_t shift_apply(int ntiles, cudaStream_t s, const SimDesc *sims, const void *consts,
+                                 const int *tsim, const void *state, void *next, const int *pos, SimDyn *dyn) {
+    ks_shift<R, N, K><<<ntiles, NT, 0, s>>>(sims, (const Consts<R> *)consts, tsim, (const R *)state, (R *)next, pos,
+                                            dyn);
+    return cudaGetLastError();
+  }
+  static cudaError_t trows(int nsims, cudaStream_t s, const SimDesc *sims, const void *consts, const int *ctr,
+                           SimDyn *dyn, double *rows) {
+    kt_rows<R><<<nsims, 128, 0, s>>>(sims, (const Consts<R> *)consts, ctr, dyn, rows);
     return cudaGetLastError();
   }
   static BatchLaunch table() {
@@ -173,6 +198,9 @@ struct BatchKernels {
     t.flags = flags;
     t.sdphi = sdphi;
     t.supd = supd;
+    t.trows = trows;
+    t.shift_pos = shift_pos;
+    t.shift_apply = shift_apply;
     t.elem = sizeof(R);
     return t;
   }

@@ -94,6 +94,27 @@ gpd::Consts<R> make_consts(const gp_derived &d) {
     }
     c.C[a] = (R)d.C[a];
   }
+  c.tgrad = d.tgrad;
+  c.bc_t[0] = d.bc_t[0];
+  c.bc_t[1] = d.bc_t[1];
+  c.Teq64 = d.Teq;
+  for (int a = 0; a < GPK_MAXN; a++) {
+    for (int i = 0; i < GPK_MAXK; i++) {
+      c.Beq64[a][i] = d.Beq[a][i];
+      c.dBbdT64[a][i] = d.dBbdT[a][i];
+      c.ceql[a][i] = d.ceql[a][i];
+      c.ceqs[a][i] = d.ceqs[a][i];
+      c.DCk[a][i] = d.DCk[a][i];
+      for (int j = 0; j < GPK_MAXK; j++) c.A64[a][i][j] = d.A[a][i][j];
+    }
+    c.DTl[a] = d.DTl[a];
+    c.DTs[a] = d.DTs[a];
+  }
+  c.tg_base = d.tg_base; c.tg_dT = d.tg_dT; c.tg_dist = d.tg_dist; c.tg_off = d.tg_off; c.tg_vel = d.tg_vel;
+  c.dx64 = d.dx; c.dy64 = d.dy; c.dt64 = d.dt;
+  c.shift = d.shift;
+  c.shiftj = (int)d.shiftj;
+  for (int i = 0; i < GPK_MAXK; i++) c.mu_fill[i] = (R)d.mu_fill[i];
   return c;
 }
 
@@ -318,6 +339,11 @@ struct gp_batch {
   gpd::TensorMapSlot *tmaps;    /* [nsims][2]: TMA maps of each simulation's mu planes in state[0], state[1] */
   int cur;
   long long *ext;               /* running extremes per simulation [nsims][2(N+K)] */
+  bool tgrad;                   /* some simulation is non-isothermal: temperature rows each step */
+  bool shift;                   /* some simulation has the moving frame: a check every 100 steps */
+  int *spos;                    /* its interface position per simulation */
+  double *trows;                /* their temperature rows (SimDesc::off_T) */
+  gpd::SimDyn *dyn;             /* per simulation moving-frame state */
   double *partials, *sums_sim;
   /* captured step sequences: graphs[(starting parity, steps)], steps <= GP_GRAPH_STEPS */
   std::map<std::pair<int, long>, cudaGraphExec_t> graphs;
@@ -356,9 +382,11 @@ static int batch_step_once(gp_batch *b, int want_sums, cudaEvent_t *ev) {
   st.tma_extra = b->tma_extra;
   st.bch_max = b->shape.bch_max;
   st.mixed = b->shape.mixed ? 1 : 0;
+  st.trows = b->tgrad ? b->trows : nullptr;
   st.bch_div = b->shape.bch_div;
   const int in = b->cur, out = b->cur ^ 1;
   if (ev) BK(cudaEventRecord(ev[0], b->stream));
+  if (b->tgrad) BK(b->L.trows(b->nsims, b->stream, b->d_desc, b->d_consts, b->counters, b->dyn, b->trows));
   BK(b->L.classify(b->ntiles, b->stream, b->d_desc, b->d_consts, b->d_tsim, b->flags[in], b->flags[out], b->glist,
                    b->blist, b->counters));
   if (!want_sums && b->grid_s > 0 && b->shape.fused && (!ev || ev[3] == nullptr)) {
@@ -394,6 +422,18 @@ static int batch_reflag(gp_batch *b, bool other_unknown) {
   return GP_OK;
 }
 
+/* The moving-frame check after a step whose number is a multiple of 100
+ * (microsim_gp.c:115-123): every simulation's state goes to the other buffer,
+ * shifted where its interface passed Shiftj, copied otherwise. */
+static int batch_shift(gp_batch *b) {
+  BK(cudaMemsetAsync(b->spos, 0, sizeof(int) * (size_t)b->nsims, b->stream));
+  BK(b->L.shift_pos(b->ntiles, b->stream, b->d_desc, b->d_consts, b->d_tsim, b->state[b->cur], b->spos));
+  BK(b->L.shift_apply(b->ntiles, b->stream, b->d_desc, b->d_consts, b->d_tsim, b->state[b->cur], b->state[b->cur ^ 1],
+                      b->spos, b->dyn));
+  b->cur ^= 1;
+  return batch_reflag(b, true);
+}
+
 static int batch_fold_stats(gp_batch *b, gp_stats *out) {
   const int N = b->N, K = b->K, ne = 2 * (N + K), ns = 2 * N + 2 * K + 1;
   k_reduce_sums<<<dim3(ns, b->nsims), 256, 0, b->stream>>>(b->partials, b->d_seg0, b->d_segn, ns, b->sums_sim);
@@ -402,9 +442,12 @@ static int batch_fold_stats(gp_batch *b, gp_stats *out) {
   std::vector<double> sums((size_t)ns * b->nsims);
   BK(cudaMemcpyAsync(mm.data(), b->ext, mm.size() * 8, cudaMemcpyDeviceToHost, b->stream));
   BK(cudaMemcpyAsync(sums.data(), b->sums_sim, sums.size() * 8, cudaMemcpyDeviceToHost, b->stream));
+  std::vector<gpd::SimDyn> dyn(b->nsims);
+  BK(cudaMemcpyAsync(dyn.data(), b->dyn, sizeof(gpd::SimDyn) * dyn.size(), cudaMemcpyDeviceToHost, b->stream));
   BK(cudaStreamSynchronize(b->stream));
   for (int s = 0; s < b->nsims; s++) {
     stats_from(&b->last[s], &mm[(size_t)s * ne], &sums[(size_t)s * ns], N, K, b->steps);
+    b->last[s].shift_offset = dyn[s].shift_off;
     if (out) out[s] = b->last[s];
   }
   return GP_OK;
@@ -442,9 +485,9 @@ static void batch_drop_graphs(gp_batch *b) {
 
 /* The graph of n steps from the current parity, captured on first use; null
  * when the cache is full (the caller then launches the steps one by one). */
-static int batch_graph(gp_batch *b, long n, cudaGraphExec_t *out) {
+static int batch_graph(gp_batch *b, long n, bool shift_at_end, cudaGraphExec_t *out) {
   *out = nullptr;
-  const auto key = std::make_pair(b->cur, n);
+  const auto key = std::make_pair(b->cur, n | (shift_at_end ? (1L << 30) : 0L));
   auto it = b->graphs.find(key);
   if (it != b->graphs.end()) {
     *out = it->second;
@@ -456,6 +499,7 @@ static int batch_graph(gp_batch *b, long n, cudaGraphExec_t *out) {
   int rc = GP_OK;
   const int cur0 = b->cur;
   for (long i = 0; i < n && rc == GP_OK; i++) rc = batch_step_once(b, 0, nullptr);
+  if (rc == GP_OK && shift_at_end) rc = batch_shift(b);
   b->steps -= n; /* captured, not run */
   b->cur = cur0;
   cudaError_t ec = cudaStreamEndCapture(b->stream, &gr);
@@ -484,7 +528,13 @@ static int batch_step_impl(gp_batch *b, long nsteps, gp_stats *stats, double *to
   long s = 0;
   const long graphed = stats ? nsteps - 1 : nsteps;   /* steps that may run inside graphs */
   while (!split && graphed - s >= 2) {
-    const long n = std::min<long>(GP_GRAPH_STEPS, graphed - s);
+    long n = std::min<long>(GP_GRAPH_STEPS, graphed - s);
+    bool sh = false;
+    if (b->shift) {   /* chunks end at the moving frame's checks */
+      const long to_check = GP_GRAPH_STEPS - (long)(b->steps % GP_GRAPH_STEPS);
+      if (n >= to_check) { n = to_check; sh = true; }
+      if (n < 2) break;
+    }
     if (b->tune_next < b->ncand && n == GP_GRAPH_STEPS) {
       /* autotuning: one 100-step chunk per candidate shape, each captured
        * afresh and timed with events; then the fastest is kept */
@@ -521,17 +571,18 @@ static int batch_step_impl(gp_batch *b, long nsteps, gp_stats *stats, double *to
       continue;
     }
     cudaGraphExec_t ge = nullptr;
-    int rc = batch_graph(b, n, &ge);
+    int rc = batch_graph(b, n, sh, &ge);
     if (rc != GP_OK) return rc;
     if (!ge) break;   /* cache full: the rest one by one */
     BK(cudaGraphLaunch(ge, b->stream));
-    if (n & 1) b->cur ^= 1;
+    if ((n & 1) ^ (sh ? 1 : 0)) b->cur ^= 1;
     b->steps += n;
     s += n;
   }
   for (; s < nsteps; s++) {
     int rc = batch_step_once(b, stats != nullptr && s == nsteps - 1, split ? b->ev : nullptr);
     if (rc != GP_OK) return rc;
+    if (b->shift && b->steps % GP_GRAPH_STEPS == 0 && (rc = batch_shift(b)) != GP_OK) return rc;
     if (split) {
       float x = 0.f, y = 0.f;
       BK(cudaEventSynchronize(b->ev[2]));
@@ -788,6 +839,9 @@ void gp_batch_destroy(gp_batch *b) {
   cudaFree(b->sums_sim);
   cudaFree(b->counters);
   cudaFree(b->tmaps);
+  cudaFree(b->trows);
+  cudaFree(b->dyn);
+  cudaFree(b->spos);
   if (b->stream) cudaStreamDestroy(b->stream);
   delete b;
 }
@@ -841,7 +895,7 @@ int gp_batch_create(gp_batch **out, int nsims, const gp_params *params, const do
   /* layout: every simulation's N+K planes back to back, pitch a multiple of 32 */
   const int N = b->N, K = b->K, ne = 2 * (N + K), ns = 2 * N + 2 * K + 1;
   long long off = 0, offd = 0;
-  int nt = 0;
+  int nt = 0, offT = 0;
   std::vector<int> tsim, seg0, segn;
   std::vector<char> consts;
   const size_t csz = b->elem == 8 ? sizeof(gpd::Consts<double>) : sizeof(gpd::Consts<float>);
@@ -857,6 +911,8 @@ int gp_batch_create(gp_batch **out, int nsims, const gp_params *params, const do
     sd.tiles_x = (sd.g.my + gpd::TY - 1) / gpd::TY;
     const int tiles_y = (sd.g.mx + gpd::TX - 1) / gpd::TX;
     sd.tile0 = nt;
+    sd.off_T = offT;
+    offT += 2 * (int)(sd.g.my + 6);
     seg0.push_back(nt);
     segn.push_back(sd.tiles_x * tiles_y);
     for (int t = 0; t < sd.tiles_x * tiles_y; t++) tsim.push_back(s);
@@ -974,6 +1030,16 @@ int gp_batch_create(gp_batch **out, int nsims, const gp_params *params, const do
   BALLOC(b->sums_sim, sizeof(double) * (size_t)ns * nsims);
   BALLOC(b->counters, gpd::CTR_COUNT * sizeof(int));
   BALLOC(b->tmaps, sizeof(gpd::TensorMapSlot) * 2 * (size_t)nsims);
+  b->tgrad = false;
+  b->shift = false;
+  for (int s = 0; s < nsims; s++) {
+    b->tgrad |= b->derived[s].tgrad != 0;
+    b->shift |= b->derived[s].shift != 0;
+  }
+  BALLOC(b->spos, sizeof(int) * (size_t)nsims);
+  if (b->shift) b->tune_next = b->ncand;   /* the first chunks end at the frame checks: no tuning */
+  BALLOC(b->trows, sizeof(double) * (size_t)std::max(offT, 1));
+  BALLOC(b->dyn, sizeof(gpd::SimDyn) * (size_t)nsims);
 #undef BALLOC
   std::vector<gpd::TensorMapSlot> tm(2 * (size_t)nsims);
   if (encode_mu_maps(b, tm.data()) != GP_OK) {
@@ -1000,6 +1066,7 @@ int gp_batch_create(gp_batch **out, int nsims, const gp_params *params, const do
   BUP(b->tmaps, tm.data(), sizeof(gpd::TensorMapSlot) * tm.size());
 #undef BUP
   if (cudaMemsetAsync(b->dphi, 0, (size_t)offd * b->elem, b->stream) != cudaSuccess ||
+      cudaMemsetAsync(b->dyn, 0, sizeof(gpd::SimDyn) * (size_t)nsims, b->stream) != cudaSuccess ||
       cudaMemsetAsync(b->counters, 0, gpd::CTR_COUNT * sizeof(int), b->stream) != cudaSuccess) {
     rc = bfail(b, GP_ECUDA, "gp_batch_create: memset failed");
     gp_batch_destroy(b);
@@ -1022,6 +1089,9 @@ int gp_batch_create(gp_batch **out, int nsims, const gp_params *params, const do
 int gp_batch_smooth(gp_batch *b, long nsteps) {
   if (!b || nsteps < 0) return bfail(b, GP_EINVAL, "gp_batch_smooth: bad argument");
   const size_t csz = b->consts_bytes;
+  /* the sweeps run before the first step: the temperature as copied at t = 0 */
+  if (b->tgrad && nsteps > 0)
+    BK(b->L.trows(b->nsims, b->stream, b->d_desc, b->d_consts, b->counters, b->dyn, b->trows));
   for (long t = 0; t < nsteps; t++) {
     for (int s = 0; s < b->nsims; s++) {
       const gpd::SimDesc &sd = b->desc[s];
@@ -1031,7 +1101,8 @@ int gp_batch_smooth(gp_batch *b, long nsteps) {
       char *dp = (char *)b->dphi + (size_t)sd.off_dphi * b->elem;
       const size_t mu_off = (size_t)b->N * sd.g.plane * b->elem;
       BK(b->L.sdphi(b->stream, cs, st, dp, sd.g));
-      BK(b->L.supd(b->stream, cs, st, st + mu_off, dp, nx, nx + mu_off, sd.g));
+      const double *tcc = b->derived[s].tgrad ? b->trows + sd.off_T + (sd.g.my + 6) : nullptr;
+      BK(b->L.supd(b->stream, cs, st, st + mu_off, dp, nx, nx + mu_off, sd.g, tcc));
     }
     b->cur ^= 1;
   }
@@ -1304,6 +1375,8 @@ int adj_check(gp_ctx *c, gpd::AdjLaunch *L) {
   gp_batch *b = c->b;
   const gp_derived &d = b->derived[0];
   if (b->elem != 8) return fail(c, GP_EUNSUPPORTED, "gp_adjoint: FP64 contexts only");
+  if (d.tgrad || d.shift)
+    return fail(c, GP_EUNSUPPORTED, "gp_adjoint: isothermal runs without a moving frame only");
   if (d.N != 2 || d.K != 1 || d.inv_mode != GP_INV_BINARY)
     return fail(c, GP_EUNSUPPORTED, "gp_adjoint: NUMPHASES=2 with one BINARY component only (have N=%d K=%d)", d.N,
                 d.K);
@@ -1543,6 +1616,8 @@ extern "C" int gp_step_noalloc(const gp_params *p, const double *phi_in, const d
   gp_derived d;
   char err[256] = "";
   if (gp_host_derive(p, &d, err, sizeof err) != GP_OK) return fail(nullptr, GP_EINVAL, "gp_step_noalloc: %s", err);
+  if (d.tgrad || d.shift)
+    return fail(nullptr, GP_EUNSUPPORTED, "gp_step_noalloc: isothermal runs without a moving frame only");
   Kern k;
   if (!pick(d.N, d.K, d.aniso != 0, &k)) return fail(nullptr, GP_EINVAL, "gp_step_noalloc: no kernel for N=%d K=%d", d.N, d.K);
   gpd::Grid g = make_grid(d, 1); /* caller's planes are contiguous [field][MESH_X][MESH_Y] */

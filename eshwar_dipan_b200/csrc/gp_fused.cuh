@@ -326,7 +326,7 @@ __device__ __forceinline__ void ring_face_terms(const CT &D, const R (*P)[S2], R
  * (calculate_divergence_phasefield.h:4-62) in the same arithmetic as dphi_tile. */
 template <typename R, int N, int K, bool ANISO, typename CT>
 __device__ __forceinline__ void ring_dphi(const CT &D, const GenSmem<R, N, K> &sm, int ri, int rj,
-                                          unsigned mask, R *d) {
+                                          unsigned mask, R *d, double Tpf) {
   const int i = ri + 1, j = rj + 1, e = LI(ri, rj);
   R ph[N];
   bool act[N];
@@ -354,16 +354,35 @@ __device__ __forceinline__ void ring_dphi(const CT &D, const GenSmem<R, N, K> &s
     gcy[a] = div2y(S[L2I(i, j + 1)] - S[L2I(i, j - 1)], D);
   }
   R psi[N];
+  if (D.tgrad) {
+    /* init_propertymatrices(T) at the cell's temperature before dpsi
+     * (calculate_divergence_phasefield.h:21-29) */
+    R E[N][K], Bt[N][K], Ct[N];
+    e_at<R, N, K>(D, Tpf, E);
+    bc_at<R, N, K>(D, Tpf, Bt, Ct);
 #pragma unroll
-  for (int b = 0; b < N; b++) {
-    R c[K], ps = R(0.0);
+    for (int b = 0; b < N; b++) {
+      R c[K], ps = R(0.0);
 #pragma unroll
-    for (int k = 0; k < K; k++) {
-      c[k] = c_mu<R, K>(D, m, b, k);
-      ps -= m[k] * c[k];
+      for (int k = 0; k < K; k++) {
+        c[k] = c_muE<R, K>(D, E[b], m, b, k);
+        ps -= m[k] * c[k];
+      }
+      ps += feBC<R, K>(D, Bt[b], Ct[b], c, b);
+      psi[b] = ps;
     }
-    ps += fe<R, K>(D, c, b);
-    psi[b] = ps;
+  } else {
+#pragma unroll
+    for (int b = 0; b < N; b++) {
+      R c[K], ps = R(0.0);
+#pragma unroll
+      for (int k = 0; k < K; k++) {
+        c[k] = c_mu<R, K>(D, m, b, k);
+        ps -= m[k] * c[k];
+      }
+      ps += fe<R, K>(D, c, b);
+      psi[b] = ps;
+    }
   }
   R cq0[NP<N>::v], cq1[NP<N>::v], cd0[NP<N>::v], cd1[NP<N>::v], cac[NP<N>::v], cq2[NP<N>::v];
   if (ANISO) {
@@ -477,7 +496,8 @@ template <typename R, int N, int K, bool ANISO, typename CT>
 __device__ __forceinline__ TileFlags general_tile(const CT &D, const Grid &g, const R *__restrict__ phi,
                                                     const R *__restrict__ mu, R *__restrict__ phin,
                                                     R *__restrict__ mun, int x0, int y0, const StatBufs &st,
-                                                    long long ext_slot, long long slot, GenSmem<R, N, K> &sm) {
+                                                    long long ext_slot, long long slot, GenSmem<R, N, K> &sm,
+                                                    const double *__restrict__ tpf, const double *__restrict__ tcc) {
   constexpr int L = N - 1;
   const R cst = D.obstacle ? D.jat_obst : D.jat_well;
 
@@ -582,7 +602,7 @@ __device__ __forceinline__ TileFlags general_tile(const CT &D, const Grid &g, co
     const int e = sm.LIST[q];
     const int ri = e / SW, rj = e - ri * SW;
     R d[N];
-    ring_dphi<R, N, K, ANISO>(D, sm, ri, rj, sm.ACT[e], d);
+    ring_dphi<R, N, K, ANISO>(D, sm, ri, rj, sm.ACT[e], d, D.tgrad ? tpf[y0 - 1 + rj + 3] : 0.0);
 #pragma unroll
     for (int a = 0; a < N; a++) sm.DP[a][e] = d[a];
   }
@@ -600,12 +620,16 @@ __device__ __forceinline__ TileFlags general_tile(const CT &D, const Grid &g, co
     for (int a = 0; a < N; a++) p[a] = PR(a, e);
 #pragma unroll
     for (int k = 0; k < K; k++) mm[k] = sm.M[k][e];
+    R Ec[N][K];
+    /* the ghosted column of ring cell e (cells past my+1 are not needed: clamped) */
+    if (D.tgrad) e_at<R, N, K>(D, tcc[min(y0 - 1 + e % SW + 3, g.my + 5)], Ec);
 #pragma unroll
     for (int a = 0; a < N; a++) {
       R hv = h<R, N>(p, a);
       sm.w.u.H[a][e] = hv;
 #pragma unroll
-      for (int k = 0; k < K; k++) sm.w.u.CM[a][k][e] = c_mu<R, K>(D, mm, a, k);
+      for (int k = 0; k < K; k++)
+        sm.w.u.CM[a][k][e] = D.tgrad ? c_muE<R, K>(D, Ec[a], mm, a, k) : c_mu<R, K>(D, mm, a, k);
       if (a < L)
         sm.w.u.SP[a][e] =
             (p[a] * (R(1.0) - p[a]) > R(0.0)) ? p[a] * (R(1.0) - hv) / (sqrt(p[a] * (R(1.0) - p[a]))) : R(0.0);
@@ -695,7 +719,7 @@ __device__ __forceinline__ TileFlags general_tile(const CT &D, const Grid &g, co
 #pragma unroll
     for (int k = 0; k < K; k++) m[k] = sm.M[k][c];
     commit_cell<R, N, K>(D, sm.w.u.FX, sm.w.u.FY, sm.w.u.JX, sm.w.u.JY, sm.w.u.CM, sm.w.u.H, i, j, x, y, ph, dp, m,
-                         nph, nm, dmu, st);
+                         nph, nm, dmu, st, D.tgrad ? tcc[y + 3] : 0.0);
     const long long o = (long long)x * g.pitch + y;
 #pragma unroll
     for (int a = 0; a < N; a++) phin[a * g.plane + o] = nph[a];
@@ -705,7 +729,7 @@ __device__ __forceinline__ TileFlags general_tile(const CT &D, const Grid &g, co
   }
 #undef PRIJ
 #undef PR
-  block_stats<R, N, K>(D, valid, nph, nm, dp, dmu, st, ext_slot, slot);
+  block_stats<R, N, K>(D, valid, nph, nm, dp, dmu, st, ext_slot, slot, (D.tgrad && valid) ? tcc[y + 3] : 0.0);
   return tile_flags(valid, oh, tx, ty, min(TX, g.mx - x0), min(TY, g.my - y0));
 }
 
@@ -765,7 +789,9 @@ __global__ void __launch_bounds__(NTC) kf_classify(const SimDesc *__restrict__ s
     const int lt = t - sd.tile0;
     by = lt / sd.tiles_x;
     bx = lt - by * sd.tiles_x;
-    p = bulk_phase<R>(consts[s], sd.g, flag_in, sd.tile0, sd.tiles_x, by, bx);
+    /* a non-isothermal simulation steps every tile as an interface tile
+     * (whose pure-phase cells take the bulk update at their temperature) */
+    if (!consts[s].tgrad) p = bulk_phase<R>(consts[s], sd.g, flag_in, sd.tile0, sd.tiles_x, by, bx);
   }
   const unsigned mb = __ballot_sync(0xffffffffu, t < ntiles && p >= 0);
   const unsigned mg = __ballot_sync(0xffffffffu, t < ntiles && p < 0);
@@ -1524,9 +1550,11 @@ __device__ __noinline__ void general_tiles(const SimDesc *__restrict__ sims, con
     const R *ph = state + sd.off_state;
     R *nx = next + sd.off_state;
     using CT = typename std::conditional<MUL, ConstsMul<R>, Consts<R>>::type;
+    const double *tpf = st.trows ? st.trows + sd.off_T : nullptr;
+    const double *tcc = tpf ? tpf + (sd.g.my + 6) : nullptr;
     const TileFlags f = general_tile<R, N, K, ANISO>(static_cast<const CT &>(sc), sd.g, ph, ph + (long long)N * sd.g.plane, nx,
                                                        nx + (long long)N * sd.g.plane, by * TX, bx * TY, st, s, t,
-                                                       sm);
+                                                       sm, tpf, tcc);
     if (threadIdx.x == 0) flag_out[t] = f;
     __syncthreads();
   }
@@ -1570,6 +1598,151 @@ __global__ void __launch_bounds__(NT, (N <= 3 ? 2 : 1)) kf_step(const SimDesc *_
                                           smraw);
   }
   step_finish(ctr, ndone);
+}
+
+/* Per simulation, the moving-frame state the temperature rows need: the
+ * offset of the frame, and after a shift the offset and distance the
+ * shifted temperature field was laid down with (consumed by the next step). */
+struct SimDyn {
+  long long shift_off;   /* shift_OFFSET (microsim_gp.c:122) */
+  long long shift_T;     /* the offset of the temperature field being shifted */
+  int dlast;             /* its shift distance */
+  int fresh;             /* a shift happened at the end of the last step */
+  int pos;               /* MAX_INTERFACE_POS of the last check */
+  int pad;
+};
+
+/* The temperature of every ghosted column y of a non-isothermal simulation
+ * during the coming step, one CTA per simulation.  The reference's field is
+ * temp_bottom + y*GRADIENT (apply_temperature_gradientY, Temperature_gradient.h:4-29),
+ * laid down after each step with the step's BASE_POS (microsim_gp.c:108-113;
+ * at t = 0 without the velocity term, :77-82) and copied into the ghost
+ * columns only by the next boundary copy: the phase-field pass of step t+1
+ * reads the field as laid down (as copied at t = 0, where the start-up copy
+ * came after it), the concentration pass reads it copied.  After a moving-
+ * frame shift the field holds the shifted columns (shift.h:20) until the
+ * next step lays it down again.  Rows: [0, MESH_Y+6) as the phase-field pass
+ * reads them, then [0, MESH_Y+6) as the concentration pass reads them. */
+template <typename R>
+__global__ void __launch_bounds__(128) kt_rows(const SimDesc *__restrict__ sims, const Consts<R> *__restrict__ consts,
+                                               const int *__restrict__ ctr, SimDyn *__restrict__ dyn,
+                                               double *__restrict__ trows) {
+  const int s = blockIdx.x;
+  const Consts<R> &D = consts[s];
+  if (!D.tgrad) return;
+  const SimDesc sd = sims[s];
+  const int my = sd.g.my, ry = my + 6;
+  const long t0 = (long)(unsigned)ctr[CTR_STEP];
+  const SimDyn dd = dyn[s];
+  const long long shT = dd.fresh ? dd.shift_T : dd.shift_off;
+  const long d = dd.fresh ? dd.dlast : 0;
+  double base_pos;
+  if (t0 == 0) base_pos = (D.tg_off / D.dy64) - (double)shT;
+  else base_pos = (D.tg_off / D.dy64) - (double)shT + ((D.tg_vel / D.dy64) * ((double)t0 * D.dt64));
+  const double grad = (D.tg_dT) * D.dy64 / (D.tg_dist);
+  const double tb = D.tg_base - base_pos * grad;
+  double *tpf = trows + sd.off_T, *tcc = tpf + ry;
+  for (int y = threadIdx.x; y < ry; y += blockDim.x) {
+    /* the column a ghost column is a copy of (T's own boundary types; other
+     * types copy nothing) */
+    int yr = y;
+    if (y < 3 && (D.bc_t[0] == GP_BC_NEUMANN || D.bc_t[0] == GP_BC_PERIODIC))
+      yr = remap(y - 3, my, D.bc_t[0], D.bc_t[1]) + 3;
+    else if (y >= my + 3 && (D.bc_t[1] == GP_BC_NEUMANN || D.bc_t[1] == GP_BC_PERIODIC))
+      yr = remap(y - 3, my, D.bc_t[0], D.bc_t[1]) + 3;
+    const double laid = y <= ry - 1 - d ? tb + (double)(y + d) * grad : tb + (double)y * grad;
+    const double copied = yr <= ry - 1 - d ? tb + (double)(yr + d) * grad : tb + (double)yr * grad;
+    tcc[y] = copied;
+    tpf[y] = t0 == 0 ? copied : laid;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && dd.fresh) dyn[s].fresh = 0;
+}
+
+/* ---- moving frame (Shift = 1) --------------------------------------------
+ * Every 100 steps the reference finds MAX_INTERFACE_POS, the largest column y
+ * where the liquid crosses one half upwards (check_SHIFT, shift.h:47-65, run
+ * over the rows its concentration sweep has just updated), and when it is
+ * past Shiftj moves every row down by d = MAX_INTERFACE_POS - Shiftj cells,
+ * the top d cells becoming liquid at cfill (apply_shiftY, shift.h:4-45;
+ * microsim_gp.c:115-123).  Columns are ghosted indices (interior y + 3). */
+
+/* MAX_INTERFACE_POS over the interior (pairs of interior columns y-1, y),
+ * one CTA per tile, atomic max into pos[simulation] */
+template <typename R, int N>
+__global__ void __launch_bounds__(NT) ks_pos(const SimDesc *__restrict__ sims, const Consts<R> *__restrict__ consts,
+                                             const int *__restrict__ tsim, const R *__restrict__ state,
+                                             int *__restrict__ pos) {
+  __shared__ int s_best[NT / 32];
+  const int t = blockIdx.x, s = __ldg(tsim + t);
+  if (!consts[s].shift) return;
+  const SimDesc sd = sims[s];
+  const int lt = t - sd.tile0, by = lt / sd.tiles_x, bx = lt - by * sd.tiles_x;
+  const int x = by * TX + threadIdx.x / TY, y = bx * TY + threadIdx.x % TY;
+  int best = 0;
+  if (x < sd.g.mx && y >= 1 && y < sd.g.my) {
+    const R *pl = state + sd.off_state + (long long)(N - 1) * sd.g.plane + (long long)x * sd.g.pitch;
+    const R a = pl[y - 1], b = pl[y];
+    if ((a - (R(1.0) - a) < R(0.0)) && (b - (R(1.0) - b) > R(0.0))) best = y + 3;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) best = max(best, __shfl_xor_sync(0xffffffffu, best, o));
+  if ((threadIdx.x & 31) == 0) s_best[threadIdx.x >> 5] = best;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int b = 0;
+#pragma unroll
+    for (int w = 0; w < NT / 32; w++) b = max(b, s_best[w]);
+    if (b > 0) atomicMax(pos + s, b);
+  }
+}
+
+/* The state after the check into the other buffer: shifted by d rows where
+ * pos > Shiftj, else copied.  A cell takes the cell d columns up (through
+ * the boundary copy tables past the last interior column), or the liquid
+ * fill beyond the ghost columns.  The first tile's thread 0 records the
+ * shift for the temperature rows of the next step. */
+template <typename R, int N, int K>
+__global__ void __launch_bounds__(NT) ks_shift(const SimDesc *__restrict__ sims,
+                                               const Consts<R> *__restrict__ consts, const int *__restrict__ tsim,
+                                               const R *__restrict__ state, R *__restrict__ next,
+                                               const int *__restrict__ pos, SimDyn *__restrict__ dyn) {
+  const int t = blockIdx.x, s = __ldg(tsim + t);
+  const Consts<R> &D = consts[s];
+  const SimDesc sd = sims[s];
+  const int lt = t - sd.tile0, by = lt / sd.tiles_x, bx = lt - by * sd.tiles_x;
+  const int x = by * TX + threadIdx.x / TY, y = bx * TY + threadIdx.x % TY;
+  const int p = pos[s];
+  const int d = (D.shift && p > D.shiftj) ? p - D.shiftj : 0;
+  if (lt == 0 && threadIdx.x == 0 && d > 0) {
+    SimDyn &dd = dyn[s];
+    dd.shift_T = dd.shift_off;
+    dd.dlast = d;
+    dd.fresh = 1;
+    dd.shift_off += d;
+    dd.pos = p;
+  }
+  if (x >= sd.g.mx || y >= sd.g.my) return;
+  const R *src = state + sd.off_state;
+  R *dst = next + sd.off_state;
+  const long long row = (long long)x * sd.g.pitch, o = row + y;
+  const int sy = y + d;
+  if (d == 0) {
+#pragma unroll
+    for (int f = 0; f < N + K; f++) dst[f * sd.g.plane + o] = src[f * sd.g.plane + o];
+  } else if (sy <= sd.g.my + 2) {
+    const int yp = sy < sd.g.my ? sy : remap(sy, sd.g.my, D.bc_y[0][0], D.bc_y[0][1]);
+    const int ym = sy < sd.g.my ? sy : remap(sy, sd.g.my, D.bc_y[1][0], D.bc_y[1][1]);
+#pragma unroll
+    for (int a = 0; a < N; a++) dst[a * sd.g.plane + o] = src[a * sd.g.plane + row + yp];
+#pragma unroll
+    for (int k = 0; k < K; k++) dst[(N + k) * sd.g.plane + o] = src[(N + k) * sd.g.plane + row + ym];
+  } else {
+#pragma unroll
+    for (int a = 0; a < N; a++) dst[a * sd.g.plane + o] = a == N - 1 ? R(1.0) : R(0.0);
+#pragma unroll
+    for (int k = 0; k < K; k++) dst[(N + k) * sd.g.plane + o] = D.mu_fill[k];
+  }
 }
 
 /* Flags of every tile of a state buffer from its phi (after an upload,

@@ -504,7 +504,9 @@ int gp_host_derive(const gp_params *p, gp_derived *d, char *err, size_t errlen) 
   if (N < 2 || N > GPK_MAXN) FAIL("NUMPHASES=%d: kernels take 2..%d", N, GPK_MAXN);
   if (K < 1 || K > GPK_MAXK) FAIL("NUMCOMPONENTS=%d: kernels take 2..%d", p->numcomponents, GPK_MAXK + 1);
   if (p->mesh_x < 5 || p->mesh_y < 5) FAIL("MESH_X/MESH_Y must be >= 5");
-  if (!p->isothermal) FAIL("ISOTHERMAL=0 (temperature gradient) is not implemented");
+  if (!p->isothermal && !p->tempgrady) FAIL("ISOTHERMAL=0 without Tempgrady");
+  if (!p->isothermal && (p->tempgrady_v[2] == 0.0))
+    FAIL("Tempgrady: Distance must be non-zero");
   if (p->noise_phasefield) FAIL("Noise_phasefield uses rand(); not reproducible, not implemented");
   if (p->function_f != 1) FAIL("Function_F=%d: only 1 (parabolic) exists", p->function_f);
   if (p->function_w != 1 && p->function_w != 2) FAIL("Function_W=%d: only 1 or 2", p->function_w);
@@ -577,6 +579,43 @@ int gp_host_derive(const gp_params *p, gp_derived *d, char *err, size_t errlen) 
           for (k = 0; k < K; k++) s += d->DC[b][i][j][k] * (b == q ? 1.0 : 0.0);
         d->Dbulk[q][i][j] = s;
       }
+  /* the temperature field of a non-isothermal run, and the moving frame */
+  d->tgrad = !p->isothermal;
+  d->Teq = p->Teq;
+  for (a = 0; a < N; a++)
+    for (i = 0; i < K; i++) {
+      d->Beq[a][i] = Beq[a][i];
+      d->dBbdT[a][i] = dBbdT[a][i];
+      d->ceql[a][i] = p->ceq[a][N - 1][i];
+      d->ceqs[a][i] = p->ceq[a][a][i];
+    }
+  for (a = 0; a < N - 1; a++) {
+    d->DTl[a] = 0.0;
+    d->DTs[a] = 0.0;
+    for (k = 0; k < K; k++) {
+      d->DTs[a] += p->slopes[a][a][k] * (p->ceq[a][N - 1][k] - p->ceq[a][a][k]);
+      d->DTl[a] += p->slopes[a][N - 1][k] * (p->ceq[a][N - 1][k] - p->ceq[a][a][k]);
+      d->DCk[a][k] = p->ceq[a][N - 1][k] - p->ceq[a][a][k];
+    }
+  }
+  d->tg_base = p->tempgrady_v[0];
+  d->tg_dT = p->tempgrady_v[1];
+  d->tg_dist = p->tempgrady_v[2];
+  d->tg_off = p->tempgrady_v[3];
+  d->tg_vel = p->tempgrady_v[4];
+  d->bc_t[0] = p->bc_type[2][3];
+  d->bc_t[1] = p->bc_type[2][2];
+  d->shift = p->shift != 0;
+  d->shiftj = p->shiftj;
+  if (d->shift && (p->shiftj < 1 || p->shiftj >= p->mesh_y + 5)) FAIL("Shiftj=%ld outside the grid", (long)p->shiftj);
+  for (i = 0; i < K; i++) {
+    /* Mu(c, Tfill, N-1, i) with c = cfill of the liquid (shift.h:28-35, functionF_01.h:19-29) */
+    int L = N - 1;
+    double sm = 2.0 * p->A[L][i][i] * p->cfill[L][L][i] + (Beq[L][i] + dBbdT[L][i] * (p->Tfill - p->Teq));
+    for (j = 0; j < K; j++)
+      if (i != j) sm += p->A[L][i][j] * p->cfill[L][L][j];
+    d->mu_fill[i] = sm;
+  }
   d->rot_identity = 1;
   for (a = 0; a < N; a++)
     for (b = 0; b < N; b++) {

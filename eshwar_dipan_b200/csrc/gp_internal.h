@@ -56,6 +56,22 @@ typedef struct gp_derived {
   double Dbulk[GPK_MAXN][GPK_MAXK][GPK_MAXK]; /* D_kl of a cell with phi = e_p, summed as functionD.h does */
   /* boundary index maps along x and y: ghosted index -> ghosted index; per field */
   int bc_x[2][2], bc_y[2][2];             /* [field phi/mu][low/high side] type (1 or 3) */
+  /* non-isothermal runs (ISOTHERMAL = 0): the temperature field
+   * T = temp_bottom + y*GRADIENT of apply_temperature_gradientY
+   * (Temperature_gradient.h:4-29) and what a cell needs at its temperature:
+   * E = Beq + dBbdT*(T-Teq) (functionF_01.h:22,34) and B, C of
+   * function_B/function_C (functionF_01.h:62-104) */
+  int tgrad;
+  double Teq;
+  double Beq[GPK_MAXN][GPK_MAXK], dBbdT[GPK_MAXN][GPK_MAXK];
+  double ceql[GPK_MAXN][GPK_MAXK], ceqs[GPK_MAXN][GPK_MAXK], DCk[GPK_MAXN][GPK_MAXK];
+  double DTl[GPK_MAXN], DTs[GPK_MAXN];
+  double tg_base, tg_dT, tg_dist, tg_off, tg_vel;   /* Tempgrady = {base, DeltaT, Distance, OFFSET, velocity} */
+  int bc_t[2];                                       /* T's boundary types along y [low/high side] */
+  /* moving frame (Shift = 1, shift.h:4-66) */
+  int shift;
+  long shiftj;
+  double mu_fill[GPK_MAXK];                         /* Mu(cfill of the liquid, Tfill) of the cells shifted in */
 } gp_derived;
 
 /* Host restatement of matinvnew (matrix.h:50-218): LU with the reference's

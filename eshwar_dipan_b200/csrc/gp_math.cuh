@@ -44,6 +44,19 @@ struct Consts {
   R Dbulk[GPK_MAXN][GPK_MAXK][GPK_MAXK];
   double cmu64[GPK_MAXN][GPK_MAXK][GPK_MAXK];
   double muc64[GPK_MAXN][GPK_MAXK][GPK_MAXK];
+  /* non-isothermal runs: E, B and C of a cell are functions of its
+   * temperature (see gp_derived); FP64 whatever the field type */
+  int tgrad;
+  int bc_t[2];
+  double Teq64;
+  double Beq64[GPK_MAXN][GPK_MAXK], dBbdT64[GPK_MAXN][GPK_MAXK];
+  double ceql[GPK_MAXN][GPK_MAXK], ceqs[GPK_MAXN][GPK_MAXK], DCk[GPK_MAXN][GPK_MAXK];
+  double DTl[GPK_MAXN], DTs[GPK_MAXN];
+  double A64[GPK_MAXN][GPK_MAXK][GPK_MAXK];
+  double tg_base, tg_dT, tg_dist, tg_off, tg_vel, dx64, dy64, dt64;
+  /* moving frame */
+  int shift, shiftj;
+  R mu_fill[GPK_MAXK];
 };
 
 /* h_a(phi) (functionH.h:24-36) */
@@ -111,6 +124,88 @@ __device__ __forceinline__ R fe(const Consts<R> &D, const R *c, int a) {
     s += D.B[a][i] * c[i];
   }
   s += D.C[a];
+  return s;
+}
+
+/* ---- the thermodynamics of a cell at its own temperature (non-isothermal
+ * runs, where init_propertymatrices(T) runs per cell: calculate_divergence_
+ * phasefield.h:21-29; c_mu and Mu take the cell's T: functionF_01.h:19-37) */
+
+/* E_a,k = Beq + dBbdT (T - Teq) of every phase at temperature T */
+template <typename R, int N, int K, typename CT>
+__device__ __forceinline__ void e_at(const CT &D, double T, R (&E)[N][K]) {
+#pragma unroll
+  for (int a = 0; a < N; a++)
+#pragma unroll
+    for (int k = 0; k < K; k++) E[a][k] = (R)(D.Beq64[a][k] + D.dBbdT64[a][k] * (T - D.Teq64));
+}
+
+/* B and C of every phase at temperature T: function_B and function_C
+ * (functionF_01.h:62-104), their expressions in their order */
+template <typename R, int N, int K, typename CT>
+__device__ __forceinline__ void bc_at(const CT &D, double T, R (&B)[N][K], R (&C)[N]) {
+  constexpr int L = N - 1;
+#pragma unroll
+  for (int a = 0; a < N; a++) {
+    double cl[K], cs[K];
+#pragma unroll
+    for (int i = 0; i < K; i++) {
+      double sc = 0.0, bai = 0.0;
+      if (a != L) {
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+          cl[k] = D.ceql[a][k] - (D.DCk[a][k]) * (D.Teq64 - T) / (D.DTl[a]);
+          cs[k] = D.ceqs[a][k] - (D.DCk[a][k]) * (D.Teq64 - T) / (D.DTs[a]);
+          if (k != i) sc += D.A64[L][k][i] * cl[k] - D.A64[a][k][i] * cs[k];
+        }
+        bai = (2.0 * (D.A64[L][i][i] * cl[i] - D.A64[a][i][i] * cs[i]) + sc);
+      }
+      B[a][i] = (R)bai;
+    }
+    double sc = 0.0;
+    if (a != L) {
+#pragma unroll
+      for (int k = 0; k < K; k++) {
+        cl[k] = D.ceql[a][k] - (D.DCk[a][k]) * (D.Teq64 - T) / (D.DTl[a]);
+        cs[k] = D.ceqs[a][k] - (D.DCk[a][k]) * (D.Teq64 - T) / (D.DTs[a]);
+      }
+#pragma unroll
+      for (int i = 0; i < K; i++)
+#pragma unroll
+        for (int j = 0; j < K; j++)
+          if (i <= j) sc += (D.A64[a][i][j] * cs[i] * cs[j] - D.A64[L][i][j] * cl[i] * cl[j]);
+    }
+    C[a] = (R)sc;
+  }
+}
+
+/* c_a,i(mu), Mu_a,i(c) and f_a(c) with the phase's E (and B, C) given */
+template <typename R, int K, typename CT>
+__device__ __forceinline__ R c_muE(const CT &D, const R *E, const R *m, int a, int i) {
+  R s = R(0.0);
+#pragma unroll
+  for (int k = 0; k < K; k++) s += D.cmu[a][i][k] * (m[k] - E[k]);
+  return s;
+}
+template <typename R, int K, typename CT>
+__device__ __forceinline__ R MuE(const CT &D, const R *E, const R *c, int a, int i) {
+  R s = D.twoA[a][i] * c[i] + E[i];
+#pragma unroll
+  for (int j = 0; j < K; j++)
+    if (i != j) s += D.A[a][i][j] * c[j];
+  return s;
+}
+template <typename R, int K, typename CT>
+__device__ __forceinline__ R feBC(const CT &D, const R *B, R C, const R *c, int a) {
+  R s = R(0.0);
+#pragma unroll
+  for (int i = 0; i < K; i++) {
+#pragma unroll
+    for (int j = 0; j < K; j++)
+      if (i <= j) s += D.A[a][i][j] * c[i] * c[j];
+    s += B[i] * c[i];
+  }
+  s += C;
   return s;
 }
 

@@ -92,7 +92,8 @@ __global__ void k_sdphi(const Consts<R> *__restrict__ Dp, const R *__restrict__ 
 /* calculate_divergence_concentration_smooth_2D (calculate_divergence_concentration.h:154-253) */
 template <typename R, int N, int K>
 __global__ void k_supdate(const Consts<R> *__restrict__ Dp, const R *__restrict__ phi, const R *__restrict__ mu,
-                          const R *__restrict__ dphi, R *__restrict__ phin, R *__restrict__ mun, Grid g) {
+                          const R *__restrict__ dphi, R *__restrict__ phin, R *__restrict__ mun, Grid g,
+                          const double *__restrict__ tcc) {
   const Consts<R> &D = *Dp;
   const int y = blockIdx.x * blockDim.x + threadIdx.x, x = blockIdx.y;
   if (y >= g.my) return;
@@ -131,11 +132,15 @@ __global__ void k_supdate(const Consts<R> *__restrict__ Dp, const R *__restrict_
   for (int a = 0; a < N; a++)
     if (bulk < 0 && ph[a] == R(1.0)) bulk = a;
   if (bulk >= 0) {
-    R cn[K];
+    R cn[K], E[N][K];
+    /* the cell's temperature in a non-isothermal run
+     * (calculate_divergence_concentration.h:167-170) */
+    if (D.tgrad) e_at<R, N, K>(D, tcc[y + 3], E);
 #pragma unroll
-    for (int k = 0; k < K; k++) cn[k] = c_mu<R, K>(D, m, bulk, k) + D.dt * (divflux[k]);
+    for (int k = 0; k < K; k++)
+      cn[k] = (D.tgrad ? c_muE<R, K>(D, E[bulk], m, bulk, k) : c_mu<R, K>(D, m, bulk, k)) + D.dt * (divflux[k]);
 #pragma unroll
-    for (int k = 0; k < K; k++) nm[k] = Mu<R, K>(D, cn, bulk, k);
+    for (int k = 0; k < K; k++) nm[k] = D.tgrad ? MuE<R, K>(D, E[bulk], cn, bulk, k) : Mu<R, K>(D, cn, bulk, k);
   } else {
     double dc[K], dcdmu[K][K], iv[K][K];
 #pragma unroll

@@ -430,6 +430,8 @@ struct StatBufs {
   int mbar_tries;      /* polls of a TMA box's barrier before kf_bulk gives up (MBAR_TRIES) */
   int bch_max, bch_div;  /* bulk chunks: at most bch_max (<= 16) entries, left / (bch_div * warps) */
   int mixed;           /* kf_step: odd CTAs take bulk tiles first, then interface tiles */
+  const double *trows; /* non-isothermal simulations: per simulation the temperature of each ghosted column y
+                          as the phase-field pass reads it, then as the concentration pass reads it */
   unsigned tma_extra;  /* bytes a box's barrier expects beyond the box: 0, or more to test the give-up path */
 };
 
@@ -507,7 +509,7 @@ __device__ __forceinline__ void bulk_commit_f32(const Consts<R> &D, int a, const
 template <typename R, int N, int K, bool UNI = false>
 __device__ __forceinline__ void block_stats(const Consts<R> &D, bool valid, const R *nph, const R *nm, const R *dp,
                                             const double *dmu, const StatBufs &st, long long ext_slot,
-                                            long long sum_slot) {
+                                            long long sum_slot, double Tc = 0.0) {
   constexpr int NE = 2 * (N + K), NS = 2 * N + 2 * K + 1, NW = NT / 32;
   __shared__ double red[NW][NE > NS ? NE : NS];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -554,7 +556,15 @@ __device__ __forceinline__ void block_stats(const Consts<R> &D, bool valid, cons
           int k = f - 2 * N - K;
           R comp = R(0.0);
 #pragma unroll
-          for (int b = 0; b < N; b++) comp += c_mu<R, K>(D, nm, b, k) * h<R, N>(nph, b);
+          if (D.tgrad) {
+            R E[N][K];
+            e_at<R, N, K>(D, Tc, E);
+#pragma unroll
+            for (int b = 0; b < N; b++) comp += c_muE<R, K>(D, E[b], nm, b, k) * h<R, N>(nph, b);
+          } else {
+#pragma unroll
+            for (int b = 0; b < N; b++) comp += c_mu<R, K>(D, nm, b, k) * h<R, N>(nph, b);
+          }
           v = (double)comp;
         } else {
           bool bad = false;
@@ -588,7 +598,7 @@ __device__ __forceinline__ void commit_cell(const CT &D, const R (&FX)[K][K][NXF
                                             const R (&JX)[K][NXF], const R (&JY)[K][NYF], const R (&CM)[N][K][SS],
                                             const R (&H)[N][SS], int i, int j, int x, int y, const R *ph,
                                             const R *dp, const R *m, R *nph, R *nm, double *dmu,
-                                            const StatBufs &st) {
+                                            const StatBufs &st, double Tc = 0.0) {
   const R cst = D.obstacle ? D.jat_obst : D.jat_well;
   const int c = LI(i, j);
   R divflux[K], divjat[K];
@@ -618,10 +628,20 @@ __device__ __forceinline__ void commit_cell(const CT &D, const R (&FX)[K][K][NXF
     R cn[K];
 #pragma unroll
     for (int k = 0; k < K; k++) cn[k] = CM[bulk][k][c] + D.dt * (divflux[k]) - divjat[k];
+    if (D.tgrad) {
+      R E[N][K];
+      e_at<R, N, K>(D, Tc, E);
 #pragma unroll
-    for (int k = 0; k < K; k++) {
-      nm[k] = Mu<R, K>(D, cn, bulk, k);
-      dmu[k] = (double)nm[k] - (double)m[k];
+      for (int k = 0; k < K; k++) {
+        nm[k] = MuE<R, K>(D, E[bulk], cn, bulk, k);
+        dmu[k] = (double)nm[k] - (double)m[k];
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < K; k++) {
+        nm[k] = Mu<R, K>(D, cn, bulk, k);
+        dmu[k] = (double)nm[k] - (double)m[k];
+      }
     }
 #pragma unroll
     for (int a = 0; a < N; a++) nph[a] = ph[a] + dp[a];
@@ -639,9 +659,19 @@ __device__ __forceinline__ void commit_cell(const CT &D, const R (&FX)[K][K][NXF
 #pragma unroll
       for (int k = 0; k < K; k++) sum[k] += CM[a][k][c] * sdh;
     }
+    /* non-isothermal (calculate_divergence_concentration.h:85): minus
+     * sum_a dcbdT_phase h_a * dt * (-GRADIENT * velocity); dcbdT_phase is
+     * allocated but never filled by the reference (taken as 0) and the struct
+     * member GRADIENT is never set, so the term is a signed zero */
+    R sdc = R(0.0);
+    if (D.tgrad) {
+#pragma unroll
+      for (int a = 0; a < N; a++) sdc += R(0.0) * H[a][c];
+    }
 #pragma unroll
     for (int k = 0; k < K; k++) {
-      dc[k] = (double)(D.dt * (divflux[k]) - divjat[k] - sum[k]);
+      if (D.tgrad) dc[k] = (double)(D.dt * (divflux[k]) - divjat[k] - sum[k] - sdc * D.dt * (R(-0.0) * (R)D.tg_vel));
+      else dc[k] = (double)(D.dt * (divflux[k]) - divjat[k] - sum[k]);
 #pragma unroll
       for (int l = 0; l < K; l++) {
         dcdmu[k][l] = 0.0;
@@ -935,6 +965,7 @@ struct SimDesc {
   long long off_state;   /* N phi planes then K mu planes */
   long long off_dphi;    /* N delta-phi planes (smoothing sweeps) */
   int tiles_x, tile0;    /* tiles per row, first tile */
+  int off_T;             /* non-isothermal: the step's temperature rows (two of MESH_Y+6) in StatBufs::trows */
 };
 
 template <typename R>

@@ -23,12 +23,17 @@ def input_text(N=2, K=1, mesh=(48, 40), dx=1.0, dy=None, dt=0.02, eps=4.0, tau_a
                gamma=1.0, gamma_abc=10.0, aniso=True, dab=0.02, rot=None, well=False,
                bc_phi=(1, 1, 1, 1), bc_mu=None, mode=None, T=0.97, Teq=1.0,
                d_liquid=None, d_solid=0.0, A_off=0.0, nsmooth=10, ntimesteps=100, ascii=True,
-               writecomposition=0, liquid_c=None, extra=""):
+               writecomposition=0, liquid_c=None, extra="", tempgrady=None, shift=False, shiftj=30,
+               bc_T=None):
     """Reference-format Input.in for N phases (the last one liquid) and K solutes.
 
     bc_* = (X+, X-, Y+, Y-) in the reference's BOUNDARY tuple order.
     mode: 'binary' | 'ternary' | 'dilute' | 'none' (default: binary for K=1,
     ternary for K=2).
+    tempgrady: None (isothermal), or (base temperature, DeltaT, Distance,
+    OFFSET, velocity): ISOTHERMAL = 0 with that moving temperature gradient
+    along y (directional solidification).  shift: the moving frame, which
+    follows the interface once it passes column shiftj.
     """
     dy = dx if dy is None else dy
     bc_mu = bc_phi if bc_mu is None else bc_mu
@@ -63,11 +68,12 @@ def input_text(N=2, K=1, mesh=(48, 40), dx=1.0, dy=None, dt=0.02, eps=4.0, tau_a
         add("DIFFUSIVITY = {1, %d, %s};" % (a, ", ".join(_fmt(v) for v in vals)))
     add("R = 1.0;")
     add("V = 1.0;")
-    for f, bc in (("phi", bc_phi), ("mu", bc_mu), ("c", bc_mu), ("T", bc_mu)):
+    bc_T = bc_mu if bc_T is None else bc_T
+    for f, bc in (("phi", bc_phi), ("mu", bc_mu), ("c", bc_mu), ("T", bc_T)):
         add("BOUNDARY = {%s, %d, %d, %d, %d, 0, 0};" % ((f,) + tuple(bc)))
     for f in ("phi", "mu", "c", "T"):
         add("BOUNDARY_VALUE = {%s, 0, 0, 0, 0, 0, 0};" % f)
-    add("ISOTHERMAL = 1;")
+    add("ISOTHERMAL = %d;" % (0 if tempgrady else 1))
     if mode == "binary":
         add("BINARY = 1;")
     elif mode == "ternary":
@@ -89,14 +95,15 @@ def input_text(N=2, K=1, mesh=(48, 40), dx=1.0, dy=None, dt=0.02, eps=4.0, tau_a
         add("Rotation_matrix = {%d, %d, 0, 0, %s};" % (a, b, _fmt(rot.get((a, b), 0.0))))
     add("Function_W = %d;" % (2 if well else 1))
     add("Gamma_abc = {%s};" % ", ".join(_fmt(gamma_abc) for _ in triples))
-    add("Shift = 0;")
-    add("Shiftj = 30;")
+    add("Shift = %d;" % (1 if shift else 0))
+    add("Shiftj = %d;" % shiftj)
     add("Writecomposition = %d;" % writecomposition)
     add("Noise_phasefield = 0;")
     add("Amp_Noise_Phase = 0.0;")
     add("Equilibrium_temperature = %s;" % _fmt(Teq))
     add("Filling_temperature = 1.0;")
-    add("Tempgrady = {0.96, 0.06, 800.0, 0, 0.016};")
+    tg = tempgrady if tempgrady else (0.96, 0.06, 800.0, 0, 0.016)
+    add("Tempgrady = {%s};" % ", ".join(_fmt(v) for v in tg))
     add("Function_F = 1;")
     for a in range(N):
         if K == 1:

@@ -110,6 +110,8 @@ typedef struct gp_stats {
   double comp_sum[GP_MAX_COMP];
   long long nonfinite;                    /* interior cells with a non-finite field */
   long long steps_done;                   /* time steps taken since gp_init */
+  long long shift_offset;                 /* moving frame: cells the fields have moved down since gp_init
+                                             (shift_OFFSET, microsim_gp.c:122) */
 } gp_stats;
 
 typedef struct gp_ctx gp_ctx;

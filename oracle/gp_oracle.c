@@ -36,11 +36,24 @@ struct gpo {
   int obstacle, well, aniso, inv_mode, recip_div;
   double dx, dy, dt, eps, tau;
   double T, Teq;
+  /* non-isothermal runs (ISOTHERMAL = 0, Tempgrady): the temperature of every
+   * ghosted cell, its gradient parameters and the phase-diagram constants of
+   * function_B/function_C at a temperature (functionF_01.h:62-104) */
+  int tgrad;
+  double *Tc, *Tstep;   /* the field now, and the field the last step used */
+  double tg_base, tg_dT, tg_dist, tg_off, tg_vel;
+  double ceq_l[MAXN][MAXK], ceq_s[MAXN][MAXK], DT_l[MAXN], DT_s[MAXN], DC[MAXN][MAXK];
+  /* moving frame (Shift = 1): shift every 100 steps when the interface passes
+   * column shiftj (microsim_gp.c:115-126, shift.h:4-66) */
+  int shift;
+  long shiftj, shift_off, last_shift;
+  double Tfill, cfill_l[MAXK];
+  long tstep;   /* time steps since gpo_create: the reference main's t */
   double gamma[MAXN][MAXN], gabc[MAXN][MAXN][MAXN], tau_ab[MAXN][MAXN], dab[MAXN][MAXN];
   double diff[MAXN][MAXK][MAXK], A[MAXN][MAXK][MAXK];
   double cmu[MAXN][MAXK][MAXK], B[MAXN][MAXK], C[MAXN], Beq[MAXN][MAXK], dBbdT[MAXN][MAXK];
   double R[MAXN][MAXN][3][3], Rinv[MAXN][MAXN][3][3];
-  int bctype[2][4];          /* [phi/mu][face X-, X+, Y+, Y-] */
+  int bctype[3][4];          /* [phi/mu/T][face X-, X+, Y+, Y-] */
   /* state, ghosted [field][x*ry+y] */
   double *phi, *mu, *dphi;
   /* face quantities */
@@ -243,45 +256,82 @@ static double o_dh(const gpo *o, const double *ph, int b, int a) {
   return s;
 }
 
-/* c_mu, Mu, free_energy (functionF_01.h:5-37) at the isothermal T */
-static double o_cmu(const gpo *o, const double *m, int a, int i) {
+/* c_mu, Mu, free_energy (functionF_01.h:5-37) at temperature T */
+static double o_cmu(const gpo *o, const double *m, double T, int a, int i) {
   int k;
   double s = 0.0;
-  for (k = 0; k < o->K; k++) s += o->cmu[a][i][k] * (m[k] - (o->Beq[a][k] + o->dBbdT[a][k] * (o->T - o->Teq)));
+  for (k = 0; k < o->K; k++) s += o->cmu[a][i][k] * (m[k] - (o->Beq[a][k] + o->dBbdT[a][k] * (T - o->Teq)));
   return s;
 }
 
-static double o_Mu(const gpo *o, const double *c, int a, int i) {
+static double o_Mu(const gpo *o, const double *c, double T, int a, int i) {
   int j;
-  double s = 2.0 * o->A[a][i][i] * c[i] + (o->Beq[a][i] + o->dBbdT[a][i] * (o->T - o->Teq));
+  double s = 2.0 * o->A[a][i][i] * c[i] + (o->Beq[a][i] + o->dBbdT[a][i] * (T - o->Teq));
   for (j = 0; j < o->K; j++)
     if (i != j) s += o->A[a][i][j] * c[j];
   return s;
 }
 
-static double o_fe(const gpo *o, const double *c, int a) {
+static double o_fe(const gpo *o, const double *c, int a, const double B[][MAXK], const double *C) {
   int i, j;
   double s = 0.0;
   for (i = 0; i < o->K; i++) {
     for (j = 0; j < o->K; j++)
       if (i <= j) s += o->A[a][i][j] * c[i] * c[j];
-    s += o->B[a][i] * c[i];
+    s += B[a][i] * c[i];
   }
-  s += o->C[a];
+  s += C[a];
   return s;
 }
 
-/* dpsi (functionF_01.h:41-57) */
-static double o_dpsi(const gpo *o, const double *m, const double *ph, int a) {
+/* B and C of every phase at temperature T: function_B / function_C
+ * (functionF_01.h:62-104), as init_propertymatrices(T) sets them
+ * (functionF_01.h:169-230) */
+static void o_BC(const gpo *o, double T, double B[][MAXK], double *C) {
+  int a, i, j, k, L = o->N - 1;
+  for (a = 0; a < o->N; a++) {
+    double cl[MAXK] = {0}, cs[MAXK] = {0}, sc;
+    for (i = 0; i < o->K; i++) {
+      sc = 0.0;
+      B[a][i] = 0.0;
+      if (a != L) {
+        for (k = 0; k < o->K; k++) {
+          cl[k] = o->ceq_l[a][k] - (o->DC[a][k]) * (o->Teq - T) / (o->DT_l[a]);
+          cs[k] = o->ceq_s[a][k] - (o->DC[a][k]) * (o->Teq - T) / (o->DT_s[a]);
+          if (k != i) sc += o->A[L][k][i] * cl[k] - o->A[a][k][i] * cs[k];
+        }
+        B[a][i] = (2.0 * (o->A[L][i][i] * cl[i] - o->A[a][i][i] * cs[i]) + sc);
+      }
+    }
+    sc = 0.0;
+    if (a != L) {
+      for (k = 0; k < o->K; k++) {
+        cl[k] = o->ceq_l[a][k] - (o->DC[a][k]) * (o->Teq - T) / (o->DT_l[a]);
+        cs[k] = o->ceq_s[a][k] - (o->DC[a][k]) * (o->Teq - T) / (o->DT_s[a]);
+      }
+      for (i = 0; i < o->K; i++)
+        for (j = 0; j < o->K; j++)
+          if (i <= j) sc += (o->A[a][i][j] * cs[i] * cs[j] - o->A[L][i][j] * cl[i] * cl[j]);
+    }
+    C[a] = sc;
+  }
+}
+
+/* temperature of a ghosted cell: the field of a non-isothermal run, else T */
+static double o_Tcell(const gpo *o, long c) { return o->tgrad ? o->Tc[c] : o->T; }
+
+/* dpsi (functionF_01.h:41-57) at temperature T with B, C at T */
+static double o_dpsi(const gpo *o, const double *m, double T, const double *ph, int a, const double B[][MAXK],
+                     const double *C) {
   int b, k;
   double s = 0.0;
   for (b = 0; b < o->N; b++) {
     double c[MAXK], psi = 0.0;
     for (k = 0; k < o->K; k++) {
-      c[k] = o_cmu(o, m, b, k);
+      c[k] = o_cmu(o, m, T, b, k);
       psi -= m[k] * c[k];
     }
-    psi += o_fe(o, c, b);
+    psi += o_fe(o, c, b, B, C);
     s += psi * o_dh(o, ph, b, a);
   }
   return s;
@@ -641,18 +691,24 @@ static void o_dphi_cell(const gpo *o, long c, int smooth, double *out) {
   int a, N = o->N;
   double ph[MAXN], m[MAXK], dv[MAXN], lam[MAXN], sl = 0.0;
   long act = 0;
+  const double T = o_Tcell(o, c);
+  double Bt[MAXN][MAXK], Ct[MAXN];
   gather_phi(o, c, ph);
   gather_mu(o, c, m);
   for (a = 0; a < N; a++) {
     dv[a] = (F(o->gx, o, a)[c] - F(o->gx, o, a)[c - o->ry]) / o->dx;
     dv[a] += (F(o->gy, o, a)[c] - F(o->gy, o, a)[c - 1]) / o->dy;
   }
+  /* init_propertymatrices(T) before each active phase's dpsi
+   * (calculate_divergence_phasefield.h:21-29): B, C at the cell's T */
+  if (o->tgrad) o_BC(o, T, Bt, Ct);
+  else memcpy(Bt, o->B, sizeof Bt), memcpy(Ct, o->C, sizeof Ct);
   for (a = 0; a < N; a++) {
     if (!(fabs(dv[a]) > 0.0)) continue;
     if (!smooth) {
       double dA = o->aniso ? o_dAdphi_aniso(o, ph, c, a) : o_dAdphi_iso(o, ph, c, a);
       double dd = o->aniso ? o_divdA_aniso(o, c, a) : o_divdA_iso(o, c, a);
-      lam[a] = o->eps * (-dA + dd) - (1.0 / o->eps) * o_dwdphi(o, ph, dv, a, 0) - o_dpsi(o, m, ph, a);
+      lam[a] = o->eps * (-dA + dd) - (1.0 / o->eps) * o_dwdphi(o, ph, dv, a, 0) - o_dpsi(o, m, T, ph, a, Bt, Ct);
     } else if (o->aniso) {
       /* A_01 _smooth variants return 2.0*(sum1 + 0.0): the same value as the
        * isotropic A_00 forms, since sum1 (a sum started at 0.0) is never -0 */
@@ -704,8 +760,10 @@ static void o_fluxes(gpo *o) {
         }
         for (k = 0; k < K; k++) {
           if (ng != 0.0 && y != 0 && y != o->my - 2) {
-            double cl_r = o_cmu(o, mr, L, k), cl_c = o_cmu(o, mc, L, k);
-            double cs_r = o_cmu(o, mr, a, k), cs_c = o_cmu(o, mc, a, k);
+            /* non-isothermal: each cell's own temperature (calculate_fluxes_concentration.h:66-77) */
+            double Tr = o_Tcell(o, r), Tcc = o_Tcell(o, c);
+            double cl_r = o_cmu(o, mr, Tr, L, k), cl_c = o_cmu(o, mc, Tcc, L, k);
+            double cs_r = o_cmu(o, mr, Tr, a, k), cs_c = o_cmu(o, mc, Tcc, a, k);
             double sp = gya * F(o->gy, o, L)[c];
             double atf = (1.0 - o->diff[a][k][k] / o->diff[L][k][k]);
             sp += gpx * gpx_l;
@@ -722,8 +780,9 @@ static void o_fluxes(gpo *o) {
         ng = sqrt(gpy * gpy + gxa * gxa);
         for (k = 0; k < K; k++) {
           if (ng != 0.0) {
-            double cl_f = o_cmu(o, mf, L, k), cl_c = o_cmu(o, mc, L, k);
-            double cs_f = o_cmu(o, mf, a, k), cs_c = o_cmu(o, mc, a, k);
+            double Tf = o_Tcell(o, f), Tcc = o_Tcell(o, c);
+            double cl_f = o_cmu(o, mf, Tf, L, k), cl_c = o_cmu(o, mc, Tcc, L, k);
+            double cs_f = o_cmu(o, mf, Tf, a, k), cs_c = o_cmu(o, mc, Tcc, a, k);
             double sp = gxa * F(o->gx, o, L)[c];
             double atf = (1.0 - o->diff[a][k][k] / o->diff[L][k][k]);
             sp += gpy * gpy_l;
@@ -750,9 +809,9 @@ static void o_bc(gpo *o) {
   int face, field, j;
   long rx = o->rx, ry = o->ry;
   for (face = 0; face < 4; face++)
-    for (field = 0; field < 2; field++) {
-      int t = o->bctype[field][face], nf = field ? o->K : o->N, a;
-      double *arr = field ? o->mu : o->phi;
+    for (field = 0; field < (o->tgrad ? 3 : 2); field++) {
+      int t = o->bctype[field][face], nf = field == 2 ? 1 : field ? o->K : o->N, a;
+      double *arr = field == 2 ? o->Tc : field ? o->mu : o->phi;
       long pts[3], prx[3];
       if (t != 1 && t != 3) continue;
       for (j = 0; j < 3; j++) {
@@ -810,14 +869,21 @@ static void o_conc_cell(gpo *o, long c, int smooth, double *dmu_out, double *del
   const double *dph = smooth ? o->sdphi : o->dphi;
   int interface = 1, bulk = 0;
   long bk = c - o->ry, lf = c - 1;
+  const double T = o_Tcell(o, c);
+  double sum_dcbdT[MAXK];
   gather_phi(o, c, ph);
   gather_mu(o, c, m);
-  for (k = 0; k < K; k++) sum[k] = 0.0;
+  for (k = 0; k < K; k++) sum[k] = sum_dcbdT[k] = 0.0;
   if (!smooth)
     for (a = 0; a < N; a++) {
       double sdh = 0.0;
       for (b = 0; b < N; b++) sdh += o_dh(o, ph, a, b) * F(dph, o, b)[c];
-      for (k = 0; k < K; k++) sum[k] += o_cmu(o, m, a, k) * sdh;
+      for (k = 0; k < K; k++) {
+        sum[k] += o_cmu(o, m, T, a, k) * sdh;
+        /* dcbdT_phase is allocated but never filled by the reference
+         * (reading_input_parameters.h:85): taken as 0 */
+        sum_dcbdT[k] += 0.0 * o_h(o, ph, a);
+      }
     }
   for (k = 0; k < K; k++) {
     divflux[k] = 0.0;
@@ -835,11 +901,11 @@ static void o_conc_cell(gpo *o, long c, int smooth, double *dmu_out, double *del
     if (ph[a] == 1.0) { bulk = a; interface = 0; break; }
   if (!interface) {
     for (k = 0; k < K; k++) {
-      cold[k] = o_cmu(o, m, bulk, k);
+      cold[k] = o_cmu(o, m, T, bulk, k);
       cnew[k] = smooth ? cold[k] + o->dt * (divflux[k]) : cold[k] + o->dt * (divflux[k]) - divjat[k];
     }
     for (k = 0; k < K; k++) {
-      double nv = o_Mu(o, cnew, bulk, k);
+      double nv = o_Mu(o, cnew, T, bulk, k);
       deltamu[k] = nv - m[k];
       F(o->nmu, o, k)[c] = nv;
     }
@@ -847,6 +913,9 @@ static void o_conc_cell(gpo *o, long c, int smooth, double *dmu_out, double *del
     double nm[MAXK];
     for (k = 0; k < K; k++) {
       deltac[k] = smooth ? o->dt * (divflux[k]) : o->dt * (divflux[k]) - divjat[k] - sum[k];
+      /* calculate_divergence_concentration.h:85: the struct member GRADIENT
+       * of temperature_gradientY is never set, so the term is a signed zero */
+      if (!smooth && o->tgrad) deltac[k] = deltac[k] - sum_dcbdT[k] * o->dt * (-0.0 * o->tg_vel);
       for (l = 0; l < K; l++)
         for (a = 0; a < N; a++) dcdmu[k][l] += o->cmu[a][k][l] * o_h(o, ph, a);
     }
@@ -887,6 +956,56 @@ static void o_conc_cell(gpo *o, long c, int smooth, double *dmu_out, double *del
   for (k = 0; k < K; k++) dmu_out[(long)k * o->n + c] = deltamu[k];
 }
 
+/* apply_temperature_gradientY (Temperature_gradient.h:4-29) after the
+ * reference main's BASE_POS / GRADIENT / temp_bottom for step t
+ * (microsim_gp.c:77-82 for t = 0, :108-113 after step t): every ghosted cell */
+static void o_temperature(gpo *o, long t) {
+  long x, y;
+  double base_pos, grad, tb;
+  if (t == 0) base_pos = (o->tg_off / o->dy) - o->shift_off;
+  else base_pos = (o->tg_off / o->dy) - o->shift_off + ((o->tg_vel / o->dy) * (t * o->dt));
+  grad = (o->tg_dT) * o->dy / (o->tg_dist);
+  tb = o->tg_base - base_pos * grad;
+  for (x = 0; x < o->rx; x++)
+    for (y = 0; y < o->ry; y++) o->Tc[I(o, x, y)] = tb + y * grad;
+}
+
+/* check_SHIFT (shift.h:47-65) over the rows the concentration pass updated,
+ * on the values it left (updated cells new, the others as before): the
+ * largest column y with liquid below one half at y-1 and above at y */
+static long o_interface_pos(const gpo *o) {
+  long x, y, best = 0;
+  const double *pl = F(o->phi, o, o->N - 1);
+  for (x = 1; x <= o->rx - 3; x++)
+    for (y = 1; y <= o->ry - 1; y++) {
+      double a = pl[I(o, x, y - 1)], b = pl[I(o, x, y)];
+      if ((a - (1.0 - a) < 0.0) && (b - (1.0 - b) > 0.0) && y > best) best = y;
+    }
+  return best;
+}
+
+/* apply_shiftY (shift.h:4-45): every row moves down by d = pos - shiftj
+ * cells; the top d cells become liquid at cfill with Mu at Tfill (their
+ * temperature is left as it was) */
+static void o_shift(gpo *o, long pos) {
+  long x, y, d = pos - o->shiftj;
+  int a, k, L = o->N - 1;
+  for (x = 0; x < o->rx; x++) {
+    for (y = 0; y <= (o->ry - 1 - d); y++) {
+      long c = I(o, x, y);
+      for (a = 0; a < o->N; a++) F(o->phi, o, a)[c] = F(o->phi, o, a)[c + d];
+      for (k = 0; k < o->K; k++) F(o->mu, o, k)[c] = F(o->mu, o, k)[c + d];
+      if (o->tgrad) o->Tc[c] = o->Tc[c + d];
+    }
+    for (y = o->ry - d; y <= o->ry - 1; y++) {
+      long c = I(o, x, y);
+      for (a = 0; a < L; a++) F(o->phi, o, a)[c] = 0.0;
+      F(o->phi, o, L)[c] = 1.0;
+      for (k = 0; k < o->K; k++) F(o->mu, o, k)[c] = o_Mu(o, o->cfill_l, o->Tfill, L, k);
+    }
+  }
+}
+
 static void o_commit(gpo *o) {
   double *t;
   t = o->phi; o->phi = o->nphi; o->nphi = t;
@@ -918,9 +1037,23 @@ void gpo_step(gpo *o, long nsteps) {
     for (x = 1; x <= o->rx - 3; x++)
       for (y = 1; y <= o->ry - 2; y++) o_conc_cell(o, I(o, x, y), 0, dmu, deltamu);
     o_commit(o);
-    o_bc(o);
-    o_track(o, dmu);
-    o->steps++;
+    {
+      long pos = o->shift ? o_interface_pos(o) : 0;
+      o_bc(o);
+      o_track(o, dmu);
+      o->steps++;
+      o->tstep++;
+      if (o->tgrad) {
+        memcpy(o->Tstep, o->Tc, sizeof(double) * (size_t)o->n);
+        o_temperature(o, o->tstep);
+      }
+      o->last_shift = 0;
+      if (o->shift && o->tstep % 100 == 0 && pos > o->shiftj) {
+        o_shift(o, pos);
+        o->last_shift = pos - o->shiftj;
+        o->shift_off += pos - o->shiftj;
+      }
+    }
   }
   free(dmu);
 }
@@ -962,11 +1095,11 @@ gpo *gpo_create(const gp_params *p, int recip_div, char *err, int errlen) {
   int a, b, c, i, j, f;
   long n;
   if (p->dimension != 2 || p->numphases < 2 || p->numphases > MAXN || p->numcomponents < 2 ||
-      p->numcomponents - 1 > 3 || !p->isothermal || p->mesh_x < 5 || p->mesh_y < 5) {
+      p->numcomponents - 1 > 3 || p->mesh_x < 5 || p->mesh_y < 5) {
     snprintf(err, errlen, "oracle: unsupported parameters");
     return NULL;
   }
-  for (f = 0; f < 2; f++)
+  for (f = 0; f < (p->isothermal ? 2 : 3); f++)
     for (i = 0; i < 4; i++)
       if (p->bc_type[f][i] != 1 && p->bc_type[f][i] != 3) {
         snprintf(err, errlen, "oracle: only Neumann/periodic boundaries");
@@ -1002,8 +1135,35 @@ gpo *gpo_create(const gp_params *p, int recip_div, char *err, int errlen) {
         o->A[a][i][j] = p->A[a][i][j];
       }
   o_props_full(o, p);
-  for (f = 0; f < 2; f++)
+  for (f = 0; f < 3; f++)
     for (i = 0; i < 4; i++) o->bctype[f][i] = p->bc_type[f][i];
+  {
+    int L = o->N - 1, k;
+    o->tgrad = !p->isothermal;
+    o->tg_base = p->tempgrady_v[0];
+    o->tg_dT = p->tempgrady_v[1];
+    o->tg_dist = p->tempgrady_v[2];
+    o->tg_off = p->tempgrady_v[3];
+    o->tg_vel = p->tempgrady_v[4];
+    for (a = 0; a < o->N; a++)
+      for (k = 0; k < o->K; k++) {
+        o->ceq_l[a][k] = p->ceq[a][L][k];
+        o->ceq_s[a][k] = p->ceq[a][a][k];
+      }
+    for (a = 0; a < L; a++) {
+      o->DT_l[a] = 0.0;
+      o->DT_s[a] = 0.0;
+      for (k = 0; k < o->K; k++) {
+        o->DT_s[a] += p->slopes[a][a][k] * (p->ceq[a][L][k] - p->ceq[a][a][k]);
+        o->DT_l[a] += p->slopes[a][L][k] * (p->ceq[a][L][k] - p->ceq[a][a][k]);
+        o->DC[a][k] = p->ceq[a][L][k] - p->ceq[a][a][k];
+      }
+    }
+    o->shift = p->shift != 0;
+    o->shiftj = p->shiftj;
+    o->Tfill = p->Tfill;
+    for (k = 0; k < o->K; k++) o->cfill_l[k] = p->cfill[L][L][k];
+  }
   o->phi = calloc((size_t)o->N * n, 8); o->nphi = calloc((size_t)o->N * n, 8);
   o->dphi = calloc((size_t)o->N * n, 8); o->sdphi = calloc((size_t)o->N * n, 8);
   o->mu = calloc((size_t)o->K * n, 8); o->nmu = calloc((size_t)o->K * n, 8);
@@ -1013,6 +1173,9 @@ gpo *gpo_create(const gp_params *p, int recip_div, char *err, int errlen) {
   o->gmx = calloc((size_t)o->K * n, 8); o->gmy = calloc((size_t)o->K * n, 8);
   o->Dmx = calloc((size_t)o->K * o->K * n, 8); o->Dmy = calloc((size_t)o->K * o->K * n, 8);
   o->jx = calloc((size_t)o->K * n, 8); o->jy = calloc((size_t)o->K * n, 8);
+  o->Tc = calloc((size_t)n, 8);
+  o->Tstep = calloc((size_t)n, 8);
+  if (o->tgrad) o_temperature(o, 0);
   for (a = 0; a < o->N; a++) { o->phi_max[a] = 1.0; o->phi_min[a] = 0.0; }
   for (i = 0; i < o->K; i++) { o->mu_max[i] = 1.0; o->mu_min[i] = 1.0; }
   return o;
@@ -1023,6 +1186,8 @@ void gpo_destroy(gpo *o) {
   free(o->phi); free(o->nphi); free(o->dphi); free(o->sdphi); free(o->mu); free(o->nmu);
   free(o->gx); free(o->sx); free(o->gy); free(o->sy); free(o->gcx); free(o->gcy);
   free(o->gmx); free(o->gmy); free(o->Dmx); free(o->Dmy); free(o->jx); free(o->jy);
+  free(o->Tc);
+  free(o->Tstep);
   free(o);
 }
 
@@ -1079,12 +1244,14 @@ void gpo_stats(const gpo *o, gp_stats *s) {
       for (k = 0; k < o->K; k++) {
         double comp = 0.0;
         if (!isfinite(m[k])) bad = 1;
-        for (b = 0; b < o->N; b++) comp += o_cmu(o, m, b, k) * o_h(o, ph, b);
+        /* at the temperature the last step used (the field before its update) */
+        for (b = 0; b < o->N; b++) comp += o_cmu(o, m, o->tgrad ? o->Tstep[c] : o->T, b, k) * o_h(o, ph, b);
         s->comp_sum[k] += comp;
       }
       s->nonfinite += bad;
     }
   s->steps_done = o->steps;
+  s->shift_offset = o->shift_off;
 }
 
 void gpo_consts(const gpo *o, double *cmu, double *B, double *C, double *Beq,

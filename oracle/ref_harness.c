@@ -21,7 +21,8 @@
  * DATA/NAME_<STARTTIME>.vtk, boundary copies, the t=0 file, NSMOOTH-1
  * smoothing sweeps, then NTIMESTEPS steps writing DATA/NAME_<t>.vtk and a
  * DATA/shift.dat line every SAVET steps and the progress record every
- * TRACK_PROGRESS steps on stdout (isothermal, no moving frame).
+ * TRACK_PROGRESS steps on stdout, with the temperature field of a
+ * non-isothermal run and the moving frame (Shift).
  *
  * Usage:
  *   gp_ref_harness IN FILL run   NSMOOTH NSTEPS OUT.bin   (NSMOOTH<0: from IN)
@@ -173,6 +174,38 @@ static void load_state(const char *path) {
   init_propertymatrices(T);
 }
 
+/* microsim_gp.c:77-82: the temperature field of a non-isothermal run at t = 0 */
+static void temp_init(void) {
+  if (TEMPGRADY) {
+    BASE_POS = (temperature_gradientY.gradient_OFFSET / deltay) - shift_OFFSET;
+    GRADIENT = (temperature_gradientY.DeltaT) * deltay / (temperature_gradientY.Distance);
+    temp_bottom = temperature_gradientY.base_temp - BASE_POS * GRADIENT;
+    apply_temperature_gradientY(gridinfo, shift_OFFSET, 0);
+  }
+}
+
+/* microsim_gp.c:108-126: after step t, the temperature field moves with the
+ * gradient and, with Shift, every 100 steps the frame follows the interface */
+static void after_step(long tt) {
+  if (TEMPGRADY) {
+    BASE_POS = (temperature_gradientY.gradient_OFFSET / deltay) - shift_OFFSET +
+               ((temperature_gradientY.velocity / deltay) * (tt * deltat));
+    GRADIENT = (temperature_gradientY.DeltaT) * deltay / (temperature_gradientY.Distance);
+    temp_bottom = temperature_gradientY.base_temp - BASE_POS * GRADIENT;
+    apply_temperature_gradientY(gridinfo, shift_OFFSET, tt);
+  }
+  if (tt % 100 == 0) {
+    if (SHIFT) {
+      if (MAX_INTERFACE_POS > shiftj) shift_ON = 1;
+      if (shift_ON) {
+        apply_shiftY(gridinfo, MAX_INTERFACE_POS);
+        shift_OFFSET += (MAX_INTERFACE_POS - shiftj);
+        shift_ON = 0;
+      }
+    }
+  }
+}
+
 static void smooth_steps(long ns) {
   long s;
   for (s = 1; s < ns; s++) {           /* microsim_gp.c:97-100 */
@@ -183,12 +216,13 @@ static void smooth_steps(long ns) {
 
 static void time_steps(long nsteps) {
   long s;
-  for (s = 1; s <= nsteps; s++) {      /* microsim_gp.c:102-106 */
+  for (s = 1; s <= nsteps; s++) {      /* microsim_gp.c:102-126 */
     t = (int)s;
     solverloop_phasefield(start, end);
     apply_boundary_conditions(0);
     solverloop_concentration(start, end);
     apply_boundary_conditions(0);
+    after_step(s);
   }
 }
 
@@ -234,6 +268,7 @@ int main(int argc, char *argv[]) {
   if (strcmp(mode, "run") == 0 && argc == 7) {
     long ns = atol(argv[4]);
     fill(argv);
+    temp_init();
     apply_boundary_conditions(0);
     smooth_steps(ns < 0 ? nsmooth : ns);
     time_steps(atol(argv[5]));
@@ -241,6 +276,7 @@ int main(int argc, char *argv[]) {
   } else if (strcmp(mode, "load") == 0 && argc == 8) {
     long ns = atol(argv[5]);
     load_state(argv[4]);
+    temp_init();
     apply_boundary_conditions(0);
     smooth_steps(ns < 0 ? nsmooth : ns);
     time_steps(atol(argv[6]));
@@ -248,6 +284,7 @@ int main(int argc, char *argv[]) {
   } else if (strcmp(mode, "time") == 0 && argc == 5) {
     double t0, t1;
     fill(argv);
+    temp_init();
     apply_boundary_conditions(0);
     smooth_steps(nsmooth);
     t0 = now_s();
@@ -262,6 +299,7 @@ int main(int argc, char *argv[]) {
     av[0] = argv[0]; av[1] = argv[1]; av[2] = argv[2]; av[3] = argv[5];
     mkdir("DATA", 0777);
     fill(argv);
+    temp_init();
     apply_boundary_conditions(0);
     smooth_steps(nsmooth);
     time_steps(atol(argv[4]));
@@ -278,7 +316,23 @@ int main(int argc, char *argv[]) {
       if (ASCII) readfromfile_serial2D(gridinfo, av, STARTTIME);
       else readfromfile_serial2D_binary(gridinfo, av, STARTTIME);
       init_propertymatrices(T);
+      if (SHIFT) {
+        FILE *fp = fopen("DATA/shift.dat", "r");
+        for (file_iter = 0; file_iter <= STARTTIME / saveT; file_iter++) fscanf(fp, "%ld %ld\n", &time_file, &position);
+        fclose(fp);
+        shift_position = position;
+      }
+      if (!ISOTHERMAL) {
+        if (SHIFT)
+          temperature_gradientY.gradient_OFFSET = (temperature_gradientY.gradient_OFFSET) +
+                                                  floor((temperature_gradientY.velocity) * (STARTTIME * deltat)) -
+                                                  shift_position * deltay;
+        else
+          temperature_gradientY.gradient_OFFSET = (temperature_gradientY.gradient_OFFSET) +
+                                                  floor((temperature_gradientY.velocity) * (STARTTIME * deltat));
+      }
     }
+    temp_init();
     apply_boundary_conditions(0);
     if ((RESTART == 0) || (STARTTIME == 0)) {
       if (ASCII == 0) writetofile_serial2D_binary(gridinfo, av, 0);
@@ -290,6 +344,7 @@ int main(int argc, char *argv[]) {
       apply_boundary_conditions(0);
       solverloop_concentration(start, end);
       apply_boundary_conditions(0);
+      after_step(t);
       if (t % saveT == 0) {
         if (ASCII == 0) writetofile_serial2D_binary(gridinfo, av, t + STARTTIME);
         else writetofile_serial2D(gridinfo, av, t + STARTTIME);

@@ -38,6 +38,17 @@ PARITY_CASES = {
         covers="DILUTE inversion, K=2, 3 phases, dx=1.5 (true divisions)",
         kw=dict(N=3, K=2, mesh=(36, 36), mode="dilute", dx=1.5, dt=0.04, aniso=False, dab=0.0),
         seeds=[(0, 12, 12, 6.0), (1, 24, 24, 6.0)]),
+    "dirsolid_binary": dict(
+        covers="non-isothermal: a temperature gradient moving along y (Tempgrady), solid at the bottom, "
+               "anisotropic, periodic x / Neumann y; T-dependent c(mu), Mu, B and C per cell",
+        kw=dict(N=2, K=1, mesh=(40, 64), dab=0.03, bc_phi=(3, 3, 1, 1), d_solid=0.0, T=1.0, Teq=1.0,
+                tempgrady=(0.97, 0.06, 60.0, 20.0, 0.5)),
+        cubes=[(0, 0, 0, 39, 18)], seeds=[(0, 10, 19, 3.0), (0, 27, 19, 4.0)]),
+    "dirsolid_ternary3": dict(
+        covers="non-isothermal ternary 3-phase (TERNARY inversion), two solids growing from the bottom",
+        kw=dict(N=3, K=2, mesh=(36, 56), dab=0.02, bc_phi=(3, 3, 1, 1), A_off=0.25, T=1.0, Teq=1.0,
+                tempgrady=(0.97, 0.06, 60.0, 20.0, 0.5)),
+        cubes=[(0, 0, 0, 17, 14), (1, 18, 0, 35, 14)], seeds=[(0, 9, 15, 3.0)]),
     "bin_mixed_bc": dict(
         covers="phi periodic in y, mu Neumann everywhere; different copy tables per field",
         kw=dict(N=2, K=1, mesh=(40, 40), bc_phi=(1, 1, 3, 3), bc_mu=(1, 1, 1, 1)),

@@ -68,3 +68,63 @@ def test_long_run_bitwise(tmp_path, name, scale, chunks):
     # the interface moved: the run exercises the interface tiles throughout
     solid = ph[:-1].sum()
     assert solid > 0 and not np.all((ph == 0) | (ph == 1))
+
+
+@pytest.mark.parametrize("name", ["dirsolid_binary", "dirsolid_ternary3"])
+def test_directional_solidification_bitwise(tmp_path, name):
+    """Non-isothermal runs (a temperature gradient moving along y): 300 steps
+    bit-identical to the oracle, which equals the reference on these decks."""
+    from gp_cases import PARITY_CASES, build_case
+    ip, fp = build_case(tmp_path, name)
+    p = gp.load_params(ip)
+    phi, mu = gp.fill(p, fp)
+    o = Oracle(p, recip_div=1)
+    o.set(phi, mu)
+    o.smooth(p.nsmooth - 1)
+    with gp.Simulation(p, phi, mu) as sim:
+        sim.smooth(p.nsmooth - 1)
+        _compare(sim, o, name + " after smoothing")
+        done = 0
+        for n in (1, 99, 200):
+            o.step(n)
+            st = sim.step(n)
+            done += n
+            _compare(sim, o, "%s after %d steps" % (name, done))
+        ost = o.stats()
+        for k in ("phi_max", "phi_min", "mu_max", "mu_min"):
+            assert st[k] == ost[k], k
+        for k in ("rel_change_phi", "rel_change_mu", "phi_sum", "comp_sum"):
+            np.testing.assert_allclose(st[k], ost[k], rtol=1e-10, atol=1e-300, err_msg=k)
+
+
+def test_moving_frame_bitwise(tmp_path):
+    """Directional solidification with the moving frame (Shift = 1): the
+    fields shift down at step 100 once the interface passes Shiftj, the
+    temperature field follows (its offset moves with the frame); 250 steps
+    bit-identical to the oracle, which equals the reference on this deck.
+    (After a shift the reference's ghost columns hold shifted values until its
+    next boundary copy; with solid at the bottom and liquid at the top of the
+    frame no phase is active there and the delta-phi they feed is 0 either
+    way.)"""
+    from gp_cases import PARITY_CASES
+    from eshwar_dipan_b200.workloads import write_case
+    c = PARITY_CASES["dirsolid_binary"]
+    ip, fp = write_case(str(tmp_path), "frame", dict(c["kw"], shift=True, shiftj=20), seeds=c["seeds"],
+                        cubes=c["cubes"])
+    p = gp.load_params(ip)
+    phi, mu = gp.fill(p, fp)
+    o = Oracle(p, recip_div=1)
+    o.set(phi, mu)
+    o.smooth(p.nsmooth - 1)
+    with gp.Simulation(p, phi, mu) as sim:
+        sim.smooth(p.nsmooth - 1)
+        done = 0
+        for n in (99, 1, 50, 100):   # the shift after step 100, the graph path after it
+            o.step(n)
+            st = sim.step(n)
+            done += n
+            _compare(sim, o, "moving frame after %d steps" % done)
+        ost = o.stats()
+        assert st["shift_offset"] == ost["shift_offset"] > 0
+        for k in ("phi_max", "phi_min", "mu_max", "mu_min"):
+            assert st[k] == ost[k], k

@@ -107,3 +107,27 @@ def test_oracle_matches_reference_on_shrunk_cfg2(tmp_path):
     assert bits_equal(mu, ref["mu"]), mismatch_report(mu, ref["mu"])
     inner = phi[:, 3:p.mesh_x + 3, 3:p.mesh_y + 3]
     assert not np.all((inner == 0) | (inner == 1))
+
+
+@needs_ref
+@pytest.mark.parametrize("shift", [False, True])
+def test_oracle_matches_reference_directional(tmp_path, shift):
+    """Directional solidification over 250 steps: the temperature field moves
+    with the gradient after every step (microsim_gp.c:108-113) and, with the
+    moving frame, the fields shift down at steps 100 and 200
+    (microsim_gp.c:115-126, shift.h): the oracle equals the reference bit for
+    bit (full ghosted phi and mu)."""
+    from gp_cases import PARITY_CASES
+    from eshwar_dipan_b200.workloads import write_case
+    c = PARITY_CASES["dirsolid_binary"]
+    kw = dict(c["kw"], shift=shift, shiftj=20)
+    ip, fp = write_case(str(tmp_path), "ds", kw, seeds=c["seeds"], cubes=c["cubes"])
+    p, o = _run_oracle(ip, fp, 9, 250, recip_div=0)
+    ref = harness_run(ip, fp, 9, 250, tmp_path)
+    phi, mu, _ = o.get_full()
+    assert bits_equal(phi, ref["phi"]), mismatch_report(phi, ref["phi"])
+    assert bits_equal(mu, ref["mu"]), mismatch_report(mu, ref["mu"])
+    if shift:
+        # the frame moved: the solid front sits near column shiftj, not where it grew to
+        solid_rows = (phi[0, 3:-3, 3:-3] > 0.5).sum(axis=1)
+        assert solid_rows.max() < 25
