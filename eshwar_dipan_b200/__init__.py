@@ -52,11 +52,20 @@ def fill(p, filling_path):
     return phi, mu
 
 
-def vtk_write(p, path, phi, mu, ascii=None):
+def vtk_write(p, path, phi, mu, ascii=None, temperature=None):
+    """gp_vtk_write / gp_vtk_write_temperature: a non-isothermal run also
+    writes its temperature field ([MESH_X][MESH_Y]; None = the field laid
+    down at start-up)."""
     phi = np.ascontiguousarray(phi, dtype=np.float64)
     mu = np.ascontiguousarray(mu, dtype=np.float64)
     a = p.ascii if ascii is None else int(ascii)
-    check(lib().gp_vtk_write(ctypes.byref(p), str(path).encode(), _ptr(phi), _ptr(mu), a))
+    if temperature is None:
+        check(lib().gp_vtk_write(ctypes.byref(p), str(path).encode(), _ptr(phi), _ptr(mu), a))
+        return
+    T = np.ascontiguousarray(temperature, dtype=np.float64)
+    if T.shape != (p.mesh_x, p.mesh_y):
+        raise ValueError("temperature must be [MESH_X][MESH_Y]")
+    check(lib().gp_vtk_write_temperature(ctypes.byref(p), str(path).encode(), _ptr(phi), _ptr(mu), _ptr(T), a))
 
 
 def vtk_read(p, path, ascii=None):
@@ -180,6 +189,13 @@ class Simulation:
         phi = np.ascontiguousarray(phi, dtype=np.float64)
         mu = np.ascontiguousarray(mu, dtype=np.float64)
         check(lib().gp_set(self._h, _ptr(phi), _ptr(mu)), self._h)
+
+    def temperature(self):
+        """gp_temperature: the interior temperature field [MESH_X][MESH_Y]
+        after the steps taken so far."""
+        T = np.zeros((self.params.mesh_x, self.params.mesh_y), dtype=np.float64)
+        check(lib().gp_temperature(self._h, _ptr(T)), self._h)
+        return T
 
     def vtk_write_async(self, path, ascii=None):
         """gp_vtk_write_async: write the current state to `path` in the

@@ -124,6 +124,8 @@ SIGNATURES = {
     "gp_params_load": (c_int, [POINTER(Params), ctypes.c_char_p]),
     "gp_fill": (c_int, [POINTER(Params), ctypes.c_char_p, c_void_p, c_void_p]),
     "gp_vtk_write": (c_int, [POINTER(Params), ctypes.c_char_p, c_void_p, c_void_p, c_int]),
+    "gp_vtk_write_temperature": (c_int, [POINTER(Params), ctypes.c_char_p, c_void_p, c_void_p, c_void_p, c_int]),
+    "gp_temperature": (c_int, [c_void_p, c_void_p]),
     "gp_vtk_read": (c_int, [POINTER(Params), ctypes.c_char_p, c_void_p, c_void_p, c_int]),
     "gp_vtk_write_async": (c_int, [c_void_p, ctypes.c_char_p, c_int]),
     "gp_vtk_wait": (c_int, [c_void_p]),

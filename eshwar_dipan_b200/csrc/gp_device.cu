@@ -258,10 +258,11 @@ struct gp_ctx {
   std::thread *writer;          /* the write in flight, or NULL */
   int wstatus;                  /* its result */
   char werr[256];
-  void *snap;                   /* device copy of the state being written */
+  void *snap;                   /* device copy of the state being written (then the frame state) */
+  long long wsteps;             /* steps taken when the snapshot was queued */
   cudaStream_t wstream;         /* the writer's copies */
   cudaEvent_t wready;           /* the snapshot is complete */
-  double *hphi, *hmu;           /* host copies of the snapshot */
+  double *hphi, *hmu, *htemp;   /* host copies of the snapshot; its temperature field */
 };
 
 static int fail(gp_ctx *c, int code, const char *fmt, ...) {
@@ -1166,8 +1167,31 @@ void gp_destroy(gp_ctx *c) {
   if (c->wready) cudaEventDestroy(c->wready);
   free(c->hphi);
   free(c->hmu);
+  free(c->htemp);
   gp_batch_destroy(c->b);
   free(c);
+}
+
+/* The temperature field [mx][my] of simulation 0 after `steps` steps with the
+ * frame state `dd`: the field laid down after the last step (with shift_OFFSET
+ * as it was then) and moved with the frame when the frame moved at that step,
+ * as kt_rows lays it for the next step's phase-field pass. */
+static void temperature_field(const gp_batch *b, long long steps, const gpd::SimDyn &dd, double *T) {
+  const gp_derived &d = b->derived[0];
+  const size_t mx = (size_t)d.mx, my = (size_t)d.my;
+  if (!d.tgrad) {
+    for (size_t i = 0; i < mx * my; i++) T[i] = b->params[0].T;
+    return;
+  }
+  gp_host_temperature_column(&d, steps, dd.fresh ? dd.shift_T : dd.shift_off, dd.fresh ? dd.dlast : 0, T);
+  for (size_t x = 1; x < mx; x++) memcpy(T + x * my, T, sizeof(double) * my);
+}
+
+/* Bytes of the state planes of simulation 0 in a snapshot (16-byte multiple:
+ * the frame state follows them). */
+static size_t snap_state_bytes(const gp_batch *b) {
+  const size_t n = (size_t)(b->N + b->K) * b->desc[0].g.plane * b->elem;
+  return (n + 15) & ~(size_t)15;
 }
 
 /* The writer thread of gp_vtk_write_async: wait for the snapshot, bring it
@@ -1191,6 +1215,18 @@ static void vtk_writer(gp_ctx *c, std::string path, int ascii) {
   if (e != cudaSuccess) {
     snprintf(c->werr, sizeof c->werr, "gp_vtk_write_async: %s", cudaGetErrorString(e));
     rc = GP_ECUDA;
+  } else if (b->derived[0].tgrad) {
+    gpd::SimDyn dd;
+    e = cudaMemcpyAsync(&dd, (char *)c->snap + snap_state_bytes(b), sizeof dd, cudaMemcpyDeviceToHost, c->wstream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->wstream);
+    if (e != cudaSuccess) {
+      snprintf(c->werr, sizeof c->werr, "gp_vtk_write_async: %s", cudaGetErrorString(e));
+      rc = GP_ECUDA;
+    } else {
+      temperature_field(b, c->wsteps, dd, c->htemp);
+      if ((rc = gp_vtk_write_temperature(&b->params[0], path.c_str(), c->hphi, c->hmu, c->htemp, ascii)) != GP_OK)
+        snprintf(c->werr, sizeof c->werr, "%s", gp_host_thread_error());
+    }
   } else if ((rc = gp_vtk_write(&b->params[0], path.c_str(), c->hphi, c->hmu, ascii)) != GP_OK) {
     snprintf(c->werr, sizeof c->werr, "%s", gp_host_thread_error());
   }
@@ -1217,20 +1253,24 @@ int gp_vtk_write_async(gp_ctx *c, const char *path, int ascii) {
   c->err[0] = 0;
   gp_batch *b = c->b;
   const gpd::SimDesc &sd = b->desc[0];
-  const size_t bytes = (size_t)(b->N + b->K) * sd.g.plane * b->elem;
+  const size_t bytes = snap_state_bytes(b);
   if (!c->snap) {
     const size_t cells = (size_t)sd.g.mx * sd.g.my;
-    CK(cudaMalloc(&c->snap, bytes));
+    CK(cudaMalloc(&c->snap, bytes + sizeof(gpd::SimDyn)));
     CK(cudaStreamCreateWithFlags(&c->wstream, cudaStreamNonBlocking));
     CK(cudaEventCreateWithFlags(&c->wready, cudaEventDisableTiming));
     c->hphi = (double *)malloc(sizeof(double) * cells * b->N);
     c->hmu = (double *)malloc(sizeof(double) * cells * b->K);
-    if (!c->hphi || !c->hmu) return fail(c, GP_ENOMEM, "gp_vtk_write_async: out of host memory");
+    c->htemp = (double *)malloc(sizeof(double) * cells);
+    if (!c->hphi || !c->hmu || !c->htemp) return fail(c, GP_ENOMEM, "gp_vtk_write_async: out of host memory");
   }
   /* the snapshot is ordered after the steps already queued; later steps
-   * write the other state buffer or this one after the copy has read it */
+   * write the other state buffer or this one after the copy has read it.  The
+   * frame state (which sets the temperature field) travels with it. */
   CK(cudaMemcpyAsync(c->snap, (char *)b->state[b->cur] + (size_t)sd.off_state * b->elem, bytes,
                      cudaMemcpyDeviceToDevice, b->stream));
+  CK(cudaMemcpyAsync((char *)c->snap + bytes, b->dyn, sizeof(gpd::SimDyn), cudaMemcpyDeviceToDevice, b->stream));
+  c->wsteps = b->steps;
   CK(cudaEventRecord(c->wready, b->stream));
   try {
     c->writer = new std::thread(vtk_writer, c, std::string(path), ascii);
@@ -1307,6 +1347,17 @@ int gp_step_kernel_times(gp_ctx *c, long nsteps, gp_kernel_times *t) {
 int gp_get_stats(gp_ctx *c, gp_stats *s) {
   if (!c || !s) return fail(c, GP_EINVAL, "gp_get_stats: bad argument");
   *s = c->b->last[0];
+  return GP_OK;
+}
+
+int gp_temperature(gp_ctx *c, double *T) {
+  if (!c || !T) return fail(c, GP_EINVAL, "gp_temperature: NULL argument");
+  gp_batch *b = c->b;
+  gpd::SimDyn dd;
+  CK(cudaSetDevice(b->dev));
+  CK(cudaMemcpyAsync(&dd, b->dyn, sizeof dd, cudaMemcpyDeviceToHost, b->stream));
+  CK(cudaStreamSynchronize(b->stream));
+  temperature_field(b, b->steps, dd, T);
   return GP_OK;
 }
 

@@ -271,9 +271,36 @@ static int put_row(FILE *f, const double *v, long MY, int ascii, const char *fmt
   return fwrite(buf, 1, n, f) == n ? 0 : -1;
 }
 
+/* The temperature of each interior column y of a non-isothermal run after
+ * `steps` time steps: temp_bottom + y_g*GRADIENT over the ghosted column y_g =
+ * y + 3 (apply_temperature_gradientY, Temperature_gradient.h:4-29), with
+ * BASE_POS and temp_bottom of microsim_gp.c:77-82 at steps = 0 and of
+ * microsim_gp.c:108-113 after step `steps`.  shift_off is shift_OFFSET when
+ * the field was laid down; when the frame then moved by dshift > 0 cells
+ * (apply_shiftY, shift.h:4-45) column y_g holds the value laid at y_g + dshift,
+ * the top dshift ghosted columns keep their own. */
+void gp_host_temperature_column(const gp_derived *d, long long steps, long long shift_off, long dshift, double *Ty) {
+  long y;
+  const long ry = d->my + 6;
+  double base_pos, grad, tb;
+  if (steps == 0) base_pos = (d->tg_off / d->dy) - (double)shift_off;
+  else base_pos = (d->tg_off / d->dy) - (double)shift_off + ((d->tg_vel / d->dy) * ((double)steps * d->dt));
+  grad = (d->tg_dT) * d->dy / (d->tg_dist);
+  tb = d->tg_base - base_pos * grad;
+  for (y = 0; y < d->my; y++) {
+    const long yg = y + 3;
+    Ty[y] = yg <= ry - 1 - dshift ? tb + (double)(yg + dshift) * grad : tb + (double)yg * grad;
+  }
+}
+
+int gp_vtk_write(const gp_params *p, const char *path, const double *phi, const double *mu, int ascii) {
+  return gp_vtk_write_temperature(p, path, phi, mu, NULL, ascii);
+}
+
 /* write_cells_vtk_2D / write_cells_vtk_2D_binary (file_writer.h:71-255):
  * the same bytes, written a row at a time. */
-int gp_vtk_write(const gp_params *p, const char *path, const double *phi, const double *mu, int ascii) {
+int gp_vtk_write_temperature(const gp_params *p, const char *path, const double *phi, const double *mu,
+                             const double *temperature, int ascii) {
   FILE *f;
   long x, y, MX, MY;
   int a, k, N, K, bad = 0;
@@ -281,16 +308,23 @@ int gp_vtk_write(const gp_params *p, const char *path, const double *phi, const 
   char err[256];
   int have_d = 0;
   char *buf;
-  double *row;
+  double *row, *tcol = NULL;
+  const double *T = temperature;
   size_t bufn;
   if (!p || !path || !phi || !mu) { gp_set_thread_error("gp_vtk_write: NULL argument"); return GP_EINVAL; }
   N = p->numphases; K = p->numcomponents - 1; MX = p->mesh_x; MY = p->mesh_y;
-  if (p->writecomposition) {
+  if (p->writecomposition || (!p->isothermal && !T)) {
     if (gp_host_derive(p, &d, err, sizeof err) != GP_OK) {
       gp_set_thread_error("gp_vtk_write: %s", err);
       return GP_EINVAL;
     }
     have_d = 1;
+  }
+  if (!p->isothermal && !T) {
+    /* the field laid down at start-up (microsim_gp.c:77-82) */
+    tcol = malloc(sizeof(double) * (size_t)MY);
+    if (!tcol) { gp_set_thread_error("gp_vtk_write: out of host memory"); return GP_ENOMEM; }
+    gp_host_temperature_column(&d, 0, 0, 0, tcol);
   }
   bufn = (size_t)MY * 32 + 64;   /* "%le" is at most 13 characters plus sign and separators */
   buf = malloc(bufn);
@@ -298,6 +332,7 @@ int gp_vtk_write(const gp_params *p, const char *path, const double *phi, const 
   if (!buf || !row) {
     free(buf);
     free(row);
+    free(tcol);
     gp_set_thread_error("gp_vtk_write: out of host memory");
     return GP_ENOMEM;
   }
@@ -305,6 +340,7 @@ int gp_vtk_write(const gp_params *p, const char *path, const double *phi, const 
   if (!f) {
     free(buf);
     free(row);
+    free(tcol);
     gp_set_thread_error("cannot write %s", path);
     return GP_EIO;
   }
@@ -340,8 +376,13 @@ int gp_vtk_write(const gp_params *p, const char *path, const double *phi, const 
           for (b = 0; b < N; b++) ph[b] = phi[((long)b * MX + x) * MY + y];
           for (l = 0; l < K; l++) m[l] = mu[((long)l * MX + x) * MY + y];
           for (b = 0; b < N; b++) {
-            double cmu_v = 0.0;   /* c_mu (functionF_01.h:30-37) */
-            for (l = 0; l < K; l++) cmu_v += d.cmu[b][k][l] * (m[l] - d.E[b][l]);
+            double cmu_v = 0.0;   /* c_mu (functionF_01.h:30-37), at the cell's temperature when not isothermal */
+            if (p->isothermal)
+              for (l = 0; l < K; l++) cmu_v += d.cmu[b][k][l] * (m[l] - d.E[b][l]);
+            else {
+              const double Tc = T ? T[x * MY + y] : tcol[y];
+              for (l = 0; l < K; l++) cmu_v += d.cmu[b][k][l] * (m[l] - (d.Beq[b][l] + d.dBbdT[b][l] * (Tc - d.Teq)));
+            }
             comp += cmu_v * host_hphi(ph, N, b);
           }
           row[y] = comp;
@@ -351,8 +392,15 @@ int gp_vtk_write(const gp_params *p, const char *path, const double *phi, const 
       if (ascii) fprintf(f, "\n");
     }
   }
+  if (!p->isothermal) {
+    /* the temperature block, without a closing blank line (file_writer.h:138-148, 238-250) */
+    fprintf(f, "SCALARS Temperature double 1\n");
+    fprintf(f, "LOOKUP_TABLE default\n");
+    for (x = 0; x < MX && !bad; x++) bad = put_row(f, T ? T + x * MY : tcol, MY, ascii, "%le \n", buf, bufn);
+  }
   free(buf);
   free(row);
+  free(tcol);
   if (fclose(f) != 0 || bad) { gp_set_thread_error("error writing %s", path); return GP_EIO; }
   return GP_OK;
 }

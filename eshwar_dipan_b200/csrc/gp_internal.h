@@ -90,6 +90,11 @@ void gp_host_property_matrices(const gp_params *p, double Tq,
                                double Beq[GP_MAX_PHASES][GP_MAX_COMP],
                                double dBbdT[GP_MAX_PHASES][GP_MAX_COMP]);
 
+/* The reference's temperature of each interior column [MESH_Y] of a
+ * non-isothermal run after `steps` steps, laid down with shift_OFFSET =
+ * shift_off and then moved by a frame shift of dshift cells (0: none). */
+void gp_host_temperature_column(const gp_derived *d, long long steps, long long shift_off, long dshift, double *Ty);
+
 void gp_set_thread_error(const char *fmt, ...);
 
 #ifdef __cplusplus

@@ -7,9 +7,11 @@
  * parse the input, fill (or restart from DATA/NAME_<STARTTIME>.vtk), write the
  * t=0 VTK, run NSMOOTH-1 smoothing sweeps, then NTIMESTEPS steps on the GPU,
  * writing DATA/NAME_<t>.vtk every SAVET steps (in the background, while the
- * next steps run; plus DATA/shift.dat) and the progress record every
- * TRACK_PROGRESS steps.  The progress sums cover the
- * interior cells only (see gp_stats in gp.h).
+ * next steps run; plus the frame position in DATA/shift.dat) and the progress
+ * record every TRACK_PROGRESS steps.  A restart (STARTTIME, RESTART) reads the
+ * state from DATA/NAME_<STARTTIME>.vtk and, with the moving frame, its
+ * position from DATA/shift.dat.  The progress sums cover the interior cells
+ * only (see gp_stats in gp.h).
  */
 #include <math.h>
 #include <stdio.h>
@@ -39,7 +41,7 @@ int main(int argc, char **argv) {
   gp_stats st;
   char path[1200];
   int rc, a, k, N, K, max_length;
-  long t, chunk;
+  long t, chunk, shift_position = 0;
   double *phi, *mu;
   if (argc < 4) {
     fprintf(stderr, "usage: %s Input.in Filling.in NAME\n", argv[0]);
@@ -47,10 +49,6 @@ int main(int argc, char **argv) {
   }
   mkdir("DATA", 0777);
   if ((rc = gp_params_load(&p, argv[1])) != GP_OK) return die("reading the input file", rc, NULL);
-  if (p.shift) {
-    fprintf(stderr, "gp_microsim: Shift=1 (moving frame) is not implemented\n");
-    return 1;
-  }
   N = p.numphases;
   K = p.numcomponents - 1;
   phi = malloc(sizeof(double) * (size_t)N * p.mesh_x * p.mesh_y);
@@ -61,6 +59,24 @@ int main(int argc, char **argv) {
   } else {
     snprintf(path, sizeof path, "DATA/%s_%ld.vtk", argv[3], p.starttime);
     if ((rc = gp_vtk_read(&p, path, phi, mu, p.ascii)) != GP_OK) return die("reading the restart file", rc, NULL);
+    if (p.shift) {
+      /* the frame position at STARTTIME: line STARTTIME/SAVET of DATA/shift.dat (microsim_gp.c:58-66) */
+      FILE *fs = fopen("DATA/shift.dat", "r");
+      long i, tf = 0, pos = 0;
+      if (!fs) return die("reading DATA/shift.dat", GP_EIO, NULL);
+      for (i = 0; i <= p.starttime / (p.savet > 0 ? p.savet : 1); i++)
+        if (fscanf(fs, "%ld %ld\n", &tf, &pos) != 2) break;
+      fclose(fs);
+      shift_position = pos;
+    }
+    if (!p.isothermal) {
+      /* the temperature field resumes where it was (microsim_gp.c:67-73) */
+      if (p.shift)
+        p.tempgrady_v[3] = (p.tempgrady_v[3]) + floor((p.tempgrady_v[4]) * (p.starttime * p.deltat)) -
+                           shift_position * p.deltay;
+      else
+        p.tempgrady_v[3] = (p.tempgrady_v[3]) + floor((p.tempgrady_v[4]) * (p.starttime * p.deltat));
+    }
   }
   if ((rc = gp_init(&c, &p, phi, mu, GP_FP64)) != GP_OK) return die("gp_init", rc, NULL);
   if (p.restart == 0 || p.starttime == 0) {
@@ -93,7 +109,7 @@ int main(int argc, char **argv) {
       if ((rc = gp_vtk_write_async(c, path, p.ascii)) != GP_OK) return die("writing VTK", rc, c);
       f = fopen("DATA/shift.dat", "a");
       if (f) {
-        fprintf(f, "%ld %ld\n", t + p.starttime, 0L);
+        fprintf(f, "%ld %ld\n", t + p.starttime, (long)st.shift_offset + shift_position);
         fclose(f);
       }
     }

@@ -131,8 +131,18 @@ int gp_fill(const gp_params *p, const char *filling_path, double *phi, double *m
 
 /* Legacy-VTK writer/reader of the interior.  Replaces writetofile_serial2D[_binary]
  * and readfromfile_serial2D[_binary] (file_writer.h:23-70,71-416).
- * ascii=1: "%le" text; ascii=0: big-endian float64. */
+ * ascii=1: "%le" text; ascii=0: big-endian float64.  A non-isothermal run
+ * (ISOTHERMAL = 0) also writes the Temperature field, and its optional
+ * composition fields are taken at each cell's temperature: gp_vtk_write uses
+ * the field laid down at start-up (microsim_gp.c:77-82), as a file written
+ * before the first step holds; gp_vtk_write_temperature takes the field
+ * [MESH_X][MESH_Y] (gp_temperature gives a context's; NULL = the start-up
+ * field; ignored when isothermal).  The reader reads phi and mu and skips the
+ * fields after them (the reference lays the temperature field down again
+ * after reading, microsim_gp.c:75-82). */
 int gp_vtk_write(const gp_params *p, const char *path, const double *phi, const double *mu, int ascii);
+int gp_vtk_write_temperature(const gp_params *p, const char *path, const double *phi, const double *mu,
+                             const double *temperature, int ascii);
 int gp_vtk_read(const gp_params *p, const char *path, double *phi, double *mu, int ascii);
 
 /* Write the context's current state to `path` as gp_vtk_write does, in the
@@ -155,7 +165,9 @@ int gp_vtk_wait(gp_ctx *ctx);
  * Replaces serialinfo_xy (serialinfo_xy.h:1-66) + initialize_functions_solverloop
  * (initialize_functions_solverloop.h:4-58) + apply_boundary_conditions(0) at
  * microsim_gp.c:84.  GP_EINVAL for combinations the kernels do not cover
- * (N>4, K>2, non-isothermal, noise, free/Dirichlet BCs, 3-D). */
+ * (N>4, K>2, noise, free/Dirichlet BCs, 3-D).  A non-isothermal run
+ * (ISOTHERMAL = 0) carries the temperature gradient along y of Tempgrady and,
+ * with Shift = 1, the moving frame. */
 int gp_init(gp_ctx **ctx, const gp_params *p, const double *phi, const double *mu,
             gp_precision prec);
 
@@ -188,6 +200,13 @@ int gp_get_dev(gp_ctx *ctx, double *phi_dev, double *mu_dev);
 int gp_set_dev(gp_ctx *ctx, const double *phi_dev, const double *mu_dev);
 
 int gp_get_stats(gp_ctx *ctx, gp_stats *stats);
+
+/* The temperature of every interior cell [MESH_X][MESH_Y] as the reference
+ * holds it after the steps taken so far (gridinfo[].temperature: laid down by
+ * apply_temperature_gradientY after each step, Temperature_gradient.h:4-29 and
+ * microsim_gp.c:108-113, then moved with the frame by apply_shiftY,
+ * shift.h:4-45).  An isothermal run has T everywhere. */
+int gp_temperature(gp_ctx *ctx, double *temperature);
 
 /* gp_step with CUDA events recorded on the context's stream: total_ms is the
  * device time of the nsteps steps.  A step is two kernels: the bulk-tile

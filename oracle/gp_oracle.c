@@ -1217,6 +1217,12 @@ void gpo_get(const gpo *o, double *phi, double *mu) {
       for (y = 0; y < o->my; y++) mu[((long)k * o->mx + x) * o->my + y] = F(o->mu, o, k)[I(o, x + 3, y + 3)];
 }
 
+void gpo_temperature(const gpo *o, double *T) {
+  long x, y;
+  for (x = 0; x < o->mx; x++)
+    for (y = 0; y < o->my; y++) T[x * o->my + y] = o->tgrad ? o->Tc[I(o, x + 3, y + 3)] : o->T;
+}
+
 void gpo_get_full(const gpo *o, double *phi, double *mu, double *dphi) {
   if (phi) memcpy(phi, o->phi, sizeof(double) * (size_t)o->N * o->n);
   if (mu) memcpy(mu, o->mu, sizeof(double) * (size_t)o->K * o->n);

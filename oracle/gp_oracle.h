@@ -26,6 +26,8 @@ void gpo_dims(const gpo *o, long *rows_x, long *rows_y);
 int gpo_set(gpo *o, const double *phi, const double *mu);      /* interior; applies BCs */
 void gpo_get(const gpo *o, double *phi, double *mu);           /* interior */
 void gpo_get_full(const gpo *o, double *phi, double *mu, double *dphi); /* ghosted */
+/* interior temperature field [mx][my] (gridinfo[].temperature); T when isothermal */
+void gpo_temperature(const gpo *o, double *T);
 void gpo_smooth(gpo *o, long nsteps);
 void gpo_step(gpo *o, long nsteps);
 void gpo_stats(const gpo *o, gp_stats *s);

@@ -30,7 +30,7 @@ def olib():
         L.gpo_create.restype = ctypes.c_void_p
         L.gpo_create.argtypes = [ctypes.POINTER(Params), ctypes.c_int, ctypes.c_char_p, ctypes.c_int]
         for n in ("gpo_destroy", "gpo_set", "gpo_get", "gpo_get_full", "gpo_smooth", "gpo_step",
-                  "gpo_stats", "gpo_dims", "gpo_consts"):
+                  "gpo_stats", "gpo_dims", "gpo_consts", "gpo_temperature"):
             getattr(L, n).argtypes = None
         L.gpo_smooth.argtypes = [ctypes.c_void_p, ctypes.c_long]
         L.gpo_step.argtypes = [ctypes.c_void_p, ctypes.c_long]
@@ -63,6 +63,12 @@ class Oracle:
         mu = np.zeros((self.K, self.mx, self.my))
         olib().gpo_get(self.h, _p(phi), _p(mu))
         return phi, mu
+
+    def temperature(self):
+        """the interior temperature field [mx][my] (gpo_temperature)"""
+        T = np.zeros((self.mx, self.my), dtype=np.float64)
+        olib().gpo_temperature(self.h, _p(T))
+        return T
 
     def get_full(self):
         rx, ry = self.mx + 6, self.my + 6

@@ -85,11 +85,13 @@ def test_directional_solidification_bitwise(tmp_path, name):
         sim.smooth(p.nsmooth - 1)
         _compare(sim, o, name + " after smoothing")
         done = 0
+        assert bits_equal(sim.temperature(), o.temperature()), "temperature at the start"
         for n in (1, 99, 200):
             o.step(n)
             st = sim.step(n)
             done += n
             _compare(sim, o, "%s after %d steps" % (name, done))
+            assert bits_equal(sim.temperature(), o.temperature()), "temperature after %d steps" % done
         ost = o.stats()
         for k in ("phi_max", "phi_min", "mu_max", "mu_min"):
             assert st[k] == ost[k], k
@@ -124,6 +126,8 @@ def test_moving_frame_bitwise(tmp_path):
             st = sim.step(n)
             done += n
             _compare(sim, o, "moving frame after %d steps" % done)
+            # the temperature field as the reference holds it (moved with the frame at step 100)
+            assert bits_equal(sim.temperature(), o.temperature()), "temperature after %d steps" % done
         ost = o.stats()
         assert st["shift_offset"] == ost["shift_offset"] > 0
         for k in ("phi_max", "phi_min", "mu_max", "mu_min"):

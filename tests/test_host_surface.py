@@ -76,6 +76,46 @@ def test_vtk_writer_matches_reference(tmp_path, ascii, wc):
         next((i for i, (x, y) in enumerate(zip(a, b)) if x != y), min(len(a), len(b))), len(a), len(b))
 
 
+@needs_ref
+@pytest.mark.parametrize("ascii,wc,steps,shift", [(1, 1, 0, False), (0, 1, 0, False), (1, 0, 130, True),
+                                                  (0, 1, 130, True), (0, 1, 60, False)])
+def test_vtk_writer_nonisothermal_matches_reference(tmp_path, ascii, wc, steps, shift):
+    """Directional solidification: the writer adds the Temperature field and
+    takes the composition at each cell's temperature, as the reference's
+    writer does; the field is the oracle's (laid down after the last step and
+    moved with the frame, which here moves at step 100), or at step 0 the
+    start-up field gp_vtk_write lays down itself."""
+    from gp_cases import PARITY_CASES
+    c = PARITY_CASES["dirsolid_binary"]
+    ip, fp = write_case(str(tmp_path), "n", dict(c["kw"], shift=shift, shiftj=20, ascii=ascii, writecomposition=wc),
+                        seeds=c["seeds"], cubes=c["cubes"])
+    ref_dir = tmp_path / "ref"
+    ref_dir.mkdir()
+    _run([HARNESS, os.path.abspath(ip), os.path.abspath(fp), "vtk", str(steps), "n"], ref_dir)
+    p = gp.load_params(ip)
+    phi, mu = gp.fill(p, fp)
+    o = Oracle(p, recip_div=0)
+    o.set(phi, mu)
+    o.smooth(p.nsmooth - 1)
+    o.step(steps)
+    if shift:
+        assert o.stats()["shift_offset"] > 0
+    ph, m = o.get()
+    ours = str(tmp_path / "ours.vtk")
+    gp.vtk_write(p, ours, ph, m, temperature=o.temperature() if steps else None)
+    a = open(ours, "rb").read()
+    b = (ref_dir / "DATA" / ("n_%d.vtk" % steps)).read_bytes()
+    assert b"SCALARS Temperature double 1" in b
+    assert a == b, "first difference at byte %d of %d/%d" % (
+        next((i for i, (x, y) in enumerate(zip(a, b)) if x != y), min(len(a), len(b))), len(a), len(b))
+    # the reader takes phi and mu and passes over the fields after them
+    ph2, m2 = gp.vtk_read(p, ours)
+    if ascii:
+        rnd = np.vectorize(lambda v: float("%e" % v))
+        ph, m = rnd(ph), rnd(m)
+    assert bits_equal(ph2, ph) and bits_equal(m2, m)
+
+
 @pytest.mark.parametrize("ascii", [0, 1])
 def test_vtk_read_round_trip(tmp_path, ascii):
     """gp_vtk_read returns what gp_vtk_write wrote: the same bits in binary,
@@ -167,3 +207,57 @@ def test_cli_matches_reference_main(tmp_path, ascii):
     b = (tmp_path / "ref_restart" / "DATA" / "c_40.vtk").read_bytes()
     assert a == b, "restarted DATA/c_40.vtk differs"
     assert not (tmp_path / "ours_restart" / "DATA" / "c_0.vtk").exists()
+
+
+@pytest.mark.gpu
+@needs_ref
+def test_cli_directional_moving_frame_matches_reference_main(tmp_path):
+    """Directional solidification with the moving frame through gp_microsim and
+    through the reference's main(): the same DATA/NAME_<t>.vtk files (t = 0,
+    100, 200) and the same DATA/shift.dat (frame positions); then a restart
+    from t = 100 (which reads the frame position back from DATA/shift.dat and
+    resumes the temperature field) writes the same t = 200 file in both."""
+    from gp_cases import PARITY_CASES
+    c = PARITY_CASES["dirsolid_binary"]
+
+    def deck(d, ntimesteps, starttime=0, restart=0):
+        ip, fp = write_case(str(d), "f", dict(c["kw"], shift=True, shiftj=20, ascii=0, ntimesteps=ntimesteps),
+                            seeds=c["seeds"], cubes=c["cubes"])
+        text = open(ip).read()
+        text = text.replace("SAVET = %d;" % ntimesteps, "SAVET = 100;")
+        text = text.replace("STARTTIME = 0;", "STARTTIME = %d;" % starttime)
+        text = text.replace("RESTART = 0;", "RESTART = %d;" % restart)
+        open(ip, "w").write(text)
+        return ip, fp
+
+    ip, fp = deck(tmp_path / "deck", 200)
+    dirs = {}
+    for who in ("ref", "ours"):
+        d = tmp_path / who
+        d.mkdir()
+        cmd = [HARNESS, os.path.abspath(ip), os.path.abspath(fp), "main", "f"] if who == "ref" else \
+            [CLI, os.path.abspath(ip), os.path.abspath(fp), "f"]
+        _run(cmd, d)
+        dirs[who] = d
+    for t in (0, 100, 200):
+        a = (dirs["ours"] / "DATA" / ("f_%d.vtk" % t)).read_bytes()
+        b = (dirs["ref"] / "DATA" / ("f_%d.vtk" % t)).read_bytes()
+        assert a == b, "DATA/f_%d.vtk differs" % t
+    shift_ref = (dirs["ref"] / "DATA" / "shift.dat").read_text()
+    assert (dirs["ours"] / "DATA" / "shift.dat").read_text() == shift_ref
+    assert int(shift_ref.split()[1]) > 0   # the frame moved
+
+    ip2, _ = deck(tmp_path / "deck2", 100, starttime=100, restart=1)
+    for who in ("ref", "ours"):
+        d = tmp_path / (who + "_restart")
+        (d / "DATA").mkdir(parents=True)
+        shutil.copy(dirs[who] / "DATA" / "f_100.vtk", d / "DATA" / "f_100.vtk")
+        shutil.copy(dirs[who] / "DATA" / "shift.dat", d / "DATA" / "shift.dat")
+        cmd = [HARNESS, os.path.abspath(ip2), os.path.abspath(fp), "main", "f"] if who == "ref" else \
+            [CLI, os.path.abspath(ip2), os.path.abspath(fp), "f"]
+        _run(cmd, d)
+    a = (tmp_path / "ours_restart" / "DATA" / "f_200.vtk").read_bytes()
+    b = (tmp_path / "ref_restart" / "DATA" / "f_200.vtk").read_bytes()
+    assert a == b, "restarted DATA/f_200.vtk differs"
+    assert (tmp_path / "ours_restart" / "DATA" / "shift.dat").read_text() == \
+        (tmp_path / "ref_restart" / "DATA" / "shift.dat").read_text()
