@@ -77,6 +77,13 @@ def vtk_read(p, path, ascii=None):
     return phi, mu
 
 
+def _adj_result(out, g_phi, g_mu):
+    return {"loss": out.loss, "d_tau": out.d_tau, "d_dab": out.d_dab, "d_epsilon": out.d_epsilon,
+            "d_gamma": out.d_gamma, "phi0_bar": g_phi, "mu0_bar": g_mu,
+            "ms_forward": out.ms_forward, "ms_reverse": out.ms_reverse,
+            "snapshots": out.snapshots, "recomputed": out.recomputed}
+
+
 class Simulation:
     """One simulation resident on the current CUDA device (a gp_ctx)."""
 
@@ -91,6 +98,16 @@ class Simulation:
         h = ctypes.c_void_p()
         check(lib().gp_init(ctypes.byref(h), ctypes.byref(params), _ptr(phi), _ptr(mu), int(precision)))
         self._h = h
+
+    @classmethod
+    def from_tensors(cls, params, phi, mu, precision=GP_FP64):
+        """A simulation whose start state comes from float64 CUDA tensors
+        (gp_set_dev after a gp_init of zeros): the fields are copied on the
+        device, not through host memory."""
+        sp, sm = _shapes(params)
+        sim = cls(params, np.zeros(sp), np.zeros(sm), precision)
+        sim.set_tensors(phi, mu)
+        return sim
 
     @property
     def handle(self):
@@ -125,6 +142,12 @@ class Simulation:
         return (tot.value, a.value if split else None, b.value if split else None,
                 s.as_dict(self.N, self.K) if stats else None)
 
+    def stats(self):
+        """gp_get_stats: the progress record of the last step that asked for one"""
+        s = Stats()
+        check(lib().gp_get_stats(self._h, ctypes.byref(s)), self._h)
+        return s.as_dict(self.N, self.K)
+
     def kernel_times(self, n):
         """gp_step_kernel_times: n steps launched one by one with events around
         each kernel of the launch shape in use; a dict of summed milliseconds
@@ -142,16 +165,46 @@ class Simulation:
         check(lib().gp_get(self._h, _ptr(phi), _ptr(mu)), self._h)
         return phi, mu
 
-    def adjoint(self, nsteps, target_phi=None, phi_bar=None, mu_bar=None, checkpoint_every=0):
+    def get_tensors(self):
+        """gp_get_dev: the state as float64 CUDA tensors on the current
+        device, copied on the device"""
+        import torch
+        sp, sm = _shapes(self.params)
+        phi = torch.empty(sp, dtype=torch.float64, device="cuda")
+        mu = torch.empty(sm, dtype=torch.float64, device="cuda")
+        torch.cuda.current_stream().synchronize()   # the buffers are allocated
+        check(lib().gp_get_dev(self._h, ctypes.c_void_p(phi.data_ptr()), ctypes.c_void_p(mu.data_ptr())), self._h)
+        return phi, mu
+
+    def set_tensors(self, phi, mu):
+        """gp_set_dev: the state from float64 CUDA tensors on the context's
+        device, copied on the device"""
+        import torch
+        sp, sm = _shapes(self.params)
+        phi = phi.detach().to(torch.float64).contiguous()
+        mu = mu.detach().to(torch.float64).contiguous()
+        if tuple(phi.shape) != sp or tuple(mu.shape) != sm:
+            raise ValueError("phi/mu shapes %s/%s, expected %s/%s" % (tuple(phi.shape), tuple(mu.shape), sp, sm))
+        torch.cuda.current_stream().synchronize()   # the tensors are written
+        check(lib().gp_set_dev(self._h, ctypes.c_void_p(phi.data_ptr()), ctypes.c_void_p(mu.data_ptr())), self._h)
+
+    def adjoint(self, nsteps, target_phi=None, phi_bar=None, mu_bar=None, checkpoint_every=0, snapshots=0):
         """gp_adjoint: run nsteps from the current state (the simulation ends at
         the final state) and return a dict with the loss (with target_phi), the
         parameter gradients d_tau, d_dab, d_epsilon, d_gamma (phase pair 0,1),
-        phi0_bar / mu0_bar (gradient with respect to the start state) and the
-        device times of the two passes."""
+        phi0_bar / mu0_bar (gradient with respect to the start state), the
+        device times of the two passes, the states kept and the steps
+        recomputed.  The arrays may be numpy arrays or, all of them, CUDA
+        tensors on the context's device (the gradients then come back as CUDA
+        tensors, without a copy through host memory)."""
         sp, sm = _shapes(self.params)
+        given = [a for a in (target_phi, phi_bar, mu_bar) if a is not None]
+        if given and all(getattr(a, "is_cuda", False) for a in given):
+            return self._adjoint_dev(nsteps, target_phi, phi_bar, mu_bar, checkpoint_every, snapshots)
         req = AdjReq()
         req.nsteps = int(nsteps)
         req.checkpoint_every = int(checkpoint_every)
+        req.snapshots = int(snapshots)
         keep = []
         if phi_bar is not None:
             a = np.ascontiguousarray(phi_bar, dtype=np.float64)
@@ -173,9 +226,41 @@ class Simulation:
         out.phi0_bar = g_phi.ctypes.data
         out.mu0_bar = g_mu.ctypes.data
         check(lib().gp_adjoint(self._h, ctypes.byref(req), ctypes.byref(out)), self._h)
-        return {"loss": out.loss, "d_tau": out.d_tau, "d_dab": out.d_dab, "d_epsilon": out.d_epsilon,
-                "d_gamma": out.d_gamma, "phi0_bar": g_phi, "mu0_bar": g_mu,
-                "ms_forward": out.ms_forward, "ms_reverse": out.ms_reverse}
+        return _adj_result(out, g_phi, g_mu)
+
+    def _adjoint_dev(self, nsteps, target_phi, phi_bar, mu_bar, checkpoint_every, snapshots):
+        import torch
+        sp, sm = _shapes(self.params)
+        req = AdjReq()
+        req.nsteps = int(nsteps)
+        req.checkpoint_every = int(checkpoint_every)
+        req.snapshots = int(snapshots)
+        req.device = 1
+        keep = []
+
+        def dptr(t, shape):
+            t = t.detach().to(torch.float64).contiguous()
+            if tuple(t.shape) != shape:
+                raise ValueError("shape %s, expected %s" % (tuple(t.shape), shape))
+            keep.append(t)
+            return t.data_ptr()
+        if phi_bar is not None:
+            req.phi_bar = dptr(phi_bar, sp)
+            if mu_bar is not None:
+                req.mu_bar = dptr(mu_bar, sm)
+        elif target_phi is not None:
+            req.target_phi = dptr(target_phi, sp)
+        else:
+            raise ValueError("give target_phi or phi_bar")
+        dev = keep[0].device
+        g_phi = torch.zeros(sp, dtype=torch.float64, device=dev)
+        g_mu = torch.zeros(sm, dtype=torch.float64, device=dev)
+        out = AdjOut()
+        out.phi0_bar = g_phi.data_ptr()
+        out.mu0_bar = g_mu.data_ptr()
+        torch.cuda.current_stream(dev).synchronize()   # the inputs are written
+        check(lib().gp_adjoint(self._h, ctypes.byref(req), ctypes.byref(out)), self._h)
+        return _adj_result(out, g_phi, g_mu)
 
     def adjoint_replay(self, nsteps):
         """gp_adjoint_replay: (max |difference|, number of differing values)

@@ -103,14 +103,14 @@ class Stats(ctypes.Structure):
 class AdjReq(ctypes.Structure):
     """gp_adj_req (include/gp.h)."""
     _fields_ = [("nsteps", c_long), ("phi_bar", c_void_p), ("mu_bar", c_void_p), ("target_phi", c_void_p),
-                ("checkpoint_every", c_long)]
+                ("checkpoint_every", c_long), ("snapshots", c_long), ("device", c_int)]
 
 
 class AdjOut(ctypes.Structure):
     """gp_adj_out (include/gp.h)."""
     _fields_ = [("loss", c_double), ("d_tau", c_double), ("d_dab", c_double), ("d_epsilon", c_double),
                 ("d_gamma", c_double), ("phi0_bar", c_void_p), ("mu0_bar", c_void_p),
-                ("ms_forward", c_double), ("ms_reverse", c_double)]
+                ("ms_forward", c_double), ("ms_reverse", c_double), ("snapshots", c_long), ("recomputed", c_long)]
 
 
 class KernelTimes(ctypes.Structure):
@@ -126,6 +126,9 @@ SIGNATURES = {
     "gp_vtk_write": (c_int, [POINTER(Params), ctypes.c_char_p, c_void_p, c_void_p, c_int]),
     "gp_vtk_write_temperature": (c_int, [POINTER(Params), ctypes.c_char_p, c_void_p, c_void_p, c_void_p, c_int]),
     "gp_temperature": (c_int, [c_void_p, c_void_p]),
+    "gp_set_stat_rows": (c_int, [c_void_p, ctypes.c_long, ctypes.c_long]),
+    "gp_rows_pack": (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_void_p]),
+    "gp_rows_unpack": (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_void_p]),
     "gp_vtk_read": (c_int, [POINTER(Params), ctypes.c_char_p, c_void_p, c_void_p, c_int]),
     "gp_vtk_write_async": (c_int, [c_void_p, ctypes.c_char_p, c_int]),
     "gp_vtk_wait": (c_int, [c_void_p]),

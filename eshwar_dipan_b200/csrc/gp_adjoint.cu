@@ -102,6 +102,55 @@ __global__ void __launch_bounds__(AB) ka_dphi(const Consts<double> *__restrict__
   for (int a = 0; a < N; a++) dphi[didx(g, a, x, y)] = d[a];
 }
 
+/* A ring or interior cell whose delta-phi can differ from +0.0: a phase with
+ * a non-zero discrete Laplacian there, or a negative phi (dphi_cell returns
+ * +0.0 first for every other cell). */
+template <int N, int K>
+__device__ __forceinline__ bool dphi_active(const Consts<double> *c, const Grid &g, const double *st, int x, int y) {
+  const int xm = rmx(x - 1, g, c, 0), xc = rmx(x, g, c, 0), xp = rmx(x + 1, g, c, 0);
+  const int ym = rmy(y - 1, g, c, 0), yc = rmy(y, g, c, 0), yp = rmy(y + 1, g, c, 0);
+  bool active = false;
+#pragma unroll
+  for (int a = 0; a < N; a++) {
+    const double *f = st + a * g.plane;
+    const double cc = f[(long long)xc * g.pitch + yc];
+    const double gxf = f[(long long)xp * g.pitch + yc] - cc, gxb = cc - f[(long long)xm * g.pitch + yc];
+    const double gyr = f[(long long)xc * g.pitch + yp] - cc, gyl = cc - f[(long long)xc * g.pitch + ym];
+    active |= (gxf - gxb) != 0.0 || (gyr - gyl) != 0.0 || cc < 0.0;
+  }
+  return active;
+}
+
+/* delta-phi in two launches: the grid is swept for the active cells (the
+ * others keep the +0.0 the buffer was cleared to), then one thread per
+ * listed cell evaluates dphi_cell */
+template <int N, int K>
+__global__ void __launch_bounds__(AB) ka_dphi_sort(const Consts<double> *__restrict__ c, Grid g,
+                                                   const double *__restrict__ st, int2 *__restrict__ cells,
+                                                   int *__restrict__ count);
+
+template <int N, int K, bool A>
+__global__ void __launch_bounds__(AB) ka_dphi_list(const Consts<double> *__restrict__ c, AdjParams prm, Grid g,
+                                                   const double *__restrict__ st, double *__restrict__ dphi,
+                                                   const int2 *__restrict__ cells, const int *__restrict__ count) {
+  double p[ADJ_NPARAM];
+#pragma unroll
+  for (int j = 0; j < ADJ_NPARAM; j++) p[j] = prm.v[j];
+  const AK<double> D = make_ak<double>(c, p);
+  const int n = *count;
+  for (int i = blockIdx.x * AB + threadIdx.x; i < n; i += gridDim.x * AB) {
+    const int2 e = cells[i];
+    double S[N][3][3], M[K][3][3];
+    gather<N, K>(c, g, st, e.x, e.y, S, M);
+    double m[K], d[N];
+#pragma unroll
+    for (int k = 0; k < K; k++) m[k] = M[k][1][1];
+    dphi_cell<double, N, K, A>(D, S, m, d);
+#pragma unroll
+    for (int a = 0; a < N; a++) dphi[didx(g, a, e.x, e.y)] = d[a];
+  }
+}
+
 template <int N, int K>
 __global__ void __launch_bounds__(AB) ka_update(const Consts<double> *__restrict__ c, AdjParams prm, Grid g,
                                                 const double *__restrict__ st, const double *__restrict__ dphi,
@@ -367,6 +416,15 @@ __device__ __forceinline__ void push_cell(bool want, int x, int y, int2 *__restr
 }
 
 template <int N, int K>
+__global__ void __launch_bounds__(AB) ka_dphi_sort(const Consts<double> *__restrict__ c, Grid g,
+                                                   const double *__restrict__ st, int2 *__restrict__ cells,
+                                                   int *__restrict__ count) {
+  const int y = blockIdx.x * AB + threadIdx.x - 1, x = (int)blockIdx.y - 1;
+  const bool want = y <= g.my && dphi_active<N, K>(c, g, st, x, y);
+  push_cell(want, x, y, cells, count);
+}
+
+template <int N, int K>
 __global__ void __launch_bounds__(AB) ka_rev_update(const Consts<double> *__restrict__ c, AdjParams prm, Grid g,
                                                     const double *__restrict__ st, const double *__restrict__ dphi,
                                                     const double *__restrict__ ybar, double *__restrict__ xbar,
@@ -515,6 +573,16 @@ struct AdjKernels {
     ka_dphi<N, K, A><<<grid, AB, 0, s>>>((const Consts<double> *)c, p, g, st, dp);
     return cudaGetLastError();
   }
+  static cudaError_t dphi_sparse(cudaStream_t s, const void *c, AdjParams p, Grid g, const double *st, double *dp,
+                                 int2 *cells, int *count) {
+    cudaError_t e = cudaMemsetAsync(dp, 0, sizeof(double) * (size_t)N * g.dplane, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(count, 0, sizeof(int), s);
+    if (e != cudaSuccess) return e;
+    dim3 grid((g.my + 2 + AB - 1) / AB, g.mx + 2);
+    ka_dphi_sort<N, K><<<grid, AB, 0, s>>>((const Consts<double> *)c, g, st, cells, count);
+    ka_dphi_list<N, K, A><<<list_grid(), AB, 0, s>>>((const Consts<double> *)c, p, g, st, dp, cells, count);
+    return cudaGetLastError();
+  }
   static cudaError_t update(cudaStream_t s, const void *c, AdjParams p, Grid g, const double *st, const double *dp,
                             double *next) {
     dim3 grid((g.my + AB - 1) / AB, g.mx);
@@ -556,11 +624,13 @@ bool gp_adjoint_launch(int N, int K, bool aniso, gpd::AdjLaunch *out) {
   if (N != 2 || K != 1) return false;
   if (aniso) {
     out->dphi = gpd::AdjKernels<2, 1, true>::dphi;
+    out->dphi_sparse = gpd::AdjKernels<2, 1, true>::dphi_sparse;
     out->update = gpd::AdjKernels<2, 1, true>::update;
     out->rev_update = gpd::AdjKernels<2, 1, true>::rev_update;
     out->rev_dphi = gpd::AdjKernels<2, 1, true>::rev_dphi;
   } else {
     out->dphi = gpd::AdjKernels<2, 1, false>::dphi;
+    out->dphi_sparse = gpd::AdjKernels<2, 1, false>::dphi_sparse;
     out->update = gpd::AdjKernels<2, 1, false>::update;
     out->rev_update = gpd::AdjKernels<2, 1, false>::rev_update;
     out->rev_dphi = gpd::AdjKernels<2, 1, false>::rev_dphi;

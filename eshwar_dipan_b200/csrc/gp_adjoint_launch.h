@@ -19,6 +19,10 @@ struct AdjParams {
 struct AdjLaunch {
   /* delta-phi of the interior plus ring of a state (dplane layout) */
   cudaError_t (*dphi)(cudaStream_t s, const void *consts, AdjParams p, Grid g, const double *state, double *dphi);
+  /* the same values from a sweep that lists the active cells and a pass over
+   * the list (cells/count: scratch list as below) */
+  cudaError_t (*dphi_sparse)(cudaStream_t s, const void *consts, AdjParams p, Grid g, const double *state,
+                             double *dphi, int2 *cells, int *count);
   /* the step from a state and its delta-phi, by the adjoint's cell functions */
   cudaError_t (*update)(cudaStream_t s, const void *consts, AdjParams p, Grid g, const double *state,
                         const double *dphi, double *next);

@@ -126,6 +126,8 @@ gpd::Grid make_grid(const gp_derived &d, int pitch_multiple) {
   g.plane = (long long)g.pitch * d.mx;
   g.dpitch = (int)((d.my + 2 + 31) / 32 * 32);
   g.dplane = (long long)g.dpitch * (d.mx + 2);
+  g.sx0 = 0;
+  g.sx1 = (int)d.mx;
   return g;
 }
 
@@ -817,6 +819,48 @@ static int encode_mu_maps(gp_batch *b, gpd::TensorMapSlot *out) {
   return GP_OK;
 }
 
+/* Gather (pack) or scatter rows of the current state, one CTA per row. */
+template <typename T>
+__global__ void k_rows_copy(T *__restrict__ state, long long plane, int pitch, int my, gpd::RowItems it,
+                            T *__restrict__ buf, int pack) {
+  const int i = blockIdx.x;
+  T *r = state + (long long)it.field[i] * plane + (long long)it.row[i] * pitch;
+  T *q = buf + (long long)i * my;
+  if (pack)
+    for (int y = threadIdx.x; y < my; y += blockDim.x) q[y] = r[y];
+  else
+    for (int y = threadIdx.x; y < my; y += blockDim.x) r[y] = q[y];
+}
+
+static int rows_copy(gp_ctx *c, const char *who, int n, const int *fields, const int *rows, void *buf, int pack) {
+  if (!c || !fields || !rows || !buf) return fail(c, GP_EINVAL, "%s: NULL argument", who);
+  gp_batch *b = c->b;
+  const gpd::SimDesc &sd = b->desc[0];
+  if (n < 1 || n > gpd::ROW_ITEMS_MAX) return fail(c, GP_EINVAL, "%s: %d rows (1..%d)", who, n, gpd::ROW_ITEMS_MAX);
+  gpd::RowItems it;
+  for (int i = 0; i < n; i++) {
+    if (fields[i] < 0 || fields[i] >= b->N + b->K || rows[i] < 0 || rows[i] >= sd.g.mx)
+      return fail(c, GP_EINVAL, "%s: item %d (field %d, row %d) outside the state", who, i, fields[i], rows[i]);
+    it.field[i] = fields[i];
+    it.row[i] = rows[i];
+  }
+  c->err[0] = 0;
+  CK(cudaSetDevice(b->dev));
+  char *base = (char *)b->state[b->cur] + (size_t)sd.off_state * b->elem;
+  if (b->elem == 8)
+    k_rows_copy<double><<<n, 256, 0, b->stream>>>((double *)base, sd.g.plane, sd.g.pitch, sd.g.my, it, (double *)buf,
+                                                   pack);
+  else
+    k_rows_copy<float><<<n, 256, 0, b->stream>>>((float *)base, sd.g.plane, sd.g.pitch, sd.g.my, it, (float *)buf,
+                                                  pack);
+  CK(cudaGetLastError());
+  if (!pack) {
+    const int rc = batch_reflag(b, false);   /* the tiles' phase flags follow the new rows */
+    if (rc != GP_OK) return rc;
+  }
+  return GP_OK;
+}
+
 extern "C" {
 
 void gp_batch_destroy(gp_batch *b) {
@@ -1393,6 +1437,31 @@ int gp_set_dev(gp_ctx *c, const double *phi, const double *mu) {
   return GP_OK;
 }
 
+int gp_set_stat_rows(gp_ctx *c, long x0, long x1) {
+  if (!c) return fail(nullptr, GP_EINVAL, "gp_set_stat_rows: NULL context");
+  gp_batch *b = c->b;
+  gpd::SimDesc &sd = b->desc[0];
+  if (x0 < 0 || x1 > sd.g.mx || x0 >= x1)
+    return fail(c, GP_EINVAL, "gp_set_stat_rows: rows [%ld, %ld) outside [0, %d)", x0, x1, sd.g.mx);
+  if (b->shift) return fail(c, GP_EUNSUPPORTED, "gp_set_stat_rows: the moving frame needs the whole grid");
+  c->err[0] = 0;
+  sd.g.sx0 = (int)x0;
+  sd.g.sx1 = (int)x1;
+  CK(cudaSetDevice(b->dev));
+  CK(cudaMemcpyAsync(b->d_desc, b->desc.data(), sizeof(gpd::SimDesc) * b->desc.size(), cudaMemcpyHostToDevice,
+                     b->stream));
+  CK(cudaStreamSynchronize(b->stream));
+  return GP_OK;
+}
+
+int gp_rows_pack(gp_ctx *c, int n, const int *fields, const int *rows, void *dev_buf) {
+  return rows_copy(c, "gp_rows_pack", n, fields, rows, dev_buf, 1);
+}
+
+int gp_rows_unpack(gp_ctx *c, int n, const int *fields, const int *rows, const void *dev_buf) {
+  return rows_copy(c, "gp_rows_unpack", n, fields, rows, const_cast<void *>(dev_buf), 0);
+}
+
 }  /* extern "C" */
 
 
@@ -1435,6 +1504,23 @@ int adj_check(gp_ctx *c, gpd::AdjLaunch *L) {
   return GP_OK;
 }
 
+/* Fewest forward steps that reverse l steps when the state at their start is
+ * kept and s more states can be: with s+1 checkpoints, r the least repetition
+ * number with C(s+1+r, r) >= l, the bound r*l - C(s+1+r, r-1) of binomial
+ * checkpointing (Griewank, "Achieving logarithmic growth of temporal and
+ * spatial complexity in reverse automatic differentiation", 1992). */
+long adj_rev_cost(long l, long s) {
+  if (l <= 1) return 0;
+  if (s <= 0) return l * (l - 1) / 2;
+  const long long S1 = s + 1;
+  long long r = 0, b = 1;   /* b = C(S1 + r, r) */
+  while (b < l) {
+    r++;
+    b = b * (S1 + r) / r;
+  }
+  return (long)(r * l - b * r / (S1 + 1));
+}
+
 gpd::AdjParams adj_params(const gp_params &p) {
   gpd::AdjParams a;
   a.v[gpd::ADJ_TAU] = p.tau_ab[0][1];
@@ -1462,9 +1548,23 @@ int gp_adjoint(gp_ctx *c, const gp_adj_req *req, gp_adj_out *out) {
   const int N = d.N, K = d.K;
   const size_t mx = g.mx, my = g.my, S = (size_t)(N + K) * g.plane, Sd = (size_t)N * g.dplane;
   const long T = req->nsteps;
-  long C = req->checkpoint_every > 0 ? req->checkpoint_every : (long)ceil(sqrt((double)T));
-  if (C > T) C = T;
-  const long nseg = (T + C - 1) / C;
+  const bool dev = req->device != 0;
+  const cudaMemcpyKind h2d = dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  const cudaMemcpyKind d2h = dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+  CK(cudaSetDevice(b->dev));
+
+  /* snapshots of the state besides the start state: the caller's number, or
+   * one state every checkpoint_every steps, or as many as half the free
+   * device memory holds (every state, when they fit: no step is recomputed) */
+  long nsnap;
+  if (req->snapshots > 0) nsnap = req->snapshots;
+  else if (req->checkpoint_every > 0) nsnap = (T + req->checkpoint_every - 1) / req->checkpoint_every;
+  else {
+    size_t fre = 0, tot = 0;
+    CK(cudaMemGetInfo(&fre, &tot));
+    nsnap = (long)std::min<size_t>((size_t)T, fre / 2 / (S * 8));
+  }
+  nsnap = std::max(0L, std::min(nsnap, T - 1));
   const gpd::AdjParams prm = adj_params(b->params[0]);
   const void *consts = b->d_consts;
   AdjBufs m;
@@ -1473,8 +1573,8 @@ int gp_adjoint(gp_ctx *c, const gp_adj_req *req, gp_adj_out *out) {
     if (cudaMalloc((void **)&(ptr), (n) * sizeof(double)) != cudaSuccess)                               \
       return fail(c, GP_ENOMEM, "gp_adjoint: cudaMalloc of %zu bytes failed", (size_t)(n) * sizeof(double)); \
   } while (0)
-  AALLOC(m.snap, S * nseg);
-  AALLOC(m.seg, S * C);
+  AALLOC(m.snap, S * (size_t)(nsnap + 1));   /* slot 0: the start state */
+  AALLOC(m.seg, S);                          /* the state before the last step */
   AALLOC(m.ybar, S);
   AALLOC(m.xbar, S);
   AALLOC(m.dphi, Sd);
@@ -1488,93 +1588,163 @@ int gp_adjoint(gp_ctx *c, const gp_adj_req *req, gp_adj_out *out) {
         cudaMalloc((void **)&m.ncells, sizeof(int)) != cudaSuccess)
       return fail(c, GP_ENOMEM, "gp_adjoint: cudaMalloc of the cell list failed");
   }
-  double *state = (double *)b->state[b->cur];   /* a batch of one starts at offset 0 */
   const long long steps0 = b->steps;
   cudaEvent_t e0, e1, e2;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
   CK(cudaEventCreate(&e2));
   CK(cudaEventRecord(e0, b->stream));
-
-  /* ---- forward, keeping the state at the start of every segment */
-  for (long s = 0; s < nseg; s++) {
-    state = (double *)b->state[b->cur];
-    CK(cudaMemcpyAsync(m.snap + S * s, state, S * 8, cudaMemcpyDeviceToDevice, b->stream));
-    const long n = std::min(C, T - s * C);
-    if ((rc = batch_step_impl(b, n, nullptr, nullptr, nullptr, nullptr)) != GP_OK) return rc;
-  }
-  state = (double *)b->state[b->cur];
-  CK(cudaMemcpyAsync(m.final_state, state, S * 8, cudaMemcpyDeviceToDevice, b->stream));
-  CK(cudaEventRecord(e1, b->stream));
-
-  /* ---- seed: dL/d(final state) */
-  out->loss = 0.0;
-  CK(cudaMemsetAsync(m.ybar, 0, S * 8, b->stream));
-  if (req->phi_bar) {
-    if ((rc = planes_copy(b, m.ybar, g.pitch, req->phi_bar, my, N, g.plane, mx * my, mx, my,
-                          cudaMemcpyHostToDevice)) != GP_OK)
-      return rc;
-    if (req->mu_bar &&
-        (rc = planes_copy(b, m.ybar + N * g.plane, g.pitch, req->mu_bar, my, K, g.plane, mx * my, mx, my,
-                          cudaMemcpyHostToDevice)) != GP_OK)
-      return rc;
-  } else {
-    std::vector<double> phT((size_t)N * mx * my);
-    if ((rc = planes_copy(b, phT.data(), my, state, g.pitch, N, mx * my, g.plane, mx, my,
-                          cudaMemcpyDeviceToHost)) != GP_OK)
-      return rc;
-    CK(cudaStreamSynchronize(b->stream));
-    double loss = 0.0;
-    for (size_t i = 0; i < phT.size(); i++) {
-      phT[i] -= req->target_phi[i];
-      loss += phT[i] * phT[i];
-    }
-    out->loss = 0.5 * loss;
-    if ((rc = planes_copy(b, m.ybar, g.pitch, phT.data(), my, N, g.plane, mx * my, mx, my,
-                          cudaMemcpyHostToDevice)) != GP_OK)
-      return rc;
-    CK(cudaStreamSynchronize(b->stream));
-  }
+  CK(cudaMemcpyAsync(m.snap, b->state[b->cur], S * 8, cudaMemcpyDeviceToDevice, b->stream));
   CK(cudaMemsetAsync(m.pbar, 0, gpd::ADJ_NPARAM * 8, b->stream));
+  out->loss = 0.0;
 
-  /* ---- reverse sweep, segment by segment from the last */
-  for (long s = nseg - 1; s >= 0; s--) {
-    const long n = std::min(C, T - s * C);
-    state = (double *)b->state[b->cur];
-    CK(cudaMemcpyAsync(state, m.snap + S * s, S * 8, cudaMemcpyDeviceToDevice, b->stream));
-    if ((rc = batch_reflag(b, true)) != GP_OK) return rc;
-    /* the segment's states, queued without a host round trip per step */
-    for (long j = 0; j < n; j++) {
-      state = (double *)b->state[b->cur];
-      CK(cudaMemcpyAsync(m.seg + S * j, state, S * 8, cudaMemcpyDeviceToDevice, b->stream));
-      if (j + 1 < n && (rc = batch_step_once(b, 0, nullptr)) != GP_OK) return rc;
+  /* ---- the steps are reversed by the binomial checkpointing schedule:
+   * reversing steps [a, a+l) with the state at a in a slot and s free slots
+   * advances m steps from a, keeps that state, reverses [a+m, a+l) with s-1
+   * slots and then [a, a+m) with s; m minimises the recomputed steps (the
+   * cost is convex in m).  The first chain of advances is the forward pass:
+   * when it reaches the last step's start state, one more step gives the
+   * final state and the seed of the reverse sweep.  With every state kept
+   * (nsnap = T - 1) nothing is recomputed. */
+  struct Task {
+    long a, l, s;
+    int slot;   /* the state a, or the slot to release (l = 0) */
+  };
+  std::vector<Task> stack;
+  std::vector<int> free_slots;
+  for (int i = (int)nsnap; i >= 1; i--) free_slots.push_back(i);
+  stack.push_back({0, T, nsnap, 0});
+  long work_t = 0;    /* the state the engine's buffer holds (-1: none of ours) */
+  bool seeded = false;
+  auto slot_ptr = [&](int k) { return m.snap + S * (size_t)k; };
+  auto advance = [&](long k) -> int {
+    for (long i = 0; i < k; i++) {
+      const int r = batch_step_once(b, 0, nullptr);
+      if (r != GP_OK) return r;
     }
-    if ((rc = batch_check_error(b)) != GP_OK) return rc;
-    for (long j = n - 1; j >= 0; j--) {
-      const double *x = m.seg + S * j;
-      CK(L.dphi(b->stream, consts, prm, g, x, m.dphi));
-      CK(cudaMemsetAsync(m.xbar, 0, S * 8, b->stream));
-      CK(cudaMemsetAsync(m.dphibar, 0, Sd * 8, b->stream));
-      CK(L.rev_update(b->stream, consts, prm, g, x, m.dphi, m.ybar, m.xbar, m.dphibar, m.pbar, m.cells, m.ncells));
-      CK(L.rev_dphi(b->stream, consts, prm, g, x, m.dphibar, m.xbar, m.pbar, m.cells, m.ncells));
-      std::swap(m.ybar, m.xbar);
+    work_t += k;
+    return GP_OK;
+  };
+  auto load = [&](long a, int slot) -> int {
+    if (work_t == a) return GP_OK;
+    BK(cudaMemcpyAsync(b->state[b->cur], slot_ptr(slot), S * 8, cudaMemcpyDeviceToDevice, b->stream));
+    work_t = a;
+    return batch_reflag(b, true);
+  };
+  /* the seed: dL/d(final state) from the state after the last step */
+  auto seed = [&]() -> int {
+    const double *fin = (const double *)b->state[b->cur];
+    BK(cudaMemcpyAsync(m.final_state, fin, S * 8, cudaMemcpyDeviceToDevice, b->stream));
+    BK(cudaEventRecord(e1, b->stream));
+    BK(cudaMemsetAsync(m.ybar, 0, S * 8, b->stream));
+    int r;
+    if (req->phi_bar) {
+      if ((r = planes_copy(b, m.ybar, g.pitch, req->phi_bar, my, N, g.plane, mx * my, mx, my, h2d)) != GP_OK)
+        return r;
+      if (req->mu_bar &&
+          (r = planes_copy(b, m.ybar + N * g.plane, g.pitch, req->mu_bar, my, K, g.plane, mx * my, mx, my, h2d)) !=
+              GP_OK)
+        return r;
+    } else {
+      std::vector<double> phT((size_t)N * mx * my), tgt;
+      if ((r = planes_copy(b, phT.data(), my, fin, g.pitch, N, mx * my, g.plane, mx, my, cudaMemcpyDeviceToHost)) !=
+          GP_OK)
+        return r;
+      const double *target = req->target_phi;
+      if (dev) {
+        tgt.resize(phT.size());
+        BK(cudaMemcpyAsync(tgt.data(), req->target_phi, tgt.size() * 8, cudaMemcpyDeviceToHost, b->stream));
+        target = tgt.data();
+      }
+      BK(cudaStreamSynchronize(b->stream));
+      double loss = 0.0;
+      for (size_t i = 0; i < phT.size(); i++) {
+        phT[i] -= target[i];
+        loss += phT[i] * phT[i];
+      }
+      out->loss = 0.5 * loss;
+      if ((r = planes_copy(b, m.ybar, g.pitch, phT.data(), my, N, g.plane, mx * my, mx, my,
+                           cudaMemcpyHostToDevice)) != GP_OK)
+        return r;
+      BK(cudaStreamSynchronize(b->stream));   /* phT is released on return */
     }
+    seeded = true;
+    return GP_OK;
+  };
+  /* reverse of the step from state t held at x: ybar (after) -> ybar (before) */
+  auto reverse = [&](const double *x) -> int {
+    BK(L.dphi_sparse(b->stream, consts, prm, g, x, m.dphi, m.cells, m.ncells));
+    BK(cudaMemsetAsync(m.xbar, 0, S * 8, b->stream));
+    BK(cudaMemsetAsync(m.dphibar, 0, Sd * 8, b->stream));
+    BK(L.rev_update(b->stream, consts, prm, g, x, m.dphi, m.ybar, m.xbar, m.dphibar, m.pbar, m.cells, m.ncells));
+    BK(L.rev_dphi(b->stream, consts, prm, g, x, m.dphibar, m.xbar, m.pbar, m.cells, m.ncells));
+    std::swap(m.ybar, m.xbar);
+    return GP_OK;
+  };
+  /* reverse of the step from the state the engine's buffer holds (t); the
+   * first such step is the last one (T - 1): the final state comes first */
+  auto reverse_work = [&]() -> int {
+    int r;
+    if (!seeded) {
+      BK(cudaMemcpyAsync(m.seg, b->state[b->cur], S * 8, cudaMemcpyDeviceToDevice, b->stream));
+      if ((r = advance(1)) != GP_OK || (r = seed()) != GP_OK) return r;
+      work_t = -1;
+      return reverse(m.seg);
+    }
+    return reverse((const double *)b->state[b->cur]);
+  };
+  while (!stack.empty()) {
+    const Task t = stack.back();
+    stack.pop_back();
+    if (t.l == 0) {
+      free_slots.push_back(t.slot);
+      continue;
+    }
+    if (t.l == 1) {
+      /* the state is in its slot; unless this is the last step, which comes
+       * straight after the forward pass reached it */
+      if (!seeded) {
+        if ((rc = load(t.a, t.slot)) != GP_OK || (rc = reverse_work()) != GP_OK) return rc;
+      } else if ((rc = reverse(slot_ptr(t.slot))) != GP_OK)
+        return rc;
+      continue;
+    }
+    if (t.s == 0) {
+      for (long i = t.l - 1; i >= 0; i--)
+        if ((rc = load(t.a, t.slot)) != GP_OK || (rc = advance(i)) != GP_OK || (rc = reverse_work()) != GP_OK)
+          return rc;
+      continue;
+    }
+    long lo = 1, hi = t.l - 1;
+    auto cost_at = [&](long mm) { return mm + adj_rev_cost(t.l - mm, t.s - 1) + adj_rev_cost(mm, t.s); };
+    while (lo < hi) {
+      const long mid = (lo + hi) / 2;
+      if (cost_at(mid + 1) < cost_at(mid)) lo = mid + 1;
+      else hi = mid;
+    }
+    const long mm = lo;
+    const int j = free_slots.back();
+    free_slots.pop_back();
+    if ((rc = load(t.a, t.slot)) != GP_OK || (rc = advance(mm)) != GP_OK) return rc;
+    CK(cudaMemcpyAsync(slot_ptr(j), b->state[b->cur], S * 8, cudaMemcpyDeviceToDevice, b->stream));
+    stack.push_back({t.a, mm, t.s, t.slot});
+    stack.push_back({0, 0, 0, j});
+    stack.push_back({t.a + mm, t.l - mm, t.s - 1, j});
   }
   CK(cudaEventRecord(e2, b->stream));
+  if ((rc = batch_check_error(b)) != GP_OK) return rc;
 
   /* ---- results; the context goes back to the final state */
   double pb[gpd::ADJ_NPARAM];
   CK(cudaMemcpyAsync(pb, m.pbar, sizeof pb, cudaMemcpyDeviceToHost, b->stream));
   if (out->phi0_bar &&
-      (rc = planes_copy(b, out->phi0_bar, my, m.ybar, g.pitch, N, mx * my, g.plane, mx, my,
-                        cudaMemcpyDeviceToHost)) != GP_OK)
+      (rc = planes_copy(b, out->phi0_bar, my, m.ybar, g.pitch, N, mx * my, g.plane, mx, my, d2h)) != GP_OK)
     return rc;
   if (out->mu0_bar &&
-      (rc = planes_copy(b, out->mu0_bar, my, m.ybar + N * g.plane, g.pitch, K, mx * my, g.plane, mx, my,
-                        cudaMemcpyDeviceToHost)) != GP_OK)
+      (rc = planes_copy(b, out->mu0_bar, my, m.ybar + N * g.plane, g.pitch, K, mx * my, g.plane, mx, my, d2h)) !=
+          GP_OK)
     return rc;
-  state = (double *)b->state[b->cur];
-  CK(cudaMemcpyAsync(state, m.final_state, S * 8, cudaMemcpyDeviceToDevice, b->stream));
+  CK(cudaMemcpyAsync(b->state[b->cur], m.final_state, S * 8, cudaMemcpyDeviceToDevice, b->stream));
   if ((rc = batch_reflag(b, true)) != GP_OK) return rc;
   CK(cudaStreamSynchronize(b->stream));
   b->steps = steps0 + T;
@@ -1582,6 +1752,8 @@ int gp_adjoint(gp_ctx *c, const gp_adj_req *req, gp_adj_out *out) {
   out->d_dab = pb[gpd::ADJ_DAB];
   out->d_epsilon = pb[gpd::ADJ_EPS];
   out->d_gamma = pb[gpd::ADJ_GAMMA];
+  out->snapshots = nsnap;
+  out->recomputed = adj_rev_cost(T, nsnap) - (T - 1);
   float f1 = 0.f, f2 = 0.f;
   CK(cudaEventElapsedTime(&f1, e0, e1));
   CK(cudaEventElapsedTime(&f2, e1, e2));

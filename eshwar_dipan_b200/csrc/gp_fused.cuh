@@ -729,7 +729,8 @@ __device__ __forceinline__ TileFlags general_tile(const CT &D, const Grid &g, co
   }
 #undef PRIJ
 #undef PR
-  block_stats<R, N, K>(D, valid, nph, nm, dp, dmu, st, ext_slot, slot, (D.tgrad && valid) ? tcc[y + 3] : 0.0);
+  block_stats<R, N, K>(D, valid && stat_row(g, x), nph, nm, dp, dmu, st, ext_slot, slot,
+                       (D.tgrad && valid) ? tcc[y + 3] : 0.0);
   return tile_flags(valid, oh, tx, ty, min(TX, g.mx - x0), min(TY, g.my - y0));
 }
 
@@ -1351,6 +1352,10 @@ __device__ __forceinline__ void bulk_tiles(const SimDesc *__restrict__ sims, con
             redo |= (v1 && !f1 ? 2u : 0u) << (2 * rr);
           }
           const long long o = (long long)x * g.pitch + y;
+          /* the statistics take the cells of their rows */
+          const bool srow = stat_row(g, x);
+          f0 = f0 && srow;
+          f1 = f1 && srow;
 #pragma unroll
           for (int k = 0; k < K; k++) {
             if (v1) *reinterpret_cast<double2 *>(mun + k * g.plane + o) = make_double2(n0[k], n1[k]);
@@ -1384,13 +1389,16 @@ __device__ __forceinline__ void bulk_tiles(const SimDesc *__restrict__ sims, con
             for (int k = 0; k < K; k++) m[k] = sg.M[k][i][cc];
             bulk_cell_full_f64<K, MUL>(&sg.M[0][0][0], i, cc, &D, p, m, nm, dmu);
             const long long o = (long long)x * g.pitch + y + (bit & 1);
+            const bool srow = stat_row(g, x);
 #pragma unroll
             for (int k = 0; k < K; k++) {
               mun[k * g.plane + o] = nm[k];
-              emax[k] = fmax(emax[k], nm[k]);
-              emin[k] = fmin(emin[k], nm[k]);
+              if (srow) {
+                emax[k] = fmax(emax[k], nm[k]);
+                emin[k] = fmin(emin[k], nm[k]);
+              }
             }
-            sum_cell(nm, dmu);
+            if (srow) sum_cell(nm, dmu);
           }
         }
       } else {
@@ -1425,6 +1433,7 @@ __device__ __forceinline__ void bulk_tiles(const SimDesc *__restrict__ sims, con
             LY[m] = f2sub(f2pack(ym, f2hi(o)), f2pack(f2lo(o), ym));
           }
           const long long o = (long long)x * g.pitch + y;
+          const bool srow = stat_row(g, x);
           R n0[K], n1[K];
           double d0[K], d1[K];
 #pragma unroll
@@ -1451,12 +1460,16 @@ __device__ __forceinline__ void bulk_tiles(const SimDesc *__restrict__ sims, con
             d1[k] = (double)f2hi(sdm);
             if (v1) {
               *reinterpret_cast<f2 *>(mun + k * g.plane + o) = nm;
-              emax[k] = fmax3f(emax[k], n0[k], n1[k]);
-              emin[k] = fmin3f(emin[k], n0[k], n1[k]);
+              if (srow) {
+                emax[k] = fmax3f(emax[k], n0[k], n1[k]);
+                emin[k] = fmin3f(emin[k], n0[k], n1[k]);
+              }
             } else {
               mun[k * g.plane + o] = n0[k];
-              emax[k] = fmaxf(emax[k], n0[k]);
-              emin[k] = fminf(emin[k], n0[k]);
+              if (srow) {
+                emax[k] = fmaxf(emax[k], n0[k]);
+                emin[k] = fminf(emin[k], n0[k]);
+              }
             }
           }
           if (have != p) {
@@ -1467,8 +1480,10 @@ __device__ __forceinline__ void bulk_tiles(const SimDesc *__restrict__ sims, con
               else phin[a * g.plane + o] = v;
             }
           }
-          sum_cell(n0, d0);
-          if (v1) sum_cell(n1, d1);
+          if (srow) {
+            sum_cell(n0, d0);
+            if (v1) sum_cell(n1, d1);
+          }
 #pragma unroll
           for (int m = 0; m < K; m++) P[m] = Pn[m];
         }

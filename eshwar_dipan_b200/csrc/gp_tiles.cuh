@@ -42,7 +42,19 @@ struct Grid {
   long long plane;       /* elements per state plane */
   int dpitch;            /* row pitch of the delta-phi buffer */
   long long dplane;      /* elements per delta-phi plane ((mx+2) rows) */
+  int sx0, sx1;          /* rows the progress statistics cover (a slab's own rows; all by default) */
 };
+
+/* rows moved by one gp_rows_pack / gp_rows_unpack call: item i is row
+ * row[i] of state field field[i] */
+constexpr int ROW_ITEMS_MAX = 64;
+struct RowItems {
+  int field[ROW_ITEMS_MAX];
+  int row[ROW_ITEMS_MAX];
+};
+
+/* the cell's row is counted by the progress statistics */
+__device__ __forceinline__ bool stat_row(const Grid &g, int x) { return x >= g.sx0 && x < g.sx1; }
 
 /* interior coordinate v in [-3, m+2] -> interior coordinate it is a copy of
  * (assign_buffer_points_conditions / assign_boundary_points_values,
@@ -847,7 +859,7 @@ __device__ __forceinline__ void update_tile(const Consts<R> &D, const Grid &g, c
 #pragma unroll
       for (int k = 0; k < K; k++) mun[k * g.plane + o] = nm[k];
     }
-    block_stats<R, N, K, true>(D, valid, nph, nm, dp, dmu, st, 0, slot);
+    block_stats<R, N, K, true>(D, valid && stat_row(g, x), nph, nm, dp, dmu, st, 0, slot);
     return;
   }
 
@@ -951,7 +963,7 @@ __device__ __forceinline__ void update_tile(const Consts<R> &D, const Grid &g, c
 #pragma unroll
     for (int k = 0; k < K; k++) mun[k * g.plane + o] = nm[k];
   }
-  block_stats<R, N, K>(D, valid, nph, nm, dp, dmu, st, 0, slot);
+  block_stats<R, N, K>(D, valid && stat_row(g, x), nph, nm, dp, dmu, st, 0, slot);
 }
 
 /* ------------------------------------------------------------------ */

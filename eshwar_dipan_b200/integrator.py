@@ -7,9 +7,11 @@ torch operation over the C ABI (gp_step forward, gp_adjoint backward).
     loss.backward()                               # phi0.grad, mu0.grad, theta.grad
 
 theta holds the phase pair (0,1) values of Tau (the mobility is 1/Tau), dab
-(anisotropy strength), epsilon and GAMMA (interface energy).  Tensors are
-float64 on the CPU (the library copies them to its own device buffers); the
-computation runs in the CUDA kernels behind the ABI.  Supported where
+(anisotropy strength), epsilon and GAMMA (interface energy).  The fields may be
+float64 CUDA tensors on the device the library runs on: they then go in and
+out by device pointers (gp_set_dev, gp_get_dev, gp_adjoint with device
+buffers) and never through host memory; CPU tensors are copied in and out.
+The computation runs in the CUDA kernels behind the ABI.  Supported where
 gp_adjoint is: NUMPHASES = 2, one BINARY component, FP64.
 """
 import ctypes
@@ -36,29 +38,44 @@ def with_theta(params, theta):
     return q
 
 
+def _simulation(p, phi, mu):
+    if phi.is_cuda:
+        return Simulation.from_tensors(p, phi, mu)
+    return Simulation(p, phi.detach().numpy().astype(np.float64), mu.detach().numpy().astype(np.float64))
+
+
 class _Rollout(torch.autograd.Function):
     @staticmethod
     def forward(ctx, phi0, mu0, theta, params, nsteps, checkpoint_every):
         p = with_theta(params, theta.detach().cpu().numpy())
-        a = phi0.detach().cpu().numpy().astype(np.float64)
-        m = mu0.detach().cpu().numpy().astype(np.float64)
-        with Simulation(p, a, m) as s:
+        with _simulation(p, phi0, mu0) as s:
             s.step(nsteps, stats=False)
-            phi_t, mu_t = s.get()
+            if phi0.is_cuda:
+                phi_t, mu_t = s.get_tensors()
+            else:
+                phi_t, mu_t = (torch.from_numpy(a) for a in s.get())
         ctx.save_for_backward(phi0, mu0, theta)
         ctx.params, ctx.nsteps, ctx.every = params, nsteps, checkpoint_every
-        return torch.from_numpy(phi_t), torch.from_numpy(mu_t)
+        return phi_t, mu_t
 
     @staticmethod
     def backward(ctx, g_phi, g_mu):
         phi0, mu0, theta = ctx.saved_tensors
         p = with_theta(ctx.params, theta.detach().cpu().numpy())
-        gphi = (g_phi if g_phi is not None else torch.zeros_like(phi0)).detach().cpu().numpy()
-        gmu = (g_mu if g_mu is not None else torch.zeros_like(mu0)).detach().cpu().numpy()
-        with Simulation(p, phi0.detach().cpu().numpy(), mu0.detach().cpu().numpy()) as s:
-            r = s.adjoint(ctx.nsteps, phi_bar=gphi, mu_bar=gmu, checkpoint_every=ctx.every)
-        d_theta = torch.tensor([r["d_tau"], r["d_dab"], r["d_epsilon"], r["d_gamma"]], dtype=theta.dtype)
-        return torch.from_numpy(r["phi0_bar"]), torch.from_numpy(r["mu0_bar"]), d_theta, None, None, None
+        gphi = (g_phi if g_phi is not None else torch.zeros_like(phi0)).detach()
+        gmu = (g_mu if g_mu is not None else torch.zeros_like(mu0)).detach()
+        with _simulation(p, phi0, mu0) as s:
+            if phi0.is_cuda:
+                r = s.adjoint(ctx.nsteps, phi_bar=gphi.to(phi0.device), mu_bar=gmu.to(phi0.device),
+                              checkpoint_every=ctx.every)
+                g0, m0 = r["phi0_bar"], r["mu0_bar"]
+            else:
+                r = s.adjoint(ctx.nsteps, phi_bar=gphi.cpu().numpy(), mu_bar=gmu.cpu().numpy(),
+                              checkpoint_every=ctx.every)
+                g0, m0 = torch.from_numpy(r["phi0_bar"]), torch.from_numpy(r["mu0_bar"])
+        d_theta = torch.tensor([r["d_tau"], r["d_dab"], r["d_epsilon"], r["d_gamma"]], dtype=theta.dtype,
+                               device=theta.device)
+        return g0, m0, d_theta, None, None, None
 
 
 class GPRollout:

@@ -293,17 +293,23 @@ int gp_step_noalloc(const gp_params *p, const double *phi_in, const double *mu_i
  * phases, simplex projection, bulk test): derivatives are those of the branch
  * the trajectory took.
  * The forward pass runs from the context's current state and leaves the
- * context at the final state (as gp_step would); states every
- * checkpoint_every steps are kept on the device and each segment between them
- * is recomputed once during the reverse sweep (about 2*sqrt(nsteps) stored
- * states with the default). */
+ * context at the final state (as gp_step would).  Steps are reversed in the
+ * order of binomial checkpointing: with s states kept on the device besides
+ * the start state, the schedule recomputes the fewest forward steps any
+ * schedule with s snapshots can (none when s = nsteps-1, the default whenever
+ * that many states fit in half the free device memory). */
 typedef struct gp_adj_req {
   long nsteps;                 /* time steps, >= 1 */
   const double *phi_bar;       /* NULL, or [N][X][Y]: dL/dphi of the final state */
   const double *mu_bar;        /* NULL (zero), or [K][X][Y]: dL/dmu of the final state */
   const double *target_phi;    /* used when phi_bar is NULL: L = 1/2 sum over phases and
                                   cells of (phi_final - target)^2 */
-  long checkpoint_every;       /* steps between stored states; 0 = ceil(sqrt(nsteps)) */
+  long checkpoint_every;       /* > 0 (and snapshots 0): keep nsteps/checkpoint_every states */
+  long snapshots;              /* states kept besides the start state (binomial checkpointing);
+                                  0 and checkpoint_every 0: as many as half the free device memory
+                                  holds, at most nsteps-1 (every state: nothing is recomputed) */
+  int device;                  /* 1: phi_bar, mu_bar, target_phi and the phi0_bar / mu0_bar of the
+                                  result are device pointers on the context's device */
 } gp_adj_req;
 
 typedef struct gp_adj_out {
@@ -316,6 +322,8 @@ typedef struct gp_adj_out {
   double *mu0_bar;             /* NULL, or [K][X][Y]: receives dL/dmu of the start state */
   double ms_forward;           /* device time of the forward pass */
   double ms_reverse;           /* device time of the recomputation and reverse sweep */
+  long snapshots;              /* states kept besides the start state */
+  long recomputed;             /* forward steps taken again in the reverse sweep */
 } gp_adj_out;
 
 int gp_adjoint(gp_ctx *ctx, const gp_adj_req *req, gp_adj_out *out);
@@ -326,6 +334,28 @@ int gp_adjoint(gp_ctx *ctx, const gp_adj_req *req, gp_adj_out *out);
  * value and *n_diff the number of values whose bits differ.  The context
  * advances by nsteps. */
 int gp_adjoint_replay(gp_ctx *ctx, long nsteps, double *max_abs_diff, long long *n_diff);
+
+/* ---- slabs: one grid split along x over several contexts ----------------
+ * Each context (one per GPU rank) holds its own rows of the global grid plus
+ * halo rows above and below (3 rows, the reference's ghost width) that
+ * another rank owns, or, at a periodic edge, the rows the reference's ghost
+ * copy maps there.  A step of the local grid leaves its own rows exactly as a
+ * step of the whole grid does (the step reads no further than two rows), so
+ * one halo exchange per step keeps every rank exact.  Replaces the MPI slab
+ * exchange of the reference's MPI variant (mpiinfo_xyz.h:739-787). */
+
+/* Rows [x0, x1) of the context's grid are counted by the progress statistics
+ * (gp_stats): the context's own rows.  Default: every row.  Not with the
+ * moving frame (GP_EUNSUPPORTED). */
+int gp_set_stat_rows(gp_ctx *ctx, long x0, long x1);
+
+/* Gather rows of the current state into a contiguous device buffer (pack) or
+ * scatter them from one (unpack): item i is row rows[i] of field fields[i]
+ * (0..N-1: phi_a, N..N+K-1: mu_k), MESH_Y values of the context's precision,
+ * in item order; 1 <= n <= 64.  Ordered on the context's stream (gp_stream),
+ * without a host wait; unpack also renews the tiles' phase flags. */
+int gp_rows_pack(gp_ctx *ctx, int n, const int *fields, const int *rows, void *dev_buf);
+int gp_rows_unpack(gp_ctx *ctx, int n, const int *fields, const int *rows, const void *dev_buf);
 
 /* Stream the context's work is ordered on (a cudaStream_t as an opaque pointer). */
 void *gp_stream(gp_ctx *ctx);

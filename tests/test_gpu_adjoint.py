@@ -129,25 +129,67 @@ def test_adjoint_start_state_gradient_vs_finite_differences(tmp_path):
         assert abs(ad - fd) <= 1e-5 * abs(fd) + 1e-9, "adjoint %.10e fd %.10e" % (ad, fd)
 
 
-def test_adjoint_checkpoint_spacing_does_not_change_the_gradient(tmp_path):
+def binomial_cost(l, s):
+    """fewest forward steps that reverse l steps with the start state and s
+    more states kept (binomial checkpointing: r*l - C(s+1+r, r-1) with r the
+    least repetition number such that C(s+1+r, r) >= l)"""
+    from math import comb
+    if l <= 1:
+        return 0
+    if s <= 0:
+        return l * (l - 1) // 2
+    r = 0
+    while comb(s + 1 + r, r) < l:
+        r += 1
+    return r * l - comb(s + 1 + r, r - 1)
+
+
+def test_binomial_cost_is_the_optimum():
+    """the schedule's cost bound equals the optimum of the recursion it
+    follows (advance m, reverse the rest with one slot less, then the first m)"""
+    from functools import lru_cache
+
+    @lru_cache(None)
+    def best(l, s):
+        if l <= 1:
+            return 0
+        if s == 0:
+            return l * (l - 1) // 2
+        return min(m + best(l - m, s - 1) + best(m, s) for m in range(1, l))
+    for s in range(0, 6):
+        for l in range(1, 90):
+            assert binomial_cost(l, s) == best(l, s), (l, s)
+
+
+@pytest.mark.parametrize("kw", [dict(), dict(snapshots=22), dict(snapshots=1), dict(snapshots=3),
+                                dict(snapshots=7), dict(checkpoint_every=7), dict(checkpoint_every=23)])
+def test_adjoint_schedule_does_not_change_the_gradient(tmp_path, kw):
+    """Every checkpointing schedule (the whole tape, binomial with 1, 3 or 7
+    kept states, the states of every 7th or 23rd step) gives the same
+    gradients, recomputes the binomial bound's number of steps and leaves the
+    context at the final state."""
     p, phi0, mu0 = _params(tmp_path, "dendrite_aniso")
     phi, mu = _start(p, phi0, mu0)
     nsteps = 23
     rng = np.random.default_rng(3)
     pb = rng.standard_normal(phi.shape)
-    res = []
-    for every in (0, 1, 7, 23):
-        with gp.Simulation(p, phi, mu) as s:
-            res.append(s.adjoint(nsteps, phi_bar=pb, checkpoint_every=every))
-            end = s.get()
-        with gp.Simulation(p, phi, mu) as s:
-            s.step(nsteps, stats=False)
-            ref = s.get()
-        assert np.array_equal(end[0], ref[0]) and np.array_equal(end[1], ref[1])
-    for r in res[1:]:
-        np.testing.assert_allclose(r["phi0_bar"], res[0]["phi0_bar"], rtol=1e-10, atol=1e-12)
-        for n in PARAMS:
-            assert r["d_" + n] == pytest.approx(res[0]["d_" + n], rel=1e-10, abs=1e-14)
+    with gp.Simulation(p, phi, mu) as s:
+        ref = s.adjoint(nsteps, phi_bar=pb, snapshots=nsteps - 1)
+    with gp.Simulation(p, phi, mu) as s:
+        r = s.adjoint(nsteps, phi_bar=pb, **kw)
+        end = s.get()
+    with gp.Simulation(p, phi, mu) as s:
+        s.step(nsteps, stats=False)
+        fin = s.get()
+    assert np.array_equal(end[0], fin[0]) and np.array_equal(end[1], fin[1])
+    snaps = kw.get("snapshots") or (-(-nsteps // kw["checkpoint_every"]) if "checkpoint_every" in kw else nsteps - 1)
+    snaps = min(snaps, nsteps - 1)
+    assert r["snapshots"] == snaps
+    assert r["recomputed"] == binomial_cost(nsteps, snaps) - (nsteps - 1)
+    np.testing.assert_allclose(r["phi0_bar"], ref["phi0_bar"], rtol=1e-10, atol=1e-12)
+    np.testing.assert_allclose(r["mu0_bar"], ref["mu0_bar"], rtol=1e-10, atol=1e-12)
+    for n in PARAMS:
+        assert r["d_" + n] == pytest.approx(ref["d_" + n], rel=1e-10, abs=1e-14)
 
 
 def test_adjoint_rejects_unsupported(tmp_path):
@@ -190,3 +232,59 @@ def test_torch_integrator_gradients(tmp_path):
     fd = float((lp - lm) / (2 * h))
     ad = float((th.grad * v).sum())
     assert abs(ad - fd) <= 1e-5 * abs(fd), (ad, fd)
+
+
+def test_torch_integrator_cuda_tensors(tmp_path):
+    """GPRollout on float64 CUDA tensors: the fields go in and out by device
+    pointer, the results and gradients equal those of CPU tensors."""
+    import torch
+    from eshwar_dipan_b200.integrator import GPRollout
+    p, phi0, mu0 = _params(tmp_path, "dendrite_aniso")
+    phi, mu = _start(p, phi0, mu0)
+    nsteps = 25
+    target = _target(p, phi, mu, nsteps)
+    roll = GPRollout(p, nsteps)
+    out = {}
+    for dev in ("cpu", "cuda"):
+        th = roll.theta0().clone().to(dev).requires_grad_(True)
+        a = torch.from_numpy(phi.copy()).to(dev).requires_grad_(True)
+        m = torch.from_numpy(mu.copy()).to(dev).requires_grad_(True)
+        phi_t, mu_t = roll(a, m, th)
+        assert phi_t.device.type == dev and mu_t.device.type == dev
+        loss = 0.5 * ((phi_t - torch.from_numpy(target).to(dev)) ** 2).sum()
+        loss.backward()
+        assert a.grad.device.type == dev and th.grad.device.type == dev
+        out[dev] = (phi_t.detach().cpu().numpy(), a.grad.cpu().numpy(), m.grad.cpu().numpy(), th.grad.cpu().numpy())
+    assert np.array_equal(out["cpu"][0], out["cuda"][0])
+    for i in (1, 2, 3):
+        np.testing.assert_allclose(out["cuda"][i], out["cpu"][i], rtol=1e-10, atol=1e-14)
+
+
+def test_adjoint_benchmark_size_vs_finite_differences(tmp_path):
+    """The adjoint's configuration as benchmarked: a 512x512 dendrite over
+    1000 steps, gradients of the mismatch with the run whose parameters are 5%
+    larger.  Each parameter gradient within 1e-5 relative of the central
+    difference (step 1e-5 of the value); every state is kept (no recomputed
+    step)."""
+    from eshwar_dipan_b200.workloads import workload
+    it, ft, desc, _ = workload("cfg5", 1)
+    ip, fp = str(tmp_path / "i.in"), str(tmp_path / "f.in")
+    open(ip, "w").write(it)
+    open(fp, "w").write(ft)
+    p = gp.load_params(ip)
+    phi, mu = _start(p, *gp.fill(p, fp))
+    nsteps = 1000
+    target = _target(p, phi, mu, nsteps)
+    with gp.Simulation(p, phi, mu) as s:
+        g = s.adjoint(nsteps, target_phi=target)
+    assert g["recomputed"] == 0 and g["snapshots"] == nsteps - 1
+    assert g["loss"] == pytest.approx(_loss(p, phi, mu, nsteps, target), rel=1e-12)
+    for n in PARAMS:
+        if n == "dab" and _get(p, n) == 0.0:
+            continue
+        v = _get(p, n)
+        h = 1e-5 * abs(v)
+        fd = (_loss(_with(p, n, v + h), phi, mu, nsteps, target) -
+              _loss(_with(p, n, v - h), phi, mu, nsteps, target)) / (2 * h)
+        ad = g["d_" + n]
+        assert abs(ad - fd) <= 1e-5 * abs(fd), "%s: adjoint %.10e fd %.10e (%s)" % (n, ad, fd, desc)
