@@ -1,6 +1,8 @@
 """Adjoint of the FP64 step (gp_adjoint): the cell functions it differentiates
-reproduce the step bit for bit, and its gradients agree with central finite
-differences of the forward runs."""
+reproduce the step bit for bit; its gradients agree with the FP64 tape
+reference (tests/torch_tape.py) and with central finite differences of the
+forward runs, at the test sizes and at the benchmarked 512x512, 1000-step
+configuration; every checkpointing schedule gives the same gradients."""
 import ctypes
 
 import numpy as np
@@ -127,6 +129,34 @@ def test_adjoint_start_state_gradient_vs_finite_differences(tmp_path):
               _loss(p, phi - h * vphi, mu - h * vmu, nsteps, target)) / (2 * h)
         ad = float((g["phi0_bar"] * vphi).sum() + (g["mu0_bar"] * vmu).sum())
         assert abs(ad - fd) <= 1e-5 * abs(fd) + 1e-9, "adjoint %.10e fd %.10e" % (ad, fd)
+
+
+@pytest.mark.parametrize("name", sorted(CASES) + ["well_aniso"])
+def test_adjoint_matches_the_fp64_tape(tmp_path, name):
+    """The CUDA adjoint against the FP64 tape reference: the same step written
+    in float64 torch operations (bit for bit the oracle's) and differentiated
+    by torch's autograd tape.  Loss equal, parameter gradients within 1e-9
+    relative, start-state gradients within 1e-8 of their largest entry."""
+    from torch_tape import tape_gradients
+    if name == "well_aniso":
+        from test_torch_tape import CASES as TCASES
+        c = TCASES[name]
+        ip, fp = write_case(str(tmp_path), name, c["kw"], seeds=c["seeds"])
+        p = gp.load_params(ip)
+        phi0, mu0 = gp.fill(p, fp)
+    else:
+        p, phi0, mu0 = _params(tmp_path, name)
+    phi, mu = _start(p, phi0, mu0)
+    nsteps = 30
+    target = _target(p, phi, mu, nsteps)
+    with gp.Simulation(p, phi, mu) as s:
+        g = s.adjoint(nsteps, target_phi=target)
+    loss, gth, gphi, gmu = tape_gradients(p, phi, mu, nsteps, target=target)
+    assert g["loss"] == pytest.approx(loss, rel=1e-13)
+    ad = np.array([g["d_tau"], g["d_dab"], g["d_epsilon"], g["d_gamma"]])
+    np.testing.assert_allclose(ad, gth, rtol=1e-9, atol=1e-12 * np.abs(gth).max())
+    np.testing.assert_allclose(g["phi0_bar"], gphi, rtol=0, atol=1e-8 * np.abs(gphi).max())
+    np.testing.assert_allclose(g["mu0_bar"], gmu, rtol=0, atol=1e-8 * np.abs(gmu).max())
 
 
 def binomial_cost(l, s):
