@@ -3,7 +3,7 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--workload cfg4|cfg2|cfg1|cfg3|cfg5] [--no-cpu-baseline]
-                    [--no-extras] [--precision-steps S]
+                    [--no-extras] [--precision-steps S] [--slab]
 
 Default workload (cfg4, the precision configuration the HBM-roofline target is
 stated on): 4096x4096 grid, 3 phases, ternary alloy (2 chemical potentials),
@@ -31,9 +31,10 @@ Beside it the line carries:
 
 A step is one explicit time step of the whole grid (phase-field pass +
 concentration pass + boundary handling).  Cell-updates count interior cells
-x steps.  With N>1 (torchrun) every rank runs its own replica of the grid (the
-single-grid step is not sharded: replicas only); value is the sum over ranks,
-timed as the max over ranks.
+x steps.  With N>1 (torchrun) every rank runs its own replica of the grid;
+value is the sum over ranks, timed as the max over ranks.  With --slab the
+grid is instead split along x over the ranks (eshwar_dipan_b200/slab.py), one
+halo exchange per step, and value is the one grid's cell-updates per second.
 """
 import argparse
 import concurrent.futures
@@ -778,6 +779,63 @@ def run_adjoint(args, rank, world, local, dist):
     return 0
 
 
+def run_slab(args, rank, world, local, dist):
+    """--slab: one grid of the workload split along x over the ranks (one
+    slab per GPU, 3 halo rows each side, the halo rows exchanged after every
+    step by NCCL point-to-point messages on the context's stream).  Strong
+    scaling: value is the grid's cell-updates per second, timed as the max
+    over ranks of K steps with their exchanges."""
+    import torch
+
+    import eshwar_dipan_b200 as gp
+    from eshwar_dipan_b200.slab import GpuSlab, SlabPlan, SlabRunner, TorchTransport, reduce_stats
+    K, W = args.steps, args.warmup
+    work = tempfile.mkdtemp(prefix="gpbench")
+    ip, fp, desc, kw = write_workload(work, args.workload)
+    p = gp.load_params(ip)
+    phi0, mu0 = gp.fill(p, fp)
+    plan = SlabPlan(p, world, rank)
+    slab = GpuSlab(plan, phi0, mu0)
+    run = SlabRunner(plan, slab, TorchTransport(dist, stream=slab.stream) if dist else None)
+    run.smooth(p.nsmooth - 1)
+    run.step(W)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    _barrier(dist)
+    ev0.record(slab.stream)
+    run.step(K)
+    ev1.record(slab.stream)
+    torch.cuda.synchronize()
+    _barrier(dist)
+    ms = reduce_over_ranks(dist, ev0.elapsed_time(ev1))
+    slab.step_stats(1)
+    run.exchange()
+
+    def allreduce(a, op):
+        if not dist:
+            return a
+        t = torch.from_numpy(np.ascontiguousarray(a)).cuda()
+        dist.all_reduce(t, op={"max": dist.ReduceOp.MAX, "min": dist.ReduceOp.MIN, "sum": dist.ReduceOp.SUM}[op])
+        return t.cpu().numpy()
+    st = reduce_stats(slab.stats(), allreduce)
+    slab.close()
+    cells = p.mesh_x * p.mesh_y
+    if rank == 0:
+        print(json.dumps({
+            "metric": "cell-updates/s", "value": cells * K / (ms / 1e3), "unit": "cell-updates/s",
+            "n_gpus": world, "steps": K, "warmup": W, "ms_per_step": ms / K, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": args.workload + ": " + desc, "grid": [p.mesh_x, p.mesh_y],
+                       "slabs": world, "halo_rows": plan.halo, "rows_per_rank": [plan.bounds[r + 1] - plan.bounds[r]
+                                                                             for r in range(world)],
+                       "inputs_vs_l2": "larger than L2" if 2 * (p.numphases + p.numcomponents - 1) * cells * 8
+                       > 126e6 else "smaller than L2"},
+            "stats": {"phi_max": list(st["phi_max"]), "mu_max": list(st["mu_max"]), "nonfinite": st["nonfinite"]},
+            "e2e": None,
+            "note": "one grid split over the ranks; the halo rows cross NVLink once per step"}), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -791,6 +849,8 @@ def main():
     ap.add_argument("--precision-steps", type=int, default=None,
                     help="steps of the FP32-vs-FP64 error run (default 10000 for cfg4, else 0)")
     ap.add_argument("--vtk", action="store_true", help="also time VTK output in the loop vs in the background")
+    ap.add_argument("--slab", action="store_true",
+                    help="split the grid along x over the ranks (strong scaling) instead of one replica per rank")
     ap.add_argument("--no-clock-window", action="store_true",
                     help="skip the ~1.5 s nvidia-smi clock window (short runs under a profiler)")
     args = ap.parse_args()
@@ -816,6 +876,8 @@ def main():
         rc = run_ensemble(args, rank, world, local, dist)
     elif args.workload == "cfg5":
         rc = run_adjoint(args, rank, world, local, dist)
+    elif args.slab:
+        rc = run_slab(args, rank, world, local, dist)
     else:
         rc = run_grid(args, rank, world, local, dist)
     if dist:

@@ -191,6 +191,8 @@ class SlabRunner:
         p, s = self.plan, self.stepper
         for m in p.local_copies:
             s.unpack(m.fields, m.dst_rows, s.pack(m.fields, m.src_rows))
+        if not p.sends and not p.recvs:
+            return
         out = [(m, s.pack(m.fields, m.src_rows)) for m in p.sends]
         got = self.transport.exchange(out, [(m, s.empty(len(m))) for m in p.recvs])
         for m, buf in got:
