@@ -340,6 +340,8 @@ __device__ __forceinline__ bool rev_update_cell(const Consts<double> *__restrict
     } else
     for (int base = b0; base < b1; base += ADJ_W) {
       DT Sd[N][3][3], Md[K][3][3], DPd[N][3][3], pd[ADJ_NPARAM];
+      /* seed inputs base .. base+W-1: every element compares its own
+       * (compile-time) input number, so the dual arrays stay in registers */
 #pragma unroll
       for (int a = 0; a < N; a++)
 #pragma unroll
@@ -348,6 +350,8 @@ __device__ __forceinline__ bool rev_update_cell(const Consts<double> *__restrict
           for (int dj = 0; dj < 3; dj++) {
             Sd[a][di][dj] = DT(S[a][di][dj]);
             DPd[a][di][dj] = DT(DP[a][di][dj]);
+#pragma unroll
+            for (int w = 0; w < ADJ_W; w++) Sd[a][di][dj].d[w] = (a * 9 + di * 3 + dj == base + w) ? 1.0 : 0.0;
           }
 #pragma unroll
       for (int k = 0; k < K; k++)
@@ -356,22 +360,23 @@ __device__ __forceinline__ bool rev_update_cell(const Consts<double> *__restrict
 #pragma unroll
           for (int dj = 0; dj < 3; dj++) Md[k][di][dj] = DT(M[k][di][dj]);
 #pragma unroll
-      for (int j = 0; j < ADJ_NPARAM; j++) pd[j] = DT(prm.v[j]);
-      /* seed inputs base .. base+W-1 */
-      for (int w = 0; w < ADJ_W && base + w < NIN; w++) {
-        const int id = base + w;
-        if (id < NPHI) {
-          const int a = id / 9, r = id % 9;
-          Sd[a][r / 3][r % 3].d[w] = 1.0;
-        } else if (id < NPHI + NMU) {
-          const int k = (id - NPHI) / 5, r = (id - NPHI) % 5;
-          Md[k][pi[r]][pj[r]].d[w] = 1.0;
-        } else if (id < NPHI + NMU + NDP) {
-          const int a = (id - NPHI - NMU) / 5, r = (id - NPHI - NMU) % 5;
-          DPd[a][pi[r]][pj[r]].d[w] = 1.0;
-        } else if (id < NIN) {
-          pd[id - NPHI - NMU - NDP].d[w] = 1.0;
-        }
+      for (int r = 0; r < 5; r++) {
+#pragma unroll
+        for (int k = 0; k < K; k++)
+#pragma unroll
+          for (int w = 0; w < ADJ_W; w++)
+            Md[k][pi[r]][pj[r]].d[w] = (NPHI + k * 5 + r == base + w) ? 1.0 : 0.0;
+#pragma unroll
+        for (int a = 0; a < N; a++)
+#pragma unroll
+          for (int w = 0; w < ADJ_W; w++)
+            DPd[a][pi[r]][pj[r]].d[w] = (NPHI + NMU + a * 5 + r == base + w) ? 1.0 : 0.0;
+      }
+#pragma unroll
+      for (int j = 0; j < ADJ_NPARAM; j++) {
+        pd[j] = DT(prm.v[j]);
+#pragma unroll
+        for (int w = 0; w < ADJ_W; w++) pd[j].d[w] = (NPHI + NMU + NDP + j == base + w) ? 1.0 : 0.0;
       }
       const AK<DT> D = make_ak<DT>(c, pd);
       DT nph[N], nm[K];
@@ -396,7 +401,9 @@ __device__ __forceinline__ bool rev_update_cell(const Consts<double> *__restrict
           const int a = (id - NPHI - NMU) / 5, r = (id - NPHI - NMU) % 5;
           atomicAdd(dphibar + didx(g, a, x + pi[r] - 1, y + pj[r] - 1), gsum);
         } else {
-          pacc[id - NPHI - NMU - NDP] += gsum;
+#pragma unroll
+          for (int j = 0; j < ADJ_NPARAM; j++)
+            if (id - NPHI - NMU - NDP == j) pacc[j] += gsum;
         }
       }
     }
@@ -494,21 +501,28 @@ __device__ __forceinline__ bool rev_dphi_cell(const Consts<double> *__restrict__
   if (live && any) {
     for (int base = b0; base < b1; base += ADJ_W) {
       DT Sd[N][3][3], md[K], pd[ADJ_NPARAM];
+      /* seeding by compile-time input numbers (registers, not local memory) */
 #pragma unroll
       for (int a = 0; a < N; a++)
 #pragma unroll
         for (int di = 0; di < 3; di++)
 #pragma unroll
-          for (int dj = 0; dj < 3; dj++) Sd[a][di][dj] = DT(S[a][di][dj]);
+          for (int dj = 0; dj < 3; dj++) {
+            Sd[a][di][dj] = DT(S[a][di][dj]);
 #pragma unroll
-      for (int k = 0; k < K; k++) md[k] = DT(M[k][1][1]);
+            for (int w = 0; w < ADJ_W; w++) Sd[a][di][dj].d[w] = (a * 9 + di * 3 + dj == base + w) ? 1.0 : 0.0;
+          }
 #pragma unroll
-      for (int j = 0; j < ADJ_NPARAM; j++) pd[j] = DT(prm.v[j]);
-      for (int w = 0; w < ADJ_W; w++) {
-        const int id = base + w;
-        if (id < NPHI) Sd[id / 9][(id % 9) / 3][id % 3].d[w] = 1.0;
-        else if (id < NPHI + K) md[id - NPHI].d[w] = 1.0;
-        else if (id < NIN) pd[id - NPHI - K].d[w] = 1.0;
+      for (int k = 0; k < K; k++) {
+        md[k] = DT(M[k][1][1]);
+#pragma unroll
+        for (int w = 0; w < ADJ_W; w++) md[k].d[w] = (NPHI + k == base + w) ? 1.0 : 0.0;
+      }
+#pragma unroll
+      for (int j = 0; j < ADJ_NPARAM; j++) {
+        pd[j] = DT(prm.v[j]);
+#pragma unroll
+        for (int w = 0; w < ADJ_W; w++) pd[j].d[w] = (NPHI + K + j == base + w) ? 1.0 : 0.0;
       }
       const AK<DT> D = make_ak<DT>(c, pd);
       DT d[N];
@@ -528,7 +542,9 @@ __device__ __forceinline__ bool rev_dphi_cell(const Consts<double> *__restrict__
           const int xs = rmx(x, g, c, 1), ys = rmy(y, g, c, 1);
           atomicAdd(xbar + (N + id - NPHI) * g.plane + (long long)xs * g.pitch + ys, gsum);
         } else {
-          pacc[id - NPHI - K] += gsum;
+#pragma unroll
+          for (int j = 0; j < ADJ_NPARAM; j++)
+            if (id - NPHI - K == j) pacc[j] += gsum;
         }
       }
     }

@@ -213,10 +213,12 @@ __device__ __forceinline__ void aproject(const T *ph, const bool *act, T *d) {
   for (int a = 0; a < N; a++)
     if (hit < 0 && act[a] && (ph[a] + d[a]) > 1.0) hit = a;
   if (hit >= 0) {
-    d[hit] = (1.0 - ph[hit]);
+    /* d[hit] = 1 - ph[hit], the other active phases -ph (by compile-time indices) */
 #pragma unroll
-    for (int b = 0; b < N; b++)
-      if (act[b] && b != hit) d[b] = -ph[b];
+    for (int b = 0; b < N; b++) {
+      if (b == hit) d[b] = (1.0 - ph[b]);
+      else if (act[b]) d[b] = -ph[b];
+    }
   }
 }
 
@@ -596,9 +598,18 @@ __device__ __forceinline__ void update_cell(const AK<T> &D, const T (&S)[N][3][3
   for (int a = 0; a < N; a++)
     if (bulk < 0 && ph[a] == 1.0) bulk = a;
   if (bulk >= 0) {
+    /* the bulk phase's c_mu, picked by compile-time indices (q stays in registers) */
+    T cb[K];
+#pragma unroll
+    for (int k = 0; k < K; k++) cb[k] = q[0].CM[0][k];
+#pragma unroll
+    for (int a = 1; a < N; a++)
+      if (a == bulk)
+#pragma unroll
+        for (int k = 0; k < K; k++) cb[k] = q[0].CM[a][k];
     T cn[K];
 #pragma unroll
-    for (int k = 0; k < K; k++) cn[k] = q[0].CM[bulk][k] + D.c->dt * (divflux[k]) - divjat[k];
+    for (int k = 0; k < K; k++) cn[k] = cb[k] + D.c->dt * (divflux[k]) - divjat[k];
 #pragma unroll
     for (int k = 0; k < K; k++) nm[k] = aMu<T, K>(D, cn, bulk, k);
   } else {
