@@ -323,9 +323,13 @@ __device__ __forceinline__ void ring_face_terms(const CT &D, const R (*P)[S2], R
 
 /* delta-phi of one ring cell (ring coordinates ri, rj; its phi at P row ri+1,
  * column rj+1) from the staged tile: calculate_divergence_phasefield_2D
- * (calculate_divergence_phasefield.h:4-62) in the same arithmetic as dphi_tile. */
+ * (calculate_divergence_phasefield.h:4-62) in the same arithmetic as dphi_tile.
+ * Not inlined: as a call of its own it gets its own register allocation, and
+ * the interface tiles spill far less under the 128-register cap of two CTAs
+ * per SM (FP64 ternary 3-phase: 732 bytes of spill stores inlined, about 200
+ * not; FP32: none), which made whole steps 3-8 % faster. */
 template <typename R, int N, int K, bool ANISO, typename CT>
-__device__ __forceinline__ void ring_dphi(const CT &D, const GenSmem<R, N, K> &sm, int ri, int rj,
+__device__ __noinline__ void ring_dphi(const CT &D, const GenSmem<R, N, K> &sm, int ri, int rj,
                                           unsigned mask, R *d, double Tpf) {
   const int i = ri + 1, j = rj + 1, e = LI(ri, rj);
   R ph[N];

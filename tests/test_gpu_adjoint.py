@@ -294,8 +294,9 @@ def test_adjoint_benchmark_size_vs_finite_differences(tmp_path):
     """The adjoint's configuration as benchmarked: a 512x512 dendrite over
     1000 steps, gradients of the mismatch with the run whose parameters are 5%
     larger.  Each parameter gradient within 1e-5 relative of the central
-    difference (step 1e-5 of the value); every state is kept (no recomputed
-    step)."""
+    difference (step 1e-5 of the value), and the start-state gradient along 8
+    random directions on the interface cells likewise; every state is kept
+    (no recomputed step)."""
     from eshwar_dipan_b200.workloads import workload
     it, ft, desc, _ = workload("cfg5", 1)
     ip, fp = str(tmp_path / "i.in"), str(tmp_path / "f.in")
@@ -318,3 +319,16 @@ def test_adjoint_benchmark_size_vs_finite_differences(tmp_path):
               _loss(_with(p, n, v - h), phi, mu, nsteps, target)) / (2 * h)
         ad = g["d_" + n]
         assert abs(ad - fd) <= 1e-5 * abs(fd), "%s: adjoint %.10e fd %.10e (%s)" % (n, ad, fd, desc)
+    # the start state along 8 random directions supported on the interface
+    # cells (where the step is smooth in phi); central differences, step 1e-6
+    rng = np.random.default_rng(11)
+    inner = (phi[0] > 0.05) & (phi[0] < 0.95)
+    assert inner.sum() > 100
+    h = 1e-6
+    for _ in range(8):
+        vphi = rng.standard_normal(phi.shape) * inner
+        vmu = rng.standard_normal(mu.shape) * inner
+        fd = (_loss(p, phi + h * vphi, mu + h * vmu, nsteps, target) -
+              _loss(p, phi - h * vphi, mu - h * vmu, nsteps, target)) / (2 * h)
+        ad = float((g["phi0_bar"] * vphi).sum() + (g["mu0_bar"] * vmu).sum())
+        assert abs(ad - fd) <= 1e-5 * abs(fd) + 1e-9, "start state: adjoint %.10e fd %.10e" % (ad, fd)
