@@ -32,10 +32,18 @@
 
 namespace gpd {
 
+/* seeded inputs per dual pass: of the concentration pass (ADJ_W) and of the
+ * phase-field pass (ADJ_WD).  With a thread per (cell, pass) the leanest pass
+ * of the concentration update is the fastest (wider ones spill); the
+ * phase-field pass takes GP_ADJ_WD */
 #ifndef GP_ADJ_W
-#define GP_ADJ_W 1   /* one seeded input per pass: with a thread per (cell, pass), the leanest pass is fastest (2 and 4 were slower) */
+#define GP_ADJ_W 1
+#endif
+#ifndef GP_ADJ_WD
+#define GP_ADJ_WD 1
 #endif
 constexpr int ADJ_W = GP_ADJ_W;
+constexpr int ADJ_WD = GP_ADJ_WD;
 constexpr int AB = 128;   /* threads per block along y */
 
 __device__ __forceinline__ int rmx(int x, const Grid &g, const Consts<double> *c, int f) {
@@ -471,9 +479,9 @@ __device__ __forceinline__ bool rev_dphi_cell(const Consts<double> *__restrict__
                                               const Grid &g, const double *__restrict__ st,
                                               const double *__restrict__ dphibar, double *__restrict__ xbar, int x,
                                               int y, bool live, double (&pacc)[ADJ_NPARAM], int pass = -1) {
-  using DT = Dual<ADJ_W>;
+  using DT = Dual<ADJ_WD>;
   constexpr int NPHI = 9 * N, NIN = NPHI + K + ADJ_NPARAM;
-  const int b0 = pass >= 0 ? pass * ADJ_W : 0, b1 = pass >= 0 ? min(NIN, b0 + ADJ_W) : NIN;
+  const int b0 = pass >= 0 ? pass * ADJ_WD : 0, b1 = pass >= 0 ? min(NIN, b0 + ADJ_WD) : NIN;
   double db[N];
   bool any = false;
   if (live) {
@@ -499,7 +507,7 @@ __device__ __forceinline__ bool rev_dphi_cell(const Consts<double> *__restrict__
   }
   if (SORT) return live && any;
   if (live && any) {
-    for (int base = b0; base < b1; base += ADJ_W) {
+    for (int base = b0; base < b1; base += ADJ_WD) {
       DT Sd[N][3][3], md[K], pd[ADJ_NPARAM];
       /* seeding by compile-time input numbers (registers, not local memory) */
 #pragma unroll
@@ -510,24 +518,24 @@ __device__ __forceinline__ bool rev_dphi_cell(const Consts<double> *__restrict__
           for (int dj = 0; dj < 3; dj++) {
             Sd[a][di][dj] = DT(S[a][di][dj]);
 #pragma unroll
-            for (int w = 0; w < ADJ_W; w++) Sd[a][di][dj].d[w] = (a * 9 + di * 3 + dj == base + w) ? 1.0 : 0.0;
+            for (int w = 0; w < ADJ_WD; w++) Sd[a][di][dj].d[w] = (a * 9 + di * 3 + dj == base + w) ? 1.0 : 0.0;
           }
 #pragma unroll
       for (int k = 0; k < K; k++) {
         md[k] = DT(M[k][1][1]);
 #pragma unroll
-        for (int w = 0; w < ADJ_W; w++) md[k].d[w] = (NPHI + k == base + w) ? 1.0 : 0.0;
+        for (int w = 0; w < ADJ_WD; w++) md[k].d[w] = (NPHI + k == base + w) ? 1.0 : 0.0;
       }
 #pragma unroll
       for (int j = 0; j < ADJ_NPARAM; j++) {
         pd[j] = DT(prm.v[j]);
 #pragma unroll
-        for (int w = 0; w < ADJ_W; w++) pd[j].d[w] = (NPHI + K + j == base + w) ? 1.0 : 0.0;
+        for (int w = 0; w < ADJ_WD; w++) pd[j].d[w] = (NPHI + K + j == base + w) ? 1.0 : 0.0;
       }
       const AK<DT> D = make_ak<DT>(c, pd);
       DT d[N];
       dphi_cell<DT, N, K, A>(D, Sd, md, d);
-      for (int w = 0; w < ADJ_W; w++) {
+      for (int w = 0; w < ADJ_WD; w++) {
         const int id = base + w;
         if (id >= NIN) break;
         double gsum = 0.0;
@@ -570,7 +578,7 @@ __global__ void __launch_bounds__(AB) ka_rev_dphi_list(const Consts<double> *__r
                                                        double *__restrict__ pbar, const int2 *__restrict__ cells,
                                                        const int *__restrict__ count) {
   /* one thread per (cell, dual pass) */
-  constexpr int NIN = 9 * N + K + ADJ_NPARAM, NPASS = (NIN + ADJ_W - 1) / ADJ_W;
+  constexpr int NIN = 9 * N + K + ADJ_NPARAM, NPASS = (NIN + ADJ_WD - 1) / ADJ_WD;
   double pacc[ADJ_NPARAM] = {};
   const long long n = (long long)*count * NPASS;
   for (long long i = (long long)blockIdx.x * AB + threadIdx.x; i < n; i += (long long)gridDim.x * AB) {
@@ -614,8 +622,6 @@ struct AdjKernels {
   static cudaError_t rev_update(cudaStream_t s, const void *c, AdjParams p, Grid g, const double *st,
                                 const double *dp, const double *ybar, double *xbar, double *dpbar, double *pbar,
                                 int2 *cells, int *count) {
-    cudaError_t e = cudaMemsetAsync(count, 0, sizeof(int), s);
-    if (e != cudaSuccess) return e;
     dim3 grid((g.my + AB - 1) / AB, g.mx);
     ka_rev_update<N, K><<<grid, AB, 0, s>>>((const Consts<double> *)c, p, g, st, dp, ybar, xbar, dpbar, cells, count);
     ka_rev_update_list<N, K><<<list_grid(), AB, 0, s>>>((const Consts<double> *)c, p, g, st, dp, ybar, xbar, dpbar,
@@ -624,8 +630,6 @@ struct AdjKernels {
   }
   static cudaError_t rev_dphi(cudaStream_t s, const void *c, AdjParams p, Grid g, const double *st,
                               const double *dpbar, double *xbar, double *pbar, int2 *cells, int *count) {
-    cudaError_t e = cudaMemsetAsync(count, 0, sizeof(int), s);
-    if (e != cudaSuccess) return e;
     dim3 grid((g.my + 2 + AB - 1) / AB, g.mx + 2);
     ka_rev_dphi<N, K, A><<<grid, AB, 0, s>>>((const Consts<double> *)c, p, g, st, dpbar, xbar, cells, count);
     ka_rev_dphi_list<N, K, A><<<list_grid(), AB, 0, s>>>((const Consts<double> *)c, p, g, st, dpbar, xbar, pbar,

@@ -27,11 +27,13 @@ struct AdjLaunch {
   cudaError_t (*update)(cudaStream_t s, const void *consts, AdjParams p, Grid g, const double *state,
                         const double *dphi, double *next);
   /* reverse of the concentration pass: ybar -> xbar, dphibar, pbar
-   * (accumulated); cells/count: scratch list of (mx+2)*(my+2) cells */
+   * (accumulated); cells/count: scratch list of (mx+2)*(my+2) cells, the
+   * count zero on entry (each pass takes a counter of its own) */
   cudaError_t (*rev_update)(cudaStream_t s, const void *consts, AdjParams p, Grid g, const double *state,
                             const double *dphi, const double *ybar, double *xbar, double *dphibar, double *pbar,
                             int2 *cells, int *count);
-  /* reverse of the phase-field pass: dphibar -> xbar, pbar (accumulated) */
+  /* reverse of the phase-field pass: dphibar -> xbar, pbar (accumulated);
+   * count zero on entry */
   cudaError_t (*rev_dphi)(cudaStream_t s, const void *consts, AdjParams p, Grid g, const double *state,
                           const double *dphibar, double *xbar, double *pbar, int2 *cells, int *count);
 };

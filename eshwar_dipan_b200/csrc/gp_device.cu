@@ -347,6 +347,7 @@ struct gp_batch {
   int *spos;                    /* its interface position per simulation */
   double *trows;                /* their temperature rows (SimDesc::off_T) */
   gpd::SimDyn *dyn;             /* per simulation moving-frame state */
+  double *dphi_out = nullptr;   /* the adjoint's forward steps: where the interface tiles write delta-phi */
   double *partials, *sums_sim;
   /* captured step sequences: graphs[(starting parity, steps)], steps <= GP_GRAPH_STEPS */
   std::map<std::pair<int, long>, cudaGraphExec_t> graphs;
@@ -383,6 +384,7 @@ static int batch_step_once(gp_batch *b, int want_sums, cudaEvent_t *ev) {
   st.round_step = (const unsigned *)(b->counters + gpd::CTR_STEP);
   st.mbar_tries = b->mbar_tries;
   st.tma_extra = b->tma_extra;
+  st.dphi_out = b->dphi_out;
   st.bch_max = b->shape.bch_max;
   st.mixed = b->shape.mixed ? 1 : 0;
   st.trows = b->tgrad ? b->trows : nullptr;
@@ -1482,11 +1484,13 @@ int planes_copy(gp_batch *b, double *dst, size_t dpitch, const double *src, size
 struct AdjBufs {
   double *snap = nullptr, *seg = nullptr, *ybar = nullptr, *xbar = nullptr, *dphi = nullptr, *dphibar = nullptr,
          *pbar = nullptr, *final_state = nullptr;
-  int2 *cells = nullptr;   /* cells of a reverse pass that take the dual passes */
+  double *rblk = nullptr;   /* two reverse blocks: adjoint of a state, adjoint of its delta-phi, list counters */
+  double *dtape = nullptr;  /* delta-phi of every step, written by the forward pass (whole-tape mode) */
+  int2 *cells = nullptr;    /* cells of a reverse pass that take the dual passes */
   int *ncells = nullptr;
-  ~AdjBufs() {
-    cudaFree(snap); cudaFree(seg); cudaFree(ybar); cudaFree(xbar); cudaFree(dphi); cudaFree(dphibar);
-    cudaFree(pbar); cudaFree(final_state); cudaFree(cells); cudaFree(ncells);
+  ~AdjBufs() {   /* ybar, xbar and dphibar point into rblk */
+    cudaFree(snap); cudaFree(seg); cudaFree(dphi); cudaFree(pbar); cudaFree(final_state); cudaFree(rblk);
+    cudaFree(dtape); cudaFree(cells); cudaFree(ncells);
   }
 };
 
@@ -1555,16 +1559,17 @@ int gp_adjoint(gp_ctx *c, const gp_adj_req *req, gp_adj_out *out) {
 
   /* snapshots of the state besides the start state: the caller's number, or
    * one state every checkpoint_every steps, or as many as half the free
-   * device memory holds (every state, when they fit: no step is recomputed) */
+   * device memory holds (every state, when they fit: no step is recomputed).
+   * With every state kept, the forward pass also keeps each step's delta-phi
+   * when that fits as well, and the reverse sweep does not recompute it. */
   long nsnap;
+  size_t fre = 0, tot = 0;
+  CK(cudaMemGetInfo(&fre, &tot));
   if (req->snapshots > 0) nsnap = req->snapshots;
   else if (req->checkpoint_every > 0) nsnap = (T + req->checkpoint_every - 1) / req->checkpoint_every;
-  else {
-    size_t fre = 0, tot = 0;
-    CK(cudaMemGetInfo(&fre, &tot));
-    nsnap = (long)std::min<size_t>((size_t)T, fre / 2 / (S * 8));
-  }
+  else nsnap = (long)std::min<size_t>((size_t)T, fre / 2 / (S * 8));
   nsnap = std::max(0L, std::min(nsnap, T - 1));
+  const bool dtape = nsnap == T - 1 && (size_t)T * (S + Sd) * 8 <= fre / 2;
   const gpd::AdjParams prm = adj_params(b->params[0]);
   const void *consts = b->d_consts;
   AdjBufs m;
@@ -1573,15 +1578,22 @@ int gp_adjoint(gp_ctx *c, const gp_adj_req *req, gp_adj_out *out) {
     if (cudaMalloc((void **)&(ptr), (n) * sizeof(double)) != cudaSuccess)                               \
       return fail(c, GP_ENOMEM, "gp_adjoint: cudaMalloc of %zu bytes failed", (size_t)(n) * sizeof(double)); \
   } while (0)
+  /* a reverse block: the adjoint of a state (S), of its delta-phi (Sd) and
+   * the two list counters of the reverse passes; a reverse step reads one
+   * block and clears and fills the other with one memset */
+  const size_t RB = S + Sd + 8;
   AALLOC(m.snap, S * (size_t)(nsnap + 1));   /* slot 0: the start state */
   AALLOC(m.seg, S);                          /* the state before the last step */
-  AALLOC(m.ybar, S);
-  AALLOC(m.xbar, S);
+  AALLOC(m.rblk, 2 * RB);
   AALLOC(m.dphi, Sd);
-  AALLOC(m.dphibar, Sd);
   AALLOC(m.pbar, gpd::ADJ_NPARAM);
   AALLOC(m.final_state, S);
+  if (dtape) AALLOC(m.dtape, Sd * (size_t)T);
 #undef AALLOC
+  int rcur = 0;   /* the block holding the adjoint of the state after the step being reversed */
+  auto rbar = [&](int k) { return m.rblk + RB * (size_t)k; };
+  m.ybar = rbar(0);
+  std::vector<char> have_dphi((size_t)T, 0);
   {
     const size_t ncell = (size_t)(g.mx + 2) * (g.my + 2);
     if (cudaMalloc((void **)&m.cells, ncell * sizeof(int2)) != cudaSuccess ||
@@ -1619,7 +1631,16 @@ int gp_adjoint(gp_ctx *c, const gp_adj_req *req, gp_adj_out *out) {
   auto slot_ptr = [&](int k) { return m.snap + S * (size_t)k; };
   auto advance = [&](long k) -> int {
     for (long i = 0; i < k; i++) {
+      const long t = work_t + i;   /* the step from state t */
+      if (m.dtape && !have_dphi[(size_t)t]) {
+        b->dphi_out = m.dtape + Sd * (size_t)t;
+        BK(cudaMemsetAsync(b->dphi_out, 0, Sd * 8, b->stream));   /* cells of bulk tiles: +0.0 */
+      }
       const int r = batch_step_once(b, 0, nullptr);
+      if (b->dphi_out) {
+        have_dphi[(size_t)t] = 1;
+        b->dphi_out = nullptr;
+      }
       if (r != GP_OK) return r;
     }
     work_t += k;
@@ -1672,26 +1693,31 @@ int gp_adjoint(gp_ctx *c, const gp_adj_req *req, gp_adj_out *out) {
     return GP_OK;
   };
   /* reverse of the step from state t held at x: ybar (after) -> ybar (before) */
-  auto reverse = [&](const double *x) -> int {
-    BK(L.dphi_sparse(b->stream, consts, prm, g, x, m.dphi, m.cells, m.ncells));
-    BK(cudaMemsetAsync(m.xbar, 0, S * 8, b->stream));
-    BK(cudaMemsetAsync(m.dphibar, 0, Sd * 8, b->stream));
-    BK(L.rev_update(b->stream, consts, prm, g, x, m.dphi, m.ybar, m.xbar, m.dphibar, m.pbar, m.cells, m.ncells));
-    BK(L.rev_dphi(b->stream, consts, prm, g, x, m.dphibar, m.xbar, m.pbar, m.cells, m.ncells));
-    std::swap(m.ybar, m.xbar);
+  auto reverse = [&](long t, const double *x) -> int {
+    const double *dph = m.dphi;
+    if (m.dtape && have_dphi[(size_t)t]) dph = m.dtape + Sd * (size_t)t;
+    else BK(L.dphi_sparse(b->stream, consts, prm, g, x, m.dphi, m.cells, m.ncells));
+    double *ybar = rbar(rcur), *xbar = rbar(rcur ^ 1), *dphibar = xbar + S;
+    int *cnt = (int *)(xbar + S + Sd);
+    BK(cudaMemsetAsync(xbar, 0, RB * 8, b->stream));
+    BK(L.rev_update(b->stream, consts, prm, g, x, dph, ybar, xbar, dphibar, m.pbar, m.cells, cnt));
+    BK(L.rev_dphi(b->stream, consts, prm, g, x, dphibar, xbar, m.pbar, m.cells, cnt + 1));
+    rcur ^= 1;
+    m.ybar = xbar;
     return GP_OK;
   };
   /* reverse of the step from the state the engine's buffer holds (t); the
    * first such step is the last one (T - 1): the final state comes first */
   auto reverse_work = [&]() -> int {
     int r;
+    const long t = work_t;
     if (!seeded) {
       BK(cudaMemcpyAsync(m.seg, b->state[b->cur], S * 8, cudaMemcpyDeviceToDevice, b->stream));
       if ((r = advance(1)) != GP_OK || (r = seed()) != GP_OK) return r;
       work_t = -1;
-      return reverse(m.seg);
+      return reverse(t, m.seg);
     }
-    return reverse((const double *)b->state[b->cur]);
+    return reverse(t, (const double *)b->state[b->cur]);
   };
   while (!stack.empty()) {
     const Task t = stack.back();
@@ -1705,7 +1731,7 @@ int gp_adjoint(gp_ctx *c, const gp_adj_req *req, gp_adj_out *out) {
        * straight after the forward pass reached it */
       if (!seeded) {
         if ((rc = load(t.a, t.slot)) != GP_OK || (rc = reverse_work()) != GP_OK) return rc;
-      } else if ((rc = reverse(slot_ptr(t.slot))) != GP_OK)
+      } else if ((rc = reverse(t.a, slot_ptr(t.slot))) != GP_OK)
         return rc;
       continue;
     }

@@ -611,6 +611,18 @@ __device__ __forceinline__ TileFlags general_tile(const CT &D, const Grid &g, co
     for (int a = 0; a < N; a++) sm.DP[a][e] = d[a];
   }
   __syncthreads();   /* the face-term cache is dead from here: its space holds the update's arrays */
+  if (st.dphi_out) {
+    /* the adjoint's tape: the delta-phi of the tile and of its ring cells
+     * (the domain's ring included), as the reverse sweep reads it */
+    for (int e = threadIdx.x; e < SS; e += NT) {
+      const int x = x0 - 1 + e / SW, y = y0 - 1 + e % SW;
+      if (x <= g.mx && y <= g.my) {
+#pragma unroll
+        for (int a = 0; a < N; a++)
+          st.dphi_out[a * g.dplane + (long long)(x + 1) * g.dpitch + (y + 1)] = (double)sm.DP[a][e];
+      }
+    }
+  }
   if (threadIdx.x == 0) {
     sm.nlist = 0;    /* for the CTA's next tile */
     sm.nflist = 0;

@@ -445,6 +445,9 @@ struct StatBufs {
   const double *trows; /* non-isothermal simulations: per simulation the temperature of each ghosted column y
                           as the phase-field pass reads it, then as the concentration pass reads it */
   unsigned tma_extra;  /* bytes a box's barrier expects beyond the box: 0, or more to test the give-up path */
+  double *dphi_out;    /* NULL, or (a batch of one) the step's delta-phi of every interface tile and its ring in
+                          the delta-phi layout (Grid dpitch/dplane); cells no interface tile covers are left as
+                          they are (their delta-phi is +0.0) */
 };
 
 /* ---- FP32 storage rounding ------------------------------------------------
