@@ -27,6 +27,8 @@
  */
 #include <cuda_runtime.h>
 
+#include <cstdlib>
+
 #include "gp_adjoint.cuh"
 #include "gp_adjoint_launch.h"
 
@@ -471,6 +473,293 @@ __global__ void __launch_bounds__(AB) ka_rev_update_list(const Consts<double> *_
   flush_params(pacc, pbar);
 }
 
+/* ---- hand-derived reverse of the concentration update ---------------------
+ * For two phases and one component (the adjoint's scope) the transposed
+ * local Jacobian of update_cell is written out instead of evaluated by dual
+ * passes: one thread per (listed cell, part), part 0 the cell's own terms (the
+ * phi commit, its mu, the dh/dphi * delta-phi coupling and the dc/dmu
+ * inversion), parts 1-4 one face each (x+, x-, y+, y-: the diffusion flux and
+ * the anti-trapping current through it).  Every derivative is that of the
+ * expressions update_cell evaluates, on the branch the step took (bulk or
+ * interface cell, current evaluated or not); only the rounding of the
+ * derivative arithmetic differs from the dual passes. */
+
+/* d(v / h)/dv in the step's arithmetic for spacing h (mul: v * (1/h)) */
+__device__ __forceinline__ double rdx(const Consts<double> *c) { return c->mul_dx ? c->inv_dx : 1.0 / c->dx; }
+__device__ __forceinline__ double rdy(const Consts<double> *c) { return c->mul_dy ? c->inv_dy : 1.0 / c->dy; }
+__device__ __forceinline__ double r2dy(const Consts<double> *c) { return c->mul_dy ? c->inv_2dy : 1.0 / (2.0 * c->dy); }
+
+/* obstacle anti-trapping weight s(p) = p (1 - h(p)) / sqrt(p (1 - p)) and ds/dp */
+__device__ __forceinline__ void sp_weight(double p, double &s, double &ds) {
+  const double w = p * (1.0 - p);
+  if (!(w > 0.0)) {
+    s = 0.0;
+    ds = 0.0;
+    return;
+  }
+  const double h = 3.0 * p * p - 2.0 * p * p * p, dh = 6.0 * p - 6.0 * p * p;
+  const double sq = sqrt(w), u = p * (1.0 - h);
+  s = u / sq;
+  ds = ((1.0 - h) - p * dh) / sq - u * (1.0 - 2.0 * p) / (2.0 * sq * w);
+}
+
+/* One face of the 3x3 window (xface: between (fi,fj) and (fi+1,fj); else
+ * between (fi,fj) and (fi,fj+1)) for two phases, one component: its primal
+ * current j and flux F, then, given their adjoints jb and Fb, the adjoints
+ * of the phi window (Sb), the mu window (Mb) and the solid's delta-phi window
+ * (Db).  ylo: interior y of the face's lower cell (y-faces). */
+__device__ __forceinline__ void face_rev(const AK<double> &D, const double (&S)[2][3][3], const double (&M)[1][3][3],
+                                         const double (&DP)[2][3][3], bool xface, int fi, int fj, int ylo, int my,
+                                         double &j, double &F, double jb, double Fb, bool want_j, double (&Sb)[2][3][3],
+                                         double (&Mb)[3][3], double (&Db)[3][3]) {
+  const Consts<double> *c = D.c;
+  const int i1 = xface ? fi + 1 : fi, j1 = xface ? fj : fj + 1;
+  double gr[2], cn[2];
+#pragma unroll
+  for (int a = 0; a < 2; a++) {
+    if (xface) {
+      gr[a] = adivx(S[a][i1][j1] - S[a][fi][fj], D);
+      cn[a] = 0.5 * (adiv2y(S[a][fi][fj + 1] - S[a][fi][fj - 1], D) + adiv2y(S[a][i1][fj + 1] - S[a][i1][fj - 1], D));
+    } else {
+      gr[a] = adivy(S[a][i1][j1] - S[a][fi][fj], D);
+      const double gc0 = 0.5 * (adivx(S[a][fi + 1][fj] - S[a][fi][fj], D) + adivx(S[a][fi][fj] - S[a][fi - 1][fj], D));
+      const double gc1 = 0.5 * (adivx(S[a][fi + 1][j1] - S[a][i1][j1], D) + adivx(S[a][i1][j1] - S[a][fi - 1][j1], D));
+      cn[a] = 0.5 * (gc0 + gc1);
+    }
+  }
+  const double hg = xface ? rdx(c) : rdy(c);   /* d gr / d(difference) */
+  /* ---- diffusion flux F = (D(cell 1) + D(cell 0)) / 2 * (mu1 - mu0) / h */
+  double DD0 = 0.0, DD1 = 0.0;
+#pragma unroll
+  for (int b = 0; b < 2; b++) {
+    DD0 += c->DC[b][0][0][0] * S[b][fi][fj];
+    DD1 += c->DC[b][0][0][0] * S[b][i1][j1];
+  }
+  const double dm = (DD1 + DD0) * 0.5;
+  const double gm = xface ? adivx(M[0][i1][j1] - M[0][fi][fj], D) : adivy(M[0][i1][j1] - M[0][fi][fj], D);
+  F = dm * gm;
+  {
+    const double dmb = Fb * gm, gmb = Fb * dm;
+    Mb[i1][j1] += gmb * hg;
+    Mb[fi][fj] -= gmb * hg;
+#pragma unroll
+    for (int b = 0; b < 2; b++) {
+      Sb[b][i1][j1] += 0.5 * dmb * c->DC[b][0][0][0];
+      Sb[b][fi][fj] += 0.5 * dmb * c->DC[b][0][0][0];
+    }
+  }
+  /* ---- anti-trapping current of the solid (phase 0) */
+  j = 0.0;
+  const bool yskip = !xface && (ylo + 3 == my - 2);
+  const double s2 = cn[0] * cn[0] + gr[0] * gr[0];
+  if (s2 == 0.0 || yskip) return;
+  const double ng = sqrt(s2), nl = sqrt(cn[1] * cn[1] + gr[1] * gr[1]);
+  double sp = gr[0] * gr[1];
+  sp += cn[0] * cn[1];
+  const double sp0 = sp;
+  if (nl > 0.0) sp /= (nl * ng);
+  const double m0 = M[0][fi][fj], m1 = M[0][i1][j1];
+  const double cl0 = 0.0 + c->cmu[1][0][0] * (m0 - c->E[1][0]), cs0 = 0.0 + c->cmu[0][0][0] * (m0 - c->E[0][0]);
+  const double cl1 = 0.0 + c->cmu[1][0][0] * (m1 - c->E[1][0]), cs1 = 0.0 + c->cmu[0][0][0] * (m1 - c->E[0][0]);
+  const double dp0 = DP[0][fi][fj], dp1 = DP[0][i1][j1];
+  double w0 = 1.0, w1 = 1.0, dw0 = 0.0, dw1 = 0.0;
+  if (c->obstacle) {
+    sp_weight(S[0][fi][fj], w0, dw0);
+    sp_weight(S[0][i1][j1], w1, dw1);
+  }
+  const double t0 = w0 * (cl0 - cs0), t1 = w1 * (cl1 - cs1);
+  const double br = t1 * dp1 + t0 * dp0;
+  const double half = c->obstacle ? 0.5 : c->well_half, atf = c->atf[0][0];
+  const double A1 = atf * fabs(sp) * half, A2 = A1 * br, A3 = A2 * gr[0];
+  j = A3 / ng;
+  if (!want_j || jb == 0.0) return;
+  /* reverse */
+  const double A3b = jb / ng;
+  double ngb = -jb * A3 / (ng * ng);
+  const double A2b = A3b * gr[0];
+  double gr0b = A3b * A2;
+  const double A1b = A2b * br, brb = A2b * A1;
+  const double spb = A1b * half * atf * (sp > 0.0 ? 1.0 : (sp < 0.0 ? -1.0 : 0.0));
+  double sp0b = spb, nlb = 0.0;
+  if (nl > 0.0) {
+    const double den = nl * ng;
+    sp0b = spb / den;
+    const double denb = -spb * sp / den;
+    nlb = denb * ng;
+    ngb += denb * nl;
+  }
+  (void)sp0;
+  gr0b += sp0b * gr[1];
+  double grLb = sp0b * gr[0], cn0b = sp0b * cn[1], cnLb = sp0b * cn[0];
+  gr0b += ngb * gr[0] / ng;
+  cn0b += ngb * cn[0] / ng;
+  if (nl > 0.0) {
+    grLb += nlb * gr[1] / nl;
+    cnLb += nlb * cn[1] / nl;
+  }
+  /* bracket: t1 dp1 + t0 dp0, t = w (cl - cs), cl - cs linear in mu */
+  const double t1b = brb * dp1, t0b = brb * dp0;
+  Db[i1][j1] += brb * t1;
+  Db[fi][fj] += brb * t0;
+  const double dcm = c->cmu[1][0][0] - c->cmu[0][0][0];
+  Mb[i1][j1] += t1b * w1 * dcm;
+  Mb[fi][fj] += t0b * w0 * dcm;
+  if (c->obstacle) {
+    Sb[0][i1][j1] += t1b * (cl1 - cs1) * dw1;
+    Sb[0][fi][fj] += t0b * (cl0 - cs0) * dw0;
+  }
+  /* gradients to the phi window */
+  const double grb[2] = {gr0b, grLb}, cnb[2] = {cn0b, cnLb};
+#pragma unroll
+  for (int a = 0; a < 2; a++) {
+    Sb[a][i1][j1] += grb[a] * hg;
+    Sb[a][fi][fj] -= grb[a] * hg;
+    if (xface) {
+      const double q = 0.5 * cnb[a] * r2dy(c);
+      Sb[a][fi][fj + 1] += q;
+      Sb[a][fi][fj - 1] -= q;
+      Sb[a][i1][fj + 1] += q;
+      Sb[a][i1][fj - 1] -= q;
+    } else {
+      const double q = 0.25 * cnb[a] * rdx(c);
+      Sb[a][fi + 1][fj] += q;
+      Sb[a][fi - 1][fj] -= q;
+      Sb[a][fi + 1][j1] += q;
+      Sb[a][fi - 1][j1] -= q;
+    }
+  }
+}
+
+/* part 0: the cell's own terms; parts 1-4: faces x+, x-, y+, y- */
+__device__ __forceinline__ void rev_update_hand(const Consts<double> *__restrict__ c, const AdjParams &prm,
+                                                const Grid &g, const double *__restrict__ st,
+                                                const double *__restrict__ dphi, const double *__restrict__ ybar,
+                                                double *__restrict__ xbar, double *__restrict__ dphibar, int x, int y,
+                                                int part, double (&pacc)[ADJ_NPARAM]) {
+  const long long o = (long long)x * g.pitch + y;
+  const double yb0 = ybar[o], yb1 = ybar[g.plane + o], ybm = ybar[2 * g.plane + o];
+  double S[2][3][3], M[1][3][3], DP[2][3][3];
+  gather<2, 1>(c, g, st, x, y, S, M);
+#pragma unroll
+  for (int a = 0; a < 2; a++)
+#pragma unroll
+    for (int di = 0; di < 3; di++)
+#pragma unroll
+      for (int dj = 0; dj < 3; dj++) DP[a][di][dj] = dphi[didx(g, a, x + di - 1, y + dj - 1)];
+  double p[ADJ_NPARAM];
+#pragma unroll
+  for (int k = 0; k < ADJ_NPARAM; k++) p[k] = prm.v[k];
+  const AK<double> D = make_ak<double>(c, p);
+  double Sb[2][3][3] = {}, Mb[3][3] = {}, Db[3][3] = {};
+  const double ph0 = S[0][1][1], ph1 = S[1][1][1], m = M[0][1][1];
+  const int bulk = ph0 == 1.0 ? 0 : (ph1 == 1.0 ? 1 : -1);
+  const double H0 = 3.0 * ph0 * ph0 - 2.0 * ph0 * ph0 * ph0, H1 = 3.0 * ph1 * ph1 - 2.0 * ph1 * ph1 * ph1;
+  const double dcdmu = (0.0 + c->cmu64[0][0][0] * H0) + c->cmu64[1][0][0] * H1;
+  /* d nm / d(dt*divflux - divjat) */
+  const double kap = bulk >= 0 ? (bulk == 0 ? c->twoA[0][0] : c->twoA[1][0]) : 1.0 / dcdmu;
+  const double dcb = ybm * kap;   /* adjoint of the update's dc (or of cn, bulk) */
+  const double cst = c->obstacle ? D.jat_obst : D.jat_well;
+  if (part == 0) {
+    /* nph = ph + dp */
+    const double ybp[2] = {yb0, yb1};
+#pragma unroll
+    for (int a = 0; a < 2; a++) {
+      if (ybp[a] != 0.0) {
+        atomicAdd(xbar + a * g.plane + o, ybp[a]);
+        atomicAdd(dphibar + didx(g, a, x, y), ybp[a]);
+      }
+    }
+    if (ybm != 0.0) {
+      if (bulk >= 0) {
+        Mb[1][1] += dcb * c->cmu[bulk][0][0];   /* cn = c_mu(m) + ... */
+      } else {
+        /* nm = m + dc / dcdmu, dc = dt*divflux - divjat - sum */
+        Mb[1][1] += ybm;
+        double jx[4], fx[4];
+        const bool xf[4] = {true, true, false, false};
+        const int fi[4] = {1, 0, 1, 1}, fj[4] = {1, 1, 1, 0}, yl[4] = {0, 0, y, y - 1};
+        double Sd[2][3][3] = {}, Md[3][3] = {}, Dd[3][3] = {};
+#pragma unroll
+        for (int f = 0; f < 4; f++)
+          face_rev(D, S, M, DP, xf[f], fi[f], fj[f], yl[f], g.my, jx[f], fx[f], 0.0, 0.0, false, Sd, Md, Dd);
+        double divflux = 0.0;
+        divflux += adivx(fx[0] - fx[1], D);
+        divflux += adivy(fx[2] - fx[3], D);
+        double divjat = adivx((jx[0] - jx[1]) * cst, D);
+        divjat += adivy((jx[2] - jx[3]) * cst, D);
+        const double dp0 = DP[0][1][1], dp1 = DP[1][1][1];
+        const double g0 = 6.0 * ph0 * (1.0 - ph0), g1 = 6.0 * ph1 * (1.0 - ph1);
+        const double sdh0 = (0.0 + g0 * dp0) + (0.0 * ph0) * dp1, sdh1 = (0.0 + (0.0 * ph1) * dp0) + g1 * dp1;
+        const double cm0 = 0.0 + c->cmu[0][0][0] * (m - c->E[0][0]), cm1 = 0.0 + c->cmu[1][0][0] * (m - c->E[1][0]);
+        const double sum = (0.0 + cm0 * sdh0) + cm1 * sdh1;
+        const double dc = c->dt * divflux - divjat - sum;
+        const double i00 = 1.0 / dcdmu;
+        /* dc / dcdmu */
+        const double dcdmub = -ybm * dc * i00 * i00;
+        Sb[0][1][1] += dcdmub * c->cmu64[0][0][0] * (6.0 * ph0 - 6.0 * ph0 * ph0);
+        Sb[1][1][1] += dcdmub * c->cmu64[1][0][0] * (6.0 * ph1 - 6.0 * ph1 * ph1);
+        /* - sum */
+        const double sumb = -dcb;
+        Mb[1][1] += sumb * (sdh0 * c->cmu[0][0][0] + sdh1 * c->cmu[1][0][0]);
+        const double s0b = sumb * cm0, s1b = sumb * cm1;
+        Db[1][1] += s0b * g0;
+        if (s1b * g1 != 0.0) atomicAdd(dphibar + didx(g, 1, x, y), s1b * g1);
+        Sb[0][1][1] += s0b * dp0 * (6.0 - 12.0 * ph0);
+        Sb[1][1][1] += s1b * dp1 * (6.0 - 12.0 * ph1);
+      }
+    }
+  } else if (ybm != 0.0) {
+    /* face part: divflux = (fx+ - fx-)/dx + (fy+ - fy-)/dy, divjat likewise times cst */
+    const int f = part - 1;
+    const bool xf = f < 2;
+    const double sg = (f == 0 || f == 2) ? 1.0 : -1.0, hh = xf ? rdx(c) : rdy(c);
+    const double divfluxb = dcb * c->dt, divjatb = -dcb;
+    const double jb = sg * cst * divjatb * hh, Fb = sg * divfluxb * hh;
+    double j = 0.0, F;
+    /* one call per face with its window coordinates as constants (the
+     * window arrays stay in registers) */
+    switch (f) {
+      case 0: face_rev(D, S, M, DP, true, 1, 1, 0, g.my, j, F, jb, Fb, true, Sb, Mb, Db); break;
+      case 1: face_rev(D, S, M, DP, true, 0, 1, 0, g.my, j, F, jb, Fb, true, Sb, Mb, Db); break;
+      case 2: face_rev(D, S, M, DP, false, 1, 1, y, g.my, j, F, jb, Fb, true, Sb, Mb, Db); break;
+      default: face_rev(D, S, M, DP, false, 1, 0, y - 1, g.my, j, F, jb, Fb, true, Sb, Mb, Db); break;
+    }
+    /* cst = jat_obst or jat_well = (-0.25 pi or -1) * epsilon */
+    pacc[ADJ_EPS] += sg * j * divjatb * hh * (c->obstacle ? (-0.25 * M_PI) : -1.0);
+  }
+  /* scatter through the boundary copy tables */
+#pragma unroll
+  for (int di = 0; di < 3; di++)
+#pragma unroll
+    for (int dj = 0; dj < 3; dj++) {
+      const int xs = rmx(x + di - 1, g, c, 0), ys = rmy(y + dj - 1, g, c, 0);
+#pragma unroll
+      for (int a = 0; a < 2; a++)
+        if (Sb[a][di][dj] != 0.0) atomicAdd(xbar + a * g.plane + (long long)xs * g.pitch + ys, Sb[a][di][dj]);
+      if (Mb[di][dj] != 0.0) {
+        const int xm = rmx(x + di - 1, g, c, 1), ym = rmy(y + dj - 1, g, c, 1);
+        atomicAdd(xbar + 2 * g.plane + (long long)xm * g.pitch + ym, Mb[di][dj]);
+      }
+      if (Db[di][dj] != 0.0) atomicAdd(dphibar + didx(g, 0, x + di - 1, y + dj - 1), Db[di][dj]);
+    }
+}
+
+__global__ void __launch_bounds__(AB) ka_rev_update_hand(const Consts<double> *__restrict__ c, AdjParams prm, Grid g,
+                                                         const double *__restrict__ st,
+                                                         const double *__restrict__ dphi,
+                                                         const double *__restrict__ ybar, double *__restrict__ xbar,
+                                                         double *__restrict__ dphibar, double *__restrict__ pbar,
+                                                         const int2 *__restrict__ cells,
+                                                         const int *__restrict__ count) {
+  double pacc[ADJ_NPARAM] = {};
+  const long long n = (long long)*count * 5;
+  for (long long i = (long long)blockIdx.x * AB + threadIdx.x; i < n; i += (long long)gridDim.x * AB) {
+    const int2 e = cells[i / 5];
+    rev_update_hand(c, prm, g, st, dphi, ybar, xbar, dphibar, e.x, e.y, (int)(i % 5), pacc);
+  }
+  flush_params(pacc, pbar);
+}
+
 /* Reverse of the phase-field pass at ring or interior cell (x, y).  SORT:
  * returns whether the cell has an active phase (the only cells with a
  * derivative); the dual passes run with SORT false over the list of those. */
@@ -619,13 +908,19 @@ struct AdjKernels {
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     return 16 * nsm;
   }
+  /* dual: the listed cells by dual passes instead of the hand-derived reverse */
+  template <bool DUAL>
   static cudaError_t rev_update(cudaStream_t s, const void *c, AdjParams p, Grid g, const double *st,
                                 const double *dp, const double *ybar, double *xbar, double *dpbar, double *pbar,
                                 int2 *cells, int *count) {
     dim3 grid((g.my + AB - 1) / AB, g.mx);
     ka_rev_update<N, K><<<grid, AB, 0, s>>>((const Consts<double> *)c, p, g, st, dp, ybar, xbar, dpbar, cells, count);
-    ka_rev_update_list<N, K><<<list_grid(), AB, 0, s>>>((const Consts<double> *)c, p, g, st, dp, ybar, xbar, dpbar,
-                                                        pbar, cells, count);
+    if (DUAL || N != 2 || K != 1)
+      ka_rev_update_list<N, K><<<list_grid(), AB, 0, s>>>((const Consts<double> *)c, p, g, st, dp, ybar, xbar,
+                                                          dpbar, pbar, cells, count);
+    else
+      ka_rev_update_hand<<<list_grid(), AB, 0, s>>>((const Consts<double> *)c, p, g, st, dp, ybar, xbar, dpbar, pbar,
+                                                    cells, count);
     return cudaGetLastError();
   }
   static cudaError_t rev_dphi(cudaStream_t s, const void *c, AdjParams p, Grid g, const double *st,
@@ -642,17 +937,20 @@ struct AdjKernels {
 
 bool gp_adjoint_launch(int N, int K, bool aniso, gpd::AdjLaunch *out) {
   if (N != 2 || K != 1) return false;
+  /* GP_ADJOINT_DUAL_UPDATE: the concentration pass by dual passes (the
+   * hand-derived reverse's cross-check) */
+  const bool dual = getenv("GP_ADJOINT_DUAL_UPDATE") != nullptr;
   if (aniso) {
     out->dphi = gpd::AdjKernels<2, 1, true>::dphi;
     out->dphi_sparse = gpd::AdjKernels<2, 1, true>::dphi_sparse;
     out->update = gpd::AdjKernels<2, 1, true>::update;
-    out->rev_update = gpd::AdjKernels<2, 1, true>::rev_update;
+    out->rev_update = dual ? gpd::AdjKernels<2, 1, true>::rev_update<true> : gpd::AdjKernels<2, 1, true>::rev_update<false>;
     out->rev_dphi = gpd::AdjKernels<2, 1, true>::rev_dphi;
   } else {
     out->dphi = gpd::AdjKernels<2, 1, false>::dphi;
     out->dphi_sparse = gpd::AdjKernels<2, 1, false>::dphi_sparse;
     out->update = gpd::AdjKernels<2, 1, false>::update;
-    out->rev_update = gpd::AdjKernels<2, 1, false>::rev_update;
+    out->rev_update = dual ? gpd::AdjKernels<2, 1, false>::rev_update<true> : gpd::AdjKernels<2, 1, false>::rev_update<false>;
     out->rev_dphi = gpd::AdjKernels<2, 1, false>::rev_dphi;
   }
   return true;

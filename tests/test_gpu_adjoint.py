@@ -159,6 +159,38 @@ def test_adjoint_matches_the_fp64_tape(tmp_path, name):
     np.testing.assert_allclose(g["mu0_bar"], gmu, rtol=0, atol=1e-8 * np.abs(gmu).max())
 
 
+@pytest.mark.parametrize("name", sorted(CASES) + ["well_aniso"])
+def test_hand_reverse_matches_dual_passes(tmp_path, name, monkeypatch):
+    """The concentration pass's hand-derived reverse against the dual-number
+    passes it replaces (GP_ADJOINT_DUAL_UPDATE): the same derivatives, up to
+    the rounding of the derivative arithmetic and the order of the atomic
+    sums."""
+    if name == "well_aniso":
+        from test_torch_tape import CASES as TCASES
+        c = TCASES[name]
+        ip, fp = write_case(str(tmp_path), name, c["kw"], seeds=c["seeds"])
+        p = gp.load_params(ip)
+        phi0, mu0 = gp.fill(p, fp)
+    else:
+        p, phi0, mu0 = _params(tmp_path, name)
+    phi, mu = _start(p, phi0, mu0)
+    nsteps = 30
+    target = _target(p, phi, mu, nsteps)
+    res = []
+    for dual in (False, True):
+        if dual:
+            monkeypatch.setenv("GP_ADJOINT_DUAL_UPDATE", "1")
+        else:
+            monkeypatch.delenv("GP_ADJOINT_DUAL_UPDATE", raising=False)
+        with gp.Simulation(p, phi, mu) as s:
+            res.append(s.adjoint(nsteps, target_phi=target))
+    h, d = res
+    for n in PARAMS:
+        assert h["d_" + n] == pytest.approx(d["d_" + n], rel=1e-10, abs=1e-13 * abs(d["d_tau"])), n
+    for k in ("phi0_bar", "mu0_bar"):
+        np.testing.assert_allclose(h[k], d[k], rtol=0, atol=1e-10 * np.abs(d[k]).max(), err_msg=k)
+
+
 def binomial_cost(l, s):
     """fewest forward steps that reverse l steps with the start state and s
     more states kept (binomial checkpointing: r*l - C(s+1+r, r-1) with r the
