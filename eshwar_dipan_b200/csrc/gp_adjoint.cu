@@ -630,120 +630,12 @@ __device__ __forceinline__ void face_rev(const AK<double> &D, const double (&S)[
   }
 }
 
-/* part 0: the cell's own terms; parts 1-4: faces x+, x-, y+, y- */
-__device__ __forceinline__ void rev_update_hand(const Consts<double> *__restrict__ c, const AdjParams &prm,
-                                                const Grid &g, const double *__restrict__ st,
-                                                const double *__restrict__ dphi, const double *__restrict__ ybar,
-                                                double *__restrict__ xbar, double *__restrict__ dphibar, int x, int y,
-                                                int part, double (&pacc)[ADJ_NPARAM]) {
-  const long long o = (long long)x * g.pitch + y;
-  const double yb0 = ybar[o], yb1 = ybar[g.plane + o], ybm = ybar[2 * g.plane + o];
-  double S[2][3][3], M[1][3][3], DP[2][3][3];
-  gather<2, 1>(c, g, st, x, y, S, M);
-#pragma unroll
-  for (int a = 0; a < 2; a++)
-#pragma unroll
-    for (int di = 0; di < 3; di++)
-#pragma unroll
-      for (int dj = 0; dj < 3; dj++) DP[a][di][dj] = dphi[didx(g, a, x + di - 1, y + dj - 1)];
-  double p[ADJ_NPARAM];
-#pragma unroll
-  for (int k = 0; k < ADJ_NPARAM; k++) p[k] = prm.v[k];
-  const AK<double> D = make_ak<double>(c, p);
-  double Sb[2][3][3] = {}, Mb[3][3] = {}, Db[3][3] = {};
-  const double ph0 = S[0][1][1], ph1 = S[1][1][1], m = M[0][1][1];
-  const int bulk = ph0 == 1.0 ? 0 : (ph1 == 1.0 ? 1 : -1);
-  const double H0 = 3.0 * ph0 * ph0 - 2.0 * ph0 * ph0 * ph0, H1 = 3.0 * ph1 * ph1 - 2.0 * ph1 * ph1 * ph1;
-  const double dcdmu = (0.0 + c->cmu64[0][0][0] * H0) + c->cmu64[1][0][0] * H1;
-  /* d nm / d(dt*divflux - divjat) */
-  const double kap = bulk >= 0 ? (bulk == 0 ? c->twoA[0][0] : c->twoA[1][0]) : 1.0 / dcdmu;
-  const double dcb = ybm * kap;   /* adjoint of the update's dc (or of cn, bulk) */
-  const double cst = c->obstacle ? D.jat_obst : D.jat_well;
-  if (part == 0) {
-    /* nph = ph + dp */
-    const double ybp[2] = {yb0, yb1};
-#pragma unroll
-    for (int a = 0; a < 2; a++) {
-      if (ybp[a] != 0.0) {
-        atomicAdd(xbar + a * g.plane + o, ybp[a]);
-        atomicAdd(dphibar + didx(g, a, x, y), ybp[a]);
-      }
-    }
-    if (ybm != 0.0) {
-      if (bulk >= 0) {
-        Mb[1][1] += dcb * c->cmu[bulk][0][0];   /* cn = c_mu(m) + ... */
-      } else {
-        /* nm = m + dc / dcdmu, dc = dt*divflux - divjat - sum */
-        Mb[1][1] += ybm;
-        double jx[4], fx[4];
-        const bool xf[4] = {true, true, false, false};
-        const int fi[4] = {1, 0, 1, 1}, fj[4] = {1, 1, 1, 0}, yl[4] = {0, 0, y, y - 1};
-        double Sd[2][3][3] = {}, Md[3][3] = {}, Dd[3][3] = {};
-#pragma unroll
-        for (int f = 0; f < 4; f++)
-          face_rev(D, S, M, DP, xf[f], fi[f], fj[f], yl[f], g.my, jx[f], fx[f], 0.0, 0.0, false, Sd, Md, Dd);
-        double divflux = 0.0;
-        divflux += adivx(fx[0] - fx[1], D);
-        divflux += adivy(fx[2] - fx[3], D);
-        double divjat = adivx((jx[0] - jx[1]) * cst, D);
-        divjat += adivy((jx[2] - jx[3]) * cst, D);
-        const double dp0 = DP[0][1][1], dp1 = DP[1][1][1];
-        const double g0 = 6.0 * ph0 * (1.0 - ph0), g1 = 6.0 * ph1 * (1.0 - ph1);
-        const double sdh0 = (0.0 + g0 * dp0) + (0.0 * ph0) * dp1, sdh1 = (0.0 + (0.0 * ph1) * dp0) + g1 * dp1;
-        const double cm0 = 0.0 + c->cmu[0][0][0] * (m - c->E[0][0]), cm1 = 0.0 + c->cmu[1][0][0] * (m - c->E[1][0]);
-        const double sum = (0.0 + cm0 * sdh0) + cm1 * sdh1;
-        const double dc = c->dt * divflux - divjat - sum;
-        const double i00 = 1.0 / dcdmu;
-        /* dc / dcdmu */
-        const double dcdmub = -ybm * dc * i00 * i00;
-        Sb[0][1][1] += dcdmub * c->cmu64[0][0][0] * (6.0 * ph0 - 6.0 * ph0 * ph0);
-        Sb[1][1][1] += dcdmub * c->cmu64[1][0][0] * (6.0 * ph1 - 6.0 * ph1 * ph1);
-        /* - sum */
-        const double sumb = -dcb;
-        Mb[1][1] += sumb * (sdh0 * c->cmu[0][0][0] + sdh1 * c->cmu[1][0][0]);
-        const double s0b = sumb * cm0, s1b = sumb * cm1;
-        Db[1][1] += s0b * g0;
-        if (s1b * g1 != 0.0) atomicAdd(dphibar + didx(g, 1, x, y), s1b * g1);
-        Sb[0][1][1] += s0b * dp0 * (6.0 - 12.0 * ph0);
-        Sb[1][1][1] += s1b * dp1 * (6.0 - 12.0 * ph1);
-      }
-    }
-  } else if (ybm != 0.0) {
-    /* face part: divflux = (fx+ - fx-)/dx + (fy+ - fy-)/dy, divjat likewise times cst */
-    const int f = part - 1;
-    const bool xf = f < 2;
-    const double sg = (f == 0 || f == 2) ? 1.0 : -1.0, hh = xf ? rdx(c) : rdy(c);
-    const double divfluxb = dcb * c->dt, divjatb = -dcb;
-    const double jb = sg * cst * divjatb * hh, Fb = sg * divfluxb * hh;
-    double j = 0.0, F;
-    /* one call per face with its window coordinates as constants (the
-     * window arrays stay in registers) */
-    switch (f) {
-      case 0: face_rev(D, S, M, DP, true, 1, 1, 0, g.my, j, F, jb, Fb, true, Sb, Mb, Db); break;
-      case 1: face_rev(D, S, M, DP, true, 0, 1, 0, g.my, j, F, jb, Fb, true, Sb, Mb, Db); break;
-      case 2: face_rev(D, S, M, DP, false, 1, 1, y, g.my, j, F, jb, Fb, true, Sb, Mb, Db); break;
-      default: face_rev(D, S, M, DP, false, 1, 0, y - 1, g.my, j, F, jb, Fb, true, Sb, Mb, Db); break;
-    }
-    /* cst = jat_obst or jat_well = (-0.25 pi or -1) * epsilon */
-    pacc[ADJ_EPS] += sg * j * divjatb * hh * (c->obstacle ? (-0.25 * M_PI) : -1.0);
-  }
-  /* scatter through the boundary copy tables */
-#pragma unroll
-  for (int di = 0; di < 3; di++)
-#pragma unroll
-    for (int dj = 0; dj < 3; dj++) {
-      const int xs = rmx(x + di - 1, g, c, 0), ys = rmy(y + dj - 1, g, c, 0);
-#pragma unroll
-      for (int a = 0; a < 2; a++)
-        if (Sb[a][di][dj] != 0.0) atomicAdd(xbar + a * g.plane + (long long)xs * g.pitch + ys, Sb[a][di][dj]);
-      if (Mb[di][dj] != 0.0) {
-        const int xm = rmx(x + di - 1, g, c, 1), ym = rmy(y + dj - 1, g, c, 1);
-        atomicAdd(xbar + 2 * g.plane + (long long)xm * g.pitch + ym, Mb[di][dj]);
-      }
-      if (Db[di][dj] != 0.0) atomicAdd(dphibar + didx(g, 0, x + di - 1, y + dj - 1), Db[di][dj]);
-    }
-}
-
+/* One warp takes six listed cells, five lanes each: lane 5i is cell i's own
+ * part, lanes 5i+1 .. 5i+4 its faces x+, x-, y+, y-.  A face lane reverses its
+ * face (its adjoints depend on the cell's adjoint of mu and on the cell's
+ * multiplier only) and hands the face's current and flux to the cell lane,
+ * which needs all four for the dc of the dc/dmu term; the five lanes' window
+ * adjoints are then summed by shuffles and the cell lane scatters them. */
 __global__ void __launch_bounds__(AB) ka_rev_update_hand(const Consts<double> *__restrict__ c, AdjParams prm, Grid g,
                                                          const double *__restrict__ st,
                                                          const double *__restrict__ dphi,
@@ -751,11 +643,139 @@ __global__ void __launch_bounds__(AB) ka_rev_update_hand(const Consts<double> *_
                                                          double *__restrict__ dphibar, double *__restrict__ pbar,
                                                          const int2 *__restrict__ cells,
                                                          const int *__restrict__ count) {
+  constexpr unsigned FULL = 0xffffffffu;
   double pacc[ADJ_NPARAM] = {};
-  const long long n = (long long)*count * 5;
-  for (long long i = (long long)blockIdx.x * AB + threadIdx.x; i < n; i += (long long)gridDim.x * AB) {
-    const int2 e = cells[i / 5];
-    rev_update_hand(c, prm, g, st, dphi, ybar, xbar, dphibar, e.x, e.y, (int)(i % 5), pacc);
+  const int lane = threadIdx.x & 31, slot = lane / 5, part = lane - slot * 5, base = slot * 5;
+  const long long ncell = *count, nwarps = (long long)gridDim.x * (AB / 32);
+  double p[ADJ_NPARAM];
+#pragma unroll
+  for (int k = 0; k < ADJ_NPARAM; k++) p[k] = prm.v[k];
+  const AK<double> D = make_ak<double>(c, p);
+  const double cst = c->obstacle ? D.jat_obst : D.jat_well;
+  for (long long w0 = ((long long)blockIdx.x * (AB / 32) + (threadIdx.x >> 5)) * 6; w0 < ncell; w0 += nwarps * 6) {
+    const long long ci = w0 + slot;
+    const bool live = slot < 6 && ci < ncell;
+    int x = 0, y = 0;
+    double S[2][3][3] = {}, M[1][3][3] = {}, DP[2][3][3] = {};
+    double yb0 = 0.0, yb1 = 0.0, ybm = 0.0;
+    if (live) {
+      const int2 e = cells[ci];
+      x = e.x;
+      y = e.y;
+      const long long o = (long long)x * g.pitch + y;
+      yb0 = ybar[o];
+      yb1 = ybar[g.plane + o];
+      ybm = ybar[2 * g.plane + o];
+      gather<2, 1>(c, g, st, x, y, S, M);
+#pragma unroll
+      for (int a = 0; a < 2; a++)
+#pragma unroll
+        for (int di = 0; di < 3; di++)
+#pragma unroll
+          for (int dj = 0; dj < 3; dj++) DP[a][di][dj] = dphi[didx(g, a, x + di - 1, y + dj - 1)];
+    }
+    double Sb[2][3][3] = {}, Mb[3][3] = {}, Db[3][3] = {};
+    const double ph0 = S[0][1][1], ph1 = S[1][1][1], m = M[0][1][1];
+    const int bulk = ph0 == 1.0 ? 0 : (ph1 == 1.0 ? 1 : -1);
+    const double H0 = 3.0 * ph0 * ph0 - 2.0 * ph0 * ph0 * ph0, H1 = 3.0 * ph1 * ph1 - 2.0 * ph1 * ph1 * ph1;
+    const double dcdmu = (0.0 + c->cmu64[0][0][0] * H0) + c->cmu64[1][0][0] * H1;
+    /* d nm / d(dt*divflux - divjat) */
+    const double kap = bulk >= 0 ? (bulk == 0 ? c->twoA[0][0] : c->twoA[1][0]) : (live ? 1.0 / dcdmu : 0.0);
+    const double dcb = ybm * kap;   /* adjoint of the update's dc (of cn in a bulk cell) */
+    /* ---- face lanes: the face's current and flux, and their reverse */
+    double jf = 0.0, Ff = 0.0;
+    if (live && part > 0) {
+      const int f = part - 1;
+      const bool xf = f < 2;
+      const double sg = (f == 0 || f == 2) ? 1.0 : -1.0, hh = xf ? rdx(c) : rdy(c);
+      const double divfluxb = dcb * c->dt, divjatb = -dcb;
+      const double jb = sg * cst * divjatb * hh, Fb = sg * divfluxb * hh;
+      const bool rev = ybm != 0.0;
+      switch (f) {   /* window coordinates as constants: the window arrays stay in registers */
+        case 0: face_rev(D, S, M, DP, true, 1, 1, 0, g.my, jf, Ff, jb, Fb, rev, Sb, Mb, Db); break;
+        case 1: face_rev(D, S, M, DP, true, 0, 1, 0, g.my, jf, Ff, jb, Fb, rev, Sb, Mb, Db); break;
+        case 2: face_rev(D, S, M, DP, false, 1, 1, y, g.my, jf, Ff, jb, Fb, rev, Sb, Mb, Db); break;
+        default: face_rev(D, S, M, DP, false, 1, 0, y - 1, g.my, jf, Ff, jb, Fb, rev, Sb, Mb, Db); break;
+      }
+      /* cst = jat_obst or jat_well = (-0.25 pi or -1) * epsilon */
+      pacc[ADJ_EPS] += sg * jf * divjatb * hh * (c->obstacle ? (-0.25 * M_PI) : -1.0);
+    }
+    double jx[4], fx[4];
+#pragma unroll
+    for (int f = 0; f < 4; f++) {
+      jx[f] = __shfl_sync(FULL, jf, base + 1 + f);
+      fx[f] = __shfl_sync(FULL, Ff, base + 1 + f);
+    }
+    /* ---- the cell lane: the phi commit and the cell's own terms */
+    if (live && part == 0) {
+      const long long o = (long long)x * g.pitch + y;
+      if (yb0 != 0.0) {
+        atomicAdd(xbar + o, yb0);
+        atomicAdd(dphibar + didx(g, 0, x, y), yb0);
+      }
+      if (yb1 != 0.0) {
+        atomicAdd(xbar + g.plane + o, yb1);
+        atomicAdd(dphibar + didx(g, 1, x, y), yb1);
+      }
+      if (ybm != 0.0) {
+        if (bulk >= 0) {
+          Mb[1][1] += dcb * c->cmu[bulk][0][0];   /* cn = c_mu(m) + ... */
+        } else {
+          /* nm = m + dc / dcdmu, dc = dt*divflux - divjat - sum */
+          Mb[1][1] += ybm;
+          double divflux = 0.0;
+          divflux += adivx(fx[0] - fx[1], D);
+          divflux += adivy(fx[2] - fx[3], D);
+          double divjat = adivx((jx[0] - jx[1]) * cst, D);
+          divjat += adivy((jx[2] - jx[3]) * cst, D);
+          const double dp0 = DP[0][1][1], dp1 = DP[1][1][1];
+          const double g0 = 6.0 * ph0 * (1.0 - ph0), g1 = 6.0 * ph1 * (1.0 - ph1);
+          const double sdh0 = (0.0 + g0 * dp0) + (0.0 * ph0) * dp1, sdh1 = (0.0 + (0.0 * ph1) * dp0) + g1 * dp1;
+          const double cm0 = 0.0 + c->cmu[0][0][0] * (m - c->E[0][0]), cm1 = 0.0 + c->cmu[1][0][0] * (m - c->E[1][0]);
+          const double sum = (0.0 + cm0 * sdh0) + cm1 * sdh1;
+          const double dc = c->dt * divflux - divjat - sum;
+          const double i00 = 1.0 / dcdmu;
+          /* dc / dcdmu */
+          const double dcdmub = -ybm * dc * i00 * i00;
+          Sb[0][1][1] += dcdmub * c->cmu64[0][0][0] * (6.0 * ph0 - 6.0 * ph0 * ph0);
+          Sb[1][1][1] += dcdmub * c->cmu64[1][0][0] * (6.0 * ph1 - 6.0 * ph1 * ph1);
+          /* - sum */
+          const double sumb = -dcb;
+          Mb[1][1] += sumb * (sdh0 * c->cmu[0][0][0] + sdh1 * c->cmu[1][0][0]);
+          const double s0b = sumb * cm0, s1b = sumb * cm1;
+          Db[1][1] += s0b * g0;
+          if (s1b * g1 != 0.0) atomicAdd(dphibar + didx(g, 1, x, y), s1b * g1);
+          Sb[0][1][1] += s0b * dp0 * (6.0 - 12.0 * ph0);
+          Sb[1][1][1] += s1b * dp1 * (6.0 - 12.0 * ph1);
+        }
+      }
+    }
+    /* ---- the five lanes' window adjoints, summed on the cell lane, scattered
+     * through the boundary copy tables */
+#pragma unroll
+    for (int di = 0; di < 3; di++)
+#pragma unroll
+      for (int dj = 0; dj < 3; dj++) {
+        double v[4] = {Sb[0][di][dj], Sb[1][di][dj], Mb[di][dj], Db[di][dj]};
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          double t = v[q];
+#pragma unroll
+          for (int k = 1; k < 5; k++) t += __shfl_sync(FULL, v[q], base + k);
+          v[q] = t;
+        }
+        if (live && part == 0) {
+          const int xs = rmx(x + di - 1, g, c, 0), ys = rmy(y + dj - 1, g, c, 0);
+#pragma unroll
+          for (int a = 0; a < 2; a++)
+            if (v[a] != 0.0) atomicAdd(xbar + a * g.plane + (long long)xs * g.pitch + ys, v[a]);
+          if (v[2] != 0.0) {
+            const int xm = rmx(x + di - 1, g, c, 1), ym = rmy(y + dj - 1, g, c, 1);
+            atomicAdd(xbar + 2 * g.plane + (long long)xm * g.pitch + ym, v[2]);
+          }
+          if (v[3] != 0.0) atomicAdd(dphibar + didx(g, 0, x + di - 1, y + dj - 1), v[3]);
+        }
+      }
   }
   flush_params(pacc, pbar);
 }

@@ -348,6 +348,12 @@ struct gp_batch {
   double *trows;                /* their temperature rows (SimDesc::off_T) */
   gpd::SimDyn *dyn;             /* per simulation moving-frame state */
   double *dphi_out = nullptr;   /* the adjoint's forward steps: where the interface tiles write delta-phi */
+  /* the adjoint's forward steps over its tape (a batch of one): the step reads
+   * redir_in (bulk boxes through redir_map) and writes redir_out instead of
+   * the ping-pong buffers; the flags still follow the parity */
+  const void *redir_in = nullptr;
+  void *redir_out = nullptr;
+  const gpd::TensorMapSlot *redir_map = nullptr;
   double *partials, *sums_sim;
   /* captured step sequences: graphs[(starting parity, steps)], steps <= GP_GRAPH_STEPS */
   std::map<std::pair<int, long>, cudaGraphExec_t> graphs;
@@ -390,6 +396,10 @@ static int batch_step_once(gp_batch *b, int want_sums, cudaEvent_t *ev) {
   st.trows = b->tgrad ? b->trows : nullptr;
   st.bch_div = b->shape.bch_div;
   const int in = b->cur, out = b->cur ^ 1;
+  const void *sin = b->redir_in ? b->redir_in : b->state[in];
+  void *sout = b->redir_in ? b->redir_out : b->state[out];
+  const gpd::TensorMapSlot *tmaps = b->redir_in ? b->redir_map : b->tmaps;
+  const int tbuf = b->redir_in ? 0 : in;
   if (ev) BK(cudaEventRecord(ev[0], b->stream));
   if (b->tgrad) BK(b->L.trows(b->nsims, b->stream, b->d_desc, b->d_consts, b->counters, b->dyn, b->trows));
   BK(b->L.classify(b->ntiles, b->stream, b->d_desc, b->d_consts, b->d_tsim, b->flags[in], b->flags[out], b->glist,
@@ -399,7 +409,7 @@ static int batch_step_once(gp_batch *b, int want_sums, cudaEvent_t *ev) {
      * the classification and after the step */
     if (ev) BK(cudaEventRecord(ev[1], b->stream));
     BK(b->L.step(b->grid_s, b->mul, b->diag, b->stream, b->d_desc, b->d_consts, b->d_tsim, b->blist, b->glist,
-                 b->tmaps, in, b->state[in], b->state[out], b->flags[out], b->counters, b->grid_s, st));
+                 tmaps, tbuf, sin, sout, b->flags[out], b->counters, b->grid_s, st));
     if (ev) BK(cudaEventRecord(ev[2], b->stream));
     b->cur = out;
     b->steps++;
@@ -407,10 +417,10 @@ static int batch_step_once(gp_batch *b, int want_sums, cudaEvent_t *ev) {
   }
   /* kf_bulk then kf_general; the last CTA of the two resets the lists */
   const int nd = b->grid_b + b->grid_g;
-  BK(b->L.bulk(b->grid_b, b->mul, b->diag, b->stream, b->d_desc, b->d_consts, b->d_tsim, b->blist, b->tmaps, in,
-               b->state[in], b->state[out], b->flags[out], b->counters, nd, st));
+  BK(b->L.bulk(b->grid_b, b->mul, b->diag, b->stream, b->d_desc, b->d_consts, b->d_tsim, b->blist, tmaps, tbuf,
+               sin, sout, b->flags[out], b->counters, nd, st));
   if (ev) BK(cudaEventRecord(ev[1], b->stream));
-  BK(b->L.general(b->grid_g, b->mul, b->stream, b->d_desc, b->d_consts, b->d_tsim, b->state[in], b->state[out],
+  BK(b->L.general(b->grid_g, b->mul, b->stream, b->d_desc, b->d_consts, b->d_tsim, sin, sout,
                   b->flags[out], b->glist, b->counters, nd, st));
   if (ev) BK(cudaEventRecord(ev[2], b->stream));
   b->cur = out;
@@ -797,27 +807,32 @@ static PFN_cuTensorMapEncodeTiled_v12000 encode_tiled_fn() {
 /* The TMA maps of kf_bulk: per simulation and state buffer, the K mu planes
  * as a 3-D tensor {pitch, mx, K} (strides one row, one plane) read in boxes
  * of {BW, SH, K}; coordinates outside the tensor read zeros. */
-static int encode_mu_maps(gp_batch *b, gpd::TensorMapSlot *out) {
+/* The tensor map of simulation s's K mu planes in a state buffer whose
+ * simulation-s planes start at `state` (the bulk tiles' TMA boxes). */
+static int encode_mu_map(gp_batch *b, int s, void *state, gpd::TensorMapSlot *out) {
   PFN_cuTensorMapEncodeTiled_v12000 fn = encode_tiled_fn();
-  if (!fn) return bfail(b, GP_ECUDA, "gp_batch_create: cuTensorMapEncodeTiled is not available");
+  if (!fn) return bfail(b, GP_ECUDA, "cuTensorMapEncodeTiled is not available");
   const bool f64 = b->elem == 8;
   const cuuint32_t bw = f64 ? gpd::BulkGeom<double, 1>::BW : gpd::BulkGeom<float, 1>::BW;
-  for (int s = 0; s < b->nsims; s++) {
-    const gpd::SimDesc &sd = b->desc[s];
+  const gpd::SimDesc &sd = b->desc[s];
+  void *base = (char *)state + (size_t)((long long)b->N * sd.g.plane) * b->elem;
+  const cuuint64_t dims[3] = {(cuuint64_t)sd.g.pitch, (cuuint64_t)sd.g.mx, (cuuint64_t)b->K};
+  const cuuint64_t strides[2] = {(cuuint64_t)sd.g.pitch * b->elem, (cuuint64_t)sd.g.plane * b->elem};
+  const cuuint32_t box[3] = {bw, (cuuint32_t)gpd::SH, (cuuint32_t)b->K};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = fn((CUtensorMap *)out, f64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3,
+                  base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return bfail(b, GP_ECUDA, "cuTensorMapEncodeTiled failed (%d) for simulation %d", (int)r, s);
+  return GP_OK;
+}
+
+static int encode_mu_maps(gp_batch *b, gpd::TensorMapSlot *out) {
+  for (int s = 0; s < b->nsims; s++)
     for (int p = 0; p < 2; p++) {
-      void *base = (char *)b->state[p] + (size_t)(sd.off_state + (long long)b->N * sd.g.plane) * b->elem;
-      const cuuint64_t dims[3] = {(cuuint64_t)sd.g.pitch, (cuuint64_t)sd.g.mx, (cuuint64_t)b->K};
-      const cuuint64_t strides[2] = {(cuuint64_t)sd.g.pitch * b->elem, (cuuint64_t)sd.g.plane * b->elem};
-      const cuuint32_t box[3] = {bw, (cuuint32_t)gpd::SH, (cuuint32_t)b->K};
-      const cuuint32_t estr[3] = {1, 1, 1};
-      CUresult r = fn((CUtensorMap *)&out[2 * s + p],
-                      f64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims,
-                      strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                      CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-      if (r != CUDA_SUCCESS)
-        return bfail(b, GP_ECUDA, "gp_batch_create: cuTensorMapEncodeTiled failed (%d) for simulation %d", (int)r, s);
+      const int rc = encode_mu_map(b, s, (char *)b->state[p] + (size_t)b->desc[s].off_state * b->elem, &out[2 * s + p]);
+      if (rc != GP_OK) return rc;
     }
-  }
   return GP_OK;
 }
 
@@ -1486,11 +1501,12 @@ struct AdjBufs {
          *pbar = nullptr, *final_state = nullptr;
   double *rblk = nullptr;   /* two reverse blocks: adjoint of a state, adjoint of its delta-phi, list counters */
   double *dtape = nullptr;  /* delta-phi of every step, written by the forward pass (whole-tape mode) */
+  gpd::TensorMapSlot *smaps = nullptr;   /* whole-tape mode: the tensor map of each slot's mu planes */
   int2 *cells = nullptr;    /* cells of a reverse pass that take the dual passes */
   int *ncells = nullptr;
   ~AdjBufs() {   /* ybar, xbar and dphibar point into rblk */
     cudaFree(snap); cudaFree(seg); cudaFree(dphi); cudaFree(pbar); cudaFree(final_state); cudaFree(rblk);
-    cudaFree(dtape); cudaFree(cells); cudaFree(ncells);
+    cudaFree(dtape); cudaFree(smaps); cudaFree(cells); cudaFree(ncells);
   }
 };
 
@@ -1590,6 +1606,15 @@ int gp_adjoint(gp_ctx *c, const gp_adj_req *req, gp_adj_out *out) {
   AALLOC(m.final_state, S);
   if (dtape) AALLOC(m.dtape, Sd * (size_t)T);
 #undef AALLOC
+  if (dtape) {
+    std::vector<gpd::TensorMapSlot> hm((size_t)T);
+    for (long t = 0; t < T; t++)
+      if ((rc = encode_mu_map(b, 0, m.snap + S * (size_t)t, &hm[(size_t)t])) != GP_OK) return fail(c, rc, "%s", b->err);
+    if (cudaMalloc((void **)&m.smaps, sizeof(gpd::TensorMapSlot) * (size_t)T) != cudaSuccess)
+      return fail(c, GP_ENOMEM, "gp_adjoint: cudaMalloc of the slot maps failed");
+    CK(cudaMemcpyAsync(m.smaps, hm.data(), sizeof(gpd::TensorMapSlot) * (size_t)T, cudaMemcpyHostToDevice, b->stream));
+    CK(cudaStreamSynchronize(b->stream));
+  }
   int rcur = 0;   /* the block holding the adjoint of the state after the step being reversed */
   auto rbar = [&](int k) { return m.rblk + RB * (size_t)k; };
   m.ybar = rbar(0);
@@ -1631,16 +1656,7 @@ int gp_adjoint(gp_ctx *c, const gp_adj_req *req, gp_adj_out *out) {
   auto slot_ptr = [&](int k) { return m.snap + S * (size_t)k; };
   auto advance = [&](long k) -> int {
     for (long i = 0; i < k; i++) {
-      const long t = work_t + i;   /* the step from state t */
-      if (m.dtape && !have_dphi[(size_t)t]) {
-        b->dphi_out = m.dtape + Sd * (size_t)t;
-        BK(cudaMemsetAsync(b->dphi_out, 0, Sd * 8, b->stream));   /* cells of bulk tiles: +0.0 */
-      }
       const int r = batch_step_once(b, 0, nullptr);
-      if (b->dphi_out) {
-        have_dphi[(size_t)t] = 1;
-        b->dphi_out = nullptr;
-      }
       if (r != GP_OK) return r;
     }
     work_t += k;
@@ -1654,8 +1670,8 @@ int gp_adjoint(gp_ctx *c, const gp_adj_req *req, gp_adj_out *out) {
   };
   /* the seed: dL/d(final state) from the state after the last step */
   auto seed = [&]() -> int {
-    const double *fin = (const double *)b->state[b->cur];
-    BK(cudaMemcpyAsync(m.final_state, fin, S * 8, cudaMemcpyDeviceToDevice, b->stream));
+    const double *fin = m.dtape ? m.final_state : (const double *)b->state[b->cur];
+    if (fin != m.final_state) BK(cudaMemcpyAsync(m.final_state, fin, S * 8, cudaMemcpyDeviceToDevice, b->stream));
     BK(cudaEventRecord(e1, b->stream));
     BK(cudaMemsetAsync(m.ybar, 0, S * 8, b->stream));
     int r;
@@ -1719,7 +1735,30 @@ int gp_adjoint(gp_ctx *c, const gp_adj_req *req, gp_adj_out *out) {
     }
     return reverse(t, (const double *)b->state[b->cur]);
   };
-  while (!stack.empty()) {
+  if (m.dtape) {
+    /* the whole tape: step t reads slot t and writes slot t+1 (the last one
+     * the final state) directly, its bulk boxes through the slot's tensor map,
+     * and leaves its delta-phi on the tape; then every step is reversed from
+     * its slot, last first */
+    for (long t = 0; t < T; t++) {
+      b->redir_in = slot_ptr((int)t);
+      b->redir_out = t + 1 < T ? slot_ptr((int)t + 1) : m.final_state;
+      b->redir_map = m.smaps + t;
+      b->dphi_out = m.dtape + Sd * (size_t)t;
+      int r = cudaMemsetAsync(b->dphi_out, 0, Sd * 8, b->stream) == cudaSuccess ? GP_OK : GP_ECUDA;
+      if (r == GP_OK) r = batch_step_once(b, 0, nullptr);
+      b->redir_in = nullptr;
+      b->redir_out = nullptr;
+      b->redir_map = nullptr;
+      b->dphi_out = nullptr;
+      if (r != GP_OK) return r == GP_ECUDA && !c->err[0] ? fail(c, GP_ECUDA, "gp_adjoint: memset failed") : r;
+      have_dphi[(size_t)t] = 1;
+    }
+    if ((rc = seed()) != GP_OK) return rc;
+    for (long t = T - 1; t >= 0; t--)
+      if ((rc = reverse(t, slot_ptr((int)t))) != GP_OK) return rc;
+  }
+  while (!m.dtape && !stack.empty()) {
     const Task t = stack.back();
     stack.pop_back();
     if (t.l == 0) {
