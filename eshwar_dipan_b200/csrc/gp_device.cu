@@ -1745,7 +1745,13 @@ int gp_adjoint(gp_ctx *c, const gp_adj_req *req, gp_adj_out *out) {
       b->redir_out = t + 1 < T ? slot_ptr((int)t + 1) : m.final_state;
       b->redir_map = m.smaps + t;
       b->dphi_out = m.dtape + Sd * (size_t)t;
-      int r = cudaMemsetAsync(b->dphi_out, 0, Sd * 8, b->stream) == cudaSuccess ? GP_OK : GP_ECUDA;
+      /* the slot written holds nothing the output flags describe: "unknown"
+       * makes the bulk tiles write their phi too */
+      int r = cudaMemsetAsync(b->dphi_out, 0, Sd * 8, b->stream) == cudaSuccess &&
+                      cudaMemsetAsync(b->flags[b->cur ^ 1], 0xfe, sizeof(gpd::TileFlags) * (size_t)b->ntiles,
+                                      b->stream) == cudaSuccess
+                  ? GP_OK
+                  : GP_ECUDA;
       if (r == GP_OK) r = batch_step_once(b, 0, nullptr);
       b->redir_in = nullptr;
       b->redir_out = nullptr;
