@@ -475,14 +475,16 @@ __global__ void __launch_bounds__(AB) ka_rev_update_list(const Consts<double> *_
 
 /* ---- hand-derived reverse of the concentration update ---------------------
  * For two phases and one component (the adjoint's scope) the transposed
- * local Jacobian of update_cell is written out instead of evaluated by dual
- * passes: one thread per (listed cell, part), part 0 the cell's own terms (the
- * phi commit, its mu, the dh/dphi * delta-phi coupling and the dc/dmu
- * inversion), parts 1-4 one face each (x+, x-, y+, y-: the diffusion flux and
- * the anti-trapping current through it).  Every derivative is that of the
- * expressions update_cell evaluates, on the branch the step took (bulk or
- * interface cell, current evaluated or not); only the rounding of the
- * derivative arithmetic differs from the dual passes. */
+ * local Jacobian of update_cell written out, beside its evaluation by dual
+ * passes (the default, which is faster: thirty threads per listed cell hide
+ * latency better than five); the two cross-check each other.  Five parts per
+ * listed cell: part 0 the cell's own terms (the phi commit, its mu, the
+ * dh/dphi * delta-phi coupling and the dc/dmu inversion), parts 1-4 one face
+ * each (x+, x-, y+, y-: the diffusion flux and the anti-trapping current
+ * through it).  Every derivative is that of the expressions update_cell
+ * evaluates, on the branch the step took (bulk or interface cell, current
+ * evaluated or not); only the rounding of the derivative arithmetic differs
+ * from the dual passes. */
 
 /* d(v / h)/dv in the step's arithmetic for spacing h (mul: v * (1/h)) */
 __device__ __forceinline__ double rdx(const Consts<double> *c) { return c->mul_dx ? c->inv_dx : 1.0 / c->dx; }
@@ -928,7 +930,7 @@ struct AdjKernels {
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     return 16 * nsm;
   }
-  /* dual: the listed cells by dual passes instead of the hand-derived reverse */
+  /* DUAL: the listed cells by dual passes, else by the hand-derived reverse */
   template <bool DUAL>
   static cudaError_t rev_update(cudaStream_t s, const void *c, AdjParams p, Grid g, const double *st,
                                 const double *dp, const double *ybar, double *xbar, double *dpbar, double *pbar,
@@ -957,9 +959,10 @@ struct AdjKernels {
 
 bool gp_adjoint_launch(int N, int K, bool aniso, gpd::AdjLaunch *out) {
   if (N != 2 || K != 1) return false;
-  /* GP_ADJOINT_DUAL_UPDATE: the concentration pass by dual passes (the
-   * hand-derived reverse's cross-check) */
-  const bool dual = getenv("GP_ADJOINT_DUAL_UPDATE") != nullptr;
+  /* the concentration pass by dual passes; GP_ADJOINT_HAND_UPDATE: by the
+   * hand-derived reverse (the two cross-check each other; the dual passes,
+   * thirty threads per listed cell, hide latency better and are faster) */
+  const bool dual = getenv("GP_ADJOINT_HAND_UPDATE") == nullptr;
   if (aniso) {
     out->dphi = gpd::AdjKernels<2, 1, true>::dphi;
     out->dphi_sparse = gpd::AdjKernels<2, 1, true>::dphi_sparse;

@@ -161,8 +161,8 @@ def test_adjoint_matches_the_fp64_tape(tmp_path, name):
 
 @pytest.mark.parametrize("name", sorted(CASES) + ["well_aniso"])
 def test_hand_reverse_matches_dual_passes(tmp_path, name, monkeypatch):
-    """The concentration pass's hand-derived reverse against the dual-number
-    passes it replaces (GP_ADJOINT_DUAL_UPDATE): the same derivatives, up to
+    """The concentration pass's hand-derived reverse (GP_ADJOINT_HAND_UPDATE)
+    against its dual-number passes (the default): the same derivatives, up to
     the rounding of the derivative arithmetic and the order of the atomic
     sums."""
     if name == "well_aniso":
@@ -179,9 +179,9 @@ def test_hand_reverse_matches_dual_passes(tmp_path, name, monkeypatch):
     res = []
     for dual in (False, True):
         if dual:
-            monkeypatch.setenv("GP_ADJOINT_DUAL_UPDATE", "1")
+            monkeypatch.delenv("GP_ADJOINT_HAND_UPDATE", raising=False)
         else:
-            monkeypatch.delenv("GP_ADJOINT_DUAL_UPDATE", raising=False)
+            monkeypatch.setenv("GP_ADJOINT_HAND_UPDATE", "1")
         with gp.Simulation(p, phi, mu) as s:
             res.append(s.adjoint(nsteps, target_phi=target))
     h, d = res
@@ -250,6 +250,32 @@ def test_adjoint_schedule_does_not_change_the_gradient(tmp_path, kw):
     assert r["recomputed"] == binomial_cost(nsteps, snaps) - (nsteps - 1)
     np.testing.assert_allclose(r["phi0_bar"], ref["phi0_bar"], rtol=1e-10, atol=1e-12)
     np.testing.assert_allclose(r["mu0_bar"], ref["mu0_bar"], rtol=1e-10, atol=1e-12)
+    for n in PARAMS:
+        assert r["d_" + n] == pytest.approx(ref["d_" + n], rel=1e-10, abs=1e-14)
+
+
+def test_adjoint_tape_does_not_read_stale_memory(tmp_path):
+    """Whole-tape mode steps from slot to slot; the slots' memory may hold an
+    earlier adjoint's states (here: of another start state of the same size).
+    The gradients and the final state equal those of a schedule that steps in
+    the context's own buffers (3 kept states)."""
+    p, phi0, mu0 = _params(tmp_path, "dendrite_aniso")
+    phi, mu = _start(p, phi0, mu0)
+    nsteps = 40
+    rng = np.random.default_rng(5)
+    pb = rng.standard_normal(phi.shape)
+    other_phi = np.clip(phi[:, ::-1, :].copy(), 0.0, 1.0)   # the seed mirrored: different tiles
+    with gp.Simulation(p, other_phi, mu) as s:
+        s.adjoint(nsteps, phi_bar=pb)
+    with gp.Simulation(p, phi, mu) as s:
+        r = s.adjoint(nsteps, phi_bar=pb)
+        end = s.get()
+    with gp.Simulation(p, phi, mu) as s:
+        ref = s.adjoint(nsteps, phi_bar=pb, snapshots=3)
+        fin = s.get()
+    assert r["snapshots"] == nsteps - 1 and ref["recomputed"] > 0
+    assert np.array_equal(end[0], fin[0]) and np.array_equal(end[1], fin[1])
+    np.testing.assert_allclose(r["phi0_bar"], ref["phi0_bar"], rtol=1e-10, atol=1e-12)
     for n in PARAMS:
         assert r["d_" + n] == pytest.approx(ref["d_" + n], rel=1e-10, abs=1e-14)
 
