@@ -61,8 +61,8 @@ PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one kf_step
 # launch in FP64, from ncu captures of the step at these workloads (the
-# summaries are under profiles/)
-NCU_TRAFFIC = {"cfg2": 116.6e6}
+# summaries are under profiles/; cfg4: an early step, as the timed ones are)
+NCU_TRAFFIC = {"cfg2": 116.6e6, "cfg4": 638.8e6}
 
 # steps run untimed before the warm-up: the launch-shape autotuner times one
 # 100-step chunk per candidate shape (at most five), then the chosen shape's
