@@ -23,6 +23,8 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <condition_variable>
+#include <functional>
 #include <algorithm>
 #include <map>
 #include <mutex>
@@ -636,24 +638,94 @@ struct StagePair {
 static StagePair g_stage[GP_STAGE_MAX_DEVICES];
 static std::mutex g_stage_mutex;
 
-/* Host-side copy of n bytes (or conversion of n elements) split over a few
- * threads when it is large: a single thread moves about 10 GB/s, below what
- * the DMA engines take from pinned memory. */
+/* A few host threads that stay up for the staging copies: a chunk's copy is
+ * split over them and the caller, without a thread start per chunk (a 671 MB
+ * transfer is ~80 chunks).  One job at a time: the staging copies run under
+ * g_stage_mutex. */
+class HostPool {
+ public:
+  static constexpr int MAXW = 7;   /* workers besides the caller */
+  static HostPool &get() {
+    static HostPool pool;
+    return pool;
+  }
+  /* run part(i) for i in [0, n) on the workers and the caller; returns when all are done */
+  void run(int n, const std::function<void(int)> &part) {
+    std::unique_lock<std::mutex> lk(mu_);
+    job_ = &part;
+    njobs_ = n;
+    next_ = 0;
+    finished_ = 0;
+    gen_++;
+    cv_.notify_all();
+    while (true) {
+      if (next_ >= njobs_) break;
+      const int i = next_++;
+      lk.unlock();
+      part(i);
+      lk.lock();
+      finished_++;
+    }
+    done_.wait(lk, [this] { return finished_ == njobs_; });
+    job_ = nullptr;
+  }
+  ~HostPool() {
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      stop_ = true;
+    }
+    cv_.notify_all();
+    for (auto &t : th_) t.join();
+  }
+
+ private:
+  HostPool() {
+    const unsigned hc = std::thread::hardware_concurrency();
+    const int nw = (int)std::min<unsigned>(MAXW, hc > 1 ? hc - 1 : 0);
+    for (int w = 0; w < nw; w++) th_.emplace_back([this] { loop(); });
+  }
+  void loop() {
+    long seen = 0;
+    std::unique_lock<std::mutex> lk(mu_);
+    while (true) {
+      cv_.wait(lk, [&] { return stop_ || (gen_ != seen && job_ && next_ < njobs_); });
+      if (stop_) return;
+      seen = gen_;
+      while (job_ && next_ < njobs_) {
+        const int i = next_++;
+        const std::function<void(int)> *f = job_;
+        lk.unlock();
+        (*f)(i);
+        lk.lock();
+        if (++finished_ == njobs_) done_.notify_all();
+      }
+    }
+  }
+  std::vector<std::thread> th_;
+  std::mutex mu_;
+  std::condition_variable cv_, done_;
+  const std::function<void(int)> *job_ = nullptr;
+  int njobs_ = 0, next_ = 0, finished_ = 0;
+  long gen_ = 0;
+  bool stop_ = false;
+};
+
+/* Host-side copy of n bytes (or conversion of n elements) split over the
+ * pool when it is large: a single thread moves about 10 GB/s, below what the
+ * DMA engines take from pinned memory. */
 template <typename F>
 static void host_parallel(size_t n, size_t grain, F &&part) {
-  const int nt = (int)std::min<size_t>(8, std::max<size_t>(1, n / grain));
+  const int nt = (int)std::min<size_t>(HostPool::MAXW + 1, std::max<size_t>(1, n / grain));
   if (nt == 1) {
     part((size_t)0, n);
     return;
   }
-  std::vector<std::thread> th;
   const size_t per = (n + nt - 1) / nt;
-  for (int i = 1; i < nt; i++) {
-    const size_t lo = std::min(n, i * per), hi = std::min(n, lo + per);
-    th.emplace_back([&part, lo, hi] { part(lo, hi); });
-  }
-  part((size_t)0, std::min(n, per));
-  for (auto &t : th) t.join();
+  const std::function<void(int)> f = [&](int i) {
+    const size_t lo = std::min(n, (size_t)i * per), hi = std::min(n, lo + per);
+    if (lo < hi) part(lo, hi);
+  };
+  HostPool::get().run(nt, f);
 }
 
 /* nf device planes (rows of my elements of es bytes, dpitch bytes apart;
