@@ -307,7 +307,8 @@ typedef struct gp_adj_req {
   long checkpoint_every;       /* > 0 (and snapshots 0): keep nsteps/checkpoint_every states */
   long snapshots;              /* states kept besides the start state (binomial checkpointing);
                                   0 and checkpoint_every 0: as many as half the free device memory
-                                  holds, at most nsteps-1 (every state: nothing is recomputed) */
+                                  holds, at most nsteps-1 (every state: nothing is recomputed, and
+                                  when it fits each step's delta-phi is kept as well) */
   int device;                  /* 1: phi_bar, mu_bar, target_phi and the phi0_bar / mu0_bar of the
                                   result are device pointers on the context's device */
 } gp_adj_req;
