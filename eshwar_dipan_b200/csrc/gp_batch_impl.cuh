@@ -39,9 +39,9 @@ struct BatchLaunch {
                          StatBufs st);
   cudaError_t (*flags)(int ntiles, cudaStream_t s, const SimDesc *sims, const int *tsim, const void *state,
                        TileFlags *flags);
-  cudaError_t (*sdphi)(cudaStream_t s, const void *consts, const void *phi, void *dphi, Grid g);
-  cudaError_t (*supd)(cudaStream_t s, const void *consts, const void *phi, const void *mu, const void *dphi,
-                      void *phin, void *mun, Grid g, const double *tcc);
+  /* one smoothing sweep of a simulation (tcc: its temperature rows, or NULL) */
+  cudaError_t (*smooth)(cudaStream_t s, const void *consts, const void *phi, const void *mu, void *phin,
+                        void *mun, Grid g, const double *tcc);
   /* moving frame: interface position into pos[s] (zeroed by the caller),
    * then the shifted (or copied) state into next */
   cudaError_t (*shift_pos)(int ntiles, cudaStream_t s, const SimDesc *sims, const void *consts, const int *tsim,
@@ -159,16 +159,11 @@ struct BatchKernels {
     kf_flags<R, N><<<ntiles, NT, 0, s>>>(sims, tsim, (const R *)state, fl);
     return cudaGetLastError();
   }
-  static cudaError_t sdphi(cudaStream_t s, const void *consts, const void *phi, void *dphi, Grid g) {
+  static cudaError_t smooth(cudaStream_t s, const void *consts, const void *phi, const void *mu, void *phin,
+                            void *mun, Grid g, const double *tcc) {
     dim3 grid((g.my + 127) / 128, g.mx);
-    k_sdphi<R, N, A><<<grid, 128, 0, s>>>((const Consts<R> *)consts, (const R *)phi, (R *)dphi, g);
-    return cudaGetLastError();
-  }
-  static cudaError_t supd(cudaStream_t s, const void *consts, const void *phi, const void *mu, const void *dphi,
-                          void *phin, void *mun, Grid g, const double *tcc) {
-    dim3 grid((g.my + 127) / 128, g.mx);
-    k_supdate<R, N, K><<<grid, 128, 0, s>>>((const Consts<R> *)consts, (const R *)phi, (const R *)mu,
-                                            (const R *)dphi, (R *)phin, (R *)mun, g, tcc);
+    k_smooth<R, N, K, A><<<grid, 128, 0, s>>>((const Consts<R> *)consts, (const R *)phi, (const R *)mu, (R *)phin,
+                                              (R *)mun, g, tcc);
     return cudaGetLastError();
   }
   static cudaError_t shift_pos(int ntiles, cudaStream_t s, const SimDesc *sims, const void *consts, const int *tsim,
@@ -196,8 +191,7 @@ struct BatchKernels {
     t.step_occupancy = step_occupancy;
     t.general = general;
     t.flags = flags;
-    t.sdphi = sdphi;
-    t.supd = supd;
+    t.smooth = smooth;
     t.trows = trows;
     t.shift_pos = shift_pos;
     t.shift_apply = shift_apply;

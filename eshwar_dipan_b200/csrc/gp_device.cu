@@ -336,7 +336,6 @@ struct gp_batch {
   size_t consts_bytes;
   int *d_tsim, *d_seg0, *d_segn;
   void *state[2];               /* ping-pong: every simulation's N phi then K mu planes */
-  void *dphi;                   /* delta-phi planes of the smoothing sweeps */
   gpd::TileFlags *flags[2];     /* per tile and state buffer: one-hot phase of the tile and its edge bands */
   int *glist;                   /* interface tiles of the current step */
   int4 *blist;                  /* bulk tiles of the current step (entries written by kf_classify) */
@@ -959,7 +958,6 @@ void gp_batch_destroy(gp_batch *b) {
   for (int p = 0; p < 2; p++) cudaFree(b->state[p]);
   for (int i = 0; i < 4; i++)
     if (b->ev[i]) cudaEventDestroy(b->ev[i]);
-  cudaFree(b->dphi);
   cudaFree(b->flags[0]);   /* flags[1] is part of the same allocation */
   cudaFree(b->glist);
   cudaFree(b->blist);
@@ -1028,7 +1026,7 @@ int gp_batch_create(gp_batch **out, int nsims, const gp_params *params, const do
   }
   /* layout: every simulation's N+K planes back to back, pitch a multiple of 32 */
   const int N = b->N, K = b->K, ne = 2 * (N + K), ns = 2 * N + 2 * K + 1;
-  long long off = 0, offd = 0;
+  long long off = 0;
   int nt = 0, offT = 0;
   std::vector<int> tsim, seg0, segn;
   std::vector<char> consts;
@@ -1041,7 +1039,6 @@ int gp_batch_create(gp_batch **out, int nsims, const gp_params *params, const do
     memset(&sd, 0, sizeof sd);
     sd.g = make_grid(d, 32);
     sd.off_state = off;
-    sd.off_dphi = offd;
     sd.tiles_x = (sd.g.my + gpd::TY - 1) / gpd::TY;
     const int tiles_y = (sd.g.mx + gpd::TX - 1) / gpd::TX;
     sd.tile0 = nt;
@@ -1052,7 +1049,6 @@ int gp_batch_create(gp_batch **out, int nsims, const gp_params *params, const do
     for (int t = 0; t < sd.tiles_x * tiles_y; t++) tsim.push_back(s);
     nt += sd.tiles_x * tiles_y;
     off += (long long)(N + K) * sd.g.plane;
-    offd += (long long)N * sd.g.dplane;
     b->desc.push_back(sd);
     if (b->elem == 8) {
       gpd::Consts<double> c = make_consts<double>(d);
@@ -1149,7 +1145,6 @@ int gp_batch_create(gp_batch **out, int nsims, const gp_params *params, const do
   } while (0)
   BALLOC(b->state[0], (size_t)off * b->elem);
   BALLOC(b->state[1], (size_t)off * b->elem);
-  BALLOC(b->dphi, (size_t)offd * b->elem);
   BALLOC(b->flags[0], 2 * sizeof(gpd::TileFlags) * (size_t)nt);
   b->flags[1] = b->flags[0] + nt;
   BALLOC(b->glist, sizeof(int) * (size_t)nt);
@@ -1199,8 +1194,7 @@ int gp_batch_create(gp_batch **out, int nsims, const gp_params *params, const do
   BUP(b->ext, ext.data(), sizeof(long long) * ext.size());
   BUP(b->tmaps, tm.data(), sizeof(gpd::TensorMapSlot) * tm.size());
 #undef BUP
-  if (cudaMemsetAsync(b->dphi, 0, (size_t)offd * b->elem, b->stream) != cudaSuccess ||
-      cudaMemsetAsync(b->dyn, 0, sizeof(gpd::SimDyn) * (size_t)nsims, b->stream) != cudaSuccess ||
+  if (cudaMemsetAsync(b->dyn, 0, sizeof(gpd::SimDyn) * (size_t)nsims, b->stream) != cudaSuccess ||
       cudaMemsetAsync(b->counters, 0, gpd::CTR_COUNT * sizeof(int), b->stream) != cudaSuccess) {
     rc = bfail(b, GP_ECUDA, "gp_batch_create: memset failed");
     gp_batch_destroy(b);
@@ -1232,11 +1226,9 @@ int gp_batch_smooth(gp_batch *b, long nsteps) {
       const char *cs = (const char *)b->d_consts + csz * s;
       const char *st = (const char *)b->state[b->cur] + (size_t)sd.off_state * b->elem;
       char *nx = (char *)b->state[b->cur ^ 1] + (size_t)sd.off_state * b->elem;
-      char *dp = (char *)b->dphi + (size_t)sd.off_dphi * b->elem;
       const size_t mu_off = (size_t)b->N * sd.g.plane * b->elem;
-      BK(b->L.sdphi(b->stream, cs, st, dp, sd.g));
       const double *tcc = b->derived[s].tgrad ? b->trows + sd.off_T + (sd.g.my + 6) : nullptr;
-      BK(b->L.supd(b->stream, cs, st, st + mu_off, dp, nx, nx + mu_off, sd.g, tcc));
+      BK(b->L.smooth(b->stream, cs, st, st + mu_off, nx, nx + mu_off, sd.g, tcc));
     }
     b->cur ^= 1;
   }

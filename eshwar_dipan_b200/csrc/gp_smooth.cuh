@@ -19,12 +19,10 @@ __device__ __forceinline__ R ld_field(const R *__restrict__ f, const Consts<R> &
 }
 
 /* calculate_divergence_phasefield_smooth_2D (calculate_divergence_phasefield.h:63-158)
- * for the interior; result into the delta-phi buffer. */
+ * at interior cell (x, y): its delta-phi into d. */
 template <typename R, int N, bool ANISO>
-__global__ void k_sdphi(const Consts<R> *__restrict__ Dp, const R *__restrict__ phi, R *__restrict__ dphi, Grid g) {
-  const Consts<R> &D = *Dp;
-  const int y = blockIdx.x * blockDim.x + threadIdx.x, x = blockIdx.y;
-  if (y >= g.my) return;
+__device__ __forceinline__ void sdphi_cell(const Consts<R> &D, const R *__restrict__ phi, const Grid &g, int x, int y,
+                                           R (&d)[N]) {
   R S[N][3][3];
 #pragma unroll
   for (int a = 0; a < N; a++)
@@ -32,7 +30,7 @@ __global__ void k_sdphi(const Consts<R> *__restrict__ Dp, const R *__restrict__ 
     for (int u = 0; u < 3; u++)
 #pragma unroll
       for (int v = 0; v < 3; v++) S[a][u][v] = ld_field(phi, D, g, 0, a, x - 1 + u, y - 1 + v);
-  R ph[N], dv[N], gcx[N], gcy[N], d[N], lam[N];
+  R ph[N], dv[N], gcx[N], gcy[N], lam[N];
   bool act[N];
 #pragma unroll
   for (int a = 0; a < N; a++) {
@@ -84,19 +82,15 @@ __global__ void k_sdphi(const Consts<R> *__restrict__ Dp, const R *__restrict__ 
 #pragma unroll
   for (int a = 0; a < N; a++) d[a] = act[a] ? D.dt * (lam[a] - sl) / (tau * D.eps) : R(0.0);
   project_nw<R, N>(ph, act, d);
-  const long long o = (long long)(x + 1) * g.dpitch + (y + 1);
-#pragma unroll
-  for (int a = 0; a < N; a++) dphi[a * g.dplane + o] = d[a];
 }
 
-/* calculate_divergence_concentration_smooth_2D (calculate_divergence_concentration.h:154-253) */
+/* calculate_divergence_concentration_smooth_2D (calculate_divergence_concentration.h:154-253)
+ * at interior cell (x, y), given the cell's delta-phi of the sweep (the pass
+ * reads no other cell's) */
 template <typename R, int N, int K>
-__global__ void k_supdate(const Consts<R> *__restrict__ Dp, const R *__restrict__ phi, const R *__restrict__ mu,
-                          const R *__restrict__ dphi, R *__restrict__ phin, R *__restrict__ mun, Grid g,
-                          const double *__restrict__ tcc) {
-  const Consts<R> &D = *Dp;
-  const int y = blockIdx.x * blockDim.x + threadIdx.x, x = blockIdx.y;
-  if (y >= g.my) return;
+__device__ __forceinline__ void supd_cell(const Consts<R> &D, const R *__restrict__ phi, const R *__restrict__ mu,
+                                          const R (&dph)[N], R *__restrict__ phin, R *__restrict__ mun,
+                                          const Grid &g, const double *__restrict__ tcc, int x, int y) {
   /* cells: 0 centre, 1 front (x+1), 2 back (x-1), 3 right (y+1), 4 left (y-1) */
   const int cx[5] = {x, x + 1, x - 1, x, x}, cy[5] = {y, y, y, y + 1, y - 1};
   R P[5][N], M[5][K], Dv[5][K][K];
@@ -162,11 +156,26 @@ __global__ void k_supdate(const Consts<R> *__restrict__ Dp, const R *__restrict_
       nm[k] = (R)(s + (double)m[k]);
     }
   }
-  const long long o = (long long)x * g.pitch + y, od = (long long)(x + 1) * g.dpitch + (y + 1);
+  const long long o = (long long)x * g.pitch + y;
 #pragma unroll
-  for (int a = 0; a < N; a++) phin[a * g.plane + o] = ph[a] + dphi[a * g.dplane + od];
+  for (int a = 0; a < N; a++) phin[a * g.plane + o] = ph[a] + dph[a];
 #pragma unroll
   for (int k = 0; k < K; k++) mun[k * g.plane + o] = nm[k];
+}
+
+/* One smoothing sweep (smooth(), solverloop.h:72-90), one thread per interior
+ * cell: the phase-field pass's delta-phi of the cell, then the concentration
+ * pass's update, which reads the delta-phi of no other cell (the two passes
+ * in one launch, without a delta-phi buffer between them). */
+template <typename R, int N, int K, bool ANISO>
+__global__ void k_smooth(const Consts<R> *__restrict__ Dp, const R *__restrict__ phi, const R *__restrict__ mu,
+                         R *__restrict__ phin, R *__restrict__ mun, Grid g, const double *__restrict__ tcc) {
+  const Consts<R> &D = *Dp;
+  const int y = blockIdx.x * blockDim.x + threadIdx.x, x = blockIdx.y;
+  if (y >= g.my) return;
+  R d[N];
+  sdphi_cell<R, N, ANISO>(D, phi, g, x, y, d);
+  supd_cell<R, N, K>(D, phi, mu, d, phin, mun, g, tcc, x, y);
 }
 
 }  // namespace gpd

@@ -978,7 +978,6 @@ __device__ __forceinline__ void update_tile(const Consts<R> &D, const Grid &g, c
 struct SimDesc {
   Grid g;
   long long off_state;   /* N phi planes then K mu planes */
-  long long off_dphi;    /* N delta-phi planes (smoothing sweeps) */
   int tiles_x, tile0;    /* tiles per row, first tile */
   int off_T;             /* non-isothermal: the step's temperature rows (two of MESH_Y+6) in StatBufs::trows */
 };
