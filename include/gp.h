@@ -273,8 +273,10 @@ void gp_batch_destroy(gp_batch *b);
  * in a fixed 32 MiB array inside the library that every GPU which loads the
  * library keeps until exit; grids needing more (about 1.3 million cells with
  * 3 phases) are rejected with GP_EINVAL and a message.  The first call on a
- * device looks up that array's device address (cudaGetSymbolAddress); make
- * that first call before any stream capture.  All calls share the array, so
+ * device looks up that array's device address (cudaGetSymbolAddress).  No
+ * call may be recorded by stream capture: each one copies the step's constant
+ * block from host (pageable) memory into the library's __constant__ block,
+ * which a captured graph could not replay.  All calls share the array, so
  * calls that overlap on the GPU (other streams, other host threads) race; the
  * same holds for the constant block its kernels read.  The call is
  * asynchronous on `stream`; no progress record is produced.  Results are those
