@@ -775,14 +775,17 @@ def run_adjoint(args, rank, world, local, dist):
                "data": "synthetic (one seed at the centre)",
                "config": {"workload": "cfg5: " + desc, "grid": [p.mesh_x, p.mesh_y], "phases": 2, "components": 1,
                           "loss": "1/2 sum (phi_T - target)^2, target from Tau, dab, epsilon, GAMMA x 1.05",
-                          "checkpoints": "every ceil(sqrt(steps)) steps", "parallelism": "single"},
+                          "states_kept": g["snapshots"], "steps_recomputed": g["recomputed"],
+                          "parallelism": "single"},
                "adjoint": {"loss": g["loss"], "d_tau": g["d_tau"], "d_mobility": -g["d_tau"] * p.tau_ab[0][1] ** 2,
                            "d_dab": g["d_dab"], "d_epsilon": g["d_epsilon"], "d_gamma": g["d_gamma"],
                            "max_abs_dphi0": float(np.abs(g["phi0_bar"]).max()),
                            "ms_forward_pass": g["ms_forward"], "ms_reverse_pass": g["ms_reverse"],
                            "ms_plain_forward": fwd_ms, "cost_vs_forward": adj_ms / fwd_ms},
-               "gpu_launches": (2 * nsteps + 2 * (nsteps - int(np.ceil(nsteps / np.ceil(np.sqrt(nsteps)))))
-                                + 5 * nsteps),
+               # forward: kf_classify + kf_step per step, recomputed steps too; reverse: four
+               # kernels per step, and two more per step whose delta-phi is not on the tape
+               "gpu_launches": 2 * (nsteps + g["recomputed"]) + 4 * nsteps
+                               + (2 * nsteps if g["snapshots"] < nsteps - 1 else 0),
                "clocks": nv.summary(),
                "note": "value = cell-updates of the differentiated steps per second of forward + reverse"}
         print(json.dumps(out), flush=True)

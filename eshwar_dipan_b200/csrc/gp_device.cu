@@ -351,10 +351,14 @@ struct gp_batch {
   double *dphi_out = nullptr;   /* the adjoint's forward steps: where the interface tiles write delta-phi */
   /* the adjoint's forward steps over its tape (a batch of one): the step reads
    * redir_in (bulk boxes through redir_map) and writes redir_out instead of
-   * the ping-pong buffers; the flags still follow the parity */
+   * the ping-pong buffers; the flags still follow the parity.  redir_have
+   * stands in for the output buffer's flags in the classification: "unknown"
+   * for every tile, since redir_out holds nothing the flags describe (the
+   * bulk tiles then write their phi too) */
   const void *redir_in = nullptr;
   void *redir_out = nullptr;
   const gpd::TensorMapSlot *redir_map = nullptr;
+  const gpd::TileFlags *redir_have = nullptr;
   double *partials, *sums_sim;
   /* captured step sequences: graphs[(starting parity, steps)], steps <= GP_GRAPH_STEPS */
   std::map<std::pair<int, long>, cudaGraphExec_t> graphs;
@@ -403,8 +407,8 @@ static int batch_step_once(gp_batch *b, int want_sums, cudaEvent_t *ev) {
   const int tbuf = b->redir_in ? 0 : in;
   if (ev) BK(cudaEventRecord(ev[0], b->stream));
   if (b->tgrad) BK(b->L.trows(b->nsims, b->stream, b->d_desc, b->d_consts, b->counters, b->dyn, b->trows));
-  BK(b->L.classify(b->ntiles, b->stream, b->d_desc, b->d_consts, b->d_tsim, b->flags[in], b->flags[out], b->glist,
-                   b->blist, b->counters));
+  BK(b->L.classify(b->ntiles, b->stream, b->d_desc, b->d_consts, b->d_tsim, b->flags[in],
+                   b->redir_in ? b->redir_have : b->flags[out], b->glist, b->blist, b->counters));
   if (!want_sums && b->grid_s > 0 && b->shape.fused && (!ev || ev[3] == nullptr)) {
     /* one launch for both kinds of tile; ev (with ev[3] null): events after
      * the classification and after the step */
@@ -1560,6 +1564,30 @@ int planes_copy(gp_batch *b, double *dst, size_t dpitch, const double *src, size
   return GP_OK;
 }
 
+/* Whatever enqueue() puts on the batch's stream, captured as one CUDA graph
+ * and launched once (the executable graph is freed when that launch
+ * completes): long runs of short launches whose arguments change from one
+ * launch to the next, with the launch gaps of a graph. */
+template <typename F>
+static int run_captured(gp_batch *b, F &&enqueue) {
+  cudaGraph_t gr = nullptr;
+  BK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+  const int rc = enqueue();
+  const cudaError_t ec = cudaStreamEndCapture(b->stream, &gr);
+  if (rc != GP_OK || ec != cudaSuccess) {
+    if (gr) cudaGraphDestroy(gr);
+    return rc != GP_OK ? rc : bfail(b, GP_ECUDA, "graph capture: %s", cudaGetErrorString(ec));
+  }
+  cudaGraphExec_t ge;
+  cudaError_t ei = cudaGraphInstantiate(&ge, gr, 0);
+  cudaGraphDestroy(gr);
+  if (ei != cudaSuccess) return bfail(b, GP_ECUDA, "graph instantiate: %s", cudaGetErrorString(ei));
+  ei = cudaGraphLaunch(ge, b->stream);
+  cudaGraphExecDestroy(ge);
+  if (ei != cudaSuccess) return bfail(b, GP_ECUDA, "graph launch: %s", cudaGetErrorString(ei));
+  return GP_OK;
+}
+
 struct AdjBufs {
   double *snap = nullptr, *seg = nullptr, *ybar = nullptr, *xbar = nullptr, *dphi = nullptr, *dphibar = nullptr,
          *pbar = nullptr, *final_state = nullptr;
@@ -1568,9 +1596,10 @@ struct AdjBufs {
   gpd::TensorMapSlot *smaps = nullptr;   /* whole-tape mode: the tensor map of each slot's mu planes */
   int2 *cells = nullptr;    /* cells of a reverse pass that take the dual passes */
   int *ncells = nullptr;
+  gpd::TileFlags *unknown = nullptr;   /* whole-tape mode: "unknown" flags of every tile (redir_have) */
   ~AdjBufs() {   /* ybar, xbar and dphibar point into rblk */
     cudaFree(snap); cudaFree(seg); cudaFree(dphi); cudaFree(pbar); cudaFree(final_state); cudaFree(rblk);
-    cudaFree(dtape); cudaFree(smaps); cudaFree(cells); cudaFree(ncells);
+    cudaFree(dtape); cudaFree(smaps); cudaFree(cells); cudaFree(ncells); cudaFree(unknown);
   }
 };
 
@@ -1674,9 +1703,14 @@ int gp_adjoint(gp_ctx *c, const gp_adj_req *req, gp_adj_out *out) {
     std::vector<gpd::TensorMapSlot> hm((size_t)T);
     for (long t = 0; t < T; t++)
       if ((rc = encode_mu_map(b, 0, m.snap + S * (size_t)t, &hm[(size_t)t])) != GP_OK) return fail(c, rc, "%s", b->err);
-    if (cudaMalloc((void **)&m.smaps, sizeof(gpd::TensorMapSlot) * (size_t)T) != cudaSuccess)
+    if (cudaMalloc((void **)&m.smaps, sizeof(gpd::TensorMapSlot) * (size_t)T) != cudaSuccess ||
+        cudaMalloc((void **)&m.unknown, sizeof(gpd::TileFlags) * (size_t)b->ntiles) != cudaSuccess)
       return fail(c, GP_ENOMEM, "gp_adjoint: cudaMalloc of the slot maps failed");
     CK(cudaMemcpyAsync(m.smaps, hm.data(), sizeof(gpd::TensorMapSlot) * (size_t)T, cudaMemcpyHostToDevice, b->stream));
+    CK(cudaMemsetAsync(m.unknown, 0xfe, sizeof(gpd::TileFlags) * (size_t)b->ntiles, b->stream));
+    /* the interface tiles write the delta-phi of their cells and rings; every
+     * other cell of every step keeps this +0.0 */
+    CK(cudaMemsetAsync(m.dtape, 0, Sd * (size_t)T * 8, b->stream));
     CK(cudaStreamSynchronize(b->stream));
   }
   int rcur = 0;   /* the block holding the adjoint of the state after the step being reversed */
@@ -1803,30 +1837,42 @@ int gp_adjoint(gp_ctx *c, const gp_adj_req *req, gp_adj_out *out) {
     /* the whole tape: step t reads slot t and writes slot t+1 (the last one
      * the final state) directly, its bulk boxes through the slot's tensor map,
      * and leaves its delta-phi on the tape; then every step is reversed from
-     * its slot, last first */
-    for (long t = 0; t < T; t++) {
-      b->redir_in = slot_ptr((int)t);
-      b->redir_out = t + 1 < T ? slot_ptr((int)t + 1) : m.final_state;
-      b->redir_map = m.smaps + t;
-      b->dphi_out = m.dtape + Sd * (size_t)t;
-      /* the slot written holds nothing the output flags describe: "unknown"
-       * makes the bulk tiles write their phi too */
-      int r = cudaMemsetAsync(b->dphi_out, 0, Sd * 8, b->stream) == cudaSuccess &&
-                      cudaMemsetAsync(b->flags[b->cur ^ 1], 0xfe, sizeof(gpd::TileFlags) * (size_t)b->ntiles,
-                                      b->stream) == cudaSuccess
-                  ? GP_OK
-                  : GP_ECUDA;
-      if (r == GP_OK) r = batch_step_once(b, 0, nullptr);
-      b->redir_in = nullptr;
-      b->redir_out = nullptr;
-      b->redir_map = nullptr;
-      b->dphi_out = nullptr;
-      if (r != GP_OK) return r == GP_ECUDA && !c->err[0] ? fail(c, GP_ECUDA, "gp_adjoint: memset failed") : r;
-      have_dphi[(size_t)t] = 1;
+     * its slot, last first.  Both sweeps go to the GPU as graphs of
+     * GP_GRAPH_STEPS steps, captured once each. */
+    for (long t0 = 0; t0 < T; t0 += GP_GRAPH_STEPS) {
+      const long t1 = std::min<long>(T, t0 + GP_GRAPH_STEPS);
+      rc = run_captured(b, [&]() -> int {
+        for (long t = t0; t < t1; t++) {
+          b->redir_in = slot_ptr((int)t);
+          b->redir_out = t + 1 < T ? slot_ptr((int)t + 1) : m.final_state;
+          b->redir_map = m.smaps + t;
+          b->redir_have = m.unknown;
+          b->dphi_out = m.dtape + Sd * (size_t)t;
+          const int r = batch_step_once(b, 0, nullptr);
+          b->redir_in = nullptr;
+          b->redir_out = nullptr;
+          b->redir_map = nullptr;
+          b->redir_have = nullptr;
+          b->dphi_out = nullptr;
+          if (r != GP_OK) return r;
+        }
+        return GP_OK;
+      });
+      if (rc != GP_OK) return rc;
+      for (long t = t0; t < t1; t++) have_dphi[(size_t)t] = 1;
     }
     if ((rc = seed()) != GP_OK) return rc;
-    for (long t = T - 1; t >= 0; t--)
-      if ((rc = reverse(t, slot_ptr((int)t))) != GP_OK) return rc;
+    for (long t1 = T; t1 > 0; t1 -= GP_GRAPH_STEPS) {
+      const long t0 = std::max<long>(0, t1 - GP_GRAPH_STEPS);
+      rc = run_captured(b, [&]() -> int {
+        for (long t = t1 - 1; t >= t0; t--) {
+          const int r = reverse(t, slot_ptr((int)t));
+          if (r != GP_OK) return r;
+        }
+        return GP_OK;
+      });
+      if (rc != GP_OK) return rc;
+    }
   }
   while (!m.dtape && !stack.empty()) {
     const Task t = stack.back();
