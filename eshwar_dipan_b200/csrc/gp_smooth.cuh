@@ -168,7 +168,7 @@ __device__ __forceinline__ void supd_cell(const Consts<R> &D, const R *__restric
  * pass's update, which reads the delta-phi of no other cell (the two passes
  * in one launch, without a delta-phi buffer between them). */
 template <typename R, int N, int K, bool ANISO>
-__global__ void k_smooth(const Consts<R> *__restrict__ Dp, const R *__restrict__ phi, const R *__restrict__ mu,
+__global__ void __launch_bounds__(128, N <= 3 ? 4 : 3) k_smooth(const Consts<R> *__restrict__ Dp, const R *__restrict__ phi, const R *__restrict__ mu,
                          R *__restrict__ phin, R *__restrict__ mun, Grid g, const double *__restrict__ tcc) {
   const Consts<R> &D = *Dp;
   const int y = blockIdx.x * blockDim.x + threadIdx.x, x = blockIdx.y;
