@@ -926,9 +926,17 @@ struct AdjKernels {
   }
   /* the list passes: a persistent grid over the listed cells */
   static int list_grid() {
-    int dev = 0, nsm = 148;
-    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    return 16 * nsm;
+    /* SM count per device, looked up once (every reverse step asks; a
+     * repeated lookup writes the same value) */
+    static int nsm_of[64];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 16 * 148;
+    if (!nsm_of[dev]) {
+      int nsm = 148;
+      cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+      nsm_of[dev] = nsm;
+    }
+    return 16 * nsm_of[dev];
   }
   /* DUAL: the listed cells by dual passes, else by the hand-derived reverse */
   template <bool DUAL>

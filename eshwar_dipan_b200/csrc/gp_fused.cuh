@@ -1534,7 +1534,7 @@ __device__ __forceinline__ void bulk_release_warp(unsigned char *smraw) {
 }
 
 template <typename R, int N, int K, bool SUMS, bool MUL, bool DIAG>
-__global__ void __launch_bounds__(NT, 2) kf_bulk(const SimDesc *__restrict__ sims, const Consts<R> *__restrict__ consts,
+__global__ void __launch_bounds__(NT, sizeof(R) == 4 && K == 1 ? 3 : 2) kf_bulk(const SimDesc *__restrict__ sims, const Consts<R> *__restrict__ consts,
                                                  const int *__restrict__ tsim, const int4 *__restrict__ blist,
                                                  const TensorMapSlot *__restrict__ tmaps, int buf,
                                                  const R *__restrict__ state, R *__restrict__ next,
