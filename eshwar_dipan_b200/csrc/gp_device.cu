@@ -1564,12 +1564,12 @@ int planes_copy(gp_batch *b, double *dst, size_t dpitch, const double *src, size
   return GP_OK;
 }
 
-/* Whatever enqueue() puts on the batch's stream, captured as one CUDA graph
- * and launched once (the executable graph is freed when that launch
- * completes): long runs of short launches whose arguments change from one
- * launch to the next, with the launch gaps of a graph. */
+/* Whatever enqueue() puts on the batch's stream, captured as one executable
+ * CUDA graph (nothing runs): long runs of short launches whose arguments
+ * change from one launch to the next get the launch gaps of a graph. */
 template <typename F>
-static int run_captured(gp_batch *b, F &&enqueue) {
+static int capture_graph(gp_batch *b, F &&enqueue, cudaGraphExec_t *out) {
+  *out = nullptr;
   cudaGraph_t gr = nullptr;
   BK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
   const int rc = enqueue();
@@ -1578,13 +1578,22 @@ static int run_captured(gp_batch *b, F &&enqueue) {
     if (gr) cudaGraphDestroy(gr);
     return rc != GP_OK ? rc : bfail(b, GP_ECUDA, "graph capture: %s", cudaGetErrorString(ec));
   }
-  cudaGraphExec_t ge;
-  cudaError_t ei = cudaGraphInstantiate(&ge, gr, 0);
+  const cudaError_t ei = cudaGraphInstantiate(out, gr, 0);
   cudaGraphDestroy(gr);
-  if (ei != cudaSuccess) return bfail(b, GP_ECUDA, "graph instantiate: %s", cudaGetErrorString(ei));
-  ei = cudaGraphLaunch(ge, b->stream);
-  cudaGraphExecDestroy(ge);
-  if (ei != cudaSuccess) return bfail(b, GP_ECUDA, "graph launch: %s", cudaGetErrorString(ei));
+  if (ei != cudaSuccess) {
+    *out = nullptr;
+    return bfail(b, GP_ECUDA, "graph instantiate: %s", cudaGetErrorString(ei));
+  }
+  return GP_OK;
+}
+
+/* Launch an executable graph once; *ge is freed when that launch completes
+ * and set to NULL. */
+static int launch_once(gp_batch *b, cudaGraphExec_t *ge) {
+  const cudaError_t e = cudaGraphLaunch(*ge, b->stream);
+  cudaGraphExecDestroy(*ge);
+  *ge = nullptr;
+  if (e != cudaSuccess) return bfail(b, GP_ECUDA, "graph launch: %s", cudaGetErrorString(e));
   return GP_OK;
 }
 
@@ -1597,7 +1606,10 @@ struct AdjBufs {
   int2 *cells = nullptr;    /* cells of a reverse pass that take the dual passes */
   int *ncells = nullptr;
   gpd::TileFlags *unknown = nullptr;   /* whole-tape mode: "unknown" flags of every tile (redir_have) */
+  cudaGraphExec_t first[2] = {nullptr, nullptr};   /* whole-tape mode: the first graph of each sweep */
   ~AdjBufs() {   /* ybar, xbar and dphibar point into rblk */
+    for (cudaGraphExec_t ge : first)
+      if (ge) cudaGraphExecDestroy(ge);
     cudaFree(snap); cudaFree(seg); cudaFree(dphi); cudaFree(pbar); cudaFree(final_state); cudaFree(rblk);
     cudaFree(dtape); cudaFree(smaps); cudaFree(cells); cudaFree(ncells); cudaFree(unknown);
   }
@@ -1728,9 +1740,6 @@ int gp_adjoint(gp_ctx *c, const gp_adj_req *req, gp_adj_out *out) {
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
   CK(cudaEventCreate(&e2));
-  CK(cudaEventRecord(e0, b->stream));
-  CK(cudaMemcpyAsync(m.snap, b->state[b->cur], S * 8, cudaMemcpyDeviceToDevice, b->stream));
-  CK(cudaMemsetAsync(m.pbar, 0, gpd::ADJ_NPARAM * 8, b->stream));
   out->loss = 0.0;
 
   /* ---- the steps are reversed by the binomial checkpointing schedule:
@@ -1833,44 +1842,85 @@ int gp_adjoint(gp_ctx *c, const gp_adj_req *req, gp_adj_out *out) {
     }
     return reverse(t, (const double *)b->state[b->cur]);
   };
+  /* whole tape: step t reads slot t and writes slot t+1 (the last one the
+   * final state) directly, its bulk boxes through the slot's tensor map, and
+   * leaves its delta-phi on the tape; then every step is reversed from its
+   * slot, last first.  Both sweeps go to the GPU as graphs of GP_GRAPH_STEPS
+   * steps, each captured once and launched once (the steps' arguments differ
+   * from graph to graph): the host captures a graph while the GPU runs the
+   * one before it, and the first graph of each sweep before the timed
+   * region, as a plain run's graphs are captured before it runs. */
+  auto capture_forward = [&](long t0, cudaGraphExec_t *ge) -> int {
+    const long t1 = std::min<long>(T, t0 + GP_GRAPH_STEPS);
+    return capture_graph(
+        b,
+        [&]() -> int {
+          for (long t = t0; t < t1; t++) {
+            b->redir_in = slot_ptr((int)t);
+            b->redir_out = t + 1 < T ? slot_ptr((int)t + 1) : m.final_state;
+            b->redir_map = m.smaps + t;
+            b->redir_have = m.unknown;
+            b->dphi_out = m.dtape + Sd * (size_t)t;
+            const int r = batch_step_once(b, 0, nullptr);
+            b->redir_in = nullptr;
+            b->redir_out = nullptr;
+            b->redir_map = nullptr;
+            b->redir_have = nullptr;
+            b->dphi_out = nullptr;
+            if (r != GP_OK) return r;
+          }
+          return GP_OK;
+        },
+        ge);
+  };
+  auto capture_reverse = [&](long t1, cudaGraphExec_t *ge) -> int {
+    const long t0 = std::max<long>(0, t1 - GP_GRAPH_STEPS);
+    return capture_graph(
+        b,
+        [&]() -> int {
+          for (long t = t1 - 1; t >= t0; t--) {
+            const int r = reverse(t, slot_ptr((int)t));
+            if (r != GP_OK) return r;
+          }
+          return GP_OK;
+        },
+        ge);
+  };
+  int rcur_seed = rcur, rcur_after = rcur;
+  double *ybar_seed = m.ybar, *ybar_after = m.ybar;
+  const void *start = b->state[b->cur];   /* a capture of steps moves b->cur on */
   if (m.dtape) {
-    /* the whole tape: step t reads slot t and writes slot t+1 (the last one
-     * the final state) directly, its bulk boxes through the slot's tensor map,
-     * and leaves its delta-phi on the tape; then every step is reversed from
-     * its slot, last first.  Both sweeps go to the GPU as graphs of
-     * GP_GRAPH_STEPS steps, captured once each. */
+    /* every step's delta-phi is on the tape by the time the reverse sweep reads it */
+    std::fill(have_dphi.begin(), have_dphi.end(), 1);
+    if ((rc = capture_forward(0, &m.first[0])) != GP_OK || (rc = capture_reverse(T, &m.first[1])) != GP_OK)
+      return rc;
+    /* the seed goes into the block the first reverse graph reads */
+    rcur_after = rcur;
+    ybar_after = m.ybar;
+    rcur = rcur_seed;
+    m.ybar = ybar_seed;
+  }
+  CK(cudaEventRecord(e0, b->stream));
+  CK(cudaMemcpyAsync(m.snap, start, S * 8, cudaMemcpyDeviceToDevice, b->stream));
+  CK(cudaMemsetAsync(m.pbar, 0, gpd::ADJ_NPARAM * 8, b->stream));
+  if (m.dtape) {
     for (long t0 = 0; t0 < T; t0 += GP_GRAPH_STEPS) {
-      const long t1 = std::min<long>(T, t0 + GP_GRAPH_STEPS);
-      rc = run_captured(b, [&]() -> int {
-        for (long t = t0; t < t1; t++) {
-          b->redir_in = slot_ptr((int)t);
-          b->redir_out = t + 1 < T ? slot_ptr((int)t + 1) : m.final_state;
-          b->redir_map = m.smaps + t;
-          b->redir_have = m.unknown;
-          b->dphi_out = m.dtape + Sd * (size_t)t;
-          const int r = batch_step_once(b, 0, nullptr);
-          b->redir_in = nullptr;
-          b->redir_out = nullptr;
-          b->redir_map = nullptr;
-          b->redir_have = nullptr;
-          b->dphi_out = nullptr;
-          if (r != GP_OK) return r;
-        }
-        return GP_OK;
-      });
+      if (t0 == 0) rc = launch_once(b, &m.first[0]);
+      else {
+        cudaGraphExec_t ge;
+        if ((rc = capture_forward(t0, &ge)) == GP_OK) rc = launch_once(b, &ge);
+      }
       if (rc != GP_OK) return rc;
-      for (long t = t0; t < t1; t++) have_dphi[(size_t)t] = 1;
     }
     if ((rc = seed()) != GP_OK) return rc;
+    rcur = rcur_after;
+    m.ybar = ybar_after;
     for (long t1 = T; t1 > 0; t1 -= GP_GRAPH_STEPS) {
-      const long t0 = std::max<long>(0, t1 - GP_GRAPH_STEPS);
-      rc = run_captured(b, [&]() -> int {
-        for (long t = t1 - 1; t >= t0; t--) {
-          const int r = reverse(t, slot_ptr((int)t));
-          if (r != GP_OK) return r;
-        }
-        return GP_OK;
-      });
+      if (t1 == T) rc = launch_once(b, &m.first[1]);
+      else {
+        cudaGraphExec_t ge;
+        if ((rc = capture_reverse(t1, &ge)) == GP_OK) rc = launch_once(b, &ge);
+      }
       if (rc != GP_OK) return rc;
     }
   }

@@ -324,7 +324,9 @@ typedef struct gp_adj_out {
   double *phi0_bar;            /* NULL, or [N][X][Y]: receives dL/dphi of the start state */
   double *mu0_bar;             /* NULL, or [K][X][Y]: receives dL/dmu of the start state */
   double ms_forward;           /* device time of the forward pass */
-  double ms_reverse;           /* device time of the recomputation and reverse sweep */
+  double ms_reverse;           /* device time of the recomputation and reverse sweep (with every
+                                  state kept, both sweeps run as CUDA graphs of 100 steps; the
+                                  first graph of each is captured before these times start) */
   long snapshots;              /* states kept besides the start state */
   long recomputed;             /* forward steps taken again in the reverse sweep */
 } gp_adj_out;
