@@ -11,25 +11,38 @@
 
 namespace gpd {
 
+/* Offsets of the cells (x-1..x+1, y-1..y+1) of interior cell (x, y) in a
+ * field's planes, ghosts through the boundary remap of that field (0 phi,
+ * 1 mu): o(u, v) = row[u] + col[v].  Computed once per cell; 32 bits hold
+ * any offset inside a plane (a plane of 2^32 FP64 cells is 32 GB). */
+struct Nbr3 {
+  unsigned row[3], col[3];
+  __device__ __forceinline__ unsigned o(int u, int v) const { return row[u] + col[v]; }
+};
 template <typename R>
-__device__ __forceinline__ R ld_field(const R *__restrict__ f, const Consts<R> &D, const Grid &g, int field, int a,
-                                      int x, int y) {
-  int sx = remap(x, g.mx, D.bc_x[field][0], D.bc_x[field][1]), sy = remap(y, g.my, D.bc_y[field][0], D.bc_y[field][1]);
-  return __ldg(f + a * g.plane + (long long)sx * g.pitch + sy);
+__device__ __forceinline__ Nbr3 nbr3(const Consts<R> &D, const Grid &g, int field, int x, int y) {
+  Nbr3 n;
+  const int bx0 = D.bc_x[field][0], bx1 = D.bc_x[field][1], by0 = D.bc_y[field][0], by1 = D.bc_y[field][1];
+#pragma unroll
+  for (int u = 0; u < 3; u++) {
+    n.row[u] = (unsigned)remap(x - 1 + u, g.mx, bx0, bx1) * (unsigned)g.pitch;
+    n.col[u] = (unsigned)remap(y - 1 + u, g.my, by0, by1);
+  }
+  return n;
 }
 
 /* calculate_divergence_phasefield_smooth_2D (calculate_divergence_phasefield.h:63-158)
  * at interior cell (x, y): its delta-phi into d. */
 template <typename R, int N, bool ANISO>
-__device__ __forceinline__ void sdphi_cell(const Consts<R> &D, const R *__restrict__ phi, const Grid &g, int x, int y,
-                                           R (&d)[N]) {
+__device__ __forceinline__ void sdphi_cell(const Consts<R> &D, const R *__restrict__ phi, const Grid &g,
+                                           const Nbr3 &np, R (&d)[N]) {
   R S[N][3][3];
 #pragma unroll
   for (int a = 0; a < N; a++)
 #pragma unroll
     for (int u = 0; u < 3; u++)
 #pragma unroll
-      for (int v = 0; v < 3; v++) S[a][u][v] = ld_field(phi, D, g, 0, a, x - 1 + u, y - 1 + v);
+      for (int v = 0; v < 3; v++) S[a][u][v] = __ldg(phi + a * g.plane + np.o(u, v));
   R ph[N], dv[N], gcx[N], gcy[N], lam[N];
   bool act[N];
 #pragma unroll
@@ -90,16 +103,17 @@ __device__ __forceinline__ void sdphi_cell(const Consts<R> &D, const R *__restri
 template <typename R, int N, int K>
 __device__ __forceinline__ void supd_cell(const Consts<R> &D, const R *__restrict__ phi, const R *__restrict__ mu,
                                           const R (&dph)[N], R *__restrict__ phin, R *__restrict__ mun,
-                                          const Grid &g, const double *__restrict__ tcc, int x, int y) {
+                                          const Grid &g, const double *__restrict__ tcc, const Nbr3 &np,
+                                          const Nbr3 &nq, int x, int y) {
   /* cells: 0 centre, 1 front (x+1), 2 back (x-1), 3 right (y+1), 4 left (y-1) */
-  const int cx[5] = {x, x + 1, x - 1, x, x}, cy[5] = {y, y, y, y + 1, y - 1};
+  const int cu[5] = {1, 2, 0, 1, 1}, cv[5] = {1, 1, 1, 2, 0};
   R P[5][N], M[5][K], Dv[5][K][K];
 #pragma unroll
   for (int q = 0; q < 5; q++) {
 #pragma unroll
-    for (int a = 0; a < N; a++) P[q][a] = ld_field(phi, D, g, 0, a, cx[q], cy[q]);
+    for (int a = 0; a < N; a++) P[q][a] = __ldg(phi + a * g.plane + np.o(cu[q], cv[q]));
 #pragma unroll
-    for (int k = 0; k < K; k++) M[q][k] = ld_field(mu, D, g, 1, k, cx[q], cy[q]);
+    for (int k = 0; k < K; k++) M[q][k] = __ldg(mu + k * g.plane + nq.o(cu[q], cv[q]));
 #pragma unroll
     for (int k = 0; k < K; k++)
 #pragma unroll
@@ -173,9 +187,10 @@ __global__ void __launch_bounds__(128, N <= 3 ? 4 : 3) k_smooth(const Consts<R> 
   const Consts<R> &D = *Dp;
   const int y = blockIdx.x * blockDim.x + threadIdx.x, x = blockIdx.y;
   if (y >= g.my) return;
+  const Nbr3 np = nbr3(D, g, 0, x, y), nq = nbr3(D, g, 1, x, y);
   R d[N];
-  sdphi_cell<R, N, ANISO>(D, phi, g, x, y, d);
-  supd_cell<R, N, K>(D, phi, mu, d, phin, mun, g, tcc, x, y);
+  sdphi_cell<R, N, ANISO>(D, phi, g, np, d);
+  supd_cell<R, N, K>(D, phi, mu, d, phin, mun, g, tcc, np, nq, x, y);
 }
 
 }  // namespace gpd
