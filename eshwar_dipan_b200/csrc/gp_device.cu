@@ -1736,10 +1736,16 @@ int gp_adjoint(gp_ctx *c, const gp_adj_req *req, gp_adj_out *out) {
       return fail(c, GP_ENOMEM, "gp_adjoint: cudaMalloc of the cell list failed");
   }
   const long long steps0 = b->steps;
-  cudaEvent_t e0, e1, e2;
-  CK(cudaEventCreate(&e0));
-  CK(cudaEventCreate(&e1));
-  CK(cudaEventCreate(&e2));
+  /* the three timing events, destroyed on every return */
+  struct Events {
+    cudaEvent_t e[3] = {nullptr, nullptr, nullptr};
+    ~Events() {
+      for (cudaEvent_t x : e)
+        if (x) cudaEventDestroy(x);
+    }
+  } ev;
+  for (cudaEvent_t &x : ev.e) CK(cudaEventCreate(&x));
+  cudaEvent_t e0 = ev.e[0], e1 = ev.e[1], e2 = ev.e[2];
   out->loss = 0.0;
 
   /* ---- the steps are reversed by the binomial checkpointing schedule:
@@ -1990,9 +1996,6 @@ int gp_adjoint(gp_ctx *c, const gp_adj_req *req, gp_adj_out *out) {
   CK(cudaEventElapsedTime(&f2, e1, e2));
   out->ms_forward = f1;
   out->ms_reverse = f2;
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
-  cudaEventDestroy(e2);
   return GP_OK;
 }
 
