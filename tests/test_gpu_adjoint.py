@@ -280,6 +280,33 @@ def test_adjoint_tape_does_not_read_stale_memory(tmp_path):
         assert r["d_" + n] == pytest.approx(ref["d_" + n], rel=1e-10, abs=1e-14)
 
 
+@pytest.mark.parametrize("nsteps", [99, 100, 101, 257])
+def test_whole_tape_graph_chunks(tmp_path, nsteps):
+    """The whole tape goes to the GPU in graphs of 100 steps per sweep (the
+    first of each captured before the forward pass, a last one shorter): at
+    lengths around and across the chunk size the gradients, the target loss
+    and the final state equal those of a schedule that launches its steps
+    one by one (a few kept states, steps recomputed)."""
+    p, phi0, mu0 = _params(tmp_path, "dendrite_aniso")
+    phi, mu = _start(p, phi0, mu0)
+    target = _target(p, phi, mu, nsteps)
+    with gp.Simulation(p, phi, mu) as s:
+        r = s.adjoint(nsteps, target_phi=target)
+        end = s.get()
+    with gp.Simulation(p, phi, mu) as s:
+        ref = s.adjoint(nsteps, target_phi=target, snapshots=4)
+    with gp.Simulation(p, phi, mu) as s:
+        s.step(nsteps, stats=False)
+        fin = s.get()
+    assert r["snapshots"] == nsteps - 1 and r["recomputed"] == 0 and ref["recomputed"] > 0
+    assert np.array_equal(end[0], fin[0]) and np.array_equal(end[1], fin[1])
+    assert r["loss"] == pytest.approx(ref["loss"], rel=1e-13)
+    np.testing.assert_allclose(r["phi0_bar"], ref["phi0_bar"], rtol=1e-10, atol=1e-12)
+    np.testing.assert_allclose(r["mu0_bar"], ref["mu0_bar"], rtol=1e-10, atol=1e-12)
+    for n in PARAMS:
+        assert r["d_" + n] == pytest.approx(ref["d_" + n], rel=1e-10, abs=1e-14)
+
+
 def test_adjoint_rejects_unsupported(tmp_path):
     from gp_cases import build_case
     ip, fp = build_case(tmp_path, "ternary3_aniso_periodic")
